@@ -1,0 +1,455 @@
+#!/usr/bin/env python
+"""Benchmark of the KPM DOS hot path on B200: vector-moments/s of the
+rescaled Chebyshev recurrence, mixed precision (FP32 matrices/vectors, FP64
+rescale and moment dots) against plain FP64, on the non-orthogonal LCAO
+diamond workload (N = 262,144, 8x8 BSR, sandwich Z^H H Z, R = 128
+Rademacher vectors, 1024 moments).
+
+One step = one full moment recurrence (1024 moments, 512 sandwich
+applications = 1536 SpMMs) over the R sample vectors, inputs resident in
+HBM; every panel (134-268 MB) is larger than the 126 MB L2.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun, one rank per GPU) each rank runs its own 128 sample
+columns (global columns rank*128 ...), the moments are summed with one NCCL
+all-reduce, and the time is the max over ranks.  Prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from datetime import timedelta
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+METRIC = "KPM moments/sec & BSR SpMM HBM GB/s: mixed-prec vs FP64, at DOS err ≤1e-5"
+UNIT = "vector-moments/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--workload", choices=["diamond", "graphene"], default="diamond")
+    p.add_argument("--small", action="store_true", help="reduced sizes, for a quick check")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-moments", type=int, default=8,
+                   help="moments in the bounded CPU baseline sample")
+    return p.parse_args()
+
+
+# ------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device_index = device_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        if self.proc is None or not self.path:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        for line in Path(self.path).read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), float(parts[3]), parts[4:]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            for name, flag in zip(names, r[3][1:]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        loaded = [r for r in rows if r[2] > 200.0] or rows
+        return {"sm_mhz": statistics.median(r[0] for r in loaded),
+                "sm_max_mhz": max(r[1] for r in rows),
+                "power_w_max": max(r[2] for r in rows),
+                "samples": len(rows), "reasons": sorted(reasons)}
+
+
+# -------------------------------------------------------------- distributed
+
+class Dist:
+    def __init__(self):
+        import torch
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+        self.torch = torch
+        if torch.cuda.is_available():
+            torch.cuda.set_device(self.local_rank)
+        if self.world > 1:
+            import torch.distributed as dist
+            dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                    device_id=torch.device("cuda", self.local_rank))
+            self.dist = dist
+        else:
+            self.dist = None
+
+    def barrier(self):
+        if self.dist is not None:
+            self.dist.barrier()
+
+    def max(self, x: float) -> float:
+        if self.dist is None:
+            return x
+        t = self.torch.tensor([x], dtype=self.torch.float64, device="cuda")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_array(self, a: np.ndarray) -> np.ndarray:
+        if self.dist is None:
+            return a
+        t = self.torch.as_tensor(np.ascontiguousarray(a)).cuda()
+        self.dist.all_reduce(t)
+        return t.cpu().numpy()
+
+    def close(self):
+        if self.dist is not None:
+            self.dist.barrier()
+            self.dist.destroy_process_group()
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text())
+        except json.JSONDecodeError:
+            pass
+    return {}
+
+
+# ------------------------------------------------------------ measurements
+
+def dos_grid(emin: float, emax: float, n_moments: int):
+    """ComputeDos's grid for the dE that n_moments resolves (observables.hpp:
+    346-375): dE = 7.396 * half_width / N, nt = ceil(span / dE)."""
+    hw = (emax - emin) / 2
+    de = math.sqrt(8 * math.log(2)) * math.pi * hw / n_moments
+    nt = max(1, math.ceil((emax - emin) / de))
+    i = np.arange(nt)
+    return np.concatenate([(i - nt) / nt, i / nt]), nt
+
+
+def run_moments(wl, cheby, psi, dist):
+    from rsatb_b200.calc import kpm_dos_moments
+    mu = kpm_dos_moments(cheby, psi, wl.n_moments)
+    if dist.world > 1:
+        s = dist.sum_array(np.concatenate([mu.real, mu.imag]) * wl.R)
+        mu = (s[:wl.n_moments] + 1j * s[wl.n_moments:]) / (wl.R * dist.world)
+    return mu
+
+
+def time_recurrence(wl, precision, steps, warmup, dist):
+    """(ms per step, max over ranks; moments of the last step; kernel
+    launches per step)."""
+    import torch
+    cheby = wl.cheby64 if precision == "f64" else wl.cheby32
+    psi = wl.psi(wl.vec_dtype(precision))
+    for _ in range(warmup):
+        mu = run_moments(wl, cheby, psi, dist)
+    torch.cuda.synchronize()
+    dist.barrier()
+    ctx = cheby.H.ctx
+    l0 = ctx.launch_count()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(steps):
+        mu = run_moments(wl, cheby, psi, dist)
+    e.record()
+    torch.cuda.synchronize()
+    dist.barrier()
+    launches = (ctx.launch_count() - l0) / steps
+    ms = dist.max(s.elapsed_time(e) / steps)
+    return ms, mu, launches
+
+
+def time_e2e(wl, precision, steps, dist):
+    """Same recurrence with the sample panel copied from pinned host memory
+    every step and the moments returned to the host by the C-ABI call."""
+    import torch
+    cheby = wl.cheby64 if precision == "f64" else wl.cheby32
+    host = wl.psi(wl.vec_dtype(precision)).cpu().pin_memory()
+    dev = torch.empty_like(host, device="cuda")
+    torch.cuda.synchronize()
+    dist.barrier()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(steps):
+        dev.copy_(host, non_blocking=True)
+        run_moments(wl, cheby, dev, dist)
+    e.record()
+    torch.cuda.synchronize()
+    dist.barrier()
+    ms = dist.max(s.elapsed_time(e) / steps)
+    n_dot_slots = 1 + wl.n_moments // 2
+    W = wl.R * (2 if wl.complex_vectors else 1)
+    return ms, host.numel() * host.element_size(), n_dot_slots * 2 * W * 8
+
+
+def time_spmm(A, n_rows, R, dtype, reps=20):
+    """Average duration (ms) of one mult_dense launch, CUDA events."""
+    import torch
+    X = torch.randn(A.shape[1], R, dtype=dtype, device="cuda")
+    Y = torch.empty(n_rows, R, dtype=dtype, device="cuda")
+    for _ in range(3):
+        A.mult_dense(X, Y)
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(reps):
+        A.mult_dense(X, Y)
+    e.record()
+    torch.cuda.synchronize()
+    return s.elapsed_time(e) / reps
+
+
+def roofline(wl, hbm_peak, peak_note, fma_peaks):
+    """Dominant kernel: the fused block SpMM of the sandwich at the run's
+    panel width (each of the 3 SpMMs per application is this kernel)."""
+    import torch
+    from rsatb_b200.workloads import spmm_bytes, spmm_flops
+    Z32 = wl.cheby32.M.Z
+    dt = wl.vec_dtype("f32")
+    item = torch.empty(0, dtype=dt).element_size()
+    ms = time_spmm(Z32, wl.n_rows, wl.R, dt)
+    nbytes = spmm_bytes(Z32, wl.R, item)
+    flops = spmm_flops(Z32, wl.R, wl.complex_vectors)
+    gbs = nbytes / (ms * 1e-3) / 1e9
+    tfs = flops / (ms * 1e-3) / 1e12
+    out = {"bound": "hbm", "achieved": round(gbs, 1), "peak": hbm_peak, "unit": "GB/s",
+           "frac": round(gbs / hbm_peak, 4), "traffic": None,
+           "kernel": "cheb_step_kernel<float,float,8,4> (Y = A X, FP32, R=%d)" % wl.R,
+           "algorithmic_bytes_per_launch": nbytes, "ms_per_launch": round(ms, 4),
+           "peak_source": peak_note,
+           "compute": {"bound": "fp32_fma", "achieved": round(tfs, 2),
+                       "peak": round(fma_peaks["f32"] / 1e12, 2), "unit": "TFLOP/s",
+                       "frac": round(tfs * 1e12 / fma_peaks["f32"], 4),
+                       "flops_per_launch": flops,
+                       "peak_source": "rsatb_measure_fma_peak (FMA chains, this run)"}}
+    # The same SpMM in FP64, and the memory-bound narrow panels.
+    Z64 = wl.cheby64.M.Z
+    dt64 = wl.vec_dtype("f64")
+    ms64 = time_spmm(Z64, wl.n_rows, wl.R, dt64)
+    out["fp64_same_kernel"] = {
+        "ms_per_launch": round(ms64, 4),
+        "gbs": round(spmm_bytes(Z64, wl.R, 2 * item) / (ms64 * 1e-3) / 1e9, 1),
+        "tflops": round(spmm_flops(Z64, wl.R, wl.complex_vectors) / (ms64 * 1e-3) / 1e12, 2),
+        "fma_frac": round(spmm_flops(Z64, wl.R, wl.complex_vectors) / (ms64 * 1e-3)
+                          / fma_peaks["f64"], 4)}
+    sweep = {}
+    for R in (8, 16):
+        for prec, A in (("f32", Z32), ("f64", Z64)):
+            d = torch.float32 if prec == "f32" else torch.float64
+            m = time_spmm(A, wl.n_rows, R, d)
+            b = spmm_bytes(A, R, torch.empty(0, dtype=d).element_size())
+            g = b / (m * 1e-3) / 1e9
+            sweep[f"{prec}_R{R}"] = {"gbs": round(g, 1), "frac": round(g / hbm_peak, 4),
+                                     "ms": round(m, 4)}
+    out["hbm_sweep_narrow_panels"] = sweep
+    return out
+
+
+def cpu_baseline(wl, n_moments: int):
+    """The oracle's FP64 recurrence (oracle/kpm_oracle.c) on the host cores,
+    on the same operator and samples, over a bounded number of moments."""
+    import oracle
+    from rsatb_b200.isqrt import EIGEN_CLAMP  # noqa: F401  (same factor as the GPU)
+    H = oracle.Bsr(wl.H.n_block_rows, wl.H.n_block_rows, wl.H.block_size, wl.H.row_ptr,
+                   wl.H.col_ind, wl.H.values)
+    if wl.Z is not None:
+        Z = oracle.Bsr(wl.Z.n_block_rows, wl.Z.n_block_rows, wl.Z.block_size, wl.Z.row_ptr,
+                       wl.Z.col_ind, wl.Z.values)
+        op = oracle.make_op(H, (wl.emax + wl.emin) / 2, (wl.emax - wl.emin) / 2, Z,
+                            oracle.bsr_adjoint(Z))
+    else:
+        op = oracle.make_op(H, (wl.emax + wl.emin) / 2, (wl.emax - wl.emin) / 2)
+    n_atoms = wl.n_rows // wl.orbitals
+    psi = oracle.set_random(20240917, 0 if wl.complex_vectors else 1, True,
+                            np.arange(n_atoms), wl.orbitals, wl.n_rows, wl.R,
+                            wl.complex_vectors, first_column=wl.first_column)
+    t0 = time.perf_counter()
+    mu = oracle.kpm_moments(op, psi, n_moments)
+    dt = time.perf_counter() - t0
+    return {"value": n_moments * wl.R / dt, "unit": UNIT, "cores": oracle.num_threads(),
+            "kind": "port", "seconds": round(dt, 3),
+            "sample": f"{n_moments} moments ({(n_moments + 1) // 2} operator applications) of "
+                      f"the same workload, all {wl.R} vectors, FP64, OpenMP"}, mu
+
+
+def fma_peaks() -> dict:
+    import ctypes as C
+    from rsatb_b200 import _capi
+    from rsatb_b200.vbcsr import context
+    ctx = context()
+    out = {}
+    for name, dp in (("f64", 1), ("f32", 0)):
+        v = C.c_double()
+        _capi.check(_capi.lib().rsatb_measure_fma_peak(ctx.handle, dp, C.byref(v)))
+        out[name] = v.value
+    return out
+
+
+def build_workload(args, rank):
+    from rsatb_b200 import workloads
+    if args.workload == "graphene":
+        return workloads.graphene_dos(30 if args.small else 60, 30 if args.small else 60,
+                                      rank=rank)
+    if args.small:
+        return workloads.diamond_sandwich(L=6, R=32, n_moments=256, rank=rank)
+    return workloads.diamond_sandwich(rank=rank)
+
+
+def config_of(wl) -> dict:
+    return {"workload": wl.name + (": diamond LCAO 16^3 conventional cells, 32768 atoms x 8 "
+                                   "orbitals, 8x8 BSR to the 3rd shell (29 blocks/row), "
+                                   "operator Z^H H Z with the graph-local S^-1/2"
+                                   if wl.name == "diamond_sandwich" else ": pz graphene"),
+            "n_rows": wl.n_rows, "vectors_per_gpu": wl.R, "n_moments": wl.n_moments,
+            "block_size": wl.H.block_size, "nnz_blocks": int(wl.H.nnz_blocks),
+            "bounds_ev": [round(wl.emin, 4), round(wl.emax, 4)],
+            "sample_vectors": "complex random phase" if wl.complex_vectors else "Rademacher",
+            "l2": "inputs larger than L2 (every panel >= 134 MB > 126 MB L2)"
+            if wl.n_rows * wl.R * 4 > 126e6 else "working set may be L2-resident"}
+
+
+def reference_arm(args, dist):
+    """The reference's CPU path (the oracle port; the reference itself cannot
+    be built here) on rank 0, bounded steps."""
+    if dist.rank != 0:
+        return
+    wl = build_workload(args, 0)
+    n_mom = max(2, args.cpu_moments // 2)
+    samples = []
+    for k in range(args.warmup + args.steps):
+        base, _ = cpu_baseline(wl, n_mom)
+        if k >= args.warmup:
+            samples.append(base)
+    secs = [s["seconds"] for s in samples]
+    value = n_mom * wl.R / (sum(secs) / len(secs))
+    base = dict(samples[-1])
+    base["value"] = value
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * sum(secs) / len(secs), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_of(wl), "cpu_baseline": base,
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "note": "RSATB cannot be built here (vbcsr, PRIMME, MPI, FFTW, HDF5 absent); the "
+                    "timed CPU path is the oracle's FP64 restatement of the same recurrence"}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    dist = Dist()
+    if args.impl == "reference":
+        reference_arm(args, dist)
+        dist.close()
+        return
+    import torch
+    from rsatb_b200.calc import evaluate_kpm_density
+
+    wl = build_workload(args, dist.rank)
+    peaks = measured_peaks()
+    hbm_peak = float(peaks.get("hbm_gbs", FALLBACK_HBM_GBS))
+    peak_note = ("MEASURED_PEAKS.json hbm_gbs (measured copy, burst)" if "hbm_gbs" in peaks
+                 else "fallback 6650 GB/s")
+    fpk = fma_peaks()
+
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        ms64, mu64, _ = time_recurrence(wl, "f64", args.steps, args.warmup, dist)
+        ms32, mu32, launches = time_recurrence(wl, "f32", args.steps, args.warmup, dist)
+    clocks = clk.summary()
+    e2e_ms, h2d, d2h = time_e2e(wl, "f32", args.steps, dist)
+    roof = roofline(wl, hbm_peak, peak_note, fpk)
+
+    x, nt = dos_grid(wl.emin, wl.emax, wl.n_moments)
+    rho64 = 2 * evaluate_kpm_density(mu64, x, 0.5 / nt)
+    rho32 = 2 * evaluate_kpm_density(mu32, x, 0.5 / nt)
+    dos_err = float(np.abs(rho32 - rho64).max() / np.abs(rho64).max())
+
+    units = wl.n_moments * wl.R * dist.world
+    value = units / (ms32 * 1e-3)
+    value64 = units / (ms64 * 1e-3)
+    base = None
+    if dist.rank == 0 and not args.no_cpu_baseline and dist.world == 1:
+        base, mu_cpu = cpu_baseline(wl, args.cpu_moments)
+        base["moments_vs_gpu_fp64_max_abs"] = float(np.abs(mu_cpu - mu64[:args.cpu_moments]).max())
+
+    if dist.rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": dist.world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms32, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 (FP64 rescale + moment dots)", "data": "synthetic (seeded generators)",
+            "config": dict(config_of(wl), parallelism=f"samples sharded over {dist.world} GPU(s)"),
+            "fp64_path": {"value": round(value64, 1), "ms_per_step": round(ms64, 3),
+                          "mixed_over_fp64": round(ms64 / ms32, 3)},
+            "dos_err_mixed_vs_fp64": dos_err,
+            "roofline": roof,
+            "cpu_baseline": base,
+            "e2e": {"value": round(units / (e2e_ms * 1e-3), 1), "unit": UNIT,
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "ms_per_step": round(e2e_ms, 3)},
+            "gpu_launches": int(round(launches * args.steps)),
+            "launches_per_step": launches,
+            "fma_peaks_tflops": {k: round(v / 1e12, 2) for k, v in fpk.items()},
+            "clocks": clocks,
+            "setup_seconds": {k: round(v, 2) for k, v in wl.setup_seconds.items()},
+        }
+        print(json.dumps(line), flush=True)
+    dist.close()
+
+
+if __name__ == "__main__":
+    main()

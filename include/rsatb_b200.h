@@ -1,0 +1,221 @@
+/*
+ * rsatb_b200.h -- C ABI of the B200 (sm_100a) implementation of RSATB's
+ * KPM / S^-1/2 / FFT-Chebyshev hot path.
+ *
+ * Plain C: opaque handles, raw pointers and sizes, integer status codes.
+ * No exception crosses this boundary; on failure a function returns a
+ * non-zero rsatb_status and rsatb_last_error() holds a message for the
+ * calling thread.
+ *
+ * Every call is asynchronous with respect to the host unless its comment
+ * says it copies results to host memory (those synchronise the context's
+ * stream before returning).  A context owns one CUDA stream and is not
+ * re-entrant: one host thread at a time per context.
+ *
+ * Data layouts (all row-major, matching vbcsr's DistMultiVector):
+ *   multivector   N x R, element (row, col) at [row * R + col]; a complex
+ *                 multivector stores (re, im) pairs, so it is N x 2R reals.
+ *   BSR matrix    uniform b x b blocks; block k of block row i holds
+ *                 A[i*b + r, col_ind[k]*b + c] at values[k*b*b + r*b + c]
+ *                 (vbcsr MatrixLayout::RowMajor); complex values interleaved.
+ */
+#ifndef RSATB_B200_H
+#define RSATB_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define RSATB_API __attribute__((visibility("default")))
+#else
+#define RSATB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  0..6 mirror rsatb::calc::isqrt::Status
+ * (rsatb/calc/isqrt_action.hpp:84-92, in that order); the rest are device
+ * conditions the CPU reference does not have. */
+typedef enum {
+    RSATB_SUCCESS = 0,
+    RSATB_INVALID_ARGUMENT = 1,
+    RSATB_FAST_PATH_REJECTED = 2,
+    RSATB_RANK_BREAKDOWN = 3,
+    RSATB_NOT_POSITIVE_DEFINITE = 4,
+    RSATB_NEAR_SINGULAR = 5,
+    RSATB_NUMERICAL_FAILURE = 6,   /* isqrt::Status::LapackFailure */
+    RSATB_CUDA_ERROR = 16,
+    RSATB_OUT_OF_MEMORY = 17,
+    RSATB_NOT_SUPPORTED = 18,
+    RSATB_DIVERGED = 19,
+    RSATB_INTERRUPTED = 20
+} rsatb_status;
+
+/* Element types of matrices and multivectors. */
+typedef enum {
+    RSATB_F64 = 0,
+    RSATB_F32 = 1,
+    RSATB_C128 = 2,   /* complex<double>, interleaved */
+    RSATB_C64 = 3     /* complex<float>, interleaved */
+} rsatb_dtype;
+
+/* Operator forms, rsatb::calc::ChebyOpForm (rsatb/calc/cheby.hpp:78-82).
+ * The Solve form (CG per matvec) is not implemented on the device. */
+typedef enum {
+    RSATB_FORM_ORTHOGONAL = 0,
+    RSATB_FORM_SANDWICH = 1
+} rsatb_form;
+
+/* Summation kernels, rsatb::calc::KpmKernel (rsatb/calc/kpm.hpp:49). */
+typedef enum {
+    RSATB_KPM_NONE = 0,
+    RSATB_KPM_JACKSON = 1,
+    RSATB_KPM_COSTAPER = 2,
+    RSATB_KPM_VPTAPER = 3
+} rsatb_kpm_kernel;
+
+/* Sample-vector distributions for rsatb_set_random. */
+typedef enum {
+    RSATB_RANDOM_PHASE = 0,       /* e^{i theta}, theta uniform; complex only */
+    RSATB_RANDOM_RADEMACHER = 1,  /* +-1 */
+    RSATB_RANDOM_UNIFORM = 2      /* uniform in [-1, 1) (real and imaginary) */
+} rsatb_random_kind;
+
+/* rsatb_bsr_create flags. */
+#define RSATB_BSR_DEVICE_POINTERS 1u  /* row_ptr/col_ind/values are device pointers */
+#define RSATB_BSR_IMAGINARY_UNIT  2u  /* real values W; the matrix is i*W */
+
+typedef struct rsatb_context* rsatb_ctx_t;
+typedef struct rsatb_bsr_matrix* rsatb_bsr_t;
+
+/* ------------------------------------------------------------------ errors */
+
+/* Message of the last failure on the calling thread ("" if none). */
+RSATB_API const char* rsatb_last_error(void);
+/* Library version, major*10000 + minor*100 + patch. */
+RSATB_API int rsatb_version(void);
+
+/* ----------------------------------------------------------- context, memory */
+
+/* Creates a context on `device` with its own non-blocking stream. */
+RSATB_API int rsatb_ctx_create(int device, rsatb_ctx_t* out);
+RSATB_API int rsatb_ctx_destroy(rsatb_ctx_t ctx);
+/* Launches on the caller's cudaStream_t (passed as void*) from now on; NULL
+ * is the legacy default stream.  Work already queued on the previous stream
+ * is waited for first. */
+RSATB_API int rsatb_ctx_set_stream(rsatb_ctx_t ctx, void* stream);
+/* The stream the context launches on (a cudaStream_t). */
+RSATB_API void* rsatb_ctx_stream(rsatb_ctx_t ctx);
+RSATB_API int rsatb_ctx_synchronize(rsatb_ctx_t ctx);
+/* Number of kernels the context has launched so far (all entry points). */
+RSATB_API int64_t rsatb_ctx_launch_count(rsatb_ctx_t ctx);
+
+RSATB_API int rsatb_device_alloc(rsatb_ctx_t ctx, size_t bytes, void** out);
+RSATB_API int rsatb_device_free(rsatb_ctx_t ctx, void* ptr);
+/* Stream-ordered copies; the *_sync forms return after the copy landed. */
+RSATB_API int rsatb_copy_to_device(rsatb_ctx_t ctx, void* dst, const void* src, size_t bytes);
+RSATB_API int rsatb_copy_to_host_sync(rsatb_ctx_t ctx, void* dst, const void* src, size_t bytes);
+
+/* ------------------------------------------------------------- BSR matrices */
+
+/* vbcsr BlockSpMat<T> with a uniform block size (construct + add_block +
+ * assemble in one call).  row_ptr has n_block_rows+1 entries, col_ind
+ * nnz_blocks entries (sorted within a row), values nnz_blocks*b*b
+ * elements of `dtype`.  Host pointers are copied; with
+ * RSATB_BSR_DEVICE_POINTERS they are copied device-to-device. */
+RSATB_API int rsatb_bsr_create(rsatb_ctx_t ctx, int n_block_rows, int n_block_cols,
+                     int block_size, int64_t nnz_blocks, const int32_t* row_ptr,
+                     const int32_t* col_ind, const void* values, rsatb_dtype dtype,
+                     unsigned flags, rsatb_bsr_t* out);
+RSATB_API int rsatb_bsr_destroy(rsatb_bsr_t A);
+/* A^H as a new matrix (BlockSpMat::mult_dense_adjoint's operator, built once
+ * so that every later apply uses the forward row-gather kernel). */
+RSATB_API int rsatb_bsr_adjoint(rsatb_ctx_t ctx, rsatb_bsr_t A, rsatb_bsr_t* out);
+/* Copy of A with values converted to `dtype` (F64 <-> F32, C128 <-> C64). */
+RSATB_API int rsatb_bsr_convert(rsatb_ctx_t ctx, rsatb_bsr_t A, rsatb_dtype dtype, rsatb_bsr_t* out);
+RSATB_API int rsatb_bsr_info(rsatb_bsr_t A, int* n_block_rows, int* n_block_cols, int* block_size,
+                   int64_t* nnz_blocks, int* dtype, unsigned* flags);
+/* Device pointer to the values array (nnz_blocks*b*b elements). */
+RSATB_API void* rsatb_bsr_values(rsatb_bsr_t A);
+/* Overwrites the values from host (or device with RSATB_BSR_DEVICE_POINTERS). */
+RSATB_API int rsatb_bsr_set_values(rsatb_ctx_t ctx, rsatb_bsr_t A, const void* values, unsigned flags);
+
+/* Y = alpha * A X.  BlockSpMat::mult_dense (vbcsr), called by
+ * Chebyshev::mult_by (rsatb/calc/cheby.hpp:599-606).  X, Y device, N x R of
+ * vec_dtype; a real matrix may multiply a complex multivector. */
+RSATB_API int rsatb_bsr_mult_dense(rsatb_ctx_t ctx, rsatb_bsr_t A, const void* X, void* Y,
+                         int n_vectors, rsatb_dtype vec_dtype, double alpha);
+
+/* ----------------------------------------------------- rescaled operator */
+
+/* The operator a Chebyshev<T> iterates (rsatb/calc/cheby.hpp:147-201):
+ * Orthogonal: H;  Sandwich: Z^H H Z with Z and its adjoint ZH.
+ * Every matrix must share one precision; the multivectors passed with the
+ * operator must have that precision too (F64/C128 or F32/C64). */
+typedef struct {
+    int form;            /* rsatb_form */
+    rsatb_bsr_t H;
+    rsatb_bsr_t Z;       /* sandwich only */
+    rsatb_bsr_t ZH;      /* sandwich only: Z^H (rsatb_bsr_adjoint) */
+    double center;       /* (emax + emin)/2 */
+    double half_width;   /* (emax - emin)/2 */
+} rsatb_cheb_op;
+
+/* Y = ((Op) X - center X) / half_width.  Chebyshev::apply_op NORMAL
+ * (rsatb/calc/cheby.hpp:232-235, apply_form :555-591). */
+RSATB_API int rsatb_cheb_apply_op(rsatb_ctx_t ctx, const rsatb_cheb_op* op, const void* X, void* Y,
+                        int n_vectors, rsatb_dtype vec_dtype);
+
+/* KPM trace moments averaged over the R columns of psi,
+ * rsatb::calc::kpm_dos_moments (rsatb/calc/dos.hpp:125-190): doubled
+ * (two moments per matvec) when `doubled` != 0, else the plain recurrence
+ * mu_n = <psi|T_n|psi> (Chebyshev::compute_moments, cheby.hpp:479-514).
+ * The recurrence, its rescaling and the FP64 column dots all run on the
+ * device; mu_out (host) receives n_moments complex values as 2*n_moments
+ * doubles.  col_mu_out (host, may be NULL) receives the per-column
+ * moments, [n_moments][R] complex. */
+RSATB_API int rsatb_kpm_dos_moments(rsatb_ctx_t ctx, const rsatb_cheb_op* op, const void* psi,
+                          int n_vectors, rsatb_dtype vec_dtype, int n_moments, int doubled,
+                          double* mu_out, double* col_mu_out);
+
+/* ------------------------------------------------------------ sample vectors */
+
+/* Seeded sample vectors, the device half of SampleVectors::initialize
+ * (rsatb/calc/observables.hpp:84-96, vbcsr set_random(seed, normalize,
+ * atom_index)).  Element (row, col) of the N x R output is a function of
+ * (seed, atom_index[atom], orbital-in-atom, col) only, through
+ * Philox-4x32-10, so it does not depend on the launch shape, and
+ * `normalize` scales by 1/sqrt(n_rows_global).  atom_index is a host array
+ * of n_atoms stable ids; every atom has orbitals_per_atom rows.  Column j
+ * of the output is global sample column first_column + j, so ranks that
+ * split the samples by column draw disjoint columns of one global set. */
+RSATB_API int rsatb_set_random(rsatb_ctx_t ctx, uint64_t seed, int kind, int normalize,
+                     const int64_t* atom_index, int n_atoms, int orbitals_per_atom,
+                     int64_t n_rows_global, int n_vectors, int64_t first_column,
+                     rsatb_dtype dtype, void* out);
+
+/* -------------------------------------------------------------- densities */
+
+/* rho(x_j) = (g0 mu0 + 2 sum_n g_n mu_n T_n(x_j)) / (pi sqrt(1 - x_j^2)),
+ * x clamped by edge_inset.  rsatb::calc::evaluate_kpm_density
+ * (rsatb/calc/kpm.hpp:206-241) with kpm_kernel_weights (:52-85).
+ * moments: host, 2*n_moments doubles (complex; real parts used);
+ * x, rho_out: host arrays of nx doubles.  Computed on the device. */
+RSATB_API int rsatb_evaluate_kpm_density(rsatb_ctx_t ctx, const double* moments, int n_moments,
+                               const double* x, int nx, double edge_inset, int kernel,
+                               double* rho_out);
+
+/* ------------------------------------------------------------ measurement */
+
+/* FMA-pipe throughput of this device in FLOP/s (FP64 if double_precision,
+ * else FP32), from independent FMA chains on every SM timed with CUDA
+ * events: the compute roofline of the block SpMM at wide panels. */
+RSATB_API int rsatb_measure_fma_peak(rsatb_ctx_t ctx, int double_precision, double* flops);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RSATB_B200_H */

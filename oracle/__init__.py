@@ -1,0 +1,256 @@
+"""TEST INFRASTRUCTURE: the CPU oracle for the rsatb_b200 hot path.
+
+``kpm_oracle.c`` restates the reference algorithms in plain C (FP64,
+OpenMP); this module builds it with gcc into ``oracle/_build`` and wraps it
+with ctypes, and adds the numpy exact-diagonalisation references.  Only the
+tests, ``__graft_entry__.smoke()`` and the CPU baseline legs of ``bench.py``
+use it, as the checker; the product (``rsatb_b200``) never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+BUILD = HERE / "_build"
+LIB = BUILD / "libkpm_oracle.so"
+SRC = HERE / "kpm_oracle.c"
+
+_lib = None
+
+
+def build(force: bool = False) -> Path:
+    """Compiles kpm_oracle.c (gcc -O2 -fopenmp, no FP contraction)."""
+    BUILD.mkdir(exist_ok=True)
+    if force or not LIB.exists() or LIB.stat().st_mtime < SRC.stat().st_mtime:
+        cmd = ["gcc", "-O2", "-march=x86-64-v2", "-fopenmp", "-ffp-contract=off", "-fPIC",
+               "-shared", "-o", str(LIB), str(SRC), "-lm"]
+        subprocess.run(cmd, check=True)
+    return LIB
+
+
+class OrcBsr(C.Structure):
+    _fields_ = [("n_block_rows", C.c_int), ("n_block_cols", C.c_int), ("b", C.c_int),
+                ("row_ptr", C.c_void_p), ("col_ind", C.c_void_p), ("vals", C.c_void_p),
+                ("cplx", C.c_int), ("imag", C.c_int)]
+
+
+class OrcOp(C.Structure):
+    _fields_ = [("sandwich", C.c_int), ("H", C.POINTER(OrcBsr)), ("Z", C.POINTER(OrcBsr)),
+                ("ZH", C.POINTER(OrcBsr)), ("center", C.c_double), ("half_width", C.c_double)]
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = C.CDLL(str(LIB))
+        vp, i, d, u64, i64 = C.c_void_p, C.c_int, C.c_double, C.c_uint64, C.c_int64
+        L.orc_set_random.argtypes = [u64, i, i, vp, i, i, i64, i, i64, i, vp]
+        L.orc_spmm.argtypes = [C.POINTER(OrcBsr), vp, vp, i, i, d]
+        L.orc_spmm.restype = None
+        L.orc_apply_op.argtypes = [C.POINTER(OrcOp), vp, vp, i, i, vp]
+        L.orc_apply_op.restype = None
+        L.orc_kpm_moments.argtypes = [C.POINTER(OrcOp), vp, i, i, i, i, vp, vp]
+        L.orc_kernel_weights.argtypes = [i, i, vp]
+        L.orc_kernel_weights.restype = None
+        L.orc_density.argtypes = [vp, i, vp, i, d, i, vp]
+        L.orc_density.restype = None
+        L.orc_dct3_direct.argtypes = [vp, i, i, vp]
+        L.orc_dct3_direct.restype = None
+        L.orc_dct3_fftroute.argtypes = [vp, i, i, vp]
+        L.orc_dct3_fftroute.restype = None
+        L.orc_fftcheb.argtypes = [C.POINTER(OrcOp), C.POINTER(OrcBsr), C.POINTER(OrcBsr),
+                                  C.POINTER(OrcBsr), vp, i, i, i, d, i, i, vp, vp]
+        L.orc_philox4x32_10.argtypes = [vp, vp, vp]
+        L.orc_philox4x32_10.restype = None
+        L.orc_num_threads.restype = i
+        L.orc_set_threads.argtypes = [i]
+        L.orc_set_threads.restype = None
+        _lib = L
+    return _lib
+
+
+def num_threads() -> int:
+    return lib().orc_num_threads()
+
+
+def set_threads(n: int) -> None:
+    lib().orc_set_threads(int(n))
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+class Bsr:
+    """Host BSR in the library's layout (row-major blocks, complex interleaved)."""
+
+    def __init__(self, n_block_rows, n_block_cols, b, row_ptr, col_ind, values, imag=False):
+        self.row_ptr = np.ascontiguousarray(row_ptr, dtype=np.int32)
+        self.col_ind = np.ascontiguousarray(col_ind, dtype=np.int32)
+        vals = np.asarray(values)
+        self.cplx = np.iscomplexobj(vals)
+        self.vals = np.ascontiguousarray(vals, dtype=np.complex128 if self.cplx else np.float64)
+        self.n_block_rows, self.n_block_cols, self.b = int(n_block_rows), int(n_block_cols), int(b)
+        self.imag = bool(imag)
+        self.c = OrcBsr(self.n_block_rows, self.n_block_cols, self.b, _ptr(self.row_ptr),
+                        _ptr(self.col_ind), _ptr(self.vals), int(self.cplx), int(self.imag))
+
+    @classmethod
+    def from_dense(cls, A: np.ndarray, b: int = 1, imag: bool = False, tol: float = 0.0):
+        n = A.shape[0] // b
+        m = A.shape[1] // b
+        ptr, ind, vals = [0], [], []
+        for i in range(n):
+            for j in range(m):
+                blk = A[i * b:(i + 1) * b, j * b:(j + 1) * b]
+                if np.abs(blk).max() > tol:
+                    ind.append(j)
+                    vals.append(blk)
+            ptr.append(len(ind))
+        vals = np.array(vals).reshape(len(ind), b, b) if ind else np.zeros((0, b, b), A.dtype)
+        return cls(n, m, b, ptr, ind, vals, imag=imag)
+
+    def to_dense(self) -> np.ndarray:
+        b = self.b
+        dt = np.complex128 if (self.cplx or self.imag) else np.float64
+        A = np.zeros((self.n_block_rows * b, self.n_block_cols * b), dtype=dt)
+        v = self.vals.reshape(-1, b, b)
+        for i in range(self.n_block_rows):
+            for k in range(self.row_ptr[i], self.row_ptr[i + 1]):
+                j = self.col_ind[k]
+                A[i * b:(i + 1) * b, j * b:(j + 1) * b] = v[k] * (1j if self.imag else 1.0)
+        return A
+
+
+def bsr_adjoint(A: Bsr) -> Bsr:
+    """A^H in the same layout (host counting sort by column)."""
+    n = A.n_block_rows
+    rows = np.repeat(np.arange(n), np.diff(A.row_ptr))
+    order = np.lexsort((rows, A.col_ind))
+    t_rows = A.col_ind[order]
+    ptr = np.zeros(A.n_block_cols + 1, dtype=np.int64)
+    np.add.at(ptr, t_rows + 1, 1)
+    vals = np.conj(np.transpose(A.vals.reshape(-1, A.b, A.b)[order], (0, 2, 1)))
+    if A.imag:
+        vals = -vals
+    return Bsr(A.n_block_cols, n, A.b, np.cumsum(ptr), rows[order], np.ascontiguousarray(vals),
+               imag=A.imag)
+
+
+def _as_panel(X: np.ndarray):
+    """(N, R) real or complex -> contiguous float64 view and (W, cv)."""
+    if np.iscomplexobj(X):
+        Xc = np.ascontiguousarray(X, dtype=np.complex128)
+        return Xc, 2 * X.shape[1], 1
+    Xr = np.ascontiguousarray(X, dtype=np.float64)
+    return Xr, X.shape[1], 0
+
+
+def spmm(A: Bsr, X: np.ndarray, alpha: float = 1.0) -> np.ndarray:
+    Xc, W, cv = _as_panel(X)
+    cplx_out = cv or A.cplx or A.imag
+    if cplx_out and not cv:
+        Xc, W, cv = _as_panel(X.astype(np.complex128))
+    Y = np.zeros_like(Xc)
+    lib().orc_spmm(C.byref(A.c), _ptr(Xc), _ptr(Y), W, cv, float(alpha))
+    return Y
+
+
+def make_op(H: Bsr, center: float, half_width: float, Z: Bsr | None = None,
+            ZH: Bsr | None = None) -> OrcOp:
+    op = OrcOp(1 if Z is not None else 0, C.pointer(H.c),
+               C.pointer(Z.c) if Z is not None else None,
+               C.pointer(ZH.c) if ZH is not None else None, float(center), float(half_width))
+    op._keep = (H, Z, ZH)
+    return op
+
+
+def apply_op(op: OrcOp, X: np.ndarray) -> np.ndarray:
+    Xc, W, cv = _as_panel(X)
+    Y = np.zeros_like(Xc)
+    T = np.zeros_like(Xc)
+    lib().orc_apply_op(C.byref(op), _ptr(Xc), _ptr(Y), W, cv, _ptr(T))
+    return Y
+
+
+def kpm_moments(op: OrcOp, psi: np.ndarray, n_moments: int, doubled: bool = True,
+                per_column: bool = False):
+    """dos.hpp:125 kpm_dos_moments; returns complex moments (and per-column)."""
+    Xc, W, cv = _as_panel(psi)
+    R = psi.shape[1]
+    mu = np.zeros(2 * n_moments)
+    col = np.zeros(2 * n_moments * R) if per_column else None
+    st = lib().orc_kpm_moments(C.byref(op), _ptr(Xc), R, cv, int(n_moments), int(doubled),
+                               _ptr(mu), _ptr(col) if per_column else None)
+    if st != 0:
+        raise RuntimeError(f"orc_kpm_moments failed ({st})")
+    m = mu.view(np.complex128)
+    if per_column:
+        return m, col.view(np.complex128).reshape(n_moments, R)
+    return m
+
+
+def set_random(seed: int, kind: int, normalize: bool, atom_index: np.ndarray, orbitals: int,
+               n_rows_global: int, n_vectors: int, complex_out: bool,
+               first_column: int = 0) -> np.ndarray:
+    ids = np.ascontiguousarray(atom_index, dtype=np.int64)
+    n_rows = ids.size * orbitals
+    out = np.zeros((n_rows, n_vectors), dtype=np.complex128 if complex_out else np.float64)
+    st = lib().orc_set_random(C.c_uint64(seed), kind, int(normalize), _ptr(ids), ids.size,
+                              orbitals, n_rows_global, n_vectors, int(first_column),
+                              int(complex_out), _ptr(out))
+    if st != 0:
+        raise ValueError("orc_set_random: invalid arguments")
+    return out
+
+
+def philox4x32_10(ctr, key) -> np.ndarray:
+    c = np.ascontiguousarray(ctr, dtype=np.uint32)
+    k = np.ascontiguousarray(key, dtype=np.uint32)
+    out = np.zeros(4, dtype=np.uint32)
+    lib().orc_philox4x32_10(_ptr(c), _ptr(k), _ptr(out))
+    return out
+
+
+def kernel_weights(kernel: int, n: int) -> np.ndarray:
+    g = np.zeros(n)
+    lib().orc_kernel_weights(kernel, n, _ptr(g))
+    return g
+
+
+def density(mu: np.ndarray, x: np.ndarray, edge_inset: float, kernel: int = 1) -> np.ndarray:
+    m = np.ascontiguousarray(mu, dtype=np.complex128)
+    xx = np.ascontiguousarray(x, dtype=np.float64)
+    rho = np.zeros_like(xx)
+    lib().orc_density(_ptr(m), m.size, _ptr(xx), xx.size, float(edge_inset), kernel, _ptr(rho))
+    return rho
+
+
+def dct3(x: np.ndarray, route: str = "direct") -> np.ndarray:
+    """Batched DCT-III along the last axis of a complex (batch, n) array."""
+    xx = np.ascontiguousarray(x, dtype=np.complex128)
+    out = np.zeros_like(xx)
+    f = lib().orc_dct3_direct if route == "direct" else lib().orc_dct3_fftroute
+    f(_ptr(xx), xx.shape[-1], int(np.prod(xx.shape[:-1])), _ptr(out))
+    return out
+
+
+def fftcheb(op: OrcOp, V, psi: np.ndarray, n_moments: int, formulation: int = 0,
+            prefactor: float = 1.0, sections: int = 1, kernel: int = 1):
+    """dc_spectrum_fftcheb; returns (sigma[n_moments, 6], energy[n_moments])."""
+    p = np.ascontiguousarray(psi, dtype=np.complex128)
+    sigma = np.zeros(n_moments * 6)
+    energy = np.zeros(n_moments)
+    st = lib().orc_fftcheb(C.byref(op), C.byref(V[0].c), C.byref(V[1].c), C.byref(V[2].c),
+                           _ptr(p), p.shape[1], int(n_moments), int(formulation),
+                           float(prefactor), int(sections), int(kernel), _ptr(sigma),
+                           _ptr(energy))
+    if st != 0:
+        raise RuntimeError(f"orc_fftcheb failed ({st})")
+    return sigma.reshape(n_moments, 6), energy

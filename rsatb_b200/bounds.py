@@ -1,0 +1,64 @@
+"""Spectral bounds of the Chebyshev operator by Lanczos on the GPU.
+
+The reference estimates the extreme eigenvalues with PRIMME and pads them by
+BoundsOptions::padding = 0.5 eV (rsatb/setup/spectral_bounds.hpp:67-76,
+445-490).  PRIMME is not available, so this runs a fixed number of Lanczos
+steps (full reorthogonalisation, FP64) on the unscaled operator, applied
+through the rsatb_b200 kernels, and widens each extreme Ritz value by its
+residual norm |beta_m s_m| as well as the padding, which keeps the window
+conservative when the Ritz values have not converged.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from .calc import Chebyshev
+from .vbcsr import set_random
+
+PADDING = 0.5  # eV, spectral_bounds.hpp:75
+
+
+def lanczos_extremes(cheby: Chebyshev, steps: int = 20, seed: int = 2):
+    """(theta_min, theta_max, res_min, res_max) of the operator cheby iterates
+    (its window is ignored: the operator is applied unscaled)."""
+    unit = Chebyshev(cheby.H, -1.0, 1.0, preconditioner=cheby.M)  # center 0, half_width 1
+    n = cheby.n_rows
+    dt = torch.complex128 if cheby.H.is_complex or cheby.H.imaginary else torch.float64
+    if not cheby.H.is_double:
+        dt = torch.complex64 if dt == torch.complex128 else torch.float32
+    dev = f"cuda:{cheby.H.ctx.device}"
+    v = torch.empty(n, 1, dtype=dt, device=dev)
+    set_random(v, seed, normalize=True)
+    v = v / torch.linalg.vector_norm(v.to(torch.complex128))
+    m = min(steps, n)
+    Q = torch.zeros(n, m, dtype=torch.complex128, device=dev)
+    alpha = np.zeros(m)
+    beta = np.zeros(m)
+    w = torch.empty_like(v)
+    q = v.to(torch.complex128)
+    for j in range(m):
+        Q[:, j] = q[:, 0]
+        unit.apply_op(q.to(dt).contiguous(), w)
+        wc = w.to(torch.complex128)
+        a = torch.vdot(q[:, 0], wc[:, 0]).real.item()
+        alpha[j] = a
+        wc = wc - Q[:, :j + 1] @ (Q[:, :j + 1].conj().T @ wc)   # full reorthogonalisation
+        wc = wc - Q[:, :j + 1] @ (Q[:, :j + 1].conj().T @ wc)
+        b = torch.linalg.vector_norm(wc).item()
+        beta[j] = b
+        if b < 1e-12 * max(1.0, abs(a)):
+            m = j + 1
+            break
+        q = wc / b
+    T = np.diag(alpha[:m]) + np.diag(beta[:m - 1], 1) + np.diag(beta[:m - 1], -1)
+    theta, S = np.linalg.eigh(T)
+    res = np.abs(beta[m - 1] * S[-1, :])
+    return float(theta[0]), float(theta[-1]), float(res[0]), float(res[-1])
+
+
+def estimate_spectral_bounds(cheby: Chebyshev, steps: int = 20, padding: float = PADDING,
+                             seed: int = 2):
+    """(emin, emax) to pass to Chebyshev; EstimateSpectralBounds analogue."""
+    tmin, tmax, rmin, rmax = lanczos_extremes(cheby, steps, seed)
+    return tmin - padding - rmin, tmax + padding + rmax

@@ -1,0 +1,244 @@
+"""The KPM engine of rsatb/calc, on the GPU.
+
+Mirrors the reference's calc-layer interface for the DOS path:
+
+* ``Chebyshev`` -- rsatb::calc::Chebyshev<T> (rsatb/calc/cheby.hpp:147-668):
+  the rescaled operator (H - center)/half_width in the Orthogonal or the
+  Sandwich (Z^H H Z) form, ``apply_op``, ``op_is_hermitian``,
+  ``compute_moments``.
+* ``kpm_dos_moments`` -- rsatb/calc/dos.hpp:125-190.
+* ``jackson_kernel``, ``kpm_kernel_weights``, ``evaluate_kpm_density`` --
+  rsatb/calc/kpm.hpp:18-85, 206-241.
+* ``ISQRTMPreconditioner`` (borrowing form) -- rsatb/calc/preconditioner.hpp:
+  169-240, holding Z and Z^H for the sandwich.
+
+Every numerical step runs in the rsatb_b200 CUDA library; this module only
+validates arguments and moves handles.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+import math
+
+import numpy as np
+import torch
+
+from . import _capi
+from ._capi import check, lib
+from .vbcsr import BlockSpMat, context, dtype_code
+
+
+class ChebyMode(enum.IntEnum):
+    """rsatb::calc::ChebyMode (cheby.hpp:58)."""
+    NORMAL = 0
+    ADJOINT = 1
+
+
+class ChebyOpForm(enum.IntEnum):
+    """rsatb::calc::ChebyOpForm (cheby.hpp:78-82)."""
+    Orthogonal = 0
+    Solve = 1
+    Sandwich = 2
+
+
+class KpmKernel(enum.IntEnum):
+    """rsatb::calc::KpmKernel (kpm.hpp:49)."""
+    None_ = _capi.KPM_NONE
+    Jackson = _capi.KPM_JACKSON
+    CosTaper = _capi.KPM_COSTAPER
+    VpTaper = _capi.KPM_VPTAPER
+
+
+def parse_kpm_kernel(name: str) -> KpmKernel:
+    """kpm.hpp:104-111."""
+    table = {"jackson": KpmKernel.Jackson, "costaper": KpmKernel.CosTaper,
+             "vptaper": KpmKernel.VpTaper, "none": KpmKernel.None_}
+    if name not in table:
+        raise ValueError(f"Unknown KPM kernel '{name}' (expected jackson, costaper, vptaper, or none)")
+    return table[name]
+
+
+class ISQRTMPreconditioner:
+    """Borrowing ISQRTMPreconditioner: applies a given factor Z and Z^H.
+
+    The reference's computing constructor runs inverse_sqrt (isqrtm.hpp:262);
+    here the factor comes from ``rsatb_b200.isqrt`` and is passed in.
+    ``adjoint`` defaults to Z.adjoint() built once on the device.
+    """
+
+    def __init__(self, factor: BlockSpMat, adjoint: BlockSpMat | None = None):
+        self.Z = factor
+        self.ZH = adjoint if adjoint is not None else factor.adjoint()
+
+    def factor(self) -> BlockSpMat:
+        return self.Z
+
+    def astype(self, precision: str) -> "ISQRTMPreconditioner":
+        return ISQRTMPreconditioner(self.Z.astype(precision), self.ZH.astype(precision))
+
+
+class Chebyshev:
+    """Rescaled operator Op~ = (Op - center)/half_width on the GPU.
+
+    ``Chebyshev(H, emin, emax)`` is the Orthogonal form;
+    ``Chebyshev(H, emin, emax, preconditioner=pre)`` the Sandwich form
+    Z^H H Z.  The Solve form (a CG per matvec) is not provided.
+    """
+
+    def __init__(self, H: BlockSpMat, emin: float, emax: float,
+                 preconditioner: ISQRTMPreconditioner | None = None, verbose: bool = False):
+        if H.shape[0] != H.shape[1]:
+            raise ValueError("H must be square")
+        self.H = H
+        self.M = preconditioner
+        self.form = ChebyOpForm.Sandwich if preconditioner is not None else ChebyOpForm.Orthogonal
+        self.verbose = verbose
+        self.set_window(emin, emax)
+
+    def set_window(self, emin: float, emax: float) -> None:
+        """cheby.hpp:517-520."""
+        self.center = (emax + emin) / 2.0
+        self.half_width = (emax - emin) / 2.0
+
+    @property
+    def n_rows(self) -> int:
+        return self.H.shape[0]
+
+    @property
+    def is_double(self) -> bool:
+        return self.H.is_double
+
+    def op_is_hermitian(self) -> bool:
+        """cheby.hpp:222: every form here is Hermitian."""
+        return self.form != ChebyOpForm.Solve
+
+    def astype(self, precision: str) -> "Chebyshev":
+        """A copy whose matrices are stored in 'f64' or 'f32'."""
+        pre = self.M.astype(precision) if self.M is not None else None
+        c = Chebyshev(self.H.astype(precision), self.center - self.half_width,
+                      self.center + self.half_width, preconditioner=pre)
+        return c
+
+    def c_op(self) -> _capi.ChebOp:
+        op = _capi.ChebOp()
+        op.form = _capi.FORM_SANDWICH if self.form == ChebyOpForm.Sandwich else _capi.FORM_ORTHOGONAL
+        op.H = self.H.handle
+        if self.M is not None:
+            op.Z = self.M.Z.handle
+            op.ZH = self.M.ZH.handle
+        op.center = self.center
+        op.half_width = self.half_width
+        return op
+
+    def apply_op(self, X: torch.Tensor, Y: torch.Tensor, mode: ChebyMode = ChebyMode.NORMAL):
+        """Y = Op~ X (cheby.hpp:232-235); ADJOINT equals NORMAL for these forms."""
+        ctx = self.H.ctx
+        ctx.bind_stream()
+        op = self.c_op()
+        check(lib().rsatb_cheb_apply_op(ctx.handle, C.byref(op), C.c_void_p(X.data_ptr()),
+                                        C.c_void_p(Y.data_ptr()), X.shape[1],
+                                        dtype_code(X.dtype)))
+        return Y
+
+    def compute_moments(self, V: torch.Tensor, N: int) -> np.ndarray:
+        """Per-column plain moments <v|T_n|v>, shape (N, R) (cheby.hpp:479-514)."""
+        _, col = _moments(self, V, N, doubled=False, per_column=True)
+        return col
+
+
+def _moments(cheby: Chebyshev, psi: torch.Tensor, n_moments: int, doubled: bool,
+             per_column: bool = False):
+    if n_moments <= 0:
+        raise ValueError("n_moments must be positive")
+    if not psi.is_cuda or psi.dim() != 2 or not psi.is_contiguous():
+        raise ValueError("psi must be a contiguous (N, R) CUDA tensor")
+    if psi.shape[0] != cheby.n_rows:
+        raise ValueError("psi rows differ from the operator size")
+    ctx = cheby.H.ctx
+    ctx.bind_stream()
+    op = cheby.c_op()
+    R = psi.shape[1]
+    mu = np.zeros(2 * n_moments)
+    col = np.zeros(2 * n_moments * R) if per_column else None
+    check(lib().rsatb_kpm_dos_moments(
+        ctx.handle, C.byref(op), C.c_void_p(psi.data_ptr()), R, dtype_code(psi.dtype),
+        int(n_moments), int(bool(doubled)), mu.ctypes.data_as(C.POINTER(C.c_double)),
+        col.ctypes.data_as(C.POINTER(C.c_double)) if per_column else None))
+    m = mu.view(np.complex128)
+    if per_column:
+        return m, col.view(np.complex128).reshape(n_moments, R)
+    return m, None
+
+
+def kpm_dos_moments(cheby: Chebyshev, psi_in: torch.Tensor, n_moments: int) -> np.ndarray:
+    """KPM trace moments averaged over the columns of psi_in (dos.hpp:125).
+
+    Doubled (two moments per matvec) since every form here is Hermitian;
+    ``kpm_dos_moments_plain`` runs the plain recurrence.
+    """
+    m, _ = _moments(cheby, psi_in, n_moments, doubled=cheby.op_is_hermitian())
+    return m
+
+
+def kpm_dos_moments_plain(cheby: Chebyshev, psi_in: torch.Tensor, n_moments: int) -> np.ndarray:
+    m, _ = _moments(cheby, psi_in, n_moments, doubled=False)
+    return m
+
+
+def jackson_kernel(n: int) -> np.ndarray:
+    """kpm.hpp:18-33 (host FP64)."""
+    return kpm_kernel_weights(KpmKernel.Jackson, n)
+
+
+def kpm_kernel_weights(kernel: KpmKernel, n: int) -> np.ndarray:
+    """kpm.hpp:52-85 (host FP64)."""
+    if n <= 0:
+        raise ValueError("kpm_kernel_weights: n must be positive")
+    g = np.ones(n)
+    if kernel == KpmKernel.Jackson:
+        denom = float(n + 1)
+        theta = math.pi / denom
+        cot = math.cos(theta) / math.sin(theta)
+        i = np.arange(1, n)
+        g[1:] = ((denom - i) * np.cos(theta * i) + cot * np.sin(theta * i)) / denom
+    elif kernel == KpmKernel.CosTaper:
+        n0 = n // 2
+        s = (np.arange(n0, n) - n0) / (n - n0)
+        g[n0:] = 0.5 * (1.0 + np.cos(math.pi * s))
+    elif kernel == KpmKernel.VpTaper:
+        n0 = n // 2
+        g[n0:] = (n - np.arange(n0, n)) / (n - n0)
+    return g
+
+
+def evaluate_kpm_density(moments, x_values, edge_inset: float,
+                         kernel: KpmKernel = KpmKernel.Jackson, device=None) -> np.ndarray:
+    """rho(x) from moments on the GPU (kpm.hpp:206-241)."""
+    mu = np.ascontiguousarray(np.asarray(moments, dtype=np.complex128))
+    x = np.ascontiguousarray(np.asarray(x_values, dtype=np.float64))
+    rho = np.zeros_like(x)
+    ctx = context(device)
+    P = C.POINTER(C.c_double)
+    check(lib().rsatb_evaluate_kpm_density(ctx.handle, mu.view(np.float64).ctypes.data_as(P),
+                                           mu.size, x.ctypes.data_as(P), x.size,
+                                           float(edge_inset), int(kernel), rho.ctypes.data_as(P)))
+    return rho
+
+
+def dos_moment_count(half_width: float, de_ev: float) -> int:
+    """Moments for a Jackson FWHM of dE (observables.hpp:346-349)."""
+    jackson_fwhm = math.sqrt(8.0 * math.log(2.0)) * math.pi
+    return max(1, int(math.ceil(jackson_fwhm * half_width / de_ev)))
+
+
+def dos_energy_grid(emin: float, emax: float, de_ev: float):
+    """The uniform 2*nt grid of ComputeDos (observables.hpp:336, 370-375,
+    438-443): returns (x_grid, omega, nt)."""
+    span = emax - emin
+    nt = max(1, int(math.ceil(span / de_ev)))
+    i = np.arange(nt)
+    x = np.concatenate([(i - nt) / nt, i / nt])
+    scale, shift = span / 2.0, (emax + emin) / 2.0
+    omega = np.concatenate([(i - nt) * scale / nt + shift, i * scale / nt + shift])
+    return x, omega, nt

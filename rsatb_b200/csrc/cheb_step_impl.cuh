@@ -1,0 +1,165 @@
+// Launch-shape selection and template dispatch of the fused step, included
+// once per precision (cheb_step_f64.cu, cheb_step_f32.cu).
+#pragma once
+
+#include "cheb_kernels.cuh"
+
+#include <cstdlib>
+#include <mutex>
+#include <unordered_map>
+
+namespace rsatb_b200 {
+namespace step_detail {
+
+// Resident CTAs per SM for a kernel at a given CTA size and shared memory.
+inline int occupancy(const void* kernel, int threads, size_t smem) {
+    static std::mutex mu;
+    static std::unordered_map<uint64_t, int> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const uint64_t key = (uint64_t(reinterpret_cast<uintptr_t>(kernel)) << 8) ^
+                         (uint64_t(threads) << 40) ^ (uint64_t(smem) << 20) ^ uint64_t(dev);
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) return it->second;
+    }
+    int n = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, smem) != cudaSuccess ||
+        n < 1)
+        n = 1;
+    std::lock_guard<std::mutex> lock(mu);
+    cache[key] = n;
+    return n;
+}
+
+// Optional tuning override of the values-per-thread choice (RSATB_STEP_V).
+inline int env_v() {
+    const char* s = std::getenv("RSATB_STEP_V");
+    return s ? std::atoi(s) : 0;
+}
+
+template <typename Kernel>
+int launch(rsatb_context* ctx, Kernel kernel, int V, int64_t rows, StepArgs& a) {
+    const int L = a.W / V;
+    const int threads = L * (256 / L);
+    const int ndots = a.dot_mode == DOT_DOUBLING ? 2 : (a.dot_mode == DOT_PLAIN ? 1 : 0);
+    const size_t smem = size_t(ndots ? 2 : 0) * threads * V * sizeof(double);
+    const int64_t need = (rows * L + threads - 1) / threads;
+    const int per_sm = occupancy(reinterpret_cast<const void*>(kernel), threads, smem);
+    int64_t grid = int64_t(ctx->sm_count) * per_sm;
+    if (grid > int64_t(ctx->sm_count) * 8) grid = int64_t(ctx->sm_count) * 8;
+    if (need < grid) grid = need;
+    if (grid < 1) grid = 1;
+    kernel<<<unsigned(grid), threads, smem, ctx->stream>>>(a);
+    RSATB_LAUNCH_CHECK(ctx);
+    return RSATB_SUCCESS;
+}
+
+// Picks V (values per thread) for W real values per row.
+inline int pick_v(int W, bool cv, bool any_b, int block_size, bool dbl) {
+    const int forced = env_v();
+    auto ok = [&](int v) {
+        if (v <= 0 || W % v) return false;
+        if (cv && v % 2) return false;
+        return W / v <= 256;
+    };
+    if (forced && ok(forced) && (!any_b || forced <= 2) && forced <= 6) return forced;
+    if (any_b) {
+        if (ok(2)) return 2;
+        if (!cv && ok(1)) return 1;
+        return 0;
+    }
+    // FP64 blocks of 8 keep the register tile at 8 x 4 values.
+    const int pref_real[3] = {4, 2, 1};
+    const int pref_cplx[3] = {4, 6, 2};
+    const int* pref = cv ? pref_cplx : pref_real;
+    (void)block_size;
+    (void)dbl;
+    for (int i = 0; i < 3; ++i)
+        if (ok(pref[i])) return pref[i];
+    return 0;
+}
+
+template <typename VT, typename MT, int B, bool CM, bool CV>
+int launch_b(rsatb_context* ctx, int V, int64_t rows, StepArgs& a) {
+    switch (V) {
+        case 1:
+            if constexpr (!CV) return launch(ctx, cheb_step_kernel<VT, MT, B, 1, CM, CV>, 1, rows, a);
+            break;
+        case 2: return launch(ctx, cheb_step_kernel<VT, MT, B, 2, CM, CV>, 2, rows, a);
+        case 4: return launch(ctx, cheb_step_kernel<VT, MT, B, 4, CM, CV>, 4, rows, a);
+        case 6:
+            if constexpr (CV) return launch(ctx, cheb_step_kernel<VT, MT, B, 6, CM, CV>, 6, rows, a);
+            break;
+    }
+    return set_error(RSATB_NOT_SUPPORTED, "no step kernel for V=%d", V);
+}
+
+template <typename VT, typename MT, bool CM, bool CV>
+int launch_typed(rsatb_context* ctx, int block_size, StepArgs& a) {
+    const bool special = block_size == 1 || block_size == 5 || block_size == 8;
+    const int V = pick_v(a.W, CV, !special, block_size, sizeof(VT) == 8);
+    if (V == 0)
+        return set_error(RSATB_NOT_SUPPORTED,
+                         "panel width %d (real values per row) has no thread mapping; widths up "
+                         "to 1536 are supported", a.W);
+    const int64_t rows = a.n_block_rows;
+    switch (block_size) {
+        case 1: return launch_b<VT, MT, 1, CM, CV>(ctx, V, rows, a);
+        case 5: return launch_b<VT, MT, 5, CM, CV>(ctx, V, rows, a);
+        case 8: return launch_b<VT, MT, 8, CM, CV>(ctx, V, rows, a);
+        default:
+            if (V == 2) return launch(ctx, cheb_step_kernel_any_b<VT, MT, 2, CM, CV>, 2, rows, a);
+            if constexpr (!CV)
+                return launch(ctx, cheb_step_kernel_any_b<VT, MT, 1, CM, CV>, 1, rows, a);
+            return set_error(RSATB_NOT_SUPPORTED, "no generic step kernel for V=%d", V);
+    }
+}
+
+template <typename VT>
+int launch_step_precision(rsatb_context* ctx, const rsatb_bsr_matrix* A, int vec_dtype,
+                          StepArgs& a) {
+    const bool cm = dtype_is_complex(A->dtype);
+    const bool cv = dtype_is_complex(vec_dtype);
+    if (cm && !cv)
+        return set_error(RSATB_INVALID_ARGUMENT, "a complex matrix needs a complex multivector");
+    if ((A->flags & RSATB_BSR_IMAGINARY_UNIT) && !cv)
+        return set_error(RSATB_INVALID_ARGUMENT,
+                         "an imaginary-unit matrix needs a complex multivector");
+    a.imag = (A->flags & RSATB_BSR_IMAGINARY_UNIT) ? 1 : 0;
+    a.n_block_rows = A->n_block_rows;
+    a.row_ptr = A->row_ptr;
+    a.col_ind = A->col_ind;
+    a.vals = A->values;
+    a.block_size = A->block_size;
+    if (cm) return launch_typed<VT, VT, true, true>(ctx, A->block_size, a);
+    if (cv) return launch_typed<VT, VT, false, true>(ctx, A->block_size, a);
+    return launch_typed<VT, VT, false, false>(ctx, A->block_size, a);
+}
+
+template <typename VT>
+int launch_coldot_precision(rsatb_context* ctx, int vec_dtype, int64_t n_rows, StepArgs& a) {
+    const bool cv = dtype_is_complex(vec_dtype);
+    const int V = pick_v(a.W, cv, false, 1, sizeof(VT) == 8);
+    if (V == 0) return set_error(RSATB_NOT_SUPPORTED, "panel width %d not supported", a.W);
+    a.dot_mode = DOT_PLAIN;
+    a.n_block_rows = n_rows;
+    if (cv) {
+        switch (V) {
+            case 2: return launch(ctx, coldot_kernel<VT, 2, true>, 2, n_rows, a);
+            case 4: return launch(ctx, coldot_kernel<VT, 4, true>, 4, n_rows, a);
+            case 6: return launch(ctx, coldot_kernel<VT, 6, true>, 6, n_rows, a);
+        }
+    } else {
+        switch (V) {
+            case 1: return launch(ctx, coldot_kernel<VT, 1, false>, 1, n_rows, a);
+            case 2: return launch(ctx, coldot_kernel<VT, 2, false>, 2, n_rows, a);
+            case 4: return launch(ctx, coldot_kernel<VT, 4, false>, 4, n_rows, a);
+        }
+    }
+    return set_error(RSATB_NOT_SUPPORTED, "no dot kernel for V=%d", V);
+}
+
+}  // namespace step_detail
+}  // namespace rsatb_b200

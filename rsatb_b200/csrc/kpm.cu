@@ -1,0 +1,334 @@
+// Chebyshev operator application and the KPM moment recurrence
+// (rsatb/calc/cheby.hpp apply_form, rsatb/calc/dos.hpp kpm_dos_moments),
+// driven from the host, computed on the device.
+#include "cheb_kernels.cuh"
+
+#include <cmath>
+#include <complex>
+#include <vector>
+
+namespace rsatb_b200 {
+
+int run_step(rsatb_context* ctx, const rsatb_bsr_matrix* A, int vdt, const StepArgs& a) {
+    return dtype_is_double(vdt) ? launch_cheb_step_f64(ctx, A, vdt, a)
+                                : launch_cheb_step_f32(ctx, A, vdt, a);
+}
+
+int run_coldot(rsatb_context* ctx, int vdt, int64_t n_rows, const StepArgs& a) {
+    return dtype_is_double(vdt) ? launch_coldot_f64(ctx, vdt, n_rows, a)
+                                : launch_coldot_f32(ctx, vdt, n_rows, a);
+}
+
+namespace {
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+StepArgs blank_args(int W) {
+    StepArgs a{};
+    a.W = W;
+    a.s_in = 1.0;
+    a.c = 0.0;
+    a.s_out = 1.0;
+    a.s2 = 1.0;
+    a.g_p = 0.0;
+    a.dot_mode = DOT_NONE;
+    return a;
+}
+
+struct OpShape {
+    int64_t n_rows;  // scalar rows N
+    bool sandwich;
+};
+
+int check_matrix_square(const rsatb_bsr_matrix* A, const char* name) {
+    RSATB_TRY(check_bsr(A, name));
+    if (A->n_block_rows != A->n_block_cols)
+        return set_error(RSATB_INVALID_ARGUMENT, "%s must be square (%d x %d blocks)", name,
+                         A->n_block_rows, A->n_block_cols);
+    return RSATB_SUCCESS;
+}
+
+int check_vec_dtype(const rsatb_bsr_matrix* A, int vdt, const char* name) {
+    if (!dtype_valid(vdt)) return set_error(RSATB_INVALID_ARGUMENT, "bad multivector dtype %d", vdt);
+    if (dtype_is_double(A->dtype) != dtype_is_double(vdt))
+        return set_error(RSATB_INVALID_ARGUMENT,
+                         "%s precision (dtype %d) differs from the multivector's (dtype %d)", name,
+                         A->dtype, vdt);
+    if (dtype_is_complex(A->dtype) && !dtype_is_complex(vdt))
+        return set_error(RSATB_INVALID_ARGUMENT, "%s is complex but the multivector is real", name);
+    return RSATB_SUCCESS;
+}
+
+int check_op(const rsatb_cheb_op* op, int vdt, OpShape* shape) {
+    if (!op) return set_error(RSATB_INVALID_ARGUMENT, "null operator");
+    RSATB_TRY(check_matrix_square(op->H, "H"));
+    RSATB_TRY(check_vec_dtype(op->H, vdt, "H"));
+    if (!(op->half_width > 0.0) || !std::isfinite(op->half_width) || !std::isfinite(op->center))
+        return set_error(RSATB_INVALID_ARGUMENT, "spectral window needs half_width > 0 (got %g)",
+                         op->half_width);
+    shape->n_rows = int64_t(op->H->n_block_rows) * op->H->block_size;
+    if (op->form == RSATB_FORM_ORTHOGONAL) {
+        shape->sandwich = false;
+    } else if (op->form == RSATB_FORM_SANDWICH) {
+        shape->sandwich = true;
+        RSATB_TRY(check_matrix_square(op->Z, "Z"));
+        RSATB_TRY(check_matrix_square(op->ZH, "ZH"));
+        RSATB_TRY(check_vec_dtype(op->Z, vdt, "Z"));
+        RSATB_TRY(check_vec_dtype(op->ZH, vdt, "ZH"));
+        const int64_t nz = int64_t(op->Z->n_block_rows) * op->Z->block_size;
+        const int64_t nzh = int64_t(op->ZH->n_block_rows) * op->ZH->block_size;
+        if (nz != shape->n_rows || nzh != shape->n_rows)
+            return set_error(RSATB_INVALID_ARGUMENT, "Z, Z^H and H sizes differ (%lld, %lld, %lld)",
+                             (long long)nz, (long long)nzh, (long long)shape->n_rows);
+    } else {
+        return set_error(RSATB_NOT_SUPPORTED,
+                         "operator form %d is not available on the device (the Solve form needs "
+                         "a CG per matvec)", op->form);
+    }
+    return RSATB_SUCCESS;
+}
+
+int panel_width(int n_vectors, int vdt, int* W) {
+    if (n_vectors <= 0) return set_error(RSATB_INVALID_ARGUMENT, "n_vectors must be positive");
+    *W = n_vectors * (dtype_is_complex(vdt) ? 2 : 1);
+    if (*W > 1536)
+        return set_error(RSATB_NOT_SUPPORTED,
+                         "%d vectors exceed the widest panel (1536 real values per row); split "
+                         "the multivector", n_vectors);
+    return RSATB_SUCCESS;
+}
+
+size_t round256(size_t b) { return (b + 255) & ~size_t(255); }
+
+// y = ((Op) in - c x) * s_out * s2 + g_p * p with the dots of `dots`; `in`
+// is the operand of the first factor (x itself for a plain application).
+// u, w: sandwich intermediates.
+int apply_fused(rsatb_context* ctx, const rsatb_cheb_op* op, const OpShape& sh, int vdt,
+                int W, const void* in, const void* x, const void* p, void* y, void* u,
+                void* w, double s_out, double s2, double g_p, int dot_mode, const void* psi0,
+                double* partials, double* dots_out, unsigned* counter) {
+    StepArgs last = blank_args(W);
+    last.x = x;
+    last.p = p;
+    last.psi0 = psi0;
+    last.y = y;
+    last.c = op->center;
+    last.s_out = s_out;
+    last.s2 = s2;
+    last.g_p = g_p;
+    last.dot_mode = dot_mode;
+    last.partials = partials;
+    last.dots_out = dots_out;
+    last.counter = counter;
+    if (!sh.sandwich) {
+        last.in = in;
+        return run_step(ctx, op->H, vdt, last);
+    }
+    StepArgs a = blank_args(W);
+    a.in = in;
+    a.y = u;
+    RSATB_TRY(run_step(ctx, op->Z, vdt, a));   // u = Z in
+    a.in = u;
+    a.y = w;
+    RSATB_TRY(run_step(ctx, op->H, vdt, a));   // w = H u
+    last.in = w;
+    return run_step(ctx, op->ZH, vdt, last);   // y = Z^H w, fused epilogue
+}
+
+}  // namespace
+}  // namespace rsatb_b200
+
+using namespace rsatb_b200;
+
+extern "C" {
+
+int rsatb_bsr_mult_dense(rsatb_ctx_t ctx, rsatb_bsr_t A, const void* X, void* Y, int n_vectors,
+                         rsatb_dtype vec_dtype, double alpha) {
+    clear_error();
+    RSATB_TRY(check_ctx(ctx));
+    RSATB_TRY(check_bsr(A, "A"));
+    RSATB_TRY(check_vec_dtype(A, vec_dtype, "A"));
+    int W = 0;
+    RSATB_TRY(panel_width(n_vectors, vec_dtype, &W));
+    if (!X || !Y) return set_error(RSATB_INVALID_ARGUMENT, "null multivector");
+    if (!aligned16(X) || !aligned16(Y))
+        return set_error(RSATB_INVALID_ARGUMENT, "multivectors must be 16-byte aligned");
+    if (X == Y) return set_error(RSATB_INVALID_ARGUMENT, "mult_dense cannot run in place");
+    StepArgs a = blank_args(W);
+    a.in = X;
+    a.y = Y;
+    a.s_in = alpha;
+    return run_step(ctx, A, vec_dtype, a);
+}
+
+int rsatb_cheb_apply_op(rsatb_ctx_t ctx, const rsatb_cheb_op* op, const void* X, void* Y,
+                        int n_vectors, rsatb_dtype vec_dtype) {
+    clear_error();
+    RSATB_TRY(check_ctx(ctx));
+    OpShape sh{};
+    RSATB_TRY(check_op(op, vec_dtype, &sh));
+    int W = 0;
+    RSATB_TRY(panel_width(n_vectors, vec_dtype, &W));
+    if (!X || !Y) return set_error(RSATB_INVALID_ARGUMENT, "null multivector");
+    if (!aligned16(X) || !aligned16(Y))
+        return set_error(RSATB_INVALID_ARGUMENT, "multivectors must be 16-byte aligned");
+    if (X == Y) return set_error(RSATB_INVALID_ARGUMENT, "apply_op cannot run in place");
+    const size_t vbytes = round256(size_t(sh.n_rows) * W * dtype_real_size(vec_dtype));
+    void* u = nullptr;
+    void* w = nullptr;
+    if (sh.sandwich) {
+        void* s = nullptr;
+        RSATB_TRY(ctx_scratch(ctx, 2 * vbytes, &s));
+        u = s;
+        w = static_cast<char*>(s) + vbytes;
+    }
+    return apply_fused(ctx, op, sh, vec_dtype, W, X, X, nullptr, Y, u, w, 1.0 / op->half_width,
+                       1.0, 0.0, DOT_NONE, nullptr, nullptr, nullptr, nullptr);
+}
+
+int rsatb_kpm_dos_moments(rsatb_ctx_t ctx, const rsatb_cheb_op* op, const void* psi,
+                          int n_vectors, rsatb_dtype vec_dtype, int n_moments, int doubled,
+                          double* mu_out, double* col_mu_out) {
+    clear_error();
+    RSATB_TRY(check_ctx(ctx));
+    OpShape sh{};
+    RSATB_TRY(check_op(op, vec_dtype, &sh));
+    int W = 0;
+    RSATB_TRY(panel_width(n_vectors, vec_dtype, &W));
+    if (n_moments <= 0) return set_error(RSATB_INVALID_ARGUMENT, "n_moments must be positive");
+    if (!psi || !mu_out) return set_error(RSATB_INVALID_ARGUMENT, "null psi or mu_out");
+    if (!aligned16(psi)) return set_error(RSATB_INVALID_ARGUMENT, "psi must be 16-byte aligned");
+    const bool cv = dtype_is_complex(vec_dtype);
+    const int R = n_vectors;
+
+    // Number of operator applications.
+    int n_steps = 0;
+    if (n_moments > 1) {
+        if (doubled) {
+            n_steps = 1;
+            for (int n = 1; 2 * n + 1 < n_moments; ++n) ++n_steps;
+        } else {
+            n_steps = n_moments - 1;
+        }
+    }
+    const int ndots = doubled ? 2 : 1;
+
+    // Scratch: three rotating panels, the sandwich pair, partial sums, dots.
+    const size_t vbytes = round256(size_t(sh.n_rows) * W * dtype_real_size(vec_dtype));
+    const size_t max_ctas = size_t(ctx->sm_count) * 8;
+    const size_t part_bytes = round256(max_ctas * 2 * W * sizeof(double));
+    const size_t dots_bytes = round256(size_t(n_steps + 1) * 2 * W * sizeof(double));
+    const int n_panels = 3 + (sh.sandwich ? 2 : 0);
+    const size_t total = n_panels * vbytes + part_bytes + dots_bytes;
+    void* s = nullptr;
+    RSATB_TRY(ctx_scratch(ctx, total, &s));
+    char* base = static_cast<char*>(s);
+    void* buf[3] = {base, base + vbytes, base + 2 * vbytes};
+    void* u = sh.sandwich ? base + 3 * vbytes : nullptr;
+    void* w = sh.sandwich ? base + 4 * vbytes : nullptr;
+    double* partials = reinterpret_cast<double*>(base + n_panels * vbytes);
+    double* dots = reinterpret_cast<double*>(base + n_panels * vbytes + part_bytes);
+    unsigned* counter = nullptr;
+    RSATB_TRY(ctx_counters(ctx, 1, &counter));
+
+    // mu_0 = <psi|psi> per column.
+    {
+        StepArgs a = blank_args(W);
+        a.x = psi;
+        a.in = psi;
+        a.partials = partials;
+        a.dots_out = dots;
+        a.counter = counter;
+        RSATB_TRY(run_coldot(ctx, vec_dtype, sh.n_rows, a));
+    }
+    const double inv_hw = 1.0 / op->half_width;
+    // Step 1: psi_1 = Op~ psi_0.  Later steps: psi_{s} = 2 Op~ psi_{s-1} - psi_{s-2}.
+    const void* prev = nullptr;   // psi_{s-2}
+    const void* cur = psi;        // psi_{s-1}
+    int slot = 0;
+    for (int sidx = 1; sidx <= n_steps; ++sidx) {
+        void* out = buf[slot];
+        slot = (slot + 1) % 3;
+        double* dslot = dots + size_t(sidx) * 2 * W;
+        if (sidx == 1) {
+            RSATB_TRY(apply_fused(ctx, op, sh, vec_dtype, W, cur, cur, nullptr, out, u, w, inv_hw,
+                                  1.0, 0.0, doubled ? DOT_DOUBLING : DOT_PLAIN, psi, partials,
+                                  dslot, counter));
+        } else {
+            RSATB_TRY(apply_fused(ctx, op, sh, vec_dtype, W, cur, cur, prev, out, u, w, inv_hw,
+                                  2.0, -1.0, doubled ? DOT_DOUBLING : DOT_PLAIN, psi, partials,
+                                  dslot, counter));
+        }
+        prev = cur;
+        cur = out;
+    }
+
+    std::vector<double> h(size_t(n_steps + 1) * 2 * W);
+    RSATB_CUDA_TRY(cudaMemcpyAsync(h.data(), dots, sizeof(double) * h.size(),
+                                   cudaMemcpyDeviceToHost, ctx->stream));
+    RSATB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+
+    using cd = std::complex<double>;
+    // Per-column dot of slot s, dot d, column q.
+    auto coldot = [&](int sidx, int d, int q) -> cd {
+        const double* p = h.data() + size_t(sidx) * 2 * W + size_t(d) * W;
+        return cv ? cd(p[2 * q], p[2 * q + 1]) : cd(p[q], 0.0);
+    };
+    // Per-column moments, then the column average in column order
+    // (dos.hpp:134-138 averages the per-column dots the same way).
+    std::vector<cd> colmu(size_t(n_moments) * R, cd(0.0, 0.0));
+    for (int q = 0; q < R; ++q) {
+        colmu[q] = coldot(0, 0, q);
+        if (n_moments == 1) continue;
+        if (doubled) {
+            const cd mu0 = colmu[q];
+            const cd mu1 = std::conj(coldot(1, 0, q));  // t0.dot(t1) = conj(<psi1|psi0>)
+            colmu[size_t(1) * R + q] = mu1;
+            for (int sidx = 1; sidx <= n_steps; ++sidx) {
+                if (2 * sidx - 1 < n_moments && 2 * sidx - 1 > 1)
+                    colmu[size_t(2 * sidx - 1) * R + q] = 2.0 * coldot(sidx, 0, q) - mu1;
+                if (2 * sidx < n_moments)
+                    colmu[size_t(2 * sidx) * R + q] = 2.0 * coldot(sidx, 1, q) - mu0;
+            }
+        } else {
+            for (int sidx = 1; sidx <= n_steps; ++sidx)
+                colmu[size_t(sidx) * R + q] = coldot(sidx, 0, q);
+        }
+    }
+    for (int n = 0; n < n_moments; ++n) {
+        cd sum(0.0, 0.0);
+        if (doubled && n >= 1) {
+            // mu_n = 2 * avg(d) - mu_{0 or 1}: average the dots first, as the
+            // reference does, then apply the doubling formula.
+            const int sidx = (n + 1) / 2;
+            const bool odd = n % 2 == 1;
+            cd dsum(0.0, 0.0);
+            for (int q = 0; q < R; ++q) {
+                if (n == 1) dsum += std::conj(coldot(1, 0, q));
+                else dsum += coldot(sidx, odd ? 0 : 1, q);
+            }
+            const cd avg = dsum / double(R);
+            if (n == 1) {
+                sum = avg;
+            } else {
+                cd base(0.0, 0.0);
+                for (int q = 0; q < R; ++q) base += odd ? std::conj(coldot(1, 0, q)) : coldot(0, 0, q);
+                sum = 2.0 * avg - base / double(R);
+            }
+        } else {
+            for (int q = 0; q < R; ++q) sum += colmu[size_t(n) * R + q];
+            sum /= double(R);
+        }
+        mu_out[2 * n] = sum.real();
+        mu_out[2 * n + 1] = sum.imag();
+    }
+    if (col_mu_out) {
+        for (size_t i = 0; i < colmu.size(); ++i) {
+            col_mu_out[2 * i] = colmu[i].real();
+            col_mu_out[2 * i + 1] = colmu[i].imag();
+        }
+    }
+    return RSATB_SUCCESS;
+}
+
+}  // extern "C"

@@ -1,0 +1,63 @@
+// Measured FMA-pipe peak (FP64 or FP32), the denominator of the compute
+// roofline of the SpMM at wide panels, where the block SpMM is bound by the
+// CUDA-core FMA rate rather than by HBM.  Every SM runs independent FMA
+// chains; the result is FLOP/s = 2 * FMAs / elapsed time (CUDA events).
+#include "common.cuh"
+
+namespace rsatb_b200 {
+namespace {
+
+template <typename T>
+__global__ void __launch_bounds__(256) fma_chains(T* out, int iters, T a, T b) {
+    T x0 = T(threadIdx.x) * T(1e-3), x1 = x0 + T(1), x2 = x0 + T(2), x3 = x0 + T(3);
+    T x4 = x0 + T(4), x5 = x0 + T(5), x6 = x0 + T(6), x7 = x0 + T(7);
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            x0 = fma(x0, a, b); x1 = fma(x1, a, b); x2 = fma(x2, a, b); x3 = fma(x3, a, b);
+            x4 = fma(x4, a, b); x5 = fma(x5, a, b); x6 = fma(x6, a, b); x7 = fma(x7, a, b);
+        }
+    }
+    const T s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+    if (s == T(-12345.678)) out[threadIdx.x] = s;  // keeps the chains live
+}
+
+}  // namespace
+}  // namespace rsatb_b200
+
+using namespace rsatb_b200;
+
+extern "C" int rsatb_measure_fma_peak(rsatb_ctx_t ctx, int double_precision, double* flops) {
+    clear_error();
+    RSATB_TRY(check_ctx(ctx));
+    if (!flops) return set_error(RSATB_INVALID_ARGUMENT, "null output");
+    void* sink = nullptr;
+    RSATB_TRY(ctx_scratch(ctx, 4096, &sink));
+    const int threads = 256;
+    const int grid = ctx->sm_count * 8;
+    const int iters = double_precision ? 4096 : 8192;
+    cudaEvent_t e0, e1;
+    RSATB_CUDA_TRY(cudaEventCreate(&e0));
+    RSATB_CUDA_TRY(cudaEventCreate(&e1));
+    float best_ms = 1e30f;
+    for (int rep = 0; rep < 4; ++rep) {
+        RSATB_CUDA_TRY(cudaEventRecord(e0, ctx->stream));
+        if (double_precision)
+            fma_chains<double><<<grid, threads, 0, ctx->stream>>>((double*)sink, iters,
+                                                                   0.999999, 1e-7);
+        else
+            fma_chains<float><<<grid, threads, 0, ctx->stream>>>((float*)sink, iters, 0.9999f,
+                                                                  1e-4f);
+        RSATB_LAUNCH_CHECK(ctx);
+        RSATB_CUDA_TRY(cudaEventRecord(e1, ctx->stream));
+        RSATB_CUDA_TRY(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        RSATB_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+        if (rep > 0 && ms < best_ms) best_ms = ms;  // first run warms up
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    const double fmas = double(grid) * threads * double(iters) * 4.0 * 8.0;
+    *flops = 2.0 * fmas / (double(best_ms) * 1e-3);
+    return RSATB_SUCCESS;
+}

@@ -1,0 +1,288 @@
+"""GPU parity of the KPM path against the CPU oracle.
+
+Tolerances: bit-exact for the seeded sample vectors; 1e-13 relative for
+single FP64 SpMM / operator applications; 1e-10 of mu_0 for FP64 moments
+(the bar of test_dos.cpp:131 and of the FP64 mode); FP32 (mixed) kernels
+against the FP64 oracle at 1e-5 relative per application and a DOS error
+<= 1e-5 of the FP64 DOS peak.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+from _util import adjoint_arrays, random_hermitian_bsr, rel_err, to_oracle
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    return torch
+
+
+def dev_bsr(A, precision="f64", imaginary=False):
+    from rsatb_b200.vbcsr import BlockSpMat
+    M = BlockSpMat(A.row_ptr, A.col_ind, A.values, A.block_size, A.n_block_cols,
+                   imaginary=imaginary)
+    return M.astype("f32") if precision == "f32" else M
+
+
+def to_dev(torch, X, dtype=None):
+    t = torch.as_tensor(np.ascontiguousarray(X)).cuda()
+    return t.to(dtype) if dtype is not None else t
+
+
+# ----------------------------------------------------------- sample vectors
+
+@pytest.mark.parametrize("kind,cplx", [(0, True), (1, False), (1, True), (2, True), (2, False)])
+def test_set_random_bit_exact(torch_cuda, kind, cplx):
+    torch = torch_cuda
+    from rsatb_b200.vbcsr import set_random
+    ids = (np.arange(300) * 7 + 11).astype(np.int64)
+    orbs, R, seed = 3, 5, 20240917
+    want = oracle.set_random(seed, kind, True, ids, orbs, 900, R, cplx)
+    out = torch.empty(900, R, dtype=torch.complex128 if cplx else torch.float64, device="cuda")
+    set_random(out, seed, normalize=True, atom_index=ids, orbitals_per_atom=orbs, kind=kind)
+    got = out.cpu().numpy()
+    assert np.array_equal(got.view(np.float64), want.view(np.float64))
+    # FP32 output is the FP64 value rounded once
+    out32 = torch.empty(900, R, dtype=torch.complex64 if cplx else torch.float32, device="cuda")
+    set_random(out32, seed, normalize=True, atom_index=ids, orbitals_per_atom=orbs, kind=kind)
+    assert np.array_equal(out32.cpu().numpy(), want.astype(np.complex64 if cplx else np.float32))
+
+
+# --------------------------------------------------------------- SpMM
+
+CASES = [
+    # (n_blocks, b, degree, complex matrix, imaginary flag, R, complex vectors)
+    (300, 1, 3, False, False, 8, True),
+    (300, 1, 3, False, False, 3, False),
+    (120, 5, 6, False, False, 32, False),
+    (64, 8, 10, False, False, 128, False),
+    (64, 8, 10, False, False, 16, True),
+    (90, 2, 4, True, False, 4, True),
+    (70, 3, 5, False, False, 6, False),
+    (70, 3, 5, True, False, 3, True),
+    (200, 1, 8, False, True, 48, True),
+    (50, 5, 4, True, False, 2, True),
+    (40, 8, 5, True, False, 8, True),
+]
+
+
+def _panel(rng, n, R, cplx):
+    X = rng.standard_normal((n, R))
+    if cplx:
+        X = X + 1j * rng.standard_normal((n, R))
+    return X
+
+
+@pytest.mark.parametrize("case", CASES)
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_mult_dense_matches_oracle(torch_cuda, case, precision):
+    torch = torch_cuda
+    n, b, deg, cm, imag, R, cv = case
+    A = random_hermitian_bsr(n, b, deg, seed=n + b, complex_values=cm)
+    if imag:
+        A = A.with_values(A.values.real.copy())
+    rng = np.random.default_rng(3)
+    X = _panel(rng, n * b, R, cv)
+    want = oracle.spmm(to_oracle(A, imag=imag), X, alpha=0.75)
+    Ad = dev_bsr(A, precision, imaginary=imag)
+    dt = {("f64", True): torch.complex128, ("f64", False): torch.float64,
+          ("f32", True): torch.complex64, ("f32", False): torch.float32}[(precision, cv)]
+    Xd = to_dev(torch, X, dt)
+    Yd = torch.empty_like(Xd)
+    Ad.mult_dense(Xd, Yd, alpha=0.75)
+    got = Yd.cpu().numpy()
+    tol = 1e-13 if precision == "f64" else 2e-5
+    assert rel_err(got, want) < tol
+
+
+def test_adjoint_matches_host_adjoint(torch_cuda):
+    torch = torch_cuda
+    A = random_hermitian_bsr(80, 3, 4, seed=5, complex_values=True)
+    # make it non-Hermitian so the adjoint matters
+    A = A.with_values(A.values * (1.0 + 0.3j))
+    AH = adjoint_arrays(A)
+    X = _panel(np.random.default_rng(1), 240, 4, True)
+    want = oracle.spmm(to_oracle(AH), X)
+    Ad = dev_bsr(A).adjoint()
+    Xd = to_dev(torch, X)
+    Yd = torch.empty_like(Xd)
+    Ad.mult_dense(Xd, Yd)
+    assert rel_err(Yd.cpu().numpy(), want) < 1e-13
+    # imaginary-unit matrix: (i W)^H = -i W^T
+    W = random_hermitian_bsr(60, 1, 3, seed=9, complex_values=False)
+    W = W.with_values(np.random.default_rng(2).standard_normal(W.values.shape))
+    WH = adjoint_arrays(W)
+    want = oracle.spmm(to_oracle(WH, imag=True), X[:60], alpha=-1.0)
+    Wd = dev_bsr(W, imaginary=True).adjoint()
+    Xd = to_dev(torch, X[:60].copy())
+    Yd = torch.empty_like(Xd)
+    Wd.mult_dense(Xd, Yd)
+    assert rel_err(Yd.cpu().numpy(), want) < 1e-13
+
+
+# ------------------------------------------------------ operators and moments
+
+def graphene_case(n1=12, n2=12):
+    from rsatb_b200 import lattice
+    H, _, _ = lattice.graphene(n1, n2)
+    return H
+
+
+def diamond_case(L=2):
+    from rsatb_b200 import lattice
+    from rsatb_b200.isqrt import graph_inverse_sqrt_host
+    H, S = lattice.diamond_lcao(L=L, seed=3)
+    Z = graph_inverse_sqrt_host(S)
+    return H, S, Z
+
+
+def build_cheby(H, emin, emax, Z=None, precision="f64"):
+    from rsatb_b200.calc import Chebyshev, ISQRTMPreconditioner
+    pre = ISQRTMPreconditioner(dev_bsr(Z)) if Z is not None else None
+    c = Chebyshev(dev_bsr(H), emin, emax, preconditioner=pre)
+    return c.astype("f32") if precision == "f32" else c
+
+
+def oracle_op(H, emin, emax, Z=None):
+    c, hw = (emax + emin) / 2, (emax - emin) / 2
+    if Z is None:
+        return oracle.make_op(to_oracle(H), c, hw)
+    return oracle.make_op(to_oracle(H), c, hw, to_oracle(Z), to_oracle(adjoint_arrays(Z)))
+
+
+def test_apply_op_orthogonal_and_sandwich(torch_cuda):
+    torch = torch_cuda
+    H = graphene_case()
+    X = _panel(np.random.default_rng(4), H.n_rows, 8, True)
+    c = build_cheby(H, -8.7, 8.9)
+    Y = torch.empty(H.n_rows, 8, dtype=torch.complex128, device="cuda")
+    c.apply_op(to_dev(torch, X), Y)
+    assert rel_err(Y.cpu().numpy(), oracle.apply_op(oracle_op(H, -8.7, 8.9), X)) < 1e-13
+    Hd, S, Z = diamond_case()
+    X = _panel(np.random.default_rng(5), Hd.n_rows, 16, False)
+    c = build_cheby(Hd, -12.0, 11.0, Z)
+    Y = torch.empty(Hd.n_rows, 16, dtype=torch.float64, device="cuda")
+    c.apply_op(to_dev(torch, X), Y)
+    assert rel_err(Y.cpu().numpy(), oracle.apply_op(oracle_op(Hd, -12.0, 11.0, Z), X)) < 1e-13
+
+
+def _moment_err(a, b):
+    return float(np.abs(a - b).max() / np.abs(b).max())
+
+
+@pytest.mark.parametrize("doubled", [True, False])
+def test_kpm_moments_graphene_fp64(torch_cuda, doubled):
+    torch = torch_cuda
+    from rsatb_b200.calc import _moments
+    from rsatb_b200.vbcsr import set_random
+    H = graphene_case()
+    emin, emax = -8.6, 8.6
+    R, n_moments = 8, 128
+    psi = torch.empty(H.n_rows, R, dtype=torch.complex128, device="cuda")
+    set_random(psi, 20240917)
+    want_mu, want_col = oracle.kpm_moments(oracle_op(H, emin, emax), psi.cpu().numpy(),
+                                           n_moments, doubled=doubled, per_column=True)
+    mu, col = _moments(build_cheby(H, emin, emax), psi, n_moments, doubled, per_column=True)
+    assert _moment_err(mu, want_mu) < 1e-10
+    assert _moment_err(col, want_col) < 1e-10
+
+
+def test_kpm_moments_doubled_equals_plain(torch_cuda):
+    torch = torch_cuda
+    from rsatb_b200.calc import kpm_dos_moments, kpm_dos_moments_plain
+    from rsatb_b200.vbcsr import set_random
+    H = graphene_case(8, 8)
+    c = build_cheby(H, -8.6, 8.6)
+    psi = torch.empty(H.n_rows, 4, dtype=torch.complex128, device="cuda")
+    set_random(psi, 1)
+    a = kpm_dos_moments(c, psi, 64)
+    b = kpm_dos_moments_plain(c, psi, 64)
+    assert np.abs(a - b).max() < 1e-10
+
+
+def test_kpm_moments_diamond_sandwich_fp64(torch_cuda):
+    torch = torch_cuda
+    from rsatb_b200.calc import kpm_dos_moments
+    from rsatb_b200.vbcsr import set_random
+    H, S, Z = diamond_case()
+    emin, emax = -14.0, 14.0
+    psi = torch.empty(H.n_rows, 16, dtype=torch.float64, device="cuda")
+    set_random(psi, 7, orbitals_per_atom=8)
+    want = oracle.kpm_moments(oracle_op(H, emin, emax, Z), psi.cpu().numpy(), 256)
+    got = kpm_dos_moments(build_cheby(H, emin, emax, Z), psi, 256)
+    assert _moment_err(got, want) < 1e-10
+    assert np.abs(got).max() <= 1.0 + 1e-9  # spectrum inside the window
+
+
+@pytest.mark.parametrize("n_moments", [1, 2, 3, 4, 5, 33])
+def test_kpm_moments_complex_matrix_edge_counts(torch_cuda, n_moments):
+    torch = torch_cuda
+    from rsatb_b200.calc import _moments
+    A = random_hermitian_bsr(40, 2, 3, seed=21, complex_values=True, scale=0.3)
+    psi = _panel(np.random.default_rng(8), 80, 3, True)
+    bound = np.abs(np.linalg.eigvalsh(A.to_dense())).max() + 0.5
+    for doubled in (True, False):
+        want = oracle.kpm_moments(oracle_op(A, -bound, bound), psi, n_moments, doubled=doubled)
+        got, _ = _moments(build_cheby(A, -bound, bound), to_dev(torch, psi), n_moments, doubled)
+        assert got.shape == (n_moments,)
+        assert _moment_err(got, want) < 1e-10
+
+
+def dos_error(mu, mu_ref, nt=200):
+    from rsatb_b200.calc import evaluate_kpm_density
+    i = np.arange(nt)
+    x = np.concatenate([(i - nt) / nt, i / nt])
+    rho = 2 * evaluate_kpm_density(mu, x, 0.5 / nt)
+    ref = 2 * evaluate_kpm_density(mu_ref, x, 0.5 / nt)
+    return float(np.abs(rho - ref).max() / np.abs(ref).max())
+
+
+def test_mixed_precision_dos_error(torch_cuda):
+    """FP32 matrices/vectors with FP64 rescale and dots: DOS within 1e-5 of the
+    FP64 path (peak-normalised), on graphene (orthogonal) and diamond
+    (sandwich)."""
+    torch = torch_cuda
+    from rsatb_b200.calc import kpm_dos_moments
+    from rsatb_b200.vbcsr import set_random
+    H = graphene_case(30, 30)
+    c64 = build_cheby(H, -8.6, 8.6)
+    psi = torch.empty(H.n_rows, 8, dtype=torch.complex128, device="cuda")
+    set_random(psi, 20240917)
+    mu64 = kpm_dos_moments(c64, psi, 512)
+    mu32 = kpm_dos_moments(c64.astype("f32"), psi.to(torch.complex64), 512)
+    assert dos_error(mu32, mu64) < 1e-5
+    Hd, S, Z = diamond_case()
+    c64 = build_cheby(Hd, -14.0, 14.0, Z)
+    psi = torch.empty(Hd.n_rows, 32, dtype=torch.float64, device="cuda")
+    set_random(psi, 4, orbitals_per_atom=8)
+    mu64 = kpm_dos_moments(c64, psi, 1024)
+    mu32 = kpm_dos_moments(c64.astype("f32"), psi.to(torch.float32), 1024)
+    assert dos_error(mu32, mu64) < 1e-5
+
+
+def test_density_matches_oracle(torch_cuda):
+    from rsatb_b200.calc import KpmKernel, evaluate_kpm_density
+    rng = np.random.default_rng(0)
+    mu = rng.standard_normal(300) * np.exp(-np.arange(300) / 60) + 0j
+    mu[0] = 1.0
+    x = np.linspace(-1, 1, 2001)
+    for k in (KpmKernel.Jackson, KpmKernel.None_, KpmKernel.CosTaper, KpmKernel.VpTaper):
+        got = evaluate_kpm_density(mu, x, 1e-3, k)
+        want = oracle.density(mu, x, 1e-3, int(k))
+        assert rel_err(got, want) < 1e-12
+
+
+def test_lanczos_bounds_contain_spectrum(torch_cuda):
+    from rsatb_b200.bounds import estimate_spectral_bounds
+    from rsatb_b200.calc import Chebyshev
+    H = graphene_case(20, 20)
+    emin, emax = estimate_spectral_bounds(Chebyshev(dev_bsr(H), -1, 1))
+    assert emin < -8.1 and emax > 8.1 and emax < 10.5
