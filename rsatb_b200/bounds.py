@@ -28,19 +28,22 @@ def lanczos_extremes(cheby: Chebyshev, steps: int = 20, seed: int = 2):
     if not cheby.H.is_double:
         dt = torch.complex64 if dt == torch.complex128 else torch.float32
     dev = f"cuda:{cheby.H.ctx.device}"
+    real = not dt.is_complex
+    wdt = torch.float64 if real else torch.complex128   # FP64 Lanczos arithmetic
     v = torch.empty(n, 1, dtype=dt, device=dev)
     set_random(v, seed, normalize=True)
-    v = v / torch.linalg.vector_norm(v.to(torch.complex128))
+    v = v.to(wdt)
+    v = v / torch.linalg.vector_norm(v)
     m = min(steps, n)
-    Q = torch.zeros(n, m, dtype=torch.complex128, device=dev)
+    Q = torch.zeros(n, m, dtype=wdt, device=dev)
     alpha = np.zeros(m)
     beta = np.zeros(m)
     w = torch.empty_like(v)
-    q = v.to(torch.complex128)
+    q = v
     for j in range(m):
         Q[:, j] = q[:, 0]
         unit.apply_op(q.to(dt).contiguous(), w)
-        wc = w.to(torch.complex128)
+        wc = w.to(wdt)
         a = torch.vdot(q[:, 0], wc[:, 0]).real.item()
         alpha[j] = a
         wc = wc - Q[:, :j + 1] @ (Q[:, :j + 1].conj().T @ wc)   # full reorthogonalisation

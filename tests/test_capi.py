@@ -54,10 +54,12 @@ def test_invalid_arguments_are_status_codes():
     ctx = context()
     lib = _capi.lib()
     h = C.c_void_p()
-    # column out of range
-    st = lib.rsatb_bsr_create(ctx.handle, 2, 2, 1, 2, np.array([0, 1, 2], np.int32).ctypes.data,
-                              np.array([0, 5], np.int32).ctypes.data,
-                              np.ones(2).ctypes.data, _capi.F64, 0, C.byref(h))
+    # column out of range (arrays kept alive across the call)
+    ptr = np.array([0, 1, 2], np.int32)
+    ind = np.array([0, 5], np.int32)
+    vals = np.ones(2)
+    st = lib.rsatb_bsr_create(ctx.handle, 2, 2, 1, 2, ptr.ctypes.data, ind.ctypes.data,
+                              vals.ctypes.data, _capi.F64, 0, C.byref(h))
     assert st == 1 and b"out of range" in lib.rsatb_last_error()
     A = BlockSpMat([0, 1, 2], [0, 1], np.ones((2, 1, 1)), 1)
     X = torch.ones(2, 3, dtype=torch.float64, device="cuda")
