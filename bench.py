@@ -48,6 +48,10 @@ def parse_args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-moments", type=int, default=8,
                    help="moments in the bounded CPU baseline sample")
+    p.add_argument("--spmm-only", action="store_true",
+                   help="time Y = H X alone on a diamond L^3 H (the ncu profiling case)")
+    p.add_argument("--spmm-L", type=int, default=12)
+    p.add_argument("--spmm-reps", type=int, default=3)
     return p.parse_args()
 
 
@@ -389,8 +393,32 @@ def reference_arm(args, dist):
     print(json.dumps(line), flush=True)
 
 
+def spmm_only(args):
+    """Y = H X on the diamond H at R = 128 and R = 8, FP32 and FP64: the
+    small case the ncu captures of the step kernel use (every operand above
+    the 126 MB L2 for R = 128)."""
+    import torch
+    from rsatb_b200 import lattice
+    from rsatb_b200.vbcsr import BlockSpMat
+    from rsatb_b200.workloads import spmm_bytes, spmm_flops
+    H, _ = lattice.diamond_lcao(L=args.spmm_L, seed=7)
+    A64 = BlockSpMat(H.row_ptr, H.col_ind, H.values, 8)
+    A32 = A64.astype("f32")
+    out = {"n_rows": H.n_rows, "nnz_blocks": int(H.nnz_blocks)}
+    for R in (128, 8):
+        for name, A, dt in (("f32", A32, torch.float32), ("f64", A64, torch.float64)):
+            ms = time_spmm(A, H.n_rows, R, dt, reps=args.spmm_reps)
+            b = spmm_bytes(A, R, torch.empty(0, dtype=dt).element_size())
+            out[f"{name}_R{R}"] = {"ms": round(ms, 4), "gbs": round(b / ms / 1e6, 1),
+                                   "tflops": round(spmm_flops(A, R, False) / ms / 1e9, 2)}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse_args()
+    if args.spmm_only:
+        spmm_only(args)
+        return
     dist = Dist()
     if args.impl == "reference":
         reference_arm(args, dist)

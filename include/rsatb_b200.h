@@ -180,6 +180,24 @@ RSATB_API int rsatb_kpm_dos_moments(rsatb_ctx_t ctx, const rsatb_cheb_op* op, co
                           int n_vectors, rsatb_dtype vec_dtype, int n_moments, int doubled,
                           double* mu_out, double* col_mu_out);
 
+/* rsatb_kpm_dos_moments for callers that cannot allocate device memory:
+ * for example a process whose device memory is reserved in full by another
+ * allocator (a framework's caching pool sized to the whole GPU), where a new
+ * cudaMalloc fails, or a latency-critical loop that cannot take the
+ * device-wide synchronisation of cudaMalloc/cudaFree.  Same arguments,
+ * arithmetic and results as rsatb_kpm_dos_moments; it allocates nothing:
+ * all its temporaries live in one fixed 32 MiB static device array that
+ * every GPU loading the library holds until exit.  The first call on a
+ * device looks up that array's address (make it before any stream capture).
+ * Problems whose temporaries exceed 32 MiB are rejected with
+ * RSATB_INVALID_ARGUMENT; calls overlapping on the GPU share the array and
+ * race, so serialise them.  No counterpart in the reference: RSATB runs on
+ * the CPU and has no device allocations to avoid. */
+RSATB_API int rsatb_kpm_dos_moments_noalloc(rsatb_ctx_t ctx, const rsatb_cheb_op* op,
+                                            const void* psi, int n_vectors,
+                                            rsatb_dtype vec_dtype, int n_moments, int doubled,
+                                            double* mu_out, double* col_mu_out);
+
 /* ------------------------------------------------------------ sample vectors */
 
 /* Seeded sample vectors, the device half of SampleVectors::initialize

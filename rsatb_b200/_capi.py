@@ -74,6 +74,8 @@ SIGNATURES = {
     "rsatb_bsr_mult_dense": (_i, [_vp, _vp, _vp, _vp, _i, _i, _d]),
     "rsatb_cheb_apply_op": (_i, [_vp, C.POINTER(ChebOp), _vp, _vp, _i, _i]),
     "rsatb_kpm_dos_moments": (_i, [_vp, C.POINTER(ChebOp), _vp, _i, _i, _i, _i, _PD, _PD]),
+    "rsatb_kpm_dos_moments_noalloc": (_i, [_vp, C.POINTER(ChebOp), _vp, _i, _i, _i, _i, _PD,
+                                           _PD]),
     "rsatb_set_random": (_i, [_vp, _u64, _i, _i, _vp, _i, _i, _i64, _i, _i64, _i, _vp]),
     "rsatb_evaluate_kpm_density": (_i, [_vp, _PD, _i, _PD, _i, _d, _i, _PD]),
     "rsatb_measure_fma_peak": (_i, [_vp, _i, _PD]),
