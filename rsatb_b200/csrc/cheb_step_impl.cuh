@@ -3,6 +3,7 @@
 #pragma once
 
 #include "cheb_kernels.cuh"
+#include "cheb_staged.cuh"
 
 #include <cstdlib>
 #include <mutex>
@@ -81,6 +82,96 @@ inline int pick_v(int W, bool cv, bool any_b, int block_size, bool dbl) {
     return 0;
 }
 
+constexpr int kNotApplicable = 1000;
+
+inline bool env_force_v1() {
+    const char* s = std::getenv("RSATB_STEP_KERNEL");
+    return s && s[0] == 'v' && s[1] == '1';
+}
+
+// The cp.async-staged kernel (cheb_staged.cuh); kNotApplicable when the
+// panel width has no staged mapping (the caller falls back to the
+// register kernel).
+template <typename VT, typename MT, int B, int V, bool CM, bool CV>
+int launch_staged(rsatb_context* ctx, StepArgs& a) {
+    constexpr int STAGES = 3;
+    const int L = a.W / V;
+    int Lp, n_chunks;
+    if (L <= 32) {
+        if (32 % L) return kNotApplicable;
+        Lp = L;
+        n_chunks = 1;
+    } else {
+        if (L % 32) return kNotApplicable;
+        Lp = 32;
+        n_chunks = L / 32;
+    }
+    const int spw = 32 / Lp;
+    const int wb = staged_warp_bytes<VT, MT, B, V, CM, STAGES>(spw);
+    int warps = 8;
+    while (warps > n_chunks && warps > 1 && warps * wb > 112 * 1024) warps /= 2;
+    if (warps % n_chunks) return kNotApplicable;
+    const int threads = warps * 32;
+    const int ndots = a.dot_mode == DOT_NONE ? 0 : 2;
+    size_t smem = size_t(warps) * wb;
+    const size_t red = size_t(ndots) * threads * V * sizeof(double);
+    if (red > smem) smem = red;
+    if (smem > 227 * 1024) return kNotApplicable;
+    auto kernel = cheb_step_staged<VT, MT, B, V, CM, CV, STAGES>;
+    static bool attr_set = false;  // one kernel per instantiation
+    if (!attr_set) {
+        if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 227 * 1024) != cudaSuccess)
+            return set_error(RSATB_CUDA_ERROR, "cudaFuncSetAttribute (staged step) failed");
+        attr_set = true;
+    }
+    const int64_t items = a.n_block_rows * n_chunks;
+    const int64_t per_cta = int64_t(warps) * spw;
+    const int64_t need = (items + per_cta - 1) / per_cta;
+    const int per_sm = occupancy(reinterpret_cast<const void*>(kernel), threads, smem);
+    int64_t grid = int64_t(ctx->sm_count) * per_sm;
+    if (need < grid) grid = need;
+    if (grid < 1) grid = 1;
+    kernel<<<unsigned(grid), threads, smem, ctx->stream>>>(a, Lp, n_chunks);
+    RSATB_LAUNCH_CHECK(ctx);
+    return RSATB_SUCCESS;
+}
+
+template <typename VT, typename MT, int B, bool CM, bool CV>
+int launch_staged_v(rsatb_context* ctx, int V, StepArgs& a) {
+    switch (V) {
+        case 1:
+            if constexpr (!CV) return launch_staged<VT, MT, B, 1, CM, CV>(ctx, a);
+            break;
+        case 2: return launch_staged<VT, MT, B, 2, CM, CV>(ctx, a);
+        case 4: return launch_staged<VT, MT, B, 4, CM, CV>(ctx, a);
+        case 6:
+            if constexpr (CV) return launch_staged<VT, MT, B, 6, CM, CV>(ctx, a);
+            break;
+    }
+    return kNotApplicable;
+}
+
+// V for the staged kernel: FP64 blocks of 8 take 2 values per thread (the
+// register tile stays near 100 registers), everything else 4 when it fits.
+inline int pick_v_staged(int W, bool cv, int block_size, bool dbl) {
+    const int forced = env_v();
+    auto ok = [&](int v) {
+        if (v <= 0 || v > 6 || W % v) return false;
+        if (cv && v % 2) return false;
+        const int L = W / v;
+        return (L <= 32 && 32 % L == 0) || (L > 32 && L % 32 == 0 && L <= 256);
+    };
+    if (forced && ok(forced)) return forced;
+    const int real64[3] = {2, 4, 1}, real32[3] = {4, 2, 1}, cplx[3] = {4, 2, 6},
+              cplx64[3] = {2, 4, 6};
+    const int* pref = cv ? ((dbl && block_size == 8) ? cplx64 : cplx)
+                         : ((dbl && block_size == 8) ? real64 : real32);
+    for (int i = 0; i < 3; ++i)
+        if (ok(pref[i])) return pref[i];
+    return 0;
+}
+
 template <typename VT, typename MT, int B, bool CM, bool CV>
 int launch_b(rsatb_context* ctx, int V, int64_t rows, StepArgs& a) {
     switch (V) {
@@ -105,6 +196,18 @@ int launch_typed(rsatb_context* ctx, int block_size, StepArgs& a) {
                          "panel width %d (real values per row) has no thread mapping; widths up "
                          "to 1536 are supported", a.W);
     const int64_t rows = a.n_block_rows;
+    if (special && !env_force_v1()) {
+        const int Vs = pick_v_staged(a.W, CV, block_size, sizeof(VT) == 8);
+        int st = kNotApplicable;
+        if (Vs) {
+            switch (block_size) {
+                case 1: st = launch_staged_v<VT, MT, 1, CM, CV>(ctx, Vs, a); break;
+                case 5: st = launch_staged_v<VT, MT, 5, CM, CV>(ctx, Vs, a); break;
+                case 8: st = launch_staged_v<VT, MT, 8, CM, CV>(ctx, Vs, a); break;
+            }
+        }
+        if (st != kNotApplicable) return st;
+    }
     switch (block_size) {
         case 1: return launch_b<VT, MT, 1, CM, CV>(ctx, V, rows, a);
         case 5: return launch_b<VT, MT, 5, CM, CV>(ctx, V, rows, a);

@@ -286,3 +286,33 @@ def test_lanczos_bounds_contain_spectrum(torch_cuda):
     H = graphene_case(20, 20)
     emin, emax = estimate_spectral_bounds(Chebyshev(dev_bsr(H), -1, 1))
     assert emin < -8.1 and emax > 8.1 and emax < 10.5
+
+
+@pytest.mark.parametrize("case", [c for c in CASES if c[1] in (1, 5, 8)])
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_staged_kernel_matches_register_kernel(torch_cuda, case, precision, monkeypatch):
+    """The cp.async-staged step kernel against the register kernel (same
+    summation order), including the fused epilogue and dots."""
+    torch = torch_cuda
+    from rsatb_b200.calc import Chebyshev, _moments
+    n, b, deg, cm, imag, R, cv = case
+    if imag:
+        return
+    A = random_hermitian_bsr(n, b, deg, seed=n + 7 * b, complex_values=cm, scale=0.2)
+    bound = np.abs(np.linalg.eigvalsh(A.to_dense())).max() + 0.5
+    c = build_cheby(A, -bound, bound, precision=precision)
+    X = _panel(np.random.default_rng(11), n * b, R, cv)
+    dt = {("f64", True): torch.complex128, ("f64", False): torch.float64,
+          ("f32", True): torch.complex64, ("f32", False): torch.float32}[(precision, cv)]
+    Xd = to_dev(torch, X, dt)
+    monkeypatch.setenv("RSATB_STEP_KERNEL", "staged")
+    Y1 = torch.empty_like(Xd)
+    c.H.mult_dense(Xd, Y1)
+    mu1, col1 = _moments(c, Xd, 24, True, per_column=True)
+    monkeypatch.setenv("RSATB_STEP_KERNEL", "v1")
+    Y2 = torch.empty_like(Xd)
+    c.H.mult_dense(Xd, Y2)
+    mu2, col2 = _moments(c, Xd, 24, True, per_column=True)
+    tol = 1e-13 if precision == "f64" else 1e-6
+    assert rel_err(Y1.cpu().numpy(), Y2.cpu().numpy()) < tol
+    assert np.abs(col1 - col2).max() <= tol * np.abs(col2).max() * 10
