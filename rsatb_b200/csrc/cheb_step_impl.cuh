@@ -118,12 +118,17 @@ int launch_staged(rsatb_context* ctx, StepArgs& a) {
     if (red > smem) smem = red;
     if (smem > 227 * 1024) return kNotApplicable;
     auto kernel = cheb_step_staged<VT, MT, B, V, CM, CV, STAGES>;
-    static bool attr_set = false;  // one kernel per instantiation
-    if (!attr_set) {
-        if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 227 * 1024) != cudaSuccess)
-            return set_error(RSATB_CUDA_ERROR, "cudaFuncSetAttribute (staged step) failed");
-        attr_set = true;
+    // Raise the dynamic shared-memory limit of this instantiation as far as
+    // this launch needs (a process-wide setting of the function).
+    static size_t attr_bytes = 48 * 1024;
+    if (smem > attr_bytes) {
+        cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               int(smem));
+        if (err != cudaSuccess) {
+            cudaGetLastError();
+            return kNotApplicable;  // the register kernel needs no opt-in
+        }
+        attr_bytes = smem;
     }
     const int64_t items = a.n_block_rows * n_chunks;
     const int64_t per_cta = int64_t(warps) * spw;
