@@ -4,6 +4,7 @@
 
 #include "cheb_kernels.cuh"
 #include "cheb_staged.cuh"
+#include "cheb_rowsplit.cuh"
 
 #include <cstdlib>
 #include <mutex>
@@ -84,9 +85,53 @@ inline int pick_v(int W, bool cv, bool any_b, int block_size, bool dbl) {
 
 constexpr int kNotApplicable = 1000;
 
-inline bool env_force_v1() {
+// RSATB_STEP_KERNEL=v1|staged|rowsplit forces one kernel family (tuning and
+// A/B tests); unset picks by shape and precision.
+inline int env_kernel() {
     const char* s = std::getenv("RSATB_STEP_KERNEL");
-    return s && s[0] == 'v' && s[1] == '1';
+    if (!s) return 0;
+    if (s[0] == 'v' && s[1] == '1') return 1;
+    if (s[0] == 's') return 2;
+    if (s[0] == 'r') return 3;
+    return 0;
+}
+inline bool env_force_v1() { return env_kernel() == 1; }
+
+template <typename VT, int B, int KL, int WW, bool CV>
+int launch_rowsplit_k(rsatb_context* ctx, StepArgs& a) {
+    constexpr int UNROLL = WW <= 8 ? 4 : 2;
+    auto kernel = cheb_step_rowsplit<VT, B, KL, WW, CV, UNROLL>;
+    const int threads = 256;
+    const int ndots = a.dot_mode == DOT_NONE ? 0 : 2;
+    const size_t smem = size_t(ndots) * threads * (WW / KL) * sizeof(double);
+    const int64_t need = (a.n_block_rows + 7) / 8;
+    const int per_sm = occupancy(reinterpret_cast<const void*>(kernel), threads, smem);
+    int64_t grid = int64_t(ctx->sm_count) * per_sm;
+    if (need < grid) grid = need;
+    if (grid < 1) grid = 1;
+    kernel<<<unsigned(grid), threads, smem, ctx->stream>>>(a);
+    RSATB_LAUNCH_CHECK(ctx);
+    return RSATB_SUCCESS;
+}
+
+// Narrow real-matrix panels (W in {4, 8, 16}) with blocks of 5 or 8.
+template <typename VT, bool CM, bool CV>
+int launch_rowsplit(rsatb_context* ctx, int block_size, StepArgs& a) {
+    if constexpr (CM) {
+        return kNotApplicable;
+    } else {
+        if (a.W == 16) {
+            if (block_size == 8) return launch_rowsplit_k<VT, 8, 4, 16, CV>(ctx, a);
+            if (block_size == 5) return launch_rowsplit_k<VT, 5, 4, 16, CV>(ctx, a);
+        } else if (a.W == 8) {
+            if (block_size == 8) return launch_rowsplit_k<VT, 8, 4, 8, CV>(ctx, a);
+            if (block_size == 5) return launch_rowsplit_k<VT, 5, 4, 8, CV>(ctx, a);
+        } else if (a.W == 4 && !CV) {
+            if (block_size == 8) return launch_rowsplit_k<VT, 8, 4, 4, false>(ctx, a);
+            if (block_size == 5) return launch_rowsplit_k<VT, 5, 4, 4, false>(ctx, a);
+        }
+        return kNotApplicable;
+    }
 }
 
 // The cp.async-staged kernel (cheb_staged.cuh); kNotApplicable when the
@@ -178,6 +223,9 @@ inline int pick_v_staged(int W, bool cv, int block_size, bool dbl) {
 }
 
 template <typename VT, typename MT, int B, bool CM, bool CV>
+int launch_b(rsatb_context* ctx, int V, int64_t rows, StepArgs& a);
+
+template <typename VT, typename MT, int B, bool CM, bool CV>
 int launch_b(rsatb_context* ctx, int V, int64_t rows, StepArgs& a) {
     switch (V) {
         case 1:
@@ -201,7 +249,16 @@ int launch_typed(rsatb_context* ctx, int block_size, StepArgs& a) {
                          "panel width %d (real values per row) has no thread mapping; widths up "
                          "to 1536 are supported", a.W);
     const int64_t rows = a.n_block_rows;
-    if (special && !env_force_v1()) {
+    const int forced = env_kernel();
+    if ((forced == 0 || forced == 3) && (block_size == 5 || block_size == 8)) {
+        const int st = launch_rowsplit<VT, CM, CV>(ctx, block_size, a);
+        if (st != kNotApplicable) return st;
+    }
+    // Wide panels: the staged kernel hides the latency of the FP64 tile; the
+    // FP32 register kernel is faster (the smem round trip of X costs more
+    // L1 bandwidth than its latency hiding gains).
+    const bool want_staged = forced == 2 || (forced == 0 && sizeof(VT) == 8);
+    if (special && want_staged) {
         const int Vs = pick_v_staged(a.W, CV, block_size, sizeof(VT) == 8);
         int st = kNotApplicable;
         if (Vs) {
