@@ -93,6 +93,7 @@ inline int env_kernel() {
     if (s[0] == 'v' && s[1] == '1') return 1;
     if (s[0] == 's') return 2;
     if (s[0] == 'r') return 3;
+    if (s[0] == 'h') return 4;  // hybrid: A staged, X prefetched in registers
     return 0;
 }
 inline bool env_force_v1() { return env_kernel() == 1; }
@@ -137,7 +138,7 @@ int launch_rowsplit(rsatb_context* ctx, int block_size, StepArgs& a) {
 // The cp.async-staged kernel (cheb_staged.cuh); kNotApplicable when the
 // panel width has no staged mapping (the caller falls back to the
 // register kernel).
-template <typename VT, typename MT, int B, int V, bool CM, bool CV>
+template <typename VT, typename MT, int B, int V, bool CM, bool CV, bool STAGE_X>
 int launch_staged(rsatb_context* ctx, StepArgs& a) {
     constexpr int STAGES = 3;
     const int L = a.W / V;
@@ -152,7 +153,7 @@ int launch_staged(rsatb_context* ctx, StepArgs& a) {
         n_chunks = L / 32;
     }
     const int spw = 32 / Lp;
-    const int wb = staged_warp_bytes<VT, MT, B, V, CM, STAGES>(spw);
+    const int wb = staged_warp_bytes<VT, MT, B, V, CM, STAGES, STAGE_X>(spw);
     int warps = 8;
     while (warps > n_chunks && warps > 1 && warps * wb > 112 * 1024) warps /= 2;
     if (warps % n_chunks) return kNotApplicable;
@@ -162,7 +163,7 @@ int launch_staged(rsatb_context* ctx, StepArgs& a) {
     const size_t red = size_t(ndots) * threads * V * sizeof(double);
     if (red > smem) smem = red;
     if (smem > 227 * 1024) return kNotApplicable;
-    auto kernel = cheb_step_staged<VT, MT, B, V, CM, CV, STAGES>;
+    auto kernel = cheb_step_staged<VT, MT, B, V, CM, CV, STAGES, STAGE_X>;
     // Raise the dynamic shared-memory limit of this instantiation as far as
     // this launch needs (a process-wide setting of the function).
     static size_t attr_bytes = 48 * 1024;
@@ -187,16 +188,16 @@ int launch_staged(rsatb_context* ctx, StepArgs& a) {
     return RSATB_SUCCESS;
 }
 
-template <typename VT, typename MT, int B, bool CM, bool CV>
+template <typename VT, typename MT, int B, bool CM, bool CV, bool STAGE_X>
 int launch_staged_v(rsatb_context* ctx, int V, StepArgs& a) {
     switch (V) {
         case 1:
-            if constexpr (!CV) return launch_staged<VT, MT, B, 1, CM, CV>(ctx, a);
+            if constexpr (!CV) return launch_staged<VT, MT, B, 1, CM, CV, STAGE_X>(ctx, a);
             break;
-        case 2: return launch_staged<VT, MT, B, 2, CM, CV>(ctx, a);
-        case 4: return launch_staged<VT, MT, B, 4, CM, CV>(ctx, a);
+        case 2: return launch_staged<VT, MT, B, 2, CM, CV, STAGE_X>(ctx, a);
+        case 4: return launch_staged<VT, MT, B, 4, CM, CV, STAGE_X>(ctx, a);
         case 6:
-            if constexpr (CV) return launch_staged<VT, MT, B, 6, CM, CV>(ctx, a);
+            if constexpr (CV) return launch_staged<VT, MT, B, 6, CM, CV, STAGE_X>(ctx, a);
             break;
     }
     return kNotApplicable;
@@ -250,22 +251,29 @@ int launch_typed(rsatb_context* ctx, int block_size, StepArgs& a) {
                          "to 1536 are supported", a.W);
     const int64_t rows = a.n_block_rows;
     const int forced = env_kernel();
-    if ((forced == 0 || forced == 3) && (block_size == 5 || block_size == 8)) {
+    if (forced == 3 && (block_size == 5 || block_size == 8)) {
         const int st = launch_rowsplit<VT, CM, CV>(ctx, block_size, a);
         if (st != kNotApplicable) return st;
     }
-    // Wide panels: the staged kernel hides the latency of the FP64 tile; the
-    // FP32 register kernel is faster (the smem round trip of X costs more
-    // L1 bandwidth than its latency hiding gains).
-    const bool want_staged = forced == 2 || (forced == 0 && sizeof(VT) == 8);
+    // Measured choice (diamond 8x8 blocks, B200): FP64 takes the staged
+    // kernel at every width; FP32 takes it at W = 16 and the register kernel
+    // otherwise.
+    const bool want_staged = forced == 2 || forced == 4 ||
+                             (forced == 0 && (sizeof(VT) == 8 || a.W == 16));
     if (special && want_staged) {
         const int Vs = pick_v_staged(a.W, CV, block_size, sizeof(VT) == 8);
         int st = kNotApplicable;
-        if (Vs) {
+        if (Vs && forced == 4) {
             switch (block_size) {
-                case 1: st = launch_staged_v<VT, MT, 1, CM, CV>(ctx, Vs, a); break;
-                case 5: st = launch_staged_v<VT, MT, 5, CM, CV>(ctx, Vs, a); break;
-                case 8: st = launch_staged_v<VT, MT, 8, CM, CV>(ctx, Vs, a); break;
+                case 1: st = launch_staged_v<VT, MT, 1, CM, CV, false>(ctx, Vs, a); break;
+                case 5: st = launch_staged_v<VT, MT, 5, CM, CV, false>(ctx, Vs, a); break;
+                case 8: st = launch_staged_v<VT, MT, 8, CM, CV, false>(ctx, Vs, a); break;
+            }
+        } else if (Vs) {
+            switch (block_size) {
+                case 1: st = launch_staged_v<VT, MT, 1, CM, CV, true>(ctx, Vs, a); break;
+                case 5: st = launch_staged_v<VT, MT, 5, CM, CV, true>(ctx, Vs, a); break;
+                case 8: st = launch_staged_v<VT, MT, 8, CM, CV, true>(ctx, Vs, a); break;
             }
         }
         if (st != kNotApplicable) return st;
