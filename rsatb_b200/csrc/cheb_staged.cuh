@@ -89,9 +89,9 @@ __device__ __forceinline__ void lds_vals(const T* p, T (&o)[N]) {
 
 // Shared bytes one warp uses: STAGES x (X rows + one A block per sub-group),
 // rounded to 16 bytes.
-template <typename VT, typename MT, int B, int V, bool CM, int STAGES, bool STAGE_X = true>
+template <typename VT, typename MT, int B, int V, bool CM, int STAGES>
 __host__ __device__ constexpr int staged_warp_bytes(int sg_per_warp) {
-    return ((STAGES * ((STAGE_X ? B * 32 * V * int(sizeof(VT)) : 0) +
+    return ((STAGES * (B * 32 * V * int(sizeof(VT)) +
                        sg_per_warp * B * B * (CM ? 2 : 1) * int(sizeof(MT))) +
              15) / 16) * 16;
 }
@@ -144,22 +144,18 @@ __device__ __forceinline__ void reduce_dots_staged(const StepArgs& a, int Lp, in
     }
 }
 
-// STAGE_X = false: only the A blocks go through the shared-memory pipeline;
-// the X rows of block k+1 are loaded into registers while block k is
-// multiplied (less shared-memory traffic, more registers).
-template <typename VT, typename MT, int B, int V, bool CM, bool CV, int STAGES,
-          bool STAGE_X = true>
+template <typename VT, typename MT, int B, int V, bool CM, bool CV, int STAGES>
 __global__ void __launch_bounds__(256) cheb_step_staged(StepArgs a, int Lp, int n_chunks) {
     static_assert(!CV || V % 2 == 0, "complex panels need (re, im) pairs per thread");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int RW = B * (CM ? 2 : 1);       // values per block row of A
     constexpr int BBV = B * RW;                 // values per block
-    constexpr int XS = STAGE_X ? B * 32 * V : 0;  // X values per stage per warp
+    constexpr int XS = B * 32 * V;              // X values per stage per warp
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int spw = 32 / Lp;
     const int sg_local = lane / Lp, lane_in = lane - sg_local * Lp;
     unsigned char* wbase =
-        smem_raw + size_t(warp) * staged_warp_bytes<VT, MT, B, V, CM, STAGES, STAGE_X>(spw);
+        smem_raw + size_t(warp) * staged_warp_bytes<VT, MT, B, V, CM, STAGES>(spw);
     VT* xs = reinterpret_cast<VT*>(wbase);
     MT* as = reinterpret_cast<MT*>(wbase + STAGES * XS * sizeof(VT));
     const unsigned gmask =
@@ -182,14 +178,12 @@ __global__ void __launch_bounds__(256) cheb_step_staged(StepArgs a, int Lp, int 
         const int64_t i = item / n_chunks;
         const int k0 = __ldg(a.row_ptr + i), k1 = __ldg(a.row_ptr + i + 1);
         auto issue = [&](int k, int stage) {
-            if constexpr (STAGE_X) {
-                const int64_t j = __ldg(a.col_ind + k);
-                VT* xdst = xs + stage * XS + lane * V;
+            const int64_t j = __ldg(a.col_ind + k);
+            VT* xdst = xs + stage * XS + lane * V;
 #pragma unroll
-                for (int c = 0; c < B; ++c)
-                    cp_async_span<V * int(sizeof(VT))>(xdst + c * 32 * V,
-                                                       in + (j * B + c) * W + int64_t(g) * V);
-            }
+            for (int c = 0; c < B; ++c)
+                cp_async_span<V * int(sizeof(VT))>(xdst + c * 32 * V,
+                                                   in + (j * B + c) * W + int64_t(g) * V);
             constexpr int ABYTES = BBV * int(sizeof(MT));
             constexpr int C = CopyChunk<ABYTES>::value;
             constexpr int NCH = ABYTES / C;
@@ -207,40 +201,17 @@ __global__ void __launch_bounds__(256) cheb_step_staged(StepArgs a, int Lp, int 
         for (int r = 0; r < B; ++r)
 #pragma unroll
             for (int v = 0; v < V; ++v) acc[r][v] = VT(0);
-        VT xn[B][V];  // register prefetch of the next X rows (STAGE_X = false)
-        if constexpr (!STAGE_X) {
-            if (k0 < k1) {
-                const int64_t j = __ldg(a.col_ind + k0);
-#pragma unroll
-                for (int c = 0; c < B; ++c)
-                    load_vals<VT, V>(in + (j * B + c) * W + int64_t(g) * V, xn[c]);
-            }
-        }
         for (int k = k0; k < k1; ++k) {
             const int kk = k - k0;
             if (k + STAGES - 1 < k1) issue(k + STAGES - 1, (kk + STAGES - 1) % STAGES);
             cp_async_commit();
             VT xb[B][V];
-            if constexpr (!STAGE_X) {
-#pragma unroll
-                for (int c = 0; c < B; ++c)
-#pragma unroll
-                    for (int v = 0; v < V; ++v) xb[c][v] = xn[c][v];
-                if (k + 1 < k1) {
-                    const int64_t j = __ldg(a.col_ind + k + 1);
-#pragma unroll
-                    for (int c = 0; c < B; ++c)
-                        load_vals<VT, V>(in + (j * B + c) * W + int64_t(g) * V, xn[c]);
-                }
-            }
             cp_async_wait<STAGES - 1>();
             __syncwarp(gmask);
             const int stage = kk % STAGES;
-            if constexpr (STAGE_X) {
-                const VT* xsrc = xs + stage * XS + lane * V;
+            const VT* xsrc = xs + stage * XS + lane * V;
 #pragma unroll
-                for (int c = 0; c < B; ++c) lds_vals<VT, V>(xsrc + c * 32 * V, xb[c]);
-            }
+            for (int c = 0; c < B; ++c) lds_vals<VT, V>(xsrc + c * 32 * V, xb[c]);
             const MT* blk = as + (stage * spw + sg_local) * BBV;
 #pragma unroll
             for (int r = 0; r < B; ++r) {

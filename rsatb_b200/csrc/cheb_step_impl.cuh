@@ -93,7 +93,6 @@ inline int env_kernel() {
     if (s[0] == 'v' && s[1] == '1') return 1;
     if (s[0] == 's') return 2;
     if (s[0] == 'r') return 3;
-    if (s[0] == 'h') return 4;  // hybrid: A staged, X prefetched in registers
     return 0;
 }
 inline bool env_force_v1() { return env_kernel() == 1; }
@@ -138,7 +137,7 @@ int launch_rowsplit(rsatb_context* ctx, int block_size, StepArgs& a) {
 // The cp.async-staged kernel (cheb_staged.cuh); kNotApplicable when the
 // panel width has no staged mapping (the caller falls back to the
 // register kernel).
-template <typename VT, typename MT, int B, int V, bool CM, bool CV, bool STAGE_X>
+template <typename VT, typename MT, int B, int V, bool CM, bool CV>
 int launch_staged(rsatb_context* ctx, StepArgs& a) {
     constexpr int STAGES = 3;
     const int L = a.W / V;
@@ -153,7 +152,7 @@ int launch_staged(rsatb_context* ctx, StepArgs& a) {
         n_chunks = L / 32;
     }
     const int spw = 32 / Lp;
-    const int wb = staged_warp_bytes<VT, MT, B, V, CM, STAGES, STAGE_X>(spw);
+    const int wb = staged_warp_bytes<VT, MT, B, V, CM, STAGES>(spw);
     int warps = 8;
     while (warps > n_chunks && warps > 1 && warps * wb > 112 * 1024) warps /= 2;
     if (warps % n_chunks) return kNotApplicable;
@@ -163,7 +162,7 @@ int launch_staged(rsatb_context* ctx, StepArgs& a) {
     const size_t red = size_t(ndots) * threads * V * sizeof(double);
     if (red > smem) smem = red;
     if (smem > 227 * 1024) return kNotApplicable;
-    auto kernel = cheb_step_staged<VT, MT, B, V, CM, CV, STAGES, STAGE_X>;
+    auto kernel = cheb_step_staged<VT, MT, B, V, CM, CV, STAGES>;
     // Raise the dynamic shared-memory limit of this instantiation as far as
     // this launch needs (a process-wide setting of the function).
     static size_t attr_bytes = 48 * 1024;
@@ -188,16 +187,16 @@ int launch_staged(rsatb_context* ctx, StepArgs& a) {
     return RSATB_SUCCESS;
 }
 
-template <typename VT, typename MT, int B, bool CM, bool CV, bool STAGE_X>
+template <typename VT, typename MT, int B, bool CM, bool CV>
 int launch_staged_v(rsatb_context* ctx, int V, StepArgs& a) {
     switch (V) {
         case 1:
-            if constexpr (!CV) return launch_staged<VT, MT, B, 1, CM, CV, STAGE_X>(ctx, a);
+            if constexpr (!CV) return launch_staged<VT, MT, B, 1, CM, CV>(ctx, a);
             break;
-        case 2: return launch_staged<VT, MT, B, 2, CM, CV, STAGE_X>(ctx, a);
-        case 4: return launch_staged<VT, MT, B, 4, CM, CV, STAGE_X>(ctx, a);
+        case 2: return launch_staged<VT, MT, B, 2, CM, CV>(ctx, a);
+        case 4: return launch_staged<VT, MT, B, 4, CM, CV>(ctx, a);
         case 6:
-            if constexpr (CV) return launch_staged<VT, MT, B, 6, CM, CV, STAGE_X>(ctx, a);
+            if constexpr (CV) return launch_staged<VT, MT, B, 6, CM, CV>(ctx, a);
             break;
     }
     return kNotApplicable;
@@ -258,22 +257,15 @@ int launch_typed(rsatb_context* ctx, int block_size, StepArgs& a) {
     // Measured choice (diamond 8x8 blocks, B200): FP64 takes the staged
     // kernel at every width; FP32 takes it at W = 16 and the register kernel
     // otherwise.
-    const bool want_staged = forced == 2 || forced == 4 ||
-                             (forced == 0 && (sizeof(VT) == 8 || a.W == 16));
+    const bool want_staged = forced == 2 || (forced == 0 && (sizeof(VT) == 8 || a.W == 16));
     if (special && want_staged) {
         const int Vs = pick_v_staged(a.W, CV, block_size, sizeof(VT) == 8);
         int st = kNotApplicable;
-        if (Vs && forced == 4) {
+        if (Vs) {
             switch (block_size) {
-                case 1: st = launch_staged_v<VT, MT, 1, CM, CV, false>(ctx, Vs, a); break;
-                case 5: st = launch_staged_v<VT, MT, 5, CM, CV, false>(ctx, Vs, a); break;
-                case 8: st = launch_staged_v<VT, MT, 8, CM, CV, false>(ctx, Vs, a); break;
-            }
-        } else if (Vs) {
-            switch (block_size) {
-                case 1: st = launch_staged_v<VT, MT, 1, CM, CV, true>(ctx, Vs, a); break;
-                case 5: st = launch_staged_v<VT, MT, 5, CM, CV, true>(ctx, Vs, a); break;
-                case 8: st = launch_staged_v<VT, MT, 8, CM, CV, true>(ctx, Vs, a); break;
+                case 1: st = launch_staged_v<VT, MT, 1, CM, CV>(ctx, Vs, a); break;
+                case 5: st = launch_staged_v<VT, MT, 5, CM, CV>(ctx, Vs, a); break;
+                case 8: st = launch_staged_v<VT, MT, 8, CM, CV>(ctx, Vs, a); break;
             }
         }
         if (st != kNotApplicable) return st;
