@@ -225,6 +225,74 @@ RSATB_API int rsatb_evaluate_kpm_density(rsatb_ctx_t ctx, const double* moments,
                                const double* x, int nx, double edge_inset, int kernel,
                                double* rho_out);
 
+/* ------------------------------------------- batched dense inverse square root */
+
+/* Arithmetic of the batched Newton-Schulz solve. */
+typedef enum {
+    RSATB_NS_FP64 = 0,     /* every iteration in FP64 */
+    RSATB_NS_TF32X3 = 1,   /* tensor-core phase in split TF32 (hi*hi + hi*lo + lo*hi, FP32
+                              accumulation in TMEM), then FP64 refinement iterations */
+    RSATB_NS_TF32 = 2      /* tensor-core phase in plain TF32, then FP64 refinement */
+} rsatb_ns_precision;
+
+/* Options of rsatb_isqrt_columns_batched.  Zero fields take the defaults in
+ * brackets. */
+typedef struct {
+    int precision;          /* rsatb_ns_precision [RSATB_NS_FP64 when zero] */
+    int max_iter;           /* iterations of the tensor-core phase [30] */
+    int max_fp64_iter;      /* FP64 iterations [6 after a tensor-core phase, 60 alone] */
+    double tol;             /* stop when ||X - I||_F <= tol, X = Z S Z^T [1e-11] */
+    double accept;          /* a problem whose final ||X - I||_F exceeds this is reported
+                               RSATB_NUMERICAL_FAILURE [1e-6] */
+    size_t workspace_bytes; /* device workspace per chunk of problems [8 GiB] */
+    int no_graph;           /* 0: each chunk's iterations run as one captured CUDA graph */
+} rsatb_isqrt_options;
+
+/* Per-call statistics (host). */
+typedef struct {
+    int chunks;               /* chunks of problems the workspace allowed */
+    int low_iterations;       /* tensor-core iterations run (max over problems) */
+    int fp64_iterations;      /* FP64 iterations run (max over problems) */
+    int n_failed;             /* problems whose status is not RSATB_SUCCESS */
+    double max_residual;      /* max over problems of the final ||X - I||_F */
+    double low_flops;         /* FLOPs the tensor-core tiles executed (2 M N K per product,
+                                 padding included) */
+    double fp64_flops;        /* FLOPs of the FP64 GEMMs (2 n^3 per product) */
+    double useful_flops;      /* 8 n^3 per problem per iteration, both phases */
+    int64_t gemm_launches;    /* GEMM kernel launches */
+    double low_ms, fp64_ms;   /* device time of the two phases (CUDA events), all chunks */
+} rsatb_isqrt_stats;
+
+/* Columns [col_start, col_start + k_cols) of M^{-1/2} for a batch of
+ * symmetric positive definite matrices: the per-subgraph action of
+ * rsatb::calc::isqrt::inverse_sqrt_columns_inplace
+ * (rsatb/calc/isqrt_action.hpp:1343-1422) as called by graph_inverse_sqrt
+ * (rsatb/calc/isqrtm.hpp:149-232), for all subgraphs in one call.
+ *
+ * Problem p: n[p] x n[p] matrix at M + in_offset[p] (device, FP64,
+ * column-major, only the upper triangle is read, as with the reference's
+ * uplo 'U'); its result, n[p] x k_cols[p] column-major, goes to
+ * out + out_offset[p] (device).  n, col_start, k_cols, in_offset and
+ * out_offset are host arrays.  k_cols[p] <= 0 means all n[p] columns.
+ *
+ * Method: the Newton-Schulz iteration of rsatb::calc::inverse_sqrt
+ * (rsatb/calc/isqrtm.hpp:620-807), X = Z S Z^T, P = 1.875 I - 1.25 X +
+ * 0.375 X^2, Z <- P Z, from Z0 = I / sqrt(s) with s the Gershgorin bound
+ * of lambda_max, stopped per problem by the reference's rules (tolerance,
+ * 0.5 % plateau, iteration cap, divergence above 100); dense, per problem,
+ * 1 <= n <= 1024.  The result is (Z + Z^T)/2 of the last iterate.
+ *
+ * status (host, may be NULL) receives one rsatb_status per problem
+ * (RSATB_DIVERGED, or RSATB_NUMERICAL_FAILURE when the final residual
+ * exceeds `accept`); the call itself fails only for invalid arguments or
+ * device errors.  Synchronises the context's stream before returning. */
+RSATB_API int rsatb_isqrt_columns_batched(rsatb_ctx_t ctx, int n_problems, const int32_t* n,
+                                          const int32_t* col_start, const int32_t* k_cols,
+                                          const int64_t* in_offset, const double* M,
+                                          const int64_t* out_offset, double* out,
+                                          const rsatb_isqrt_options* options, int32_t* status,
+                                          rsatb_isqrt_stats* stats);
+
 /* ------------------------------------------------------------ measurement */
 
 /* FMA-pipe throughput of this device in FLOP/s (FP64 if double_precision,

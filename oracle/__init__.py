@@ -254,3 +254,64 @@ def fftcheb(op: OrcOp, V, psi: np.ndarray, n_moments: int, formulation: int = 0,
     if st != 0:
         raise RuntimeError(f"orc_fftcheb failed ({st})")
     return sigma.reshape(n_moments, 6), energy
+
+
+# ----------------------------------------------------- dense inverse square root
+
+EIGEN_CLAMP = 1.0e-12
+
+
+def isqrt_columns_eigen(A: np.ndarray, col_start: int = 0, k: int | None = None,
+                        clamp: float = EIGEN_CLAMP) -> np.ndarray:
+    """Columns [col_start, col_start + k) of the clamped A^{-1/2}: the eigen
+    route of isqrt::eigen_action (rsatb/calc/isqrt_action.hpp:766-795),
+    X = V f(w) V^T E with f(x) = x^-1/2 for x > clamp else 0, FP64 LAPACK
+    (numpy eigh) on the upper triangle."""
+    n = A.shape[0]
+    k = n if k is None or k <= 0 else k
+    w, V = np.linalg.eigh(A, UPLO="U")
+    f = np.where(w > clamp, 1.0 / np.sqrt(np.maximum(w, clamp)), 0.0)
+    return (V * f) @ V[col_start:col_start + k].T
+
+
+def ns_inverse_sqrt_dense(S: np.ndarray, tol: float = 1e-11, maxit: int = 60):
+    """Dense FP64 restatement of rsatb::calc::inverse_sqrt's Newton-Schulz
+    loop (rsatb/calc/isqrtm.hpp:613-700 and the residual of :370-405 on a
+    dense matrix, ||X - I||_F): X = Z S Z^T, P = 1.875 I - 1.25 X +
+    0.375 X^2, Z <- P Z, from Z0 = I / sqrt(max row sum |S|), while
+    norm > tol, count < maxit and |norm_pre - norm| > 0.005 norm; a residual
+    above 100 is a divergence.  Returns (Z, report dict)."""
+    n = S.shape[0]
+    s = np.abs(S).sum(axis=1).max()
+    Z = np.eye(n) / np.sqrt(s)
+    I = np.eye(n)
+
+    def resid(Z):
+        X = Z @ S @ Z.T
+        return X, float(np.linalg.norm(X - I))
+
+    X, norm = resid(Z)
+    norm_pre, count, diverged = 0.0, 0, False
+    while norm > tol and count < maxit and abs(norm_pre - norm) > 0.005 * norm:
+        if norm > 100.0:
+            diverged = True
+            break
+        norm_pre = norm
+        P = 1.875 * I - 1.25 * X + 0.375 * X @ X
+        Z = P @ Z
+        count += 1
+        X, norm = resid(Z)
+    return Z, {"residual": norm, "iterations": count, "diverged": diverged,
+               "converged": (not diverged) and norm <= tol,
+               "hit_maxiter": (not diverged) and count >= maxit and norm > tol}
+
+
+def spd_from_spectrum(lam: np.ndarray, seed: int) -> np.ndarray:
+    """Q diag(lam) Q^T with Q from the QR of a seeded Gaussian matrix, the
+    construction of the reference's isqrt benchmark problems
+    (rsatb/calc/test/benchmark_isqrt_action.cpp:87-140)."""
+    rng = np.random.default_rng(seed)
+    n = lam.size
+    Q, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    A = (Q * lam) @ Q.T
+    return 0.5 * (A + A.T)

@@ -44,6 +44,22 @@ class ChebOp(C.Structure):
                 ("center", C.c_double), ("half_width", C.c_double)]
 
 
+class IsqrtOptions(C.Structure):
+    _fields_ = [("precision", C.c_int), ("max_iter", C.c_int), ("max_fp64_iter", C.c_int),
+                ("tol", C.c_double), ("accept", C.c_double), ("workspace_bytes", C.c_size_t),
+                ("no_graph", C.c_int)]
+
+
+class IsqrtStats(C.Structure):
+    _fields_ = [("chunks", C.c_int), ("low_iterations", C.c_int), ("fp64_iterations", C.c_int),
+                ("n_failed", C.c_int), ("max_residual", C.c_double), ("low_flops", C.c_double),
+                ("fp64_flops", C.c_double), ("useful_flops", C.c_double),
+                ("gemm_launches", C.c_int64), ("low_ms", C.c_double), ("fp64_ms", C.c_double)]
+
+
+# rsatb_ns_precision
+NS_FP64, NS_TF32X3, NS_TF32 = 0, 1, 2
+
 _lib = None
 
 # name -> (restype, argtypes)
@@ -78,6 +94,8 @@ SIGNATURES = {
                                            _PD]),
     "rsatb_set_random": (_i, [_vp, _u64, _i, _i, _vp, _i, _i, _i64, _i, _i64, _i, _vp]),
     "rsatb_evaluate_kpm_density": (_i, [_vp, _PD, _i, _PD, _i, _d, _i, _PD]),
+    "rsatb_isqrt_columns_batched": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                         C.POINTER(IsqrtOptions), _vp, C.POINTER(IsqrtStats)]),
     "rsatb_measure_fma_peak": (_i, [_vp, _i, _PD]),
 }
 

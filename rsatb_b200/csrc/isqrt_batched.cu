@@ -1,0 +1,826 @@
+// Batched dense inverse square root by Newton-Schulz: the per-subgraph
+// S^-1/2 action of rsatb's graph-local factor (rsatb/calc/isqrtm.hpp:
+// 149-232, rsatb/calc/isqrt_action.hpp:1343-1422) for all subgraphs at once,
+// with the iteration and stopping rules of rsatb::calc::inverse_sqrt
+// (rsatb/calc/isqrtm.hpp:620-807) applied per problem.
+//
+// Iteration (one step, every GEMM of the form C = A B^T over row-major
+// operands, so both tensor-core operands are K-major):
+//     W = Z S^T            (= Z S, S symmetric)
+//     X = Z W^T            (= Z S Z^T)  -> ||X - I||_F, stopping rules
+//     P = 1.875 I - 1.25 X + 0.375 X X^T
+//     Z' = P Zt^T          (= P Z; Zt is the transposed copy of Z, written
+//                           by the previous Z' epilogue)
+// from Z0 = I / sqrt(s), s = max row sum of |S| >= lambda_max.
+//
+// Phases: an optional tensor-core phase (TF32 or split TF32 on tcgen05,
+// FP32 accumulation) followed by FP64 iterations (SIMT GEMMs) from the
+// symmetrised tensor-core iterate.  Each phase of a chunk is one captured
+// CUDA graph; a problem that stops early is gated off in every later kernel
+// by its `active` flag and its iterate is retired (copied out) at once.
+#include "ns_batched.cuh"
+#include "umma.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <vector>
+
+namespace rsatb_b200 {
+namespace ns {
+namespace {
+
+// ------------------------------------------------------------ kernels
+
+// S (row-major, padded, symmetric from the upper triangle of the
+// column-major input) in FP64 and, for a tensor-core phase, as TF32 hi/lo.
+__global__ void pack_kernel(const Prob* probs, const int64_t* in_off, const double* M,
+                            double* s64, float* s_hi, float* s_lo) {
+    const Prob pr = probs[blockIdx.x];
+    const double* src = M + in_off[blockIdx.x];
+    const int np = pr.n_pad, n = pr.n;
+    for (int64_t e = threadIdx.x; e < int64_t(np) * np; e += blockDim.x) {
+        const int r = int(e / np), c = int(e - int64_t(r) * np);
+        double v = 0.0;
+        if (r < n && c < n) v = (r <= c) ? src[int64_t(c) * n + r] : src[int64_t(r) * n + c];
+        s64[pr.off + e] = v;
+        if (s_hi) {
+            const float f = float(v);
+            const float h = umma::to_tf32(f);
+            s_hi[pr.off + e] = h;
+            s_lo[pr.off + e] = f - h;
+        }
+    }
+}
+
+// Gershgorin scale and the starting iterate Z0 = I / sqrt(s) (in FP32
+// hi/lo with its transposed copy, or in FP64); state reset.
+__global__ void init_kernel(const Prob* probs, const double* s64, State* st, float* z_hi,
+                            float* z_lo, float* zt_hi, float* zt_lo, double* z64,
+                            double* scale, int cap) {
+    const Prob pr = probs[blockIdx.x];
+    const int np = pr.n_pad, n = pr.n;
+    __shared__ double red[256];
+    double m = 0.0;
+    for (int r = threadIdx.x; r < n; r += blockDim.x) {
+        double s = 0.0;
+        const double* row = s64 + pr.off + int64_t(r) * np;
+        for (int c = 0; c < n; ++c) s += fabs(row[c]);
+        m = fmax(m, s);
+    }
+    red[threadIdx.x] = m;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + w]);
+        __syncthreads();
+    }
+    const double s = red[0];
+    const double z0 = s > 0.0 ? 1.0 / sqrt(s) : 0.0;
+    for (int64_t e = threadIdx.x; e < int64_t(np) * np; e += blockDim.x) {
+        const int r = int(e / np), c = int(e - int64_t(r) * np);
+        const double v = (r == c && r < n) ? z0 : 0.0;
+        if (z_hi) {
+            const float f = float(v);
+            const float h = umma::to_tf32(f);
+            z_hi[pr.off + e] = h;
+            z_lo[pr.off + e] = f - h;
+            zt_hi[pr.off + e] = h;
+            zt_lo[pr.off + e] = f - h;
+        }
+        if (z64) z64[pr.off + e] = v;
+    }
+    if (threadIdx.x == 0) {
+        scale[blockIdx.x] = s;
+        State x;
+        x.norm = 0.0;
+        x.norm_pre = 0.0;
+        x.count = 0;
+        x.active = (s > 0.0 && isfinite(s)) ? 1 : 0;
+        x.retire = 0;
+        x.status = x.active ? RSATB_SUCCESS : RSATB_NOT_POSITIVE_DEFINITE;
+        x.cap = cap;
+        x.restart = 0;
+        st[blockIdx.x] = x;
+    }
+}
+
+// Re-arms the problems for the FP64 phase.  A problem the tensor-core
+// phase left far from convergence (diverged, or stopped with ||X - I||_F
+// above restart_above: a spectrum the low precision cannot resolve) starts
+// over from Z0 in FP64 with the cap restart_cap; the others refine the
+// tensor-core iterate with the cap `cap`.  Problems not re-armed are marked
+// for the output copy of their last iterate.  The tensor-core phase's
+// update count is kept in low_count.
+__global__ void rearm_kernel(int np_count, State* st, int* low_count, int from_low, int cap,
+                             int restart_cap, double restart_above) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np_count) return;
+    State x = st[p];
+    low_count[p] = x.count;
+    x.restart = 0;
+    x.cap = cap;
+    if (from_low && (x.status == RSATB_DIVERGED ||
+                     (x.status == RSATB_SUCCESS && !(x.norm <= restart_above)))) {
+        x.status = RSATB_SUCCESS;
+        x.restart = 1;
+        x.cap = restart_cap;
+    }
+    x.active = (x.status == RSATB_SUCCESS) ? 1 : 0;
+    x.retire = x.active ? 0 : 1;
+    x.count = 0;
+    x.norm_pre = 0.0;
+    st[p] = x;
+}
+
+// Z64 = I / sqrt(s) for the problems the FP64 phase restarts.
+__global__ void restart_kernel(const Prob* probs, const State* st, const double* scale,
+                               double* z64) {
+    if (!st[blockIdx.x].restart) return;
+    const Prob pr = probs[blockIdx.x];
+    const int np = pr.n_pad;
+    const double s = scale[blockIdx.x];
+    const double z0 = s > 0.0 ? 1.0 / sqrt(s) : 0.0;
+    for (int64_t e = threadIdx.x; e < int64_t(np) * np; e += blockDim.x) {
+        const int r = int(e / np), c = int(e - int64_t(r) * np);
+        z64[pr.off + e] = (r == c && r < pr.n) ? z0 : 0.0;
+    }
+}
+
+// The loop condition of rsatb/calc/isqrtm.hpp:615-640 for every active
+// problem: continue while norm > tol, count < cap and the residual moved
+// by more than 0.5 %; a residual above 100 is a divergence.  With
+// stop_on_rise (tensor-core phase) a residual that did not fall also stops:
+// in exact arithmetic every eigenvalue error of X shrinks each step, so a
+// rise means the low-precision floor was reached.
+__global__ void control_kernel(int np_count, State* st, double* res2, double tol,
+                               int stop_on_rise) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np_count) return;
+    State x = st[p];
+    x.retire = 0;
+    if (x.active) {
+        const double norm = sqrt(res2[p]);
+        x.norm = norm;
+        bool go = norm > tol && x.count < x.cap && fabs(x.norm_pre - norm) > 0.005 * norm;
+        if (stop_on_rise && x.count > 0 && norm >= x.norm_pre) go = false;
+        if (!(norm <= 100.0)) {  // also catches NaN
+            x.active = 0;
+            x.retire = 1;
+            x.status = RSATB_DIVERGED;
+        } else if (!go) {
+            x.active = 0;
+            x.retire = 1;
+        } else {
+            x.norm_pre = norm;
+            x.count += 1;
+        }
+    }
+    res2[p] = 0.0;
+    st[p] = x;
+}
+
+// FP64 start of the refinement phase for problems the tensor-core phase
+// just stopped: Z64 = (Z + Z^T)/2 of the FP32 iterate (hi + lo).
+__global__ void retire_low_kernel(const Prob* probs, const State* st, const float* z_hi,
+                                  const float* z_lo, double* z64) {
+    if (!st[blockIdx.x].retire) return;
+    const Prob pr = probs[blockIdx.x];
+    const int np = pr.n_pad;
+    for (int64_t e = threadIdx.x; e < int64_t(np) * np; e += blockDim.x) {
+        const int r = int(e / np), c = int(e - int64_t(r) * np);
+        const int64_t t = pr.off + int64_t(c) * np + r;
+        const double a = double(z_hi[pr.off + e]) + double(z_lo[pr.off + e]);
+        const double b = double(z_hi[t]) + double(z_lo[t]);
+        z64[pr.off + e] = 0.5 * (a + b);
+    }
+}
+
+// Result of a problem the FP64 phase just stopped: columns
+// [col_start, col_start + k) of (Z + Z^T)/2, column-major n x k.
+__global__ void retire_out_kernel(const Prob* probs, const State* st, const double* z64,
+                                  const int* col_start, const int* k_cols, const int64_t* out_off,
+                                  double* out) {
+    if (!st[blockIdx.x].retire) return;
+    const Prob pr = probs[blockIdx.x];
+    const int np = pr.n_pad, n = pr.n, c0 = col_start[blockIdx.x], k = k_cols[blockIdx.x];
+    double* dst = out + out_off[blockIdx.x];
+    for (int64_t e = threadIdx.x; e < int64_t(n) * k; e += blockDim.x) {
+        const int j = int(e / n), i = int(e - int64_t(j) * n);
+        const int c = c0 + j;
+        dst[e] = 0.5 * (z64[pr.off + int64_t(i) * np + c] + z64[pr.off + int64_t(c) * np + i]);
+    }
+}
+
+struct F64Item {
+    int p, m0, n0;
+};
+
+// FP64 C = A B^T (BT) or C = A B, 64 x 64 tiles, 256 threads of 4 x 4
+// outputs (rows ty + 16 i, columns tx + 16 j), K chunks of 16 through
+// shared memory; same epilogue modes as the tensor-core kernel.
+template <bool BT>
+__global__ void __launch_bounds__(256) gemm_f64_kernel(const Prob* probs, const F64Item* items,
+                                                       int n_items, const State* st,
+                                                       const double* A, const double* B,
+                                                       double* C, int mode, const double* Xe,
+                                                       double* res2) {
+    __shared__ double As[16][64 + 1];
+    __shared__ double Bs[16][64 + 1];
+    __shared__ double red[8];
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+        const F64Item item = items[it];
+        if (!st[item.p].active) continue;
+        const Prob pr = probs[item.p];
+        const int np = pr.n_pad;
+        const double* Ap = A + pr.off;
+        const double* Bp = B + pr.off;
+        double acc[4][4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+        for (int k0 = 0; k0 < np; k0 += 16) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int idx = threadIdx.x + 256 * q;
+                const int r = idx >> 4, kk = idx & 15;
+                const int m = item.m0 + r;
+                As[kk][r] = m < np ? Ap[int64_t(m) * np + k0 + kk] : 0.0;
+                if (BT) {
+                    const int nn = item.n0 + r;
+                    Bs[kk][r] = nn < np ? Bp[int64_t(nn) * np + k0 + kk] : 0.0;
+                } else {
+                    const int kr = idx >> 6, c = idx & 63;
+                    const int nn = item.n0 + c;
+                    Bs[kr][c] = nn < np ? Bp[int64_t(k0 + kr) * np + nn] : 0.0;
+                }
+            }
+            __syncthreads();
+#pragma unroll
+            for (int kk = 0; kk < 16; ++kk) {
+                double a[4], b[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) a[i] = As[kk][ty + 16 * i];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx + 16 * j];
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+            }
+            __syncthreads();
+        }
+        double r2 = 0.0;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int m = item.m0 + ty + 16 * i;
+            if (m >= np) continue;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int nn = item.n0 + tx + 16 * j;
+                if (nn >= np) continue;
+                const bool valid = m < pr.n && nn < pr.n;
+                const int64_t e = pr.off + int64_t(m) * np + nn;
+                double x = acc[i][j];
+                if (mode == EPI_POLY) x = fma(0.375, x, fma(-1.25, Xe[e], m == nn ? 1.875 : 0.0));
+                if (!valid) x = 0.0;
+                if (mode == EPI_RESID && valid) {
+                    const double d = x - (m == nn ? 1.0 : 0.0);
+                    r2 += d * d;
+                }
+                C[e] = x;
+            }
+        }
+        if (mode == EPI_RESID) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) r2 += __shfl_xor_sync(0xffffffffu, r2, o);
+            if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = r2;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                double s = 0.0;
+                for (int w = 0; w < 8; ++w) s += red[w];
+                if (s != 0.0) atomicAdd(res2 + item.p, s);
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// ------------------------------------------------------------ host side
+
+int ceil_div(int a, int b) { return (a + b - 1) / b; }
+size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+struct Bucket {
+    int n_pad;
+    int first;   // first problem (chunk-local index)
+    int count;
+    int64_t off; // element offset of its first problem
+    int nt;      // N tile of the tensor-core GEMM
+};
+
+// Workspace of one chunk, carved from the context scratch.
+struct Chunk {
+    std::vector<int> ids;  // caller's problem index of each chunk-local problem
+    std::vector<Prob> probs;
+    std::vector<Bucket> buckets;
+    int64_t elems = 0;     // sum of n_pad^2
+};
+
+struct Arrays {
+    // tensor-core phase (nullptr when absent)
+    float *s_hi, *s_lo, *z_hi[2], *z_lo[2], *zt_hi[2], *zt_lo[2], *w_hi, *w_lo, *x_hi, *x_lo,
+        *p_hi, *p_lo;
+    // FP64 phase
+    double *s64, *z64[2], *w64, *x64, *p64;
+};
+
+size_t chunk_bytes(int64_t elems, bool low) {
+    return size_t(elems) * ((low ? 16 * 4 : 0) + 6 * 8);
+}
+
+// A tensor-core phase that stops above this residual has not resolved the
+// spectrum; the FP64 phase starts that problem over from Z0.
+constexpr double kRestartAbove = 0.25;
+
+struct Opts {
+    int precision;
+    int max_iter;
+    int max_fp64;
+    int max_fp64_restart;
+    double tol;
+    double accept;
+    size_t workspace;
+    bool graph;
+};
+
+// Device views of one chunk's tables and arrays.
+struct Dev {
+    Prob* probs;
+    int64_t* in_off;
+    int64_t* out_off;
+    int* col_start;
+    int* k_cols;
+    State* state;
+    double* res2;
+    double* scale;
+    int* low_count;
+    unsigned* error;
+    TcItem* tc_items;
+    F64Item* f64_items;
+    int n_tc_items;
+    int n_f64_items;
+    Arrays a;
+};
+
+template <typename T>
+T* carve(char*& cur, size_t count) {
+    T* p = reinterpret_cast<T*>(cur);
+    cur += align256(count * sizeof(T));
+    return p;
+}
+
+// One tensor-core GEMM over the whole chunk, in launches of at most
+// kMaxBuckets buckets.
+int tc_gemm(rsatb_context* ctx, const Chunk& ch, const Dev& d,
+            const std::vector<int>& group_item_begin, const float* a_hi, const float* a_lo,
+            const float* b_hi, const float* b_lo, float* c_hi, float* c_lo, float* ct_hi,
+            float* ct_lo, int mode, const float* xe_hi, const float* xe_lo, bool split,
+            rsatb_isqrt_stats* stats) {
+    const int nb = int(ch.buckets.size());
+    for (int g0 = 0, gi = 0; g0 < nb; g0 += kMaxBuckets, ++gi) {
+        TcMaps maps;
+        for (int b = g0; b < std::min(nb, g0 + kMaxBuckets); ++b) {
+            const Bucket& bk = ch.buckets[b];
+            const int lb = b - g0;
+            RSATB_TRY(encode_bucket_map(&maps.a_hi[lb], a_hi + bk.off, bk.n_pad, bk.count, 128));
+            RSATB_TRY(encode_bucket_map(&maps.a_lo[lb], a_lo + bk.off, bk.n_pad, bk.count, 128));
+            RSATB_TRY(encode_bucket_map(&maps.b_hi[lb], b_hi + bk.off, bk.n_pad, bk.count, bk.nt));
+            RSATB_TRY(encode_bucket_map(&maps.b_lo[lb], b_lo + bk.off, bk.n_pad, bk.count, bk.nt));
+        }
+        TcArgs args{};
+        args.probs = d.probs;
+        args.items = d.tc_items + group_item_begin[gi];
+        args.n_items = group_item_begin[gi + 1] - group_item_begin[gi];
+        args.state = d.state;
+        args.c_hi = c_hi;
+        args.c_lo = c_lo;
+        args.ct_hi = ct_hi;
+        args.ct_lo = ct_lo;
+        args.xe_hi = xe_hi;
+        args.xe_lo = xe_lo;
+        args.res2 = d.res2;
+        args.mode = mode;
+        args.split = split ? 1 : 0;
+        args.error = d.error;
+        RSATB_TRY(launch_tc_gemm(ctx, maps, args));
+        if (stats) stats->gemm_launches++;
+    }
+    return RSATB_SUCCESS;
+}
+
+template <bool BT>
+int f64_gemm(rsatb_context* ctx, const Dev& d, const double* A, const double* B, double* C,
+             int mode, const double* Xe, rsatb_isqrt_stats* stats) {
+    if (d.n_f64_items == 0) return RSATB_SUCCESS;
+    int grid = ctx->sm_count * 4;
+    if (d.n_f64_items < grid) grid = d.n_f64_items;
+    gemm_f64_kernel<BT><<<grid, 256, 0, ctx->stream>>>(d.probs, d.f64_items, d.n_f64_items,
+                                                       d.state, A, B, C, mode, Xe, d.res2);
+    RSATB_LAUNCH_CHECK(ctx);
+    if (stats) stats->gemm_launches++;
+    return RSATB_SUCCESS;
+}
+
+// Issues `body` either directly or as one captured graph on the context's
+// stream.
+template <typename F>
+int run_phase(rsatb_context* ctx, bool graph, F&& body) {
+    if (!graph || ctx->stream == nullptr) return body();
+    RSATB_CUDA_TRY(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    const int st = body();
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+    if (st != RSATB_SUCCESS) {
+        if (g) cudaGraphDestroy(g);
+        return st;
+    }
+    if (e != cudaSuccess)
+        return set_error(RSATB_CUDA_ERROR, "graph capture failed: %s", cudaGetErrorString(e));
+    cudaGraphExec_t x = nullptr;
+    cudaError_t ie = cudaGraphInstantiate(&x, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess)
+        return set_error(RSATB_CUDA_ERROR, "graph instantiation failed: %s",
+                         cudaGetErrorString(ie));
+    const cudaError_t le = cudaGraphLaunch(x, ctx->stream);
+    const cudaError_t se = cudaStreamSynchronize(ctx->stream);
+    cudaGraphExecDestroy(x);
+    if (le != cudaSuccess)
+        return set_error(RSATB_CUDA_ERROR, "graph launch failed: %s", cudaGetErrorString(le));
+    if (se != cudaSuccess)
+        return set_error(RSATB_CUDA_ERROR, "graph run failed: %s", cudaGetErrorString(se));
+    return RSATB_SUCCESS;
+}
+
+int run_chunk(rsatb_context* ctx, const Opts& o, const Chunk& ch, const int* col_start_h,
+              const int* k_cols_h, const int64_t* in_off_h, const int64_t* out_off_h,
+              const double* M, double* out, std::vector<State>& st_out,
+              std::vector<int>& low_count_out, rsatb_isqrt_stats* stats) {
+    const int P = int(ch.probs.size());
+    const bool low = o.precision != RSATB_NS_FP64;
+    const bool split = o.precision == RSATB_NS_TF32X3;
+
+    // Work items, ordered by bucket (the buckets of a launch group are
+    // contiguous), largest problems first.
+    std::vector<TcItem> tc_items;
+    std::vector<int> group_begin{0};
+    std::vector<F64Item> f64_items;
+    for (size_t b = 0; b < ch.buckets.size(); ++b) {
+        const Bucket& bk = ch.buckets[b];
+        for (int z = 0; z < bk.count; ++z) {
+            const int p = bk.first + z;
+            if (low)
+                for (int m0 = 0; m0 < bk.n_pad; m0 += 128)
+                    for (int n0 = 0; n0 < bk.n_pad; n0 += bk.nt)
+                        tc_items.push_back(TcItem{p, int(b % kMaxBuckets), z, m0, n0, bk.nt});
+            for (int m0 = 0; m0 < bk.n_pad; m0 += 64)
+                for (int n0 = 0; n0 < bk.n_pad; n0 += 64) f64_items.push_back(F64Item{p, m0, n0});
+        }
+        if ((b + 1) % kMaxBuckets == 0 || b + 1 == ch.buckets.size())
+            group_begin.push_back(int(tc_items.size()));
+    }
+
+    // Workspace.
+    const int64_t E = ch.elems;
+    size_t bytes = 0;
+    bytes += align256(P * sizeof(Prob)) + 2 * align256(P * sizeof(int64_t)) +
+             3 * align256(P * sizeof(int)) + align256(P * sizeof(State)) +
+             2 * align256(P * sizeof(double)) + 256 +
+             align256(tc_items.size() * sizeof(TcItem)) +
+             align256(f64_items.size() * sizeof(F64Item));
+    bytes += (low ? 16 * align256(E * sizeof(float)) : 0) + 6 * align256(E * sizeof(double));
+    void* ws = nullptr;
+    RSATB_TRY(ctx_scratch(ctx, bytes, &ws));
+    char* cur = static_cast<char*>(ws);
+    Dev d{};
+    d.probs = carve<Prob>(cur, P);
+    d.in_off = carve<int64_t>(cur, P);
+    d.out_off = carve<int64_t>(cur, P);
+    d.col_start = carve<int>(cur, P);
+    d.k_cols = carve<int>(cur, P);
+    d.low_count = carve<int>(cur, P);
+    d.state = carve<State>(cur, P);
+    d.res2 = carve<double>(cur, P);
+    d.scale = carve<double>(cur, P);
+    d.error = carve<unsigned>(cur, 64);
+    d.tc_items = carve<TcItem>(cur, tc_items.size());
+    d.f64_items = carve<F64Item>(cur, f64_items.size());
+    d.n_tc_items = int(tc_items.size());
+    d.n_f64_items = int(f64_items.size());
+    Arrays& a = d.a;
+    a = Arrays{};
+    if (low) {
+        a.s_hi = carve<float>(cur, E);
+        a.s_lo = carve<float>(cur, E);
+        for (int i = 0; i < 2; ++i) {
+            a.z_hi[i] = carve<float>(cur, E);
+            a.z_lo[i] = carve<float>(cur, E);
+            a.zt_hi[i] = carve<float>(cur, E);
+            a.zt_lo[i] = carve<float>(cur, E);
+        }
+        a.w_hi = carve<float>(cur, E);
+        a.w_lo = carve<float>(cur, E);
+        a.x_hi = carve<float>(cur, E);
+        a.x_lo = carve<float>(cur, E);
+        a.p_hi = carve<float>(cur, E);
+        a.p_lo = carve<float>(cur, E);
+    }
+    a.s64 = carve<double>(cur, E);
+    a.z64[0] = carve<double>(cur, E);
+    a.z64[1] = carve<double>(cur, E);
+    a.w64 = carve<double>(cur, E);
+    a.x64 = carve<double>(cur, E);
+    a.p64 = carve<double>(cur, E);
+
+    // Tables.
+    std::vector<int64_t> in_off(P), out_off(P);
+    std::vector<int> cs(P), kc(P);
+    for (int i = 0; i < P; ++i) {
+        const int id = ch.ids[i];
+        in_off[i] = in_off_h[id];
+        out_off[i] = out_off_h[id];
+        cs[i] = col_start_h ? col_start_h[id] : 0;
+        kc[i] = (k_cols_h && k_cols_h[id] > 0) ? k_cols_h[id] : ch.probs[i].n;
+    }
+    cudaStream_t s = ctx->stream;
+    RSATB_CUDA_TRY(cudaMemcpyAsync(d.probs, ch.probs.data(), P * sizeof(Prob),
+                                   cudaMemcpyHostToDevice, s));
+    RSATB_CUDA_TRY(cudaMemcpyAsync(d.in_off, in_off.data(), P * sizeof(int64_t),
+                                   cudaMemcpyHostToDevice, s));
+    RSATB_CUDA_TRY(cudaMemcpyAsync(d.out_off, out_off.data(), P * sizeof(int64_t),
+                                   cudaMemcpyHostToDevice, s));
+    RSATB_CUDA_TRY(cudaMemcpyAsync(d.col_start, cs.data(), P * sizeof(int),
+                                   cudaMemcpyHostToDevice, s));
+    RSATB_CUDA_TRY(cudaMemcpyAsync(d.k_cols, kc.data(), P * sizeof(int),
+                                   cudaMemcpyHostToDevice, s));
+    if (!tc_items.empty())
+        RSATB_CUDA_TRY(cudaMemcpyAsync(d.tc_items, tc_items.data(),
+                                       tc_items.size() * sizeof(TcItem), cudaMemcpyHostToDevice,
+                                       s));
+    RSATB_CUDA_TRY(cudaMemcpyAsync(d.f64_items, f64_items.data(),
+                                   f64_items.size() * sizeof(F64Item), cudaMemcpyHostToDevice, s));
+    RSATB_CUDA_TRY(cudaMemsetAsync(d.res2, 0, P * sizeof(double), s));
+    RSATB_CUDA_TRY(cudaMemsetAsync(d.error, 0, sizeof(unsigned), s));
+
+    // Pack S and the starting iterate.
+    pack_kernel<<<P, 256, 0, s>>>(d.probs, d.in_off, M, a.s64, a.s_hi, a.s_lo);
+    RSATB_LAUNCH_CHECK(ctx);
+    init_kernel<<<P, 256, 0, s>>>(d.probs, a.s64, d.state, a.z_hi[0], a.z_lo[0], a.zt_hi[0],
+                                  a.zt_lo[0], low ? nullptr : a.z64[0], d.scale,
+                                  low ? o.max_iter : o.max_fp64);
+    RSATB_LAUNCH_CHECK(ctx);
+    const int cb = (P + 255) / 256;
+
+    cudaEvent_t ev[3];
+    for (auto& e : ev) RSATB_CUDA_TRY(cudaEventCreate(&e));
+    struct EvGuard {
+        cudaEvent_t* e;
+        ~EvGuard() {
+            for (int i = 0; i < 3; ++i) cudaEventDestroy(e[i]);
+        }
+    } guard{ev};
+    RSATB_CUDA_TRY(cudaEventRecord(ev[0], s));
+
+    if (low) {
+        RSATB_TRY(prepare_tc_gemm());
+        RSATB_TRY(run_phase(ctx, o.graph, [&]() -> int {
+            for (int k = 0; k <= o.max_iter; ++k) {
+                const int c = k & 1;
+                // W = Z S^T, X = Z W^T (+ residual)
+                RSATB_TRY(tc_gemm(ctx, ch, d, group_begin, a.z_hi[c], a.z_lo[c], a.s_hi, a.s_lo,
+                                  a.w_hi, a.w_lo, nullptr, nullptr, EPI_STORE, nullptr, nullptr,
+                                  split, stats));
+                RSATB_TRY(tc_gemm(ctx, ch, d, group_begin, a.z_hi[c], a.z_lo[c], a.w_hi, a.w_lo,
+                                  a.x_hi, a.x_lo, nullptr, nullptr, EPI_RESID, nullptr, nullptr,
+                                  split, stats));
+                control_kernel<<<cb, 256, 0, s>>>(P, d.state, d.res2, o.tol, 1);
+                RSATB_LAUNCH_CHECK(ctx);
+                retire_low_kernel<<<P, 256, 0, s>>>(d.probs, d.state, a.z_hi[c], a.z_lo[c],
+                                                    a.z64[0]);
+                RSATB_LAUNCH_CHECK(ctx);
+                if (k == o.max_iter) break;
+                // P = 1.875 I - 1.25 X + 0.375 X X^T, Z' = P Z (and Z'^T)
+                RSATB_TRY(tc_gemm(ctx, ch, d, group_begin, a.x_hi, a.x_lo, a.x_hi, a.x_lo,
+                                  a.p_hi, a.p_lo, nullptr, nullptr, EPI_POLY, a.x_hi, a.x_lo,
+                                  split, stats));
+                RSATB_TRY(tc_gemm(ctx, ch, d, group_begin, a.p_hi, a.p_lo, a.zt_hi[c],
+                                  a.zt_lo[c], a.z_hi[c ^ 1], a.z_lo[c ^ 1], a.zt_hi[c ^ 1],
+                                  a.zt_lo[c ^ 1], EPI_STORE, nullptr, nullptr, split, stats));
+            }
+            return RSATB_SUCCESS;
+        }));
+    }
+    RSATB_CUDA_TRY(cudaEventRecord(ev[1], s));
+
+    rearm_kernel<<<cb, 256, 0, s>>>(P, d.state, d.low_count, low ? 1 : 0, o.max_fp64,
+                                    o.max_fp64_restart, kRestartAbove);
+    RSATB_LAUNCH_CHECK(ctx);
+    restart_kernel<<<P, 256, 0, s>>>(d.probs, d.state, d.scale, a.z64[0]);
+    RSATB_LAUNCH_CHECK(ctx);
+    retire_out_kernel<<<P, 256, 0, s>>>(d.probs, d.state, a.z64[0], d.col_start, d.k_cols,
+                                        d.out_off, out);
+    RSATB_LAUNCH_CHECK(ctx);
+    int fp64_steps = o.max_fp64;
+    if (low) {
+        // The FP64 loop is as long as the largest cap among the re-armed
+        // problems (a restart needs the full FP64 iteration count).
+        std::vector<State> h(P);
+        RSATB_CUDA_TRY(cudaMemcpyAsync(h.data(), d.state, P * sizeof(State),
+                                       cudaMemcpyDeviceToHost, s));
+        RSATB_CUDA_TRY(cudaStreamSynchronize(s));
+        for (const State& x : h)
+            if (x.active && x.cap > fp64_steps) fp64_steps = x.cap;
+    }
+
+    RSATB_TRY(run_phase(ctx, o.graph, [&]() -> int {
+        for (int k = 0; k <= fp64_steps; ++k) {
+            const int c = k & 1;
+            RSATB_TRY(f64_gemm<true>(ctx, d, a.z64[c], a.s64, a.w64, EPI_STORE, nullptr, stats));
+            RSATB_TRY(f64_gemm<true>(ctx, d, a.z64[c], a.w64, a.x64, EPI_RESID, nullptr, stats));
+            control_kernel<<<cb, 256, 0, s>>>(P, d.state, d.res2, o.tol, 0);
+            RSATB_LAUNCH_CHECK(ctx);
+            retire_out_kernel<<<P, 256, 0, s>>>(d.probs, d.state, a.z64[c], d.col_start,
+                                                d.k_cols, d.out_off, out);
+            RSATB_LAUNCH_CHECK(ctx);
+            if (k == fp64_steps) break;
+            RSATB_TRY(f64_gemm<true>(ctx, d, a.x64, a.x64, a.p64, EPI_POLY, a.x64, stats));
+            RSATB_TRY(f64_gemm<false>(ctx, d, a.p64, a.z64[c], a.z64[c ^ 1], EPI_STORE, nullptr,
+                                      stats));
+        }
+        return RSATB_SUCCESS;
+    }));
+    RSATB_CUDA_TRY(cudaEventRecord(ev[2], s));
+
+    // Results back.
+    st_out.resize(P);
+    low_count_out.resize(P);
+    unsigned err = 0;
+    RSATB_CUDA_TRY(cudaMemcpyAsync(st_out.data(), d.state, P * sizeof(State),
+                                   cudaMemcpyDeviceToHost, s));
+    RSATB_CUDA_TRY(cudaMemcpyAsync(low_count_out.data(), d.low_count, P * sizeof(int),
+                                   cudaMemcpyDeviceToHost, s));
+    RSATB_CUDA_TRY(cudaMemcpyAsync(&err, d.error, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    RSATB_CUDA_TRY(cudaStreamSynchronize(s));
+    if (err)
+        return set_error(RSATB_CUDA_ERROR,
+                         "tensor-core GEMM gave up on a bounded wait (code %u): a TMA load or an "
+                         "MMA did not complete within 2 s",
+                         err);
+    if (stats) {
+        float t1 = 0.f, t2 = 0.f;
+        cudaEventElapsedTime(&t1, ev[0], ev[1]);
+        cudaEventElapsedTime(&t2, ev[1], ev[2]);
+        stats->low_ms += t1;
+        stats->fp64_ms += t2;
+        for (int i = 0; i < P; ++i) {
+            const double n = ch.probs[i].n, np = ch.probs[i].n_pad;
+            const int lc = low ? low_count_out[i] : 0;
+            const int fc = st_out[i].count;
+            // Tile FLOPs: every pass computes G1, G2; full steps add G3, G4.
+            const int bucket_nt = [&] {
+                for (const Bucket& b : ch.buckets)
+                    if (i >= b.first && i < b.first + b.count) return b.nt;
+                return 0;
+            }();
+            const double tile = 2.0 * ceil_div(int(np), 128) * 128.0 * np *
+                                (ceil_div(int(np), bucket_nt ? bucket_nt : 1) * bucket_nt);
+            if (low) stats->low_flops += tile * (split ? 3 : 1) * (2.0 * (lc + 1) + 2.0 * lc);
+            stats->fp64_flops += 2.0 * n * n * n * (2.0 * (fc + 1) + 2.0 * fc);
+            stats->useful_flops += 8.0 * n * n * n * (lc + fc);
+        }
+    }
+    return RSATB_SUCCESS;
+}
+
+}  // namespace
+}  // namespace ns
+}  // namespace rsatb_b200
+
+using namespace rsatb_b200;
+
+extern "C" int rsatb_isqrt_columns_batched(rsatb_ctx_t ctx, int n_problems, const int32_t* n,
+                                           const int32_t* col_start, const int32_t* k_cols,
+                                           const int64_t* in_offset, const double* M,
+                                           const int64_t* out_offset, double* out,
+                                           const rsatb_isqrt_options* options, int32_t* status,
+                                           rsatb_isqrt_stats* stats) {
+    using namespace rsatb_b200::ns;
+    clear_error();
+    RSATB_TRY(check_ctx(ctx));
+    if (n_problems < 0) return set_error(RSATB_INVALID_ARGUMENT, "n_problems < 0");
+    if (stats) *stats = rsatb_isqrt_stats{};
+    if (n_problems == 0) return RSATB_SUCCESS;
+    if (!n || !in_offset || !out_offset || !M || !out)
+        return set_error(RSATB_INVALID_ARGUMENT, "null argument");
+    Opts o{};
+    o.precision = options ? options->precision : RSATB_NS_FP64;
+    if (o.precision < RSATB_NS_FP64 || o.precision > RSATB_NS_TF32)
+        return set_error(RSATB_INVALID_ARGUMENT, "unknown precision %d", o.precision);
+    const bool low = o.precision != RSATB_NS_FP64;
+    o.max_iter = (options && options->max_iter > 0) ? options->max_iter : 30;
+    o.max_fp64 = (options && options->max_fp64_iter > 0) ? options->max_fp64_iter
+                                                          : (low ? 6 : 60);
+    o.max_fp64_restart = std::max(o.max_fp64, 60);
+    o.tol = (options && options->tol > 0) ? options->tol : 1e-11;
+    o.accept = (options && options->accept > 0) ? options->accept : 1e-6;
+    o.workspace = (options && options->workspace_bytes) ? options->workspace_bytes
+                                                        : (size_t(8) << 30);
+    o.graph = !(options && options->no_graph);
+    for (int p = 0; p < n_problems; ++p) {
+        if (n[p] < 1 || n[p] > 1024)
+            return set_error(RSATB_INVALID_ARGUMENT, "problem %d: n = %d outside [1, 1024]", p,
+                             n[p]);
+        const int c0 = col_start ? col_start[p] : 0;
+        const int k = (k_cols && k_cols[p] > 0) ? k_cols[p] : n[p];
+        if (c0 < 0 || c0 + k > n[p])
+            return set_error(RSATB_INVALID_ARGUMENT,
+                             "problem %d: columns [%d, %d) outside the %d x %d matrix", p, c0,
+                             c0 + k, n[p], n[p]);
+        if (in_offset[p] < 0 || out_offset[p] < 0)
+            return set_error(RSATB_INVALID_ARGUMENT, "problem %d: negative offset", p);
+    }
+    if (!(reinterpret_cast<uintptr_t>(M) % 8 == 0) || !(reinterpret_cast<uintptr_t>(out) % 8 == 0))
+        return set_error(RSATB_INVALID_ARGUMENT, "M and out must be 8-byte aligned");
+
+    // Graph capture needs a capturable stream: on the legacy default stream
+    // the call runs on the context's own stream, ordered after the work
+    // already queued on the caller's.
+    struct StreamSwap {
+        rsatb_context* ctx;
+        cudaStream_t saved;
+        ~StreamSwap() { ctx->stream = saved; }
+    } swap{ctx, ctx->stream};
+    if (o.graph && ctx->stream == nullptr && ctx->own_stream != nullptr) {
+        cudaEvent_t e;
+        RSATB_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        cudaError_t r1 = cudaEventRecord(e, nullptr);
+        cudaError_t r2 = cudaStreamWaitEvent(ctx->own_stream, e, 0);
+        cudaEventDestroy(e);
+        RSATB_CUDA_TRY(r1);
+        RSATB_CUDA_TRY(r2);
+        ctx->stream = ctx->own_stream;
+    }
+
+    // Largest first, so each chunk's buckets are ordered and the persistent
+    // CTAs start on the longest tiles.
+    std::vector<int> order(n_problems);
+    std::iota(order.begin(), order.end(), 0);
+    auto npad = [&](int p) { return (n[p] + 31) / 32 * 32; };
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return npad(x) > npad(y); });
+
+    std::vector<State> st;
+    std::vector<int> lc;
+    size_t pos = 0;
+    while (pos < order.size()) {
+        Chunk ch;
+        int64_t elems = 0;
+        while (pos < order.size()) {
+            const int p = order[pos];
+            const int64_t e = int64_t(npad(p)) * npad(p);
+            if (!ch.ids.empty() && chunk_bytes(elems + e, low) > o.workspace) break;
+            const int np = npad(p);
+            if (ch.buckets.empty() || ch.buckets.back().n_pad != np) {
+                const int tiles = (np + 255) / 256;
+                const int nt = ((np + tiles - 1) / tiles + 15) / 16 * 16;
+                ch.buckets.push_back(Bucket{np, int(ch.ids.size()), 0, elems, nt});
+            }
+            ch.buckets.back().count++;
+            ch.ids.push_back(p);
+            ch.probs.push_back(Prob{n[p], np, elems});
+            elems += e;
+            ++pos;
+        }
+        ch.elems = elems;
+        RSATB_TRY(run_chunk(ctx, o, ch, col_start, k_cols, in_offset, out_offset, M, out, st, lc,
+                            stats));
+        for (size_t i = 0; i < ch.ids.size(); ++i) {
+            const State& x = st[i];
+            int s = x.status;
+            if (s == RSATB_SUCCESS && !(x.norm <= o.accept)) s = RSATB_NUMERICAL_FAILURE;
+            if (status) status[ch.ids[i]] = s;
+            if (stats) {
+                stats->low_iterations = std::max(stats->low_iterations, lc[i]);
+                stats->fp64_iterations = std::max(stats->fp64_iterations, x.count);
+                if (s != RSATB_SUCCESS) stats->n_failed++;
+                if (std::isfinite(x.norm))
+                    stats->max_residual = std::max(stats->max_residual, x.norm);
+                else
+                    stats->max_residual = INFINITY;
+            }
+        }
+        if (stats) stats->chunks++;
+    }
+    return RSATB_SUCCESS;
+}

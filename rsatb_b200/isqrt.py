@@ -9,19 +9,97 @@ pattern).  The per-problem action is selected by ``method``:
 * ``"eigen"``  -- the clamped eigendecomposition route of
   isqrt::eigen_action (rsatb/calc/isqrt_action.hpp:766-795), x -> x^-1/2 for
   x > 1e-12 else 0, which the reference takes for every n <= 256;
-* ``"ns"``     -- the batched Newton-Schulz kernels of the rsatb_b200
-  library (``rsatb_b200.ns``), when built.
+* ``"ns"``, ``"ns_tf32x3"``, ``"ns_tf32"`` -- the batched Newton-Schulz
+  solve of the rsatb_b200 library (``inverse_sqrt_columns_batched``): FP64
+  throughout, or a tcgen05 tensor-core phase (split or plain TF32) finished
+  by FP64 iterations.
 
 The problems are gathered and solved on the GPU in chunks.
 """
 from __future__ import annotations
 
+import ctypes as C
+
 import numpy as np
 import torch
 
+from . import _capi
+from ._capi import check, lib
 from .lattice import BsrArrays, subgraph_problems
+from .vbcsr import context
 
 EIGEN_CLAMP = 1.0e-12  # isqrt::Options::eigen_clamp (isqrt_action.hpp:126)
+
+NS_METHODS = {"ns": "fp64", "ns_tf32x3": "tf32x3", "ns_tf32": "tf32"}
+PRECISIONS = {"fp64": _capi.NS_FP64, "tf32x3": _capi.NS_TF32X3, "tf32": _capi.NS_TF32}
+
+
+def inverse_sqrt_columns_batched(M: torch.Tensor, n, in_offset, col_start=None, k_cols=None,
+                                 out_offset=None, precision: str = "tf32x3",
+                                 max_iter: int = 0, max_fp64_iter: int = 0, tol: float = 0.0,
+                                 accept: float = 0.0, workspace_bytes: int = 0,
+                                 graph: bool = True, out: torch.Tensor | None = None):
+    """Columns [col_start, col_start + k) of M_p^{-1/2} for every problem p
+    (isqrt::inverse_sqrt_columns_inplace, rsatb/calc/isqrt_action.hpp:1343,
+    for a batch), by the library's batched Newton-Schulz solve.
+
+    M: 1-D float64 CUDA tensor holding the matrices, problem p's n_p x n_p
+    column-major matrix at element in_offset[p] (upper triangle read).
+    Returns (out, status, stats): out a 1-D float64 CUDA tensor with problem
+    p's n_p x k_p column-major block at out_offset[p] (packed in problem
+    order when out_offset is None), status one rsatb_status per problem,
+    stats a dict of the call's counters.
+    """
+    if not (M.is_cuda and M.dtype == torch.float64 and M.dim() == 1 and M.is_contiguous()):
+        raise ValueError("M must be a contiguous 1-D float64 CUDA tensor")
+    if precision not in PRECISIONS:
+        raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
+    n = np.ascontiguousarray(np.asarray(n, dtype=np.int32))
+    P = n.size
+    in_offset = np.ascontiguousarray(np.asarray(in_offset, dtype=np.int64))
+    col_start = np.zeros(P, np.int32) if col_start is None else np.ascontiguousarray(
+        np.asarray(col_start, dtype=np.int32))
+    k = n.copy() if k_cols is None else np.ascontiguousarray(np.asarray(k_cols, dtype=np.int32))
+    k = np.where(k > 0, k, n).astype(np.int32)
+    if out_offset is None:
+        sizes = n.astype(np.int64) * k
+        out_offset = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.int64)
+        total = int(sizes.sum())
+    else:
+        out_offset = np.ascontiguousarray(np.asarray(out_offset, dtype=np.int64))
+        total = int((out_offset + n.astype(np.int64) * k).max()) if P else 0
+    if out is None:
+        out = torch.zeros(max(total, 1), dtype=torch.float64, device=M.device)
+    opt = _capi.IsqrtOptions(PRECISIONS[precision], max_iter, max_fp64_iter, tol, accept,
+                             workspace_bytes, 0 if graph else 1)
+    stats = _capi.IsqrtStats()
+    status = np.zeros(P, dtype=np.int32)
+    ctx = context(M.device.index)
+    ctx.bind_stream()
+    vp = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+    check(lib().rsatb_isqrt_columns_batched(
+        ctx.handle, P, vp(n), vp(col_start), vp(k), vp(in_offset), C.c_void_p(M.data_ptr()),
+        vp(out_offset), C.c_void_p(out.data_ptr()), C.byref(opt), vp(status),
+        C.byref(stats)))
+    return out, status, {f: getattr(stats, f) for f, _ in stats._fields_}
+
+
+def inverse_sqrt_rows_batched(M: torch.Tensor, rows: torch.Tensor, b: int,
+                              precision: str = "tf32x3") -> torch.Tensor:
+    """Block row `rows[p]` of M[p]^{-1/2} for a (P, n, n) batch of symmetric
+    matrices, through inverse_sqrt_columns_batched (the columns of a
+    symmetric matrix are its rows)."""
+    P, n, _ = M.shape
+    flat = M.contiguous().reshape(-1)
+    offs = np.arange(P, dtype=np.int64) * n * n
+    cs = (rows.to("cpu").numpy().astype(np.int64) * b).astype(np.int32)
+    out, status, _ = inverse_sqrt_columns_batched(flat, np.full(P, n, np.int32), offs, cs,
+                                                  np.full(P, b, np.int32), precision=precision)
+    bad = np.flatnonzero(status != 0)
+    if bad.size:
+        raise _capi.RsatbError(int(status[bad[0]]),
+                               f"{bad.size} of {P} subgraph problems failed (first: {bad[0]})")
+    return out[:P * n * b].reshape(P, b, n)
 
 
 def _gather_dense(vals: torch.Tensor, gather: torch.Tensor, b: int) -> torch.Tensor:
@@ -84,9 +162,8 @@ def graph_inverse_sqrt(S: BsrArrays, method: str = "eigen", device="cuda",
             X = clamped_inverse_sqrt_rows(M, s_all[start:stop], b)
         elif method == "ns_fp64":
             X = newton_schulz_rows_fp64(M, s_all[start:stop], b)
-        elif method == "ns":
-            from . import ns
-            X = ns.inverse_sqrt_rows(M, s_all[start:stop], b)
+        elif method in NS_METHODS:
+            X = inverse_sqrt_rows_batched(M, s_all[start:stop], b, NS_METHODS[method])
         else:
             raise ValueError(f"unknown isqrt method {method!r}")
         # (P, b, k*b) -> (P, k, b, b): block j of row i

@@ -1,0 +1,146 @@
+"""Batched dense inverse square root (rsatb_isqrt_columns_batched) against
+the oracle: the clamped eigen action (rsatb/calc/isqrt_action.hpp:766-795)
+and the dense Newton-Schulz restatement of rsatb/calc/isqrtm.hpp, whose
+diverging / healthy / capped chain cases follow
+rsatb/calc/test/test_isqrtm.cpp:132-186."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+DIVERGED, NUMERICAL_FAILURE = 19, 6
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    torch.cuda.set_device(0)
+    return torch
+
+
+def _batch(sizes, kappas, seed=11):
+    mats = []
+    for i, (n, kap) in enumerate(zip(sizes, kappas)):
+        lam = np.logspace(-np.log10(kap), 0.0, n) if n > 1 else np.array([0.7])
+        mats.append(oracle.spd_from_spectrum(lam, seed + i))
+    return mats
+
+
+def _pack(torch, mats):
+    offs = np.concatenate([[0], np.cumsum([m.size for m in mats])[:-1]]).astype(np.int64)
+    flat = np.concatenate([m.T.reshape(-1) for m in mats])  # column-major
+    return torch.as_tensor(flat, device="cuda"), offs
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+SIZES = [1, 5, 31, 32, 33, 64, 100, 129, 200, 257, 300, 400]
+KAPPAS = [1.0, 10.0, 1e2, 1e3, 1e5, 1e4, 1e5, 1e2, 1e5, 1e3, 1e4, 1e5]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "tf32x3", "tf32"])
+def test_columns_match_eigen_oracle(torch_cuda, precision):
+    from rsatb_b200.isqrt import inverse_sqrt_columns_batched
+    mats = _batch(SIZES, KAPPAS)
+    M, offs = _pack(torch_cuda, mats)
+    out, status, stats = inverse_sqrt_columns_batched(M, SIZES, offs, precision=precision)
+    assert list(status) == [0] * len(SIZES), status
+    host = out.cpu().numpy()
+    pos = 0
+    for A, n in zip(mats, SIZES):
+        got = host[pos:pos + n * n].reshape(n, n).T
+        pos += n * n
+        want = oracle.isqrt_columns_eigen(A)
+        assert _rel(got, want) < 1e-9, (n, _rel(got, want))
+    assert stats["max_residual"] < 1e-9
+    if precision != "fp64":
+        assert stats["low_iterations"] > 0 and stats["low_flops"] > 0
+    if precision == "tf32x3":
+        # split TF32 resolves kappa <= 1e5: only a few FP64 steps remain
+        assert stats["fp64_iterations"] <= 4
+    else:
+        assert stats["low_flops"] == 0
+
+
+def test_subcolumns_offsets_and_order(torch_cuda):
+    from rsatb_b200.isqrt import inverse_sqrt_columns_batched
+    sizes = [70, 12, 256, 40]
+    mats = _batch(sizes, [1e3, 1e2, 1e4, 1e5], seed=5)
+    M, offs = _pack(torch_cuda, mats)
+    cs = [10, 0, 200, 39]
+    ks = [8, 12, 56, 1]
+    out_off = np.array([5000, 0, 20000, 100], dtype=np.int64)
+    out = torch_cuda.full((40000,), -7.0, dtype=torch_cuda.float64, device="cuda")
+    out, status, _ = inverse_sqrt_columns_batched(M, sizes, offs, cs, ks, out_off,
+                                                  precision="tf32x3", out=out)
+    assert not status.any()
+    host = out.cpu().numpy()
+    for A, n, c, k, o in zip(mats, sizes, cs, ks, out_off):
+        got = host[o:o + n * k].reshape(k, n).T
+        assert _rel(got, oracle.isqrt_columns_eigen(A, c, k)) < 1e-9
+    assert host[4999] == -7.0 and host[1] != -7.0
+
+
+def _chain(off, n=24):
+    return np.eye(n) + off * (np.eye(n, k=1) + np.eye(n, k=-1))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "tf32x3"])
+def test_chain_diverging_healthy_capped(torch_cuda, precision):
+    """test_isqrtm.cpp:132-186: an indefinite chain diverges, a definite one
+    converges, a capped run is neither converged nor diverged."""
+    from rsatb_b200.isqrt import inverse_sqrt_columns_batched
+    mats = [_chain(0.60), _chain(0.49)]
+    M, offs = _pack(torch_cuda, mats)
+    out, status, _ = inverse_sqrt_columns_batched(M, [24, 24], offs, precision=precision,
+                                                  tol=1e-10)
+    assert status[0] == DIVERGED
+    assert status[1] == 0
+    got = out.cpu().numpy()[24 * 24:].reshape(24, 24).T
+    Z, rep = oracle.ns_inverse_sqrt_dense(mats[1], 1e-10, 20)
+    assert rep["converged"] and _rel(got, oracle.isqrt_columns_eigen(mats[1])) < 1e-9
+    _, status, _ = inverse_sqrt_columns_batched(M[24 * 24:], [24], [0], precision="fp64",
+                                                tol=1e-16, max_fp64_iter=1)
+    assert status[0] == NUMERICAL_FAILURE   # capped: above accept, not diverged
+
+
+def test_graph_and_chunks_do_not_change_results(torch_cuda):
+    from rsatb_b200.isqrt import inverse_sqrt_columns_batched
+    sizes = [48, 160, 96, 300, 33, 64]
+    mats = _batch(sizes, [1e2, 1e4, 1e3, 1e5, 10.0, 1e5], seed=21)
+    M, offs = _pack(torch_cuda, mats)
+    a, sa, st_a = inverse_sqrt_columns_batched(M, sizes, offs, precision="tf32x3")
+    b, sb, st_b = inverse_sqrt_columns_batched(M, sizes, offs, precision="tf32x3", graph=False,
+                                               workspace_bytes=4 << 20)
+    assert st_a["chunks"] == 1 and st_b["chunks"] > 1
+    assert not sa.any() and not sb.any()
+    assert torch_cuda.equal(a, b)
+
+
+def test_invalid_arguments_raise(torch_cuda):
+    from rsatb_b200._capi import RsatbError
+    from rsatb_b200.isqrt import inverse_sqrt_columns_batched
+    M = torch_cuda.eye(4, dtype=torch_cuda.float64, device="cuda").reshape(-1)
+    with pytest.raises(RsatbError):
+        inverse_sqrt_columns_batched(M, [0], [0])
+    with pytest.raises(RsatbError):
+        inverse_sqrt_columns_batched(M, [4], [0], [3], [2])
+    with pytest.raises(ValueError):
+        inverse_sqrt_columns_batched(M, [4], [0], precision="bf16")
+
+
+def test_graph_local_factor_ns_matches_eigen(torch_cuda):
+    """Z of the graph-local S^-1/2 (isqrtm.hpp:149-232) through the batched
+    solve equals the clamped-eigen route on a small diamond overlap."""
+    from rsatb_b200 import lattice
+    from rsatb_b200.isqrt import graph_inverse_sqrt
+    _, S = lattice.diamond_lcao(L=2, seed=3)
+    Ze = graph_inverse_sqrt(S, method="eigen")
+    Zn = graph_inverse_sqrt(S, method="ns_tf32x3")
+    assert _rel(Zn.values, Ze.values) < 1e-9

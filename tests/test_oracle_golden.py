@@ -263,3 +263,39 @@ def test_sandwich_equals_orthogonal_on_transformed_operator():
     sig_s, _ = oracle.fftcheb(op_s, Vb, s, 10)
     sig_o, _ = oracle.fftcheb(op_o, [oracle.Bsr.from_dense(v) for v in Vp], s, 10)
     assert np.abs(sig_s - sig_o).max() < 1e-10
+
+
+def test_dense_ns_chain_cases():
+    """rsatb/calc/test/test_isqrtm.cpp:132-186 on the dense restatement: the
+    0.6 chain is indefinite and diverges, 0.49 converges, a 1-step cap is
+    neither converged nor diverged."""
+    n = 24
+
+    def chain(off):
+        return np.eye(n) + off * (np.eye(n, k=1) + np.eye(n, k=-1))
+
+    _, r = oracle.ns_inverse_sqrt_dense(chain(0.60), 1e-10, 20)
+    assert r["diverged"] and not r["converged"]
+    Z, r = oracle.ns_inverse_sqrt_dense(chain(0.49), 1e-10, 20)
+    assert r["converged"] and not r["diverged"]
+    assert np.abs(Z @ chain(0.49) @ Z.T - np.eye(n)).max() < 1e-9
+    _, r = oracle.ns_inverse_sqrt_dense(chain(0.49), 1e-16, 1)
+    assert r["hit_maxiter"] and not r["converged"] and not r["diverged"]
+
+
+def test_dense_ns_and_eigen_route_agree_on_exact_construction():
+    """Q diag(lambda) Q^T problems (benchmark_isqrt_action.cpp:53-140): the
+    NS restatement and the clamped eigen action both reproduce the exact
+    Q diag(lambda^-1/2) Q^T."""
+    rng = np.random.default_rng(4)
+    for n, kappa in ((40, 1e2), (90, 1e5)):
+        lam = np.logspace(-np.log10(kappa), 0.0, n)
+        Q, _ = np.linalg.qr(rng.standard_normal((n, n)))
+        A = (Q * lam) @ Q.T
+        A = 0.5 * (A + A.T)
+        exact = (Q / np.sqrt(lam)) @ Q.T
+        ref = np.linalg.norm(exact)
+        assert np.linalg.norm(oracle.isqrt_columns_eigen(A) - exact) / ref < 1e-10
+        Z, r = oracle.ns_inverse_sqrt_dense(A)
+        assert r["converged"]
+        assert np.linalg.norm(Z - exact) / ref < 1e-10
