@@ -43,7 +43,12 @@ def parse_args():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["diamond", "graphene"], default="diamond")
+    p.add_argument("--workload", choices=["diamond", "graphene", "isqrt"], default="diamond")
+    p.add_argument("--isqrt-n", type=int, default=100_000,
+                   help="problems of the batched inverse-sqrt workload")
+    p.add_argument("--isqrt-precision", choices=["tf32x3", "tf32", "fp64"], default="tf32x3")
+    p.add_argument("--isqrt-ws-gb", type=float, default=24.0,
+                   help="device workspace per chunk of the batched inverse sqrt")
     p.add_argument("--small", action="store_true", help="reduced sizes, for a quick check")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-moments", type=int, default=8,
@@ -414,12 +419,108 @@ def spmm_only(args):
     print(json.dumps(out), flush=True)
 
 
+def bench_isqrt(args, dist):
+    """Batched graph-local S^-1/2: args.isqrt_n SPD problems per GPU, sizes
+    uniform in [40, 400], condition numbers log-uniform in [1e2, 1e5]; each
+    problem returns 16 columns of its inverse square root from column n/3
+    (an interior block row, as the graph-local factor takes).  One step =
+    one rsatb_isqrt_columns_batched call over the whole batch."""
+    import torch
+    import oracle
+    from rsatb_b200 import workloads
+    from rsatb_b200.isqrt import inverse_sqrt_columns_batched
+    t0 = time.perf_counter()
+    batch = workloads.batched_spd(args.isqrt_n, seed=7 + dist.rank)
+    torch.cuda.synchronize()
+    gen_s = time.perf_counter() - t0
+    n = batch.n
+    cs = (n // 3).astype(np.int32)
+    ks = np.minimum(16, n - cs).astype(np.int32)
+    out_off = np.concatenate([[0], np.cumsum(n.astype(np.int64) * ks)[:-1]]).astype(np.int64)
+    out = torch.zeros(int((n.astype(np.int64) * ks).sum()), dtype=torch.float64, device="cuda")
+    ws = int(args.isqrt_ws_gb * (1 << 30))
+
+    def run(prec):
+        return inverse_sqrt_columns_batched(batch.flat, n, batch.offset, cs, ks, out_off,
+                                            precision=prec, out=out, workspace_bytes=ws)
+
+    def timed(prec, steps, warmup):
+        for _ in range(warmup):
+            run(prec)
+        torch.cuda.synchronize()
+        dist.barrier()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record()
+        for _ in range(steps):
+            _, status, stats = run(prec)
+        ev[1].record()
+        torch.cuda.synchronize()
+        dist.barrier()
+        return dist.max(ev[0].elapsed_time(ev[1]) / steps), status, stats
+
+    peaks = measured_peaks()
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        ms, status, stats = timed(args.isqrt_precision, args.steps, args.warmup)
+    clocks = clk.summary()
+    host = out.cpu().numpy()
+    rng = np.random.default_rng(1)
+    sample = rng.choice(n.size, size=min(48, n.size), replace=False)
+    err = 0.0
+    for p in sample:
+        want = oracle.isqrt_columns_eigen(batch.matrix(p), int(cs[p]), int(ks[p]))
+        got = host[out_off[p]:out_off[p] + n[p] * ks[p]].reshape(ks[p], n[p]).T
+        err = max(err, float(np.linalg.norm(got - want) / np.linalg.norm(want)))
+    ms64 = None
+    if args.isqrt_precision != "fp64":
+        ms64, _, stats64 = timed("fp64", 1, 0)
+    fma = fma_peaks()
+    tf32_peak = 0.5 * float(peaks.get("bf16_tflops", 1590.0))
+    low_tfs = stats["low_flops"] / max(stats["low_ms"], 1e-9) / 1e9
+    f64_tfs = stats["fp64_flops"] / max(stats["fp64_ms"], 1e-9) / 1e9
+    units = n.size * dist.world
+    if dist.rank == 0:
+        line = {
+            "metric": "batched graph-local S^-1/2 throughput", "value": round(units / (ms * 1e-3), 1),
+            "unit": "matrices/s", "n_gpus": dist.world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms, 2), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": {"tf32x3": "split TF32 (FP32 accumulate) + FP64 refinement",
+                      "tf32": "TF32 (FP32 accumulate) + FP64 refinement",
+                      "fp64": "f64"}[args.isqrt_precision],
+            "data": "synthetic (seeded Q diag(l) Q^T, continuous spectra)",
+            "config": {"workload": "batched_isqrt: SPD n~U[40,400], kappa log-uniform "
+                                   "[1e2,1e5], 16 columns from n/3 per problem",
+                       "problems_per_gpu": int(n.size), "sum_n_cubed": float((n.astype(
+                           np.float64) ** 3).sum()), "workspace_gb_per_chunk": args.isqrt_ws_gb},
+            "status_failures": int((status != 0).sum()),
+            "max_rel_err_vs_eigh_sample": err, "sample_size": int(sample.size),
+            "stats": {k: (float(f"{v:.4g}") if isinstance(v, float) else v)
+                      for k, v in stats.items()},
+            "roofline": {"bound": "tensor", "achieved": round(low_tfs, 1),
+                         "peak": round(tf32_peak, 1), "unit": "TFLOP/s",
+                         "frac": round(low_tfs / tf32_peak, 4), "traffic": None,
+                         "kernel": "ns tc_gemm_kernel (tcgen05 kind::tf32, executed tile FLOPs)",
+                         "peak_source": "MEASURED_PEAKS.json bf16_tflops / 2 (dense TF32 rate)",
+                         "fp64_phase": {"achieved": round(f64_tfs, 2),
+                                        "peak": round(fma["f64"] / 1e12, 2),
+                                        "frac": round(f64_tfs * 1e12 / fma["f64"], 4)}},
+            "fp64_only_ms_per_step": round(ms64, 2) if ms64 else None,
+            "speedup_vs_fp64_only": round(ms64 / ms, 3) if ms64 else None,
+            "clocks": clocks, "generate_seconds": round(gen_s, 1),
+        }
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     if args.spmm_only:
         spmm_only(args)
         return
     dist = Dist()
+    if args.workload == "isqrt" and args.impl == "ours":
+        bench_isqrt(args, dist)
+        dist.close()
+        return
     if args.impl == "reference":
         reference_arm(args, dist)
         dist.close()

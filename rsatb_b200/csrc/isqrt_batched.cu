@@ -9,13 +9,16 @@
 //     W = Z S^T            (= Z S, S symmetric)
 //     X = Z W^T            (= Z S Z^T)  -> ||X - I||_F, stopping rules
 //     P = 1.875 I - 1.25 X + 0.375 X X^T
-//     Z' = P Zt^T          (= P Z; Zt is the transposed copy of Z, written
-//                           by the previous Z' epilogue)
+//     Z' = ((P + P^T)/2) Z (FP64)
 // from Z0 = I / sqrt(s), s = max row sum of |S| >= lambda_max.
 //
-// Phases: an optional tensor-core phase (TF32 or split TF32 on tcgen05,
-// FP32 accumulation) followed by FP64 iterations (SIMT GEMMs) from the
-// symmetrised tensor-core iterate.  Each phase of a chunk is one captured
+// Phases: an optional tensor-core phase (W, X and P in TF32 or split TF32
+// on tcgen05 with FP32 accumulation; the update of Z in FP64) followed by
+// FP64 iterations (SIMT GEMMs).  The iteration is equivariant under
+// Z -> Q Z for orthogonal Q, so rounding in the update of Z would leave a
+// rotation that no later step corrects; with that one product in FP64 and a
+// symmetric left factor, the low-precision errors only perturb X and are
+// removed by the following steps.  Each phase of a chunk is one captured
 // CUDA graph; a problem that stops early is gated off in every later kernel
 // by its `active` flag and its iterate is retired (copied out) at once.
 #include "ns_batched.cuh"
@@ -53,11 +56,10 @@ __global__ void pack_kernel(const Prob* probs, const int64_t* in_off, const doub
     }
 }
 
-// Gershgorin scale and the starting iterate Z0 = I / sqrt(s) (in FP32
-// hi/lo with its transposed copy, or in FP64); state reset.
+// Gershgorin scale and the starting iterate Z0 = I / sqrt(s) in FP64 (and
+// as TF32 hi/lo for a tensor-core phase); state reset.
 __global__ void init_kernel(const Prob* probs, const double* s64, State* st, float* z_hi,
-                            float* z_lo, float* zt_hi, float* zt_lo, double* z64,
-                            double* scale, int cap) {
+                            float* z_lo, double* z64, double* scale, int cap) {
     const Prob pr = probs[blockIdx.x];
     const int np = pr.n_pad, n = pr.n;
     __shared__ double red[256];
@@ -84,10 +86,8 @@ __global__ void init_kernel(const Prob* probs, const double* s64, State* st, flo
             const float h = umma::to_tf32(f);
             z_hi[pr.off + e] = h;
             z_lo[pr.off + e] = f - h;
-            zt_hi[pr.off + e] = h;
-            zt_lo[pr.off + e] = f - h;
         }
-        if (z64) z64[pr.off + e] = v;
+        z64[pr.off + e] = v;
     }
     if (threadIdx.x == 0) {
         scale[blockIdx.x] = s;
@@ -179,20 +179,15 @@ __global__ void control_kernel(int np_count, State* st, double* res2, double tol
     st[p] = x;
 }
 
-// FP64 start of the refinement phase for problems the tensor-core phase
-// just stopped: Z64 = (Z + Z^T)/2 of the FP32 iterate (hi + lo).
-__global__ void retire_low_kernel(const Prob* probs, const State* st, const float* z_hi,
-                                  const float* z_lo, double* z64) {
+// The FP64 phase starts from z64[0]: a problem the tensor-core phase
+// stopped while its iterate sat in z64[1] is copied over.
+__global__ void retire_low_kernel(const Prob* probs, const State* st, const double* src,
+                                  double* dst) {
     if (!st[blockIdx.x].retire) return;
     const Prob pr = probs[blockIdx.x];
     const int np = pr.n_pad;
-    for (int64_t e = threadIdx.x; e < int64_t(np) * np; e += blockDim.x) {
-        const int r = int(e / np), c = int(e - int64_t(r) * np);
-        const int64_t t = pr.off + int64_t(c) * np + r;
-        const double a = double(z_hi[pr.off + e]) + double(z_lo[pr.off + e]);
-        const double b = double(z_hi[t]) + double(z_lo[t]);
-        z64[pr.off + e] = 0.5 * (a + b);
-    }
+    for (int64_t e = threadIdx.x; e < int64_t(np) * np; e += blockDim.x)
+        dst[pr.off + e] = src[pr.off + e];
 }
 
 // Result of a problem the FP64 phase just stopped: columns
@@ -217,13 +212,16 @@ struct F64Item {
 
 // FP64 C = A B^T (BT) or C = A B, 64 x 64 tiles, 256 threads of 4 x 4
 // outputs (rows ty + 16 i, columns tx + 16 j), K chunks of 16 through
-// shared memory; same epilogue modes as the tensor-core kernel.
-template <bool BT>
+// shared memory; same epilogue modes as the tensor-core kernel.  SYM_A
+// multiplies by (A + A^T)/2 instead of A.  c_hi/c_lo (optional) receive the
+// TF32 hi/lo split of C for the next tensor-core GEMMs.
+template <bool BT, bool SYM_A>
 __global__ void __launch_bounds__(256) gemm_f64_kernel(const Prob* probs, const F64Item* items,
                                                        int n_items, const State* st,
                                                        const double* A, const double* B,
                                                        double* C, int mode, const double* Xe,
-                                                       double* res2) {
+                                                       double* res2, float* c_hi,
+                                                       float* c_lo) {
     __shared__ double As[16][64 + 1];
     __shared__ double Bs[16][64 + 1];
     __shared__ double red[8];
@@ -246,7 +244,9 @@ __global__ void __launch_bounds__(256) gemm_f64_kernel(const Prob* probs, const 
                 const int idx = threadIdx.x + 256 * q;
                 const int r = idx >> 4, kk = idx & 15;
                 const int m = item.m0 + r;
-                As[kk][r] = m < np ? Ap[int64_t(m) * np + k0 + kk] : 0.0;
+                double av = m < np ? Ap[int64_t(m) * np + k0 + kk] : 0.0;
+                if (SYM_A && m < np) av = 0.5 * (av + Ap[int64_t(k0 + kk) * np + m]);
+                As[kk][r] = av;
                 if (BT) {
                     const int nn = item.n0 + r;
                     Bs[kk][r] = nn < np ? Bp[int64_t(nn) * np + k0 + kk] : 0.0;
@@ -290,6 +290,12 @@ __global__ void __launch_bounds__(256) gemm_f64_kernel(const Prob* probs, const 
                     r2 += d * d;
                 }
                 C[e] = x;
+                if (c_hi) {
+                    const float f = float(x);
+                    const float h = umma::to_tf32(f);
+                    c_hi[e] = h;
+                    c_lo[e] = f - h;
+                }
             }
         }
         if (mode == EPI_RESID) {
@@ -330,14 +336,14 @@ struct Chunk {
 
 struct Arrays {
     // tensor-core phase (nullptr when absent)
-    float *s_hi, *s_lo, *z_hi[2], *z_lo[2], *zt_hi[2], *zt_lo[2], *w_hi, *w_lo, *x_hi, *x_lo,
+    float *s_hi, *s_lo, *z_hi, *z_lo, *w_hi, *w_lo, *x_hi, *x_lo,
         *p_hi, *p_lo;
     // FP64 phase
     double *s64, *z64[2], *w64, *x64, *p64;
 };
 
 size_t chunk_bytes(int64_t elems, bool low) {
-    return size_t(elems) * ((low ? 16 * 4 : 0) + 6 * 8);
+    return size_t(elems) * ((low ? 10 * 4 : 0) + 6 * 8);
 }
 
 // A tensor-core phase that stops above this residual has not resolved the
@@ -385,8 +391,8 @@ T* carve(char*& cur, size_t count) {
 // kMaxBuckets buckets.
 int tc_gemm(rsatb_context* ctx, const Chunk& ch, const Dev& d,
             const std::vector<int>& group_item_begin, const float* a_hi, const float* a_lo,
-            const float* b_hi, const float* b_lo, float* c_hi, float* c_lo, float* ct_hi,
-            float* ct_lo, int mode, const float* xe_hi, const float* xe_lo, bool split,
+            const float* b_hi, const float* b_lo, float* c_hi, float* c_lo, double* c64,
+            int mode, const float* xe_hi, const float* xe_lo, bool split,
             rsatb_isqrt_stats* stats) {
     const int nb = int(ch.buckets.size());
     for (int g0 = 0, gi = 0; g0 < nb; g0 += kMaxBuckets, ++gi) {
@@ -406,8 +412,7 @@ int tc_gemm(rsatb_context* ctx, const Chunk& ch, const Dev& d,
         args.state = d.state;
         args.c_hi = c_hi;
         args.c_lo = c_lo;
-        args.ct_hi = ct_hi;
-        args.ct_lo = ct_lo;
+        args.c64 = c64;
         args.xe_hi = xe_hi;
         args.xe_lo = xe_lo;
         args.res2 = d.res2;
@@ -420,14 +425,15 @@ int tc_gemm(rsatb_context* ctx, const Chunk& ch, const Dev& d,
     return RSATB_SUCCESS;
 }
 
-template <bool BT>
+template <bool BT, bool SYM_A = false>
 int f64_gemm(rsatb_context* ctx, const Dev& d, const double* A, const double* B, double* C,
-             int mode, const double* Xe, rsatb_isqrt_stats* stats) {
+             int mode, const double* Xe, rsatb_isqrt_stats* stats, float* c_hi = nullptr,
+             float* c_lo = nullptr) {
     if (d.n_f64_items == 0) return RSATB_SUCCESS;
     int grid = ctx->sm_count * 4;
     if (d.n_f64_items < grid) grid = d.n_f64_items;
-    gemm_f64_kernel<BT><<<grid, 256, 0, ctx->stream>>>(d.probs, d.f64_items, d.n_f64_items,
-                                                       d.state, A, B, C, mode, Xe, d.res2);
+    gemm_f64_kernel<BT, SYM_A><<<grid, 256, 0, ctx->stream>>>(
+        d.probs, d.f64_items, d.n_f64_items, d.state, A, B, C, mode, Xe, d.res2, c_hi, c_lo);
     RSATB_LAUNCH_CHECK(ctx);
     if (stats) stats->gemm_launches++;
     return RSATB_SUCCESS;
@@ -500,7 +506,7 @@ int run_chunk(rsatb_context* ctx, const Opts& o, const Chunk& ch, const int* col
              2 * align256(P * sizeof(double)) + 256 +
              align256(tc_items.size() * sizeof(TcItem)) +
              align256(f64_items.size() * sizeof(F64Item));
-    bytes += (low ? 16 * align256(E * sizeof(float)) : 0) + 6 * align256(E * sizeof(double));
+    bytes += (low ? 10 * align256(E * sizeof(float)) : 0) + 6 * align256(E * sizeof(double));
     void* ws = nullptr;
     RSATB_TRY(ctx_scratch(ctx, bytes, &ws));
     char* cur = static_cast<char*>(ws);
@@ -524,12 +530,8 @@ int run_chunk(rsatb_context* ctx, const Opts& o, const Chunk& ch, const int* col
     if (low) {
         a.s_hi = carve<float>(cur, E);
         a.s_lo = carve<float>(cur, E);
-        for (int i = 0; i < 2; ++i) {
-            a.z_hi[i] = carve<float>(cur, E);
-            a.z_lo[i] = carve<float>(cur, E);
-            a.zt_hi[i] = carve<float>(cur, E);
-            a.zt_lo[i] = carve<float>(cur, E);
-        }
+        a.z_hi = carve<float>(cur, E);
+        a.z_lo = carve<float>(cur, E);
         a.w_hi = carve<float>(cur, E);
         a.w_lo = carve<float>(cur, E);
         a.x_hi = carve<float>(cur, E);
@@ -577,8 +579,7 @@ int run_chunk(rsatb_context* ctx, const Opts& o, const Chunk& ch, const int* col
     // Pack S and the starting iterate.
     pack_kernel<<<P, 256, 0, s>>>(d.probs, d.in_off, M, a.s64, a.s_hi, a.s_lo);
     RSATB_LAUNCH_CHECK(ctx);
-    init_kernel<<<P, 256, 0, s>>>(d.probs, a.s64, d.state, a.z_hi[0], a.z_lo[0], a.zt_hi[0],
-                                  a.zt_lo[0], low ? nullptr : a.z64[0], d.scale,
+    init_kernel<<<P, 256, 0, s>>>(d.probs, a.s64, d.state, a.z_hi, a.z_lo, a.z64[0], d.scale,
                                   low ? o.max_iter : o.max_fp64);
     RSATB_LAUNCH_CHECK(ctx);
     const int cb = (P + 255) / 256;
@@ -598,26 +599,31 @@ int run_chunk(rsatb_context* ctx, const Opts& o, const Chunk& ch, const int* col
         RSATB_TRY(run_phase(ctx, o.graph, [&]() -> int {
             for (int k = 0; k <= o.max_iter; ++k) {
                 const int c = k & 1;
-                // W = Z S^T, X = Z W^T (+ residual)
-                RSATB_TRY(tc_gemm(ctx, ch, d, group_begin, a.z_hi[c], a.z_lo[c], a.s_hi, a.s_lo,
-                                  a.w_hi, a.w_lo, nullptr, nullptr, EPI_STORE, nullptr, nullptr,
-                                  split, stats));
-                RSATB_TRY(tc_gemm(ctx, ch, d, group_begin, a.z_hi[c], a.z_lo[c], a.w_hi, a.w_lo,
-                                  a.x_hi, a.x_lo, nullptr, nullptr, EPI_RESID, nullptr, nullptr,
-                                  split, stats));
+                // W = Z S^T, X = Z W^T (+ residual) on the tensor cores
+                RSATB_TRY(tc_gemm(ctx, ch, d, group_begin, a.z_hi, a.z_lo, a.s_hi, a.s_lo,
+                                  a.w_hi, a.w_lo, nullptr, EPI_STORE, nullptr, nullptr, split,
+                                  stats));
+                RSATB_TRY(tc_gemm(ctx, ch, d, group_begin, a.z_hi, a.z_lo, a.w_hi, a.w_lo,
+                                  a.x_hi, a.x_lo, nullptr, EPI_RESID, nullptr, nullptr, split,
+                                  stats));
                 control_kernel<<<cb, 256, 0, s>>>(P, d.state, d.res2, o.tol, 1);
                 RSATB_LAUNCH_CHECK(ctx);
-                retire_low_kernel<<<P, 256, 0, s>>>(d.probs, d.state, a.z_hi[c], a.z_lo[c],
-                                                    a.z64[0]);
-                RSATB_LAUNCH_CHECK(ctx);
+                if (c == 1) {
+                    retire_low_kernel<<<P, 256, 0, s>>>(d.probs, d.state, a.z64[1], a.z64[0]);
+                    RSATB_LAUNCH_CHECK(ctx);
+                }
                 if (k == o.max_iter) break;
-                // P = 1.875 I - 1.25 X + 0.375 X X^T, Z' = P Z (and Z'^T)
+                // P = 1.875 I - 1.25 X + 0.375 X X^T on the tensor cores (and in
+                // FP64), then Z' = ((P + P^T)/2) Z in FP64: a symmetric factor on
+                // the left only moves Z off the solution set {Q S^-1/2}, which
+                // later steps undo, while rounding in the product itself would
+                // add a rotation Q that no step removes.
                 RSATB_TRY(tc_gemm(ctx, ch, d, group_begin, a.x_hi, a.x_lo, a.x_hi, a.x_lo,
-                                  a.p_hi, a.p_lo, nullptr, nullptr, EPI_POLY, a.x_hi, a.x_lo,
-                                  split, stats));
-                RSATB_TRY(tc_gemm(ctx, ch, d, group_begin, a.p_hi, a.p_lo, a.zt_hi[c],
-                                  a.zt_lo[c], a.z_hi[c ^ 1], a.z_lo[c ^ 1], a.zt_hi[c ^ 1],
-                                  a.zt_lo[c ^ 1], EPI_STORE, nullptr, nullptr, split, stats));
+                                  a.p_hi, a.p_lo, a.p64, EPI_POLY, a.x_hi, a.x_lo, split,
+                                  stats));
+                const int st_z = f64_gemm<false, true>(ctx, d, a.p64, a.z64[c], a.z64[c ^ 1],
+                                                       EPI_STORE, nullptr, stats, a.z_hi, a.z_lo);
+                RSATB_TRY(st_z);
             }
             return RSATB_SUCCESS;
         }));
@@ -656,8 +662,9 @@ int run_chunk(rsatb_context* ctx, const Opts& o, const Chunk& ch, const int* col
             RSATB_LAUNCH_CHECK(ctx);
             if (k == fp64_steps) break;
             RSATB_TRY(f64_gemm<true>(ctx, d, a.x64, a.x64, a.p64, EPI_POLY, a.x64, stats));
-            RSATB_TRY(f64_gemm<false>(ctx, d, a.p64, a.z64[c], a.z64[c ^ 1], EPI_STORE, nullptr,
-                                      stats));
+            const int st_z = f64_gemm<false, true>(ctx, d, a.p64, a.z64[c], a.z64[c ^ 1],
+                                                   EPI_STORE, nullptr, stats);
+            RSATB_TRY(st_z);
         }
         return RSATB_SUCCESS;
     }));

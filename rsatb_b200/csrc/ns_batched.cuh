@@ -59,8 +59,7 @@ struct TcArgs {
     const State* state;      // state[p].active gates the tile
     float* c_hi;             // C = A B^T: TF32-rounded value
     float* c_lo;             // and the residual value - c_hi (exact)
-    float* ct_hi;            // optional transposed copy of C (nullptr: none)
-    float* ct_lo;
+    double* c64;             // optional FP64 copy of C (c_hi + c_lo), nullptr: none
     const float* xe_hi;      // EPI_POLY: X (hi + lo) for P = 1.875 I - 1.25 X + 0.375 X X^T
     const float* xe_lo;
     double* res2;            // EPI_RESID: per-problem sum of (C - I)^2 over the valid corner

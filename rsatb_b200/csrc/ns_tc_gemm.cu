@@ -11,8 +11,8 @@
 // commits each stage back to the producer.  After the last chunk all four
 // warps read the accumulator out of TMEM (warp w owns rows 32w..32w+31) and
 // run the epilogue: the Newton-Schulz polynomial or the residual
-// ||C - I||_F^2, the TF32 hi/lo split of the result, and optionally a
-// transposed copy (coalesced, one column per register across the lanes).
+// ||C - I||_F^2, the TF32 hi/lo split of the result and, optionally, its
+// FP64 value.
 #include "ns_batched.cuh"
 #include "umma.cuh"
 
@@ -182,13 +182,12 @@ __global__ void __launch_bounds__(128, 1)
                     ch[q] = make_float4(hi[4 * q], hi[4 * q + 1], hi[4 * q + 2], hi[4 * q + 3]);
                     cl[q] = make_float4(lo[4 * q], lo[4 * q + 1], lo[4 * q + 2], lo[4 * q + 3]);
                 }
-                if (args.ct_hi) {
+                if (args.c64) {
+                    double2* cd = reinterpret_cast<double2*>(args.c64 + base);
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) {
-                        const int64_t t = pr.off + int64_t(col0 + j) * np + row;
-                        args.ct_hi[t] = hi[j];
-                        args.ct_lo[t] = lo[j];
-                    }
+                    for (int q = 0; q < 8; ++q)
+                        cd[q] = make_double2(double(hi[2 * q]) + double(lo[2 * q]),
+                                             double(hi[2 * q + 1]) + double(lo[2 * q + 1]));
                 }
             }
             if (args.mode == EPI_RESID) {

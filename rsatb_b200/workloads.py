@@ -64,7 +64,7 @@ def _dev(A: lattice.BsrArrays, imaginary: bool = False) -> BlockSpMat:
 
 
 def diamond_sandwich(L: int = 16, R: int = 128, n_moments: int = 1024, seed: int = 7,
-                     rank: int = 0, isqrt_method: str = "ns_fp64") -> KpmWorkload:
+                     rank: int = 0, isqrt_method: str = "ns") -> KpmWorkload:
     t = {}
     t0 = time.perf_counter()
     H, S = lattice.diamond_lcao(L=L, seed=seed)
@@ -117,3 +117,59 @@ def spmm_flops(A: BlockSpMat, n_vectors: int, complex_vectors: bool) -> float:
     elif complex_vectors:
         per *= 2.0
     return per
+
+
+@dataclasses.dataclass
+class SpdBatch:
+    """A batch of dense SPD problems packed for rsatb_isqrt_columns_batched:
+    problem p is the n[p] x n[p] matrix at element offset[p] of `flat`
+    (symmetric, so row- and column-major agree)."""
+    flat: torch.Tensor
+    n: np.ndarray
+    offset: np.ndarray
+    kappa: np.ndarray
+    seed: int
+
+    def matrix(self, p: int) -> np.ndarray:
+        n = int(self.n[p])
+        o = int(self.offset[p])
+        return self.flat[o:o + n * n].reshape(n, n).cpu().numpy()
+
+
+def batched_spd(n_problems: int = 100_000, n_min: int = 40, n_max: int = 400,
+                kappa_min: float = 1e2, kappa_max: float = 1e5, family: str = "continuous",
+                seed: int = 7, device="cuda") -> SpdBatch:
+    """Seeded batched inverse-sqrt problems: sizes uniform in [n_min, n_max],
+    condition numbers log-uniform in [kappa_min, kappa_max], A = Q diag(l) Q^T
+    with Q from the QR of a Gaussian matrix and l the reference benchmark's
+    spectrum families (rsatb/calc/test/benchmark_isqrt_action.cpp:53-85):
+    "continuous" (log-spread over [1/kappa, 1]) or "gapped" (n/20 values in
+    [1/kappa, 10/kappa], the rest in [0.2, 2])."""
+    rng = np.random.default_rng(seed)
+    n = np.sort(rng.integers(n_min, n_max + 1, size=n_problems)).astype(np.int32)
+    kappa = np.exp(rng.uniform(np.log(kappa_min), np.log(kappa_max), size=n_problems))
+    offset = np.concatenate([[0], np.cumsum(n.astype(np.int64) ** 2)[:-1]]).astype(np.int64)
+    flat = torch.empty(int((n.astype(np.int64) ** 2).sum()), dtype=torch.float64, device=device)
+    gen = torch.Generator(device=device)
+    for size in np.unique(n):
+        idx = np.flatnonzero(n == size)
+        gen.manual_seed(seed * 1_000_003 + int(size))
+        for start in range(0, idx.size, 512):
+            part = idx[start:start + 512]
+            c = part.size
+            G = torch.randn(c, size, size, dtype=torch.float64, device=device, generator=gen)
+            Q, _ = torch.linalg.qr(G)
+            lk = torch.as_tensor(np.log(kappa[part]), device=device)[:, None]
+            t = torch.linspace(0.0, 1.0, int(size), dtype=torch.float64, device=device)[None, :]
+            if family == "continuous":
+                lam = torch.exp(-lk + t * lk)
+            else:
+                u = torch.rand(c, int(size), dtype=torch.float64, device=device, generator=gen)
+                n_low = max(1, int(size) // 20)
+                lam = 0.2 + 1.8 * u
+                lam[:, :n_low] = torch.exp(-lk) * torch.exp(u[:, :n_low] * np.log(10.0))
+            A = (Q * lam[:, None, :]) @ Q.transpose(1, 2)
+            A = 0.5 * (A + A.transpose(1, 2))
+            o = int(offset[part[0]])  # equal sizes are contiguous (n is sorted)
+            flat[o:o + c * int(size) ** 2] = A.reshape(-1)
+    return SpdBatch(flat, n, offset, kappa, seed)
