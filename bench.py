@@ -410,7 +410,7 @@ def spmm_only(args):
     A64 = BlockSpMat(H.row_ptr, H.col_ind, H.values, 8)
     A32 = A64.astype("f32")
     out = {"n_rows": H.n_rows, "nnz_blocks": int(H.nnz_blocks)}
-    for R in (128, 16, 8):
+    for R in (128, 32, 16, 8):
         for name, A, dt in (("f32", A32, torch.float32), ("f64", A64, torch.float64)):
             ms = time_spmm(A, H.n_rows, R, dt, reps=args.spmm_reps)
             b = spmm_bytes(A, R, torch.empty(0, dtype=dt).element_size())

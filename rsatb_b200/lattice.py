@@ -206,3 +206,124 @@ def subgraph_problems(P: BsrArrays):
     pos = np.minimum(pos, key.size - 1)
     gather = np.where(key[pos] == q, pos, -1).astype(np.int64)
     return members, slot, gather
+
+
+# ----------------------------------------------------- twisted bilayer graphene
+
+def _rot(theta: float) -> np.ndarray:
+    c, s = math.cos(theta), math.sin(theta)
+    return np.array([[c, -s], [s, c]])
+
+
+def _layer_atoms(t1: np.ndarray, t2: np.ndarray, b1: np.ndarray, b2: np.ndarray,
+                 delta: np.ndarray, span: int) -> np.ndarray:
+    """Honeycomb sites (lattice b1, b2, basis {0, delta}) inside the cell
+    spanned by t1, t2, as 2-D positions wrapped into the cell."""
+    Tinv = np.linalg.inv(np.stack([t1, t2], axis=1))
+    n = np.arange(-span, span + 1)
+    n1, n2 = np.meshgrid(n, n, indexing="ij")
+    base = n1.reshape(-1, 1) * b1 + n2.reshape(-1, 1) * b2
+    out = []
+    for off in (np.zeros(2), delta):
+        p = base + off
+        f = p @ Tinv.T
+        keep = np.all((f > -1e-9) & (f < 1.0 - 1e-9), axis=1)
+        out.append(p[keep])
+    return np.concatenate(out)
+
+
+def twisted_bilayer_graphene(m: int = 31, tiles=(4, 4), t: float = -2.7, a_cc: float = 1.42,
+                             d0: float = 3.35, v0: float = 0.48, decay: float = 0.45,
+                             cutoff: float = 6.0):
+    """Commensurate twisted bilayer graphene (pz), periodic in-plane.
+
+    Moire cell of index m: cos(theta) = (3m^2 + 3m + 1/2) / (3m^2 + 3m + 1),
+    4 (3m^2 + 3m + 1) atoms (m = 31: theta = 1.0501 deg, 11,908 atoms),
+    tiled tiles[0] x tiles[1].  Intralayer nearest neighbours hop t;
+    interlayer pairs within `cutoff` hop v0 exp(-(d - d0) / decay).  Atoms
+    are ordered layer-major inside each moire cell, cells in tile order.
+    Returns (H BsrArrays with b = 1, positions[n, 3], cell[3, 3],
+    displacements[nnz, 3]): displacements are the minimum-image bond vectors
+    r_j + R - r_i of the stored pattern, for commutator velocities."""
+    from scipy.spatial import cKDTree
+
+    a = math.sqrt(3.0) * a_cc
+    a1 = np.array([a, 0.0])
+    a2 = np.array([a / 2.0, a * math.sqrt(3.0) / 2.0])
+    delta = (a1 + a2) / 3.0
+    theta = math.acos((3 * m * m + 3 * m + 0.5) / (3 * m * m + 3 * m + 1.0))
+    t1 = m * a1 + (m + 1) * a2
+    t2 = -(m + 1) * a1 + (2 * m + 1) * a2
+    per_layer = 2 * (3 * m * m + 3 * m + 1)
+    span = 3 * m + 4
+    L1 = _layer_atoms(t1, t2, a1, a2, delta, span)
+    # Layer 2 is layer 1 rotated by theta; the moire vectors are lattice
+    # vectors of both layers (checked), so its sites tile the same cell.
+    Rm = _rot(theta)
+    b1, b2 = Rm @ a1, Rm @ a2
+    B = np.stack([b1, b2], axis=1)
+    for tv in (t1, t2):
+        c = np.linalg.solve(B, tv)
+        if not np.allclose(c, np.round(c), atol=1e-6):
+            raise AssertionError("moire vector is not a lattice vector of the rotated layer")
+    L2 = _layer_atoms(t1, t2, b1, b2, Rm @ delta, 4 * span)
+    if L1.shape[0] != per_layer or L2.shape[0] != per_layer:
+        raise AssertionError(f"site count {L1.shape[0]}, {L2.shape[0]} != {per_layer}")
+    cell_pos = np.concatenate([np.c_[L1, np.zeros(per_layer)], np.c_[L2, np.full(per_layer, d0)]])
+    layer_cell = np.r_[np.zeros(per_layer, np.int8), np.ones(per_layer, np.int8)]
+    T1 = np.r_[t1, 0.0]
+    T2 = np.r_[t2, 0.0]
+    n_cell = cell_pos.shape[0]
+    pos = []
+    for q in range(tiles[1]):
+        for p in range(tiles[0]):
+            pos.append(cell_pos + p * T1 + q * T2)
+    pos = np.concatenate(pos)
+    layer = np.tile(layer_cell, tiles[0] * tiles[1])
+    n = pos.shape[0]
+    S1, S2 = tiles[0] * T1, tiles[1] * T2
+    # Periodic neighbour search over the 3 x 3 images of the supercell.
+    shifts = [(u, v) for u in (-1, 0, 1) for v in (-1, 0, 1)]
+    img = np.concatenate([pos + u * S1 + v * S2 for u, v in shifts])
+    tree = cKDTree(img)
+    pairs = tree.query_ball_point(pos, cutoff + 1e-9, return_sorted=True)
+    rows = np.repeat(np.arange(n), [len(p) for p in pairs])
+    cols_img = np.concatenate([np.asarray(p, dtype=np.int64) for p in pairs])
+    cols = cols_img % n
+    disp = img[cols_img] - pos[rows]
+    dist = np.linalg.norm(disp, axis=1)
+    same = layer[rows] == layer[cols]
+    keep = (dist > 1e-6) & ((~same) | (dist < 0.5 * (a_cc + a)))
+    rows, cols, disp, dist, same = rows[keep], cols[keep], disp[keep], dist[keep], same[keep]
+    vals = np.where(same, t, v0 * np.exp(-(dist - d0) / decay))
+    row_ptr, col_ind, order = csr_from_pairs(n, rows, cols)
+    H = BsrArrays(row_ptr, col_ind, vals[order].reshape(-1, 1, 1), 1)
+    cell = np.array([S1, S2, [0.0, 0.0, 20.0]])
+    return H, pos, cell, disp[order]
+
+
+def commutator_velocity(H: BsrArrays, displacements: np.ndarray):
+    """Real parts W_a of the velocities V_a = i W_a at the Gamma point:
+    W_a,ij = (r_j + R - r_i)_a H_ij, the bond moment of
+    rsatb/operator/commutator_velocity.hpp:100-255 (BuildCommutatorVelocity,
+    factor i, kDisplacement weights) for b = 1 and a single image per bond.
+    Returns three BsrArrays sharing H's pattern, to be stored with the
+    imaginary-unit flag."""
+    if H.block_size != 1:
+        raise ValueError("commutator_velocity: pz (b = 1) operators only")
+    out = []
+    for axis in range(3):
+        w = H.values[:, 0, 0] * displacements[:, axis]
+        out.append(BsrArrays(H.row_ptr, H.col_ind, w.reshape(-1, 1, 1), 1))
+    return out
+
+
+def graphene_displacements(H: BsrArrays, pos: np.ndarray, cell: np.ndarray) -> np.ndarray:
+    """Minimum-image bond vectors r_j + R - r_i of graphene()'s pattern."""
+    rows = np.repeat(np.arange(H.n_block_rows), np.diff(H.row_ptr))
+    d = pos[H.col_ind] - pos[rows]
+    C = cell[:2, :2]
+    f = d[:, :2] @ np.linalg.inv(C)
+    f -= np.round(f)
+    d[:, :2] = f @ C
+    return d
