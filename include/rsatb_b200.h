@@ -225,6 +225,43 @@ RSATB_API int rsatb_evaluate_kpm_density(rsatb_ctx_t ctx, const double* moments,
                                const double* x, int nx, double edge_inset, int kernel,
                                double* rho_out);
 
+/* ------------------------------------------------ FFT-Chebyshev transport */
+
+/* Counters of one rsatb_dc_spectrum_fftcheb call. */
+typedef struct {
+    int sections;             /* row sections (the recurrence runs once per section) */
+    int64_t fft_chunks;       /* row chunks of the transform stage */
+    double recurrence_ms;     /* device time of the recurrences and stores */
+    double transform_ms;      /* device time of the DCT-III and contraction stage */
+    size_t store_bytes;       /* bytes of the moment stores of one section */
+} rsatb_fftcheb_stats;
+
+/* Kubo-Greenwood DC conductivity by the FFT-Chebyshev method,
+ * rsatb::calc::dc_spectrum_fftcheb (rsatb/calc/fftcheb_transport.hpp:
+ * 543-660) with accumulate_fftcheb_block (:270-525) for one block of all
+ * n_vectors samples: left chain J_a T_m(Op~) psi and right chains
+ * T_m(Op~) J_a psi, J_a = -(1/(2 half_width)) V_a (current, rsatb/calc/
+ * ac.hpp:35-60; dressed as Z^H V_a Z in the Sandwich form), the DCT-III of
+ * (g_m/pi) x_m per row, axis and sample (fft.hpp:125-154), and
+ * K(E_k) = sum conj(L3) R3 / max(1e-14, 1 - eps_k^2), averaged over the
+ * samples.  Vx, Vy, Vz: velocity matrices (RSATB_BSR_IMAGINARY_UNIT for the
+ * i*W of a real k-point, or complex), H's shape and precision.  psi: device
+ * N x n_vectors complex (C128, or C64 for FP32 vectors; the transform and
+ * the contraction are FP64 either way).  formulation 0 (Greenwood) only;
+ * partition_sections > 0 asks for at least that many row sections,
+ * max_workspace_bytes bounds the device memory (0: 80 % of what is free).
+ * sigma_out (host) receives n_moments x 6 (xx xy xz yy yz zz; Greenwood
+ * fills xx, yy, zz) scaled by prefactor, energy_out (host) the ascending
+ * energies c + hw cos(pi (M - 1 - k + 1/2) / M).  stats may be NULL.
+ * Synchronises the context's stream. */
+RSATB_API int rsatb_dc_spectrum_fftcheb(rsatb_ctx_t ctx, const rsatb_cheb_op* op,
+                                        rsatb_bsr_t Vx, rsatb_bsr_t Vy, rsatb_bsr_t Vz,
+                                        const void* psi, int n_vectors, rsatb_dtype vec_dtype,
+                                        int n_moments, int formulation, double prefactor,
+                                        int partition_sections, size_t max_workspace_bytes,
+                                        int kernel, double* sigma_out, double* energy_out,
+                                        rsatb_fftcheb_stats* stats);
+
 /* ------------------------------------------- batched dense inverse square root */
 
 /* Arithmetic of the batched Newton-Schulz solve. */

@@ -57,6 +57,11 @@ class IsqrtStats(C.Structure):
                 ("gemm_launches", C.c_int64), ("low_ms", C.c_double), ("fp64_ms", C.c_double)]
 
 
+class FftchebStats(C.Structure):
+    _fields_ = [("sections", C.c_int), ("fft_chunks", C.c_int64), ("recurrence_ms", C.c_double),
+                ("transform_ms", C.c_double), ("store_bytes", C.c_size_t)]
+
+
 # rsatb_ns_precision
 NS_FP64, NS_TF32X3, NS_TF32 = 0, 1, 2
 
@@ -94,6 +99,9 @@ SIGNATURES = {
                                            _PD]),
     "rsatb_set_random": (_i, [_vp, _u64, _i, _i, _vp, _i, _i, _i64, _i, _i64, _i, _vp]),
     "rsatb_evaluate_kpm_density": (_i, [_vp, _PD, _i, _PD, _i, _d, _i, _PD]),
+    "rsatb_dc_spectrum_fftcheb": (_i, [_vp, C.POINTER(ChebOp), _vp, _vp, _vp, _vp, _i, _i, _i,
+                                       _i, _d, _i, _sz, _i, _PD, _PD,
+                                       C.POINTER(FftchebStats)]),
     "rsatb_isqrt_columns_batched": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                          C.POINTER(IsqrtOptions), _vp, C.POINTER(IsqrtStats)]),
     "rsatb_measure_fma_peak": (_i, [_vp, _i, _PD]),

@@ -1,0 +1,556 @@
+// FFT-Chebyshev Kubo-Greenwood transport on the device: the
+// dc_spectrum_fftcheb / accumulate_fftcheb_block path of
+// rsatb/calc/fftcheb_transport.hpp:270-660 with the Greenwood formulation.
+//
+// Per sample block (all R samples at once) and per section of rows:
+//   left chain   l_m = T_m(Op~) psi,          stored as J_a l_m for a = x, y, z
+//   right chains r_m^a = T_m(Op~) J_a psi,    stored as they are
+// with J_a = -(1 / 2 hw) V_a (current, rsatb/calc/ac.hpp:35-60, through
+// Chebyshev::apply_dual, cheby.hpp:249-291), then per row, axis and sample
+// the DCT-III of (g_m / pi) x_m (fft.hpp:125-154) for both chains and the
+// contraction K_k += sum conj(L3_k) R3_k / max(1e-14, 1 - eps_k^2)
+// (fftcheb_transport.hpp:481-495).
+//
+// B200 layout (the reference's per-row FFTW layout is not kept):
+// * the three right chains are one N x 3R panel ([row][axis][sample]), so a
+//   moment is one wide fused step for them and one narrow one for l;
+// * the stores are moment-major, S[m][axis][row][sample], so every moment's
+//   rows land with coalesced writes;
+// * the DCT-III of a chunk of rows is a strided batched inverse 2M-point
+//   FFT (cuFFT, sequences interleaved: stride = batch) of the half-grid
+//   phased even extension, built and read back with coalesced accesses;
+// * the contraction gives each energy k to one CTA per chunk: no atomics,
+//   the same summation order on every run.
+#include "cheb_kernels.cuh"
+
+#include <cufft.h>
+
+#include <cmath>
+#include <complex>
+#include <vector>
+
+namespace rsatb_b200 {
+
+int run_step(rsatb_context* ctx, const rsatb_bsr_matrix* A, int vdt, const StepArgs& a);
+void kpm_kernel_weights(int kernel, int n, double* g);
+
+namespace {
+
+#define RSATB_CUFFT_TRY(call)                                                              \
+    do {                                                                                   \
+        cufftResult r_ = (call);                                                           \
+        if (r_ != CUFFT_SUCCESS)                                                           \
+            return set_error(RSATB_CUDA_ERROR, "%s failed (cufftResult %d)", #call, int(r_)); \
+    } while (0)
+
+// Right-chain panel from the three J_a psi buffers: P[row][a][s] = J[a][row][s].
+template <typename T>
+__global__ void pack_axes_kernel(int64_t n_rows, int R, const T* j0, const T* j1, const T* j2,
+                                 T* panel) {
+    const int64_t total = n_rows * 3 * R;  // complex entries
+    for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total;
+         e += int64_t(gridDim.x) * blockDim.x) {
+        const int s = int(e % R);
+        const int a = int((e / R) % 3);
+        const int64_t row = e / (3 * int64_t(R));
+        const T* src = a == 0 ? j0 : (a == 1 ? j1 : j2);
+        panel[2 * e] = src[2 * (row * R + s)];
+        panel[2 * e + 1] = src[2 * (row * R + s) + 1];
+    }
+}
+
+// Rows [row0, row0 + rows) of the right panel into store slot m:
+// S[m][a][row][s] (complex entries), slot size 3 * rows * R.
+template <typename T>
+__global__ void store_right_kernel(int64_t row0, int64_t rows, int R, const T* panel, T* slot) {
+    const int64_t total = rows * 3 * R;
+    for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total;
+         e += int64_t(gridDim.x) * blockDim.x) {
+        // e indexes the destination: a-major
+        const int s = int(e % R);
+        const int64_t row = (e / R) % rows;
+        const int a = int(e / (rows * R));
+        const int64_t src = ((row0 + row) * 3 + a) * R + s;
+        slot[2 * e] = panel[2 * src];
+        slot[2 * e + 1] = panel[2 * src + 1];
+    }
+}
+
+// Even extension with the half-grid phase of fft.hpp:125-154 for a chunk of
+// sequences: sequence q (0 <= q < nq, q = (a * chunk_rows + row) * R + s,
+// rows offset row_off inside the section) of store S (slot stride
+// slot_elems complex entries, section rows sec_rows) weighted by w_m:
+//   E[0][q] = w_0 x_0,   E[m][q] = w_m x_m e^{i pi m / 2M},
+//   E[2M - m][q] = w_m x_m e^{-i pi m / 2M}  (1 <= m < M),   E[M][q] = 0.
+template <typename T>
+__global__ void extend_kernel(int M, int64_t nq, int chunk_rows, int R, int64_t sec_rows,
+                              int64_t row_off, int64_t slot_elems, const T* S, const double* w,
+                              double2* E) {
+    const int m = blockIdx.y;
+    const double th = M_PI * double(m) / (2.0 * double(M));
+    const double c = cos(th), sn = sin(th);
+    for (int64_t q = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; q < nq;
+         q += int64_t(gridDim.x) * blockDim.x) {
+        const int s = int(q % R);
+        const int64_t row = (q / R) % chunk_rows;
+        const int a = int(q / (int64_t(chunk_rows) * R));
+        const int64_t src = int64_t(m) * slot_elems + (a * sec_rows + row_off + row) * R + s;
+        const double xr = w[m] * double(S[2 * src]), xi = w[m] * double(S[2 * src + 1]);
+        if (m == 0) {
+            E[q] = make_double2(xr, xi);
+            E[int64_t(M) * nq + q] = make_double2(0.0, 0.0);
+        } else {
+            E[int64_t(m) * nq + q] = make_double2(xr * c - xi * sn, xr * sn + xi * c);
+            E[int64_t(2 * M - m) * nq + q] = make_double2(xr * c + xi * sn, -xr * sn + xi * c);
+        }
+    }
+}
+
+// K[k][a] += sum over the chunk's (row, s) of conj(L3[k][q]) R3[k][q] /
+// max(1e-14, 1 - eps_k^2): one CTA per energy k, fixed order.
+__global__ void __launch_bounds__(256) greenwood_contract_kernel(int M, int64_t nq,
+                                                                 int64_t per_axis,
+                                                                 const double2* L3,
+                                                                 const double2* R3,
+                                                                 double* K) {
+    const int k = blockIdx.x;
+    const double eps = cos(M_PI * (double(k) + 0.5) / double(M));
+    const double wden = 1.0 - eps * eps;
+    const double inv = 1.0 / (wden > 1e-14 ? wden : 1e-14);
+    __shared__ double red[3][2][256];
+    double acc[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+    const double2* l = L3 + int64_t(k) * nq;
+    const double2* r = R3 + int64_t(k) * nq;
+    for (int a = 0; a < 3; ++a)
+        for (int64_t q = threadIdx.x; q < per_axis; q += blockDim.x) {
+            const double2 x = l[a * per_axis + q], y = r[a * per_axis + q];
+            acc[a][0] += x.x * y.x + x.y * y.y;
+            acc[a][1] += x.x * y.y - x.y * y.x;
+        }
+    for (int a = 0; a < 3; ++a) {
+        red[a][0][threadIdx.x] = acc[a][0];
+        red[a][1][threadIdx.x] = acc[a][1];
+    }
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w)
+            for (int a = 0; a < 3; ++a) {
+                red[a][0][threadIdx.x] += red[a][0][threadIdx.x + w];
+                red[a][1][threadIdx.x] += red[a][1][threadIdx.x + w];
+            }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int a = 0; a < 3; ++a) {
+            // components xx, yy, zz of the 6-component tensor (xx xy xz yy yz zz)
+            const int comp = a == 0 ? 0 : (a == 1 ? 3 : 5);
+            K[2 * (int64_t(k) * 6 + comp)] += red[a][0][0] * inv;
+            K[2 * (int64_t(k) * 6 + comp) + 1] += red[a][1][0] * inv;
+        }
+}
+
+// Owning device buffer released on scope exit.
+struct DevBuf {
+    void* p = nullptr;
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+    int alloc(size_t bytes) {
+        if (bytes == 0) bytes = 16;
+        RSATB_CUDA_TRY(cudaMalloc(&p, bytes));
+        return RSATB_SUCCESS;
+    }
+    template <typename T>
+    T* as() const {
+        return static_cast<T*>(p);
+    }
+};
+
+struct Plan {
+    cufftHandle h = 0;
+    bool made = false;
+    ~Plan() {
+        if (made) cufftDestroy(h);
+    }
+};
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+StepArgs plain_args(int W) {
+    StepArgs a{};
+    a.W = W;
+    a.s_in = 1.0;
+    a.s_out = 1.0;
+    a.s2 = 1.0;
+    a.dot_mode = DOT_NONE;
+    return a;
+}
+
+// Matrix restricted to block rows [b0, b1): row_ptr keeps absolute block
+// indices, so values, column indices and the input panel are unchanged and
+// output row i of the launch is block row b0 + i.
+rsatb_bsr_matrix row_view(const rsatb_bsr_matrix* A, int b0, int b1) {
+    rsatb_bsr_matrix v = *A;
+    v.row_ptr = A->row_ptr + b0;
+    v.n_block_rows = b1 - b0;
+    return v;
+}
+
+struct Ctx {
+    rsatb_context* ctx;
+    const rsatb_cheb_op* op;
+    bool sandwich;
+    int vdt;
+};
+
+// out = s2 * (Op in - c in) / hw + g_p * prev (Chebyshev::apply_form and the
+// recurrence axpby), W real values per row; u, w: sandwich scratch.
+int op_step(const Ctx& c, int W, const void* in, const void* prev, void* out, void* u, void* w,
+            double s2, double g_p) {
+    StepArgs last = plain_args(W);
+    last.x = in;
+    last.p = prev;
+    last.y = out;
+    last.c = c.op->center;
+    last.s_out = 1.0 / c.op->half_width;
+    last.s2 = s2;
+    last.g_p = g_p;
+    if (!c.sandwich) {
+        last.in = in;
+        return run_step(c.ctx, c.op->H, c.vdt, last);
+    }
+    StepArgs a = plain_args(W);
+    a.in = in;
+    a.y = u;
+    RSATB_TRY(run_step(c.ctx, c.op->Z, c.vdt, a));
+    a.in = u;
+    a.y = w;
+    RSATB_TRY(run_step(c.ctx, c.op->H, c.vdt, a));
+    last.in = w;
+    return run_step(c.ctx, c.op->ZH, c.vdt, last);
+}
+
+// J_a x = -(1 / 2 hw) * (dressed V_a) x on block rows [b0, b1), written
+// compactly to out (rows b0.. of the result at out[0..]).  Sandwich: Z^H V Z.
+int current_rows(const Ctx& c, const rsatb_bsr_matrix* V, int W, const void* x, void* out,
+                 int b0, int b1, void* u, void* w) {
+    const double scale = -1.0 / (2.0 * c.op->half_width);
+    StepArgs a = plain_args(W);
+    if (!c.sandwich) {
+        const rsatb_bsr_matrix view = row_view(V, b0, b1);
+        a.in = x;
+        a.y = out;
+        a.s_in = scale;
+        return run_step(c.ctx, &view, c.vdt, a);
+    }
+    a.in = x;
+    a.y = u;
+    RSATB_TRY(run_step(c.ctx, c.op->Z, c.vdt, a));
+    a.in = u;
+    a.y = w;
+    RSATB_TRY(run_step(c.ctx, V, c.vdt, a));
+    const rsatb_bsr_matrix view = row_view(c.op->ZH, b0, b1);
+    a.in = w;
+    a.y = out;
+    a.s_in = scale;
+    return run_step(c.ctx, &view, c.vdt, a);
+}
+
+unsigned grid_for(int64_t n, int sm) {
+    int64_t g = (n + 255) / 256;
+    if (g > int64_t(sm) * 16) g = int64_t(sm) * 16;
+    return unsigned(g < 1 ? 1 : g);
+}
+
+template <typename T>
+int fftcheb_impl(const Ctx& c, const rsatb_bsr_matrix* const* V, const T* psi, int R, int M,
+                 double prefactor, int sections, size_t workspace, int kernel, double* sigma_out,
+                 double* energy_out, rsatb_fftcheb_stats* stats) {
+    rsatb_context* ctx = c.ctx;
+    cudaStream_t st = ctx->stream;
+    const int b = c.op->H->block_size;
+    const int nb = c.op->H->n_block_rows;
+    const int64_t N = int64_t(nb) * b;
+    const int W1 = 2 * R, W3 = 6 * R;  // real values per row: left, right panel
+    const size_t cplx = 2 * sizeof(T);
+
+    // Store per block row: both chains, all moments, 3 axes x R samples.
+    const size_t store_per_brow = 2 * size_t(M) * b * 3 * R * cplx;
+    const size_t fixed = size_t(N) * cplx * (3 * R /*rinit*/ + 3 * 3 * R /*r*/ + 3 * R /*l*/ +
+                                            3 * R /*J psi*/ + (c.sandwich ? 2 * 3 * R : 0));
+    if (workspace == 0) {
+        size_t free_b = 0, total_b = 0;
+        RSATB_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+        workspace = free_b / 10 * 8;
+    }
+    if (workspace <= fixed + store_per_brow)
+        return set_error(RSATB_OUT_OF_MEMORY,
+                         "workspace of %zu bytes holds no section (needs %zu + %zu per block row)",
+                         workspace, fixed, store_per_brow);
+    // FFT chunk: rows whose 2 x (2M x 3 rows R) double2 extensions fit a
+    // quarter of what remains after the fixed buffers.
+    const size_t avail = workspace - fixed;
+    const size_t fft_budget = avail / 4;
+    const size_t fft_per_row = 2 * 2 * size_t(M) * 3 * R * sizeof(double2) * 2;  // + cuFFT work
+    int64_t chunk_rows = int64_t(fft_budget / fft_per_row);
+    if (chunk_rows < 1) chunk_rows = 1;
+    int64_t sec_brows = int64_t((avail - fft_budget) / store_per_brow);
+    if (sec_brows < 1)
+        return set_error(RSATB_OUT_OF_MEMORY, "workspace too small for one block row of stores");
+    if (sections > 0) {
+        const int64_t want = (nb + sections - 1) / sections;
+        if (want < sec_brows) sec_brows = want;
+    }
+    if (sec_brows > nb) sec_brows = nb;
+    const int n_sections = int((nb + sec_brows - 1) / sec_brows);
+    if (chunk_rows > sec_brows * b) chunk_rows = sec_brows * b;
+
+    // Buffers.
+    DevBuf bJ, bRinit, bR, bL, bU, bW, bS, bE, bK, bWts;
+    RSATB_TRY(bJ.alloc(size_t(N) * 3 * R * cplx));
+    RSATB_TRY(bRinit.alloc(size_t(N) * 3 * R * cplx));
+    RSATB_TRY(bR.alloc(size_t(N) * 3 * 3 * R * cplx));
+    RSATB_TRY(bL.alloc(size_t(N) * 3 * R * cplx));
+    if (c.sandwich) {
+        RSATB_TRY(bU.alloc(size_t(N) * 3 * R * cplx));
+        RSATB_TRY(bW.alloc(size_t(N) * 3 * R * cplx));
+    }
+    const int64_t sec_rows_max = sec_brows * b;
+    const int64_t slot = 3 * sec_rows_max * R;  // complex entries per moment slot
+    RSATB_TRY(bS.alloc(2 * size_t(M) * slot * cplx));
+    const int64_t nq_max = 3 * chunk_rows * R;
+    RSATB_TRY(bE.alloc(2 * 2 * size_t(M) * nq_max * sizeof(double2)));
+    RSATB_TRY(bK.alloc(size_t(M) * 12 * sizeof(double)));
+    RSATB_TRY(bWts.alloc(size_t(M) * sizeof(double)));
+    T* J[3];
+    for (int a = 0; a < 3; ++a) J[a] = bJ.as<T>() + size_t(a) * N * 2 * R;
+    T* rinit = bRinit.as<T>();
+    T* r[3];
+    T* l[3];
+    for (int i = 0; i < 3; ++i) {
+        r[i] = bR.as<T>() + size_t(i) * N * 6 * R;
+        l[i] = bL.as<T>() + size_t(i) * N * 2 * R;
+    }
+    T* SL = bS.as<T>();
+    T* SR = SL + 2 * size_t(M) * slot;
+    double2* EL = bE.as<double2>();
+    double2* ER = EL + 2 * size_t(M) * nq_max;
+    double* K = bK.as<double>();
+
+    std::vector<double> g(M), wts(M);
+    kpm_kernel_weights(kernel, M, g.data());
+    for (int m = 0; m < M; ++m) wts[m] = g[m] / M_PI;  // phi3_weight (fftcheb_transport.hpp)
+    RSATB_CUDA_TRY(cudaMemcpyAsync(bWts.p, wts.data(), M * sizeof(double),
+                                   cudaMemcpyHostToDevice, st));
+    RSATB_CUDA_TRY(cudaMemsetAsync(K, 0, size_t(M) * 12 * sizeof(double), st));
+
+    // cuFFT plans: full chunks and the last, shorter chunk of a section.
+    Plan plans[2];
+    int64_t plan_nq[2] = {0, 0};
+    auto plan_for = [&](int64_t nq, cufftHandle* out) -> int {
+        for (int i = 0; i < 2; ++i)
+            if (plans[i].made && plan_nq[i] == nq) {
+                *out = plans[i].h;
+                return RSATB_SUCCESS;
+            }
+        int slot_i = plans[0].made ? 1 : 0;
+        if (plans[slot_i].made) {
+            cufftDestroy(plans[slot_i].h);
+            plans[slot_i].made = false;
+        }
+        int n2 = 2 * M;
+        int emb = 2 * M;
+        RSATB_CUFFT_TRY(cufftPlanMany(&plans[slot_i].h, 1, &n2, &emb, int(nq), 1, &emb, int(nq), 1,
+                                      CUFFT_Z2Z, int(nq)));
+        plans[slot_i].made = true;
+        plan_nq[slot_i] = nq;
+        RSATB_CUFFT_TRY(cufftSetStream(plans[slot_i].h, st));
+        *out = plans[slot_i].h;
+        return RSATB_SUCCESS;
+    };
+
+    cudaEvent_t ev0, ev1;
+    RSATB_CUDA_TRY(cudaEventCreate(&ev0));
+    RSATB_CUDA_TRY(cudaEventCreate(&ev1));
+    struct EvG {
+        cudaEvent_t a, b;
+        ~EvG() {
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+        }
+    } evg{ev0, ev1};
+    float rec_ms = 0.f, dct_ms = 0.f;
+
+    // J_a psi and the right-chain start.
+    for (int a = 0; a < 3; ++a)
+        RSATB_TRY(current_rows(c, V[a], W1, psi, J[a], 0, nb, bU.p, bW.p));
+    pack_axes_kernel<T><<<grid_for(N * 3 * R, ctx->sm_count), 256, 0, st>>>(N, R, J[0], J[1],
+                                                                           J[2], rinit);
+    RSATB_LAUNCH_CHECK(ctx);
+
+    int64_t chunks = 0;
+    for (int sec = 0; sec < n_sections; ++sec) {
+        const int sb0 = int(sec * sec_brows);
+        const int sb1 = int(std::min<int64_t>(nb, sb0 + sec_brows));
+        const int64_t rows0 = int64_t(sb0) * b;
+        const int64_t rows = int64_t(sb1 - sb0) * b;
+        const int64_t sslot = 3 * rows * R;  // this section's slot size
+        RSATB_CUDA_TRY(cudaEventRecord(ev0, st));
+        RSATB_CUDA_TRY(cudaMemcpyAsync(r[0], rinit, size_t(N) * 3 * R * cplx,
+                                       cudaMemcpyDeviceToDevice, st));
+        const T* lp = psi;       // l_{m-1}
+        const T* lc = nullptr;   // l_m
+        int ri_prev = 0, ri_cur = -1;
+        int li = 0;
+        for (int m = 0; m < M; ++m) {
+            const T* lm;  // l_m
+            int rm;       // index of r_m
+            if (m == 0) {
+                lm = psi;
+                rm = 0;
+            } else if (m == 1) {
+                T* lo = l[li];
+                li = (li + 1) % 3;
+                RSATB_TRY(op_step(c, W1, lp, nullptr, lo, bU.p, bW.p, 1.0, 0.0));
+                RSATB_TRY(op_step(c, W3, r[ri_prev], nullptr, r[1], bU.p, bW.p, 1.0, 0.0));
+                lc = lo;
+                ri_cur = 1;
+                lm = lc;
+                rm = 1;
+            } else {
+                T* lo = l[li];
+                li = (li + 1) % 3;
+                const int rn = 3 - ri_prev - ri_cur;
+                RSATB_TRY(op_step(c, W1, lc, lp, lo, bU.p, bW.p, 2.0, -1.0));
+                RSATB_TRY(op_step(c, W3, r[ri_cur], r[ri_prev], r[rn], bU.p, bW.p, 2.0, -1.0));
+                lp = lc;
+                lc = lo;
+                ri_prev = ri_cur;
+                ri_cur = rn;
+                lm = lc;
+                rm = rn;
+            }
+            T* sl = SL + 2 * size_t(m) * sslot;
+            for (int a = 0; a < 3; ++a)
+                RSATB_TRY(current_rows(c, V[a], W1, lm, sl + 2 * size_t(a) * rows * R, sb0, sb1,
+                                       bU.p, bW.p));
+            store_right_kernel<T><<<grid_for(sslot, ctx->sm_count), 256, 0, st>>>(
+                rows0, rows, R, r[rm], SR + 2 * size_t(m) * sslot);
+            RSATB_LAUNCH_CHECK(ctx);
+        }
+        RSATB_CUDA_TRY(cudaEventRecord(ev1, st));
+        RSATB_CUDA_TRY(cudaEventSynchronize(ev1));
+        float t = 0.f;
+        cudaEventElapsedTime(&t, ev0, ev1);
+        rec_ms += t;
+
+        // Row stage in chunks of rows.
+        RSATB_CUDA_TRY(cudaEventRecord(ev0, st));
+        for (int64_t c0 = 0; c0 < rows; c0 += chunk_rows) {
+            const int64_t cr = std::min<int64_t>(chunk_rows, rows - c0);
+            const int64_t nq = 3 * cr * R;
+            cufftHandle plan;
+            RSATB_TRY(plan_for(nq, &plan));
+            dim3 grid(grid_for(nq, ctx->sm_count) > 64 ? 64 : grid_for(nq, ctx->sm_count), M);
+            extend_kernel<T><<<grid, 256, 0, st>>>(M, nq, int(cr), R, rows, c0, sslot, SL,
+                                                   bWts.as<double>(), EL);
+            RSATB_LAUNCH_CHECK(ctx);
+            extend_kernel<T><<<grid, 256, 0, st>>>(M, nq, int(cr), R, rows, c0, sslot, SR,
+                                                   bWts.as<double>(), ER);
+            RSATB_LAUNCH_CHECK(ctx);
+            RSATB_CUFFT_TRY(cufftExecZ2Z(plan, reinterpret_cast<cufftDoubleComplex*>(EL),
+                                         reinterpret_cast<cufftDoubleComplex*>(EL),
+                                         CUFFT_INVERSE));
+            RSATB_CUFFT_TRY(cufftExecZ2Z(plan, reinterpret_cast<cufftDoubleComplex*>(ER),
+                                         reinterpret_cast<cufftDoubleComplex*>(ER),
+                                         CUFFT_INVERSE));
+            greenwood_contract_kernel<<<M, 256, 0, st>>>(M, nq, cr * R, EL, ER, K);
+            RSATB_LAUNCH_CHECK(ctx);
+            ++chunks;
+        }
+        RSATB_CUDA_TRY(cudaEventRecord(ev1, st));
+        RSATB_CUDA_TRY(cudaEventSynchronize(ev1));
+        cudaEventElapsedTime(&t, ev0, ev1);
+        dct_ms += t;
+    }
+
+    std::vector<double> Kh(size_t(M) * 12);
+    RSATB_CUDA_TRY(cudaMemcpyAsync(Kh.data(), K, Kh.size() * sizeof(double),
+                                   cudaMemcpyDeviceToHost, st));
+    RSATB_CUDA_TRY(cudaStreamSynchronize(st));
+    // Sample average and the ascending energy grid of
+    // fftcheb_transport.hpp:602-659: E_k = c + hw cos(pi (M - 1 - k + 1/2) / M).
+    for (int k = 0; k < M; ++k) {
+        const int src = M - 1 - k;
+        energy_out[k] = c.op->center +
+                        c.op->half_width * std::cos(M_PI * (double(src) + 0.5) / double(M));
+        for (int comp = 0; comp < 6; ++comp)
+            sigma_out[k * 6 + comp] = prefactor * Kh[2 * (size_t(src) * 6 + comp)] / double(R);
+    }
+    if (stats) {
+        stats->sections = n_sections;
+        stats->fft_chunks = chunks;
+        stats->recurrence_ms = rec_ms;
+        stats->transform_ms = dct_ms;
+        stats->store_bytes = 2 * size_t(M) * slot * cplx;
+    }
+    return RSATB_SUCCESS;
+}
+
+}  // namespace
+}  // namespace rsatb_b200
+
+using namespace rsatb_b200;
+
+extern "C" int rsatb_dc_spectrum_fftcheb(rsatb_ctx_t ctx, const rsatb_cheb_op* op, rsatb_bsr_t Vx,
+                                         rsatb_bsr_t Vy, rsatb_bsr_t Vz, const void* psi,
+                                         int n_vectors, rsatb_dtype vec_dtype, int n_moments,
+                                         int formulation, double prefactor,
+                                         int partition_sections, size_t max_workspace_bytes,
+                                         int kernel, double* sigma_out, double* energy_out,
+                                         rsatb_fftcheb_stats* stats) {
+    clear_error();
+    RSATB_TRY(check_ctx(ctx));
+    if (!op || !psi || !sigma_out || !energy_out)
+        return set_error(RSATB_INVALID_ARGUMENT, "null argument");
+    if (op->form != RSATB_FORM_ORTHOGONAL && op->form != RSATB_FORM_SANDWICH)
+        return set_error(RSATB_NOT_SUPPORTED, "operator form %d is not available on the device",
+                         op->form);
+    const bool sandwich = op->form == RSATB_FORM_SANDWICH;
+    const rsatb_bsr_matrix* mats[6] = {op->H, sandwich ? op->Z : op->H,
+                                       sandwich ? op->ZH : op->H, Vx, Vy, Vz};
+    const char* names[6] = {"H", "Z", "ZH", "Vx", "Vy", "Vz"};
+    for (int i = 0; i < 6; ++i) {
+        RSATB_TRY(check_bsr(mats[i], names[i]));
+        if (mats[i]->n_block_rows != op->H->n_block_rows ||
+            mats[i]->n_block_cols != op->H->n_block_rows ||
+            mats[i]->block_size != op->H->block_size)
+            return set_error(RSATB_INVALID_ARGUMENT, "%s does not match H's shape", names[i]);
+        if (dtype_is_double(mats[i]->dtype) != dtype_is_double(vec_dtype))
+            return set_error(RSATB_INVALID_ARGUMENT, "%s precision differs from the vectors'",
+                             names[i]);
+    }
+    if (!dtype_is_complex(vec_dtype))
+        return set_error(RSATB_INVALID_ARGUMENT, "transport needs complex sample vectors");
+    if (!(op->half_width > 0.0))
+        return set_error(RSATB_INVALID_ARGUMENT, "half_width must be positive");
+    if (n_vectors <= 0 || n_moments <= 0)
+        return set_error(RSATB_INVALID_ARGUMENT, "n_vectors and n_moments must be positive");
+    if (6 * n_vectors > 1536)
+        return set_error(RSATB_NOT_SUPPORTED, "%d samples exceed one block (256 at most)",
+                         n_vectors);
+    if (formulation != 0)
+        return set_error(RSATB_NOT_SUPPORTED,
+                         "formulation %d: only Greenwood (0) runs on the device", formulation);
+    if (!aligned16(psi)) return set_error(RSATB_INVALID_ARGUMENT, "psi must be 16-byte aligned");
+    if (stats) *stats = rsatb_fftcheb_stats{};
+    const rsatb_bsr_matrix* V[3] = {Vx, Vy, Vz};
+    Ctx c{ctx, op, sandwich, int(vec_dtype)};
+    if (dtype_is_double(vec_dtype))
+        return fftcheb_impl<double>(c, V, static_cast<const double*>(psi), n_vectors, n_moments,
+                                    prefactor, partition_sections, max_workspace_bytes, kernel,
+                                    sigma_out, energy_out, stats);
+    return fftcheb_impl<float>(c, V, static_cast<const float*>(psi), n_vectors, n_moments,
+                               prefactor, partition_sections, max_workspace_bytes, kernel,
+                               sigma_out, energy_out, stats);
+}

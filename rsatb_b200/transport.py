@@ -1,0 +1,58 @@
+"""FFT-Chebyshev Kubo-Greenwood transport on the GPU.
+
+``dc_spectrum_fftcheb`` mirrors rsatb::calc::dc_spectrum_fftcheb
+(rsatb/calc/fftcheb_transport.hpp:543-660): same arguments (Chebyshev
+operator, three velocity matrices, sample block, moment count, formulation,
+prefactor, partition sections, workspace bound, kernel) and results
+(sigma[n_moments, 6] on the ascending energy grid).  The recurrences, the
+per-row DCT-III and the contraction run in the rsatb_b200 library
+(rsatb_dc_spectrum_fftcheb); this module validates arguments and moves
+handles.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _capi
+from ._capi import check, lib
+from .calc import Chebyshev, KpmKernel
+from .vbcsr import BlockSpMat, dtype_code
+
+GREENWOOD, BASTIN = 0, 1
+
+
+def dc_spectrum_fftcheb(cheby: Chebyshev, Vx: BlockSpMat, Vy: BlockSpMat, Vz: BlockSpMat,
+                        psi: torch.Tensor, n_moments: int, formulation: int = GREENWOOD,
+                        prefactor: float = 1.0, partition_sections: int = 0,
+                        max_workspace_mb: float = 0.0, kernel: KpmKernel = KpmKernel.Jackson,
+                        return_stats: bool = False):
+    """Returns (sigma[n_moments, 6], energy[n_moments]) and, with
+    return_stats, the call's counters.  psi: (N, R) complex CUDA tensor
+    (complex128, or complex64 for FP32 vectors)."""
+    if n_moments <= 0:
+        raise ValueError("n_moments must be positive")
+    if not psi.is_cuda or psi.dim() != 2 or not psi.is_contiguous() or not psi.is_complex():
+        raise ValueError("psi must be a contiguous (N, R) complex CUDA tensor")
+    if psi.shape[0] != cheby.n_rows:
+        raise ValueError("psi rows differ from the operator size")
+    if formulation != GREENWOOD:
+        raise NotImplementedError("only the Greenwood formulation runs on the GPU")
+    ctx = cheby.H.ctx
+    ctx.bind_stream()
+    op = cheby.c_op()
+    sigma = np.zeros(n_moments * 6)
+    energy = np.zeros(n_moments)
+    stats = _capi.FftchebStats()
+    P = C.POINTER(C.c_double)
+    check(lib().rsatb_dc_spectrum_fftcheb(
+        ctx.handle, C.byref(op), Vx.handle, Vy.handle, Vz.handle, C.c_void_p(psi.data_ptr()),
+        psi.shape[1], dtype_code(psi.dtype), int(n_moments), int(formulation), float(prefactor),
+        int(partition_sections), int(max_workspace_mb * (1 << 20)), int(kernel),
+        sigma.ctypes.data_as(P), energy.ctypes.data_as(P), C.byref(stats)))
+    out = (sigma.reshape(n_moments, 6), energy)
+    if return_stats:
+        return out + ({f: getattr(stats, f) for f, _ in stats._fields_},)
+    return out

@@ -1,0 +1,160 @@
+"""FFT-Chebyshev Kubo-Greenwood transport (rsatb_dc_spectrum_fftcheb)
+against the oracle's restatement of dc_spectrum_fftcheb
+(rsatb/calc/fftcheb_transport.hpp:270-660), itself pinned to the reference's
+O(M^2) moment reference and DCT-III checks (tests/test_oracle_golden.py)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle
+from _util import adjoint_arrays, rel_err, to_oracle
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    torch.cuda.set_device(0)
+    return torch
+
+
+def _dev(A, imaginary=False, precision="f64"):
+    from rsatb_b200.vbcsr import BlockSpMat
+    M = BlockSpMat(A.row_ptr, A.col_ind, A.values, A.block_size, A.n_block_cols,
+                   imaginary=imaginary)
+    return M.astype("f32") if precision == "f32" else M
+
+
+def _tbg(m=1, tiles=(4, 4)):
+    from rsatb_b200 import lattice
+    H, pos, cell, disp = lattice.twisted_bilayer_graphene(m=m, tiles=tiles)
+    V = lattice.commutator_velocity(H, disp)
+    return H, V
+
+
+def _phases(n, R, seed=5):
+    rng = np.random.default_rng(seed)
+    return np.exp(2j * np.pi * rng.random((n, R))) / np.sqrt(n)
+
+
+def _bounds(H):
+    w = np.linalg.eigvalsh(H.to_dense())
+    return w[0] - 0.5, w[-1] + 0.5
+
+
+def _gpu(torch, H, V, psi, M, emin, emax, precision="f64", Z=None, **kw):
+    from rsatb_b200.calc import Chebyshev, ISQRTMPreconditioner
+    from rsatb_b200.transport import dc_spectrum_fftcheb
+    pre = ISQRTMPreconditioner(_dev(Z)) if Z is not None else None
+    c = Chebyshev(_dev(H), emin, emax, preconditioner=pre)
+    Vd = [_dev(v, imaginary=True) for v in V]
+    dt = torch.complex128
+    if precision == "f32":
+        c = c.astype("f32")
+        Vd = [v.astype("f32") for v in Vd]
+        dt = torch.complex64
+    p = torch.as_tensor(psi).cuda().to(dt).contiguous()
+    return dc_spectrum_fftcheb(c, *Vd, p, M, return_stats=True, **kw)
+
+
+def _oracle(H, V, psi, M, emin, emax, Z=None, sections=1):
+    c, hw = (emax + emin) / 2, (emax - emin) / 2
+    if Z is None:
+        op = oracle.make_op(to_oracle(H), c, hw)
+    else:
+        op = oracle.make_op(to_oracle(H), c, hw, to_oracle(Z), to_oracle(adjoint_arrays(Z)))
+    Vo = [to_oracle(v, imag=True) for v in V]
+    return oracle.fftcheb(op, Vo, psi, M, formulation=0, prefactor=1.0, sections=sections)
+
+
+@pytest.mark.parametrize("M", [1, 2, 17, 64])
+def test_greenwood_matches_oracle_tbg(torch_cuda, M):
+    H, V = _tbg()
+    emin, emax = _bounds(H)
+    psi = _phases(H.n_rows, 3)
+    (sig, en, st) = _gpu(torch_cuda, H, V, psi, M, emin, emax)
+    sig_o, en_o = _oracle(H, V, psi, M, emin, emax)
+    assert np.allclose(en, en_o, rtol=0, atol=1e-13)
+    assert rel_err(sig, sig_o) < 1e-10
+    assert np.all(sig[:, [1, 2, 4]] == 0.0)   # Greenwood fills the diagonal only
+
+
+def test_sections_and_workspace_do_not_change_sigma(torch_cuda):
+    H, V = _tbg()
+    emin, emax = _bounds(H)
+    psi = _phases(H.n_rows, 2, seed=9)
+    s1, _, st1 = _gpu(torch_cuda, H, V, psi, 40, emin, emax)
+    s3, _, st3 = _gpu(torch_cuda, H, V, psi, 40, emin, emax, partition_sections=3)
+    s_small, _, st_s = _gpu(torch_cuda, H, V, psi, 40, emin, emax, max_workspace_mb=6.0)
+    assert st1["sections"] == 1 and st3["sections"] >= 3 and st_s["fft_chunks"] > 1
+    assert rel_err(s3, s1) < 1e-12 and rel_err(s_small, s1) < 1e-12
+
+
+def test_fp32_vectors_against_fp64(torch_cuda):
+    """FP32 vectors and matrices, FP64 transform and contraction."""
+    H, V = _tbg()
+    emin, emax = _bounds(H)
+    psi = _phases(H.n_rows, 4, seed=3)
+    s64, _, _ = _gpu(torch_cuda, H, V, psi, 64, emin, emax)
+    s32, _, _ = _gpu(torch_cuda, H, V, psi, 64, emin, emax, precision="f32")
+    assert rel_err(s32, s64) < 1e-4
+
+
+def test_sandwich_form_matches_oracle(torch_cuda):
+    """Non-orthogonal sandwich Z^H H Z with dressed currents Z^H V Z."""
+    from rsatb_b200 import lattice
+    from rsatb_b200.isqrt import graph_inverse_sqrt_host
+    H, V = _tbg(m=1, tiles=(3, 3))
+    # S = I + 0.015 |H| on H's pattern plus the diagonal: SPD, non-orthogonal
+    n = H.n_rows
+    Sd = np.eye(n) + 0.015 * np.abs(H.to_dense())
+    rows = np.repeat(np.arange(n), np.diff(H.row_ptr))
+    pr, pc = np.r_[rows, np.arange(n)], np.r_[H.col_ind, np.arange(n)]
+    rp, ci, _ = lattice.csr_from_pairs(n, pr, pc)
+    P = lattice.BsrArrays(rp, ci, np.zeros((ci.size, 1, 1)), 1)
+    S = lattice.BsrArrays(*_pattern_from_dense(Sd, P))
+    Z = graph_inverse_sqrt_host(S)
+    Zd = Z.to_dense()
+    Hs = Zd.T @ H.to_dense() @ Zd
+    w = np.linalg.eigvalsh(0.5 * (Hs + Hs.T))
+    emin, emax = w[0] - 0.5, w[-1] + 0.5
+    psi = _phases(H.n_rows, 2, seed=4)
+    sig, _, _ = _gpu(torch_cuda, H, V, psi, 24, emin, emax, Z=Z)
+    sig_o, _ = _oracle(H, V, psi, 24, emin, emax, Z=Z)
+    assert rel_err(sig, sig_o) < 1e-10
+
+
+def _pattern_from_dense(D, P):
+    """Values of dense D on the pattern of P (b = 1)."""
+    rows = np.repeat(np.arange(P.n_block_rows), np.diff(P.row_ptr))
+    vals = D[rows, P.col_ind].reshape(-1, 1, 1)
+    return P.row_ptr, P.col_ind, vals, 1
+
+
+def test_graphene_is_isotropic_in_plane(torch_cuda):
+    from rsatb_b200 import lattice
+    H, pos, cell = lattice.graphene(12, 12)
+    d = lattice.graphene_displacements(H, pos, cell)
+    V = lattice.commutator_velocity(H, d)
+    psi = _phases(H.n_rows, 8, seed=1)
+    sig, en, _ = _gpu(torch_cuda, H, V, psi, 64, -9.2, 9.2)
+    xx, yy, zz = sig[:, 0], sig[:, 3], sig[:, 5]
+    assert np.abs(zz).max() == 0.0
+    assert xx.max() > 0
+    assert rel_err(yy, xx) < 0.3   # stochastic trace with 8 samples
+
+
+def test_bastin_and_bad_arguments_refused(torch_cuda):
+    from rsatb_b200._capi import RsatbError
+    from rsatb_b200.calc import Chebyshev
+    from rsatb_b200.transport import dc_spectrum_fftcheb
+    H, V = _tbg()
+    c = Chebyshev(_dev(H), -10, 10)
+    Vd = [_dev(v, imaginary=True) for v in V]
+    p = torch_cuda.as_tensor(_phases(H.n_rows, 1)).cuda()
+    with pytest.raises(NotImplementedError):
+        dc_spectrum_fftcheb(c, *Vd, p, 8, formulation=1)
+    with pytest.raises(RsatbError):   # FP32 vectors with FP64 matrices
+        dc_spectrum_fftcheb(c, *Vd, p.to(torch_cuda.complex64), 8)
