@@ -43,7 +43,12 @@ def parse_args():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["diamond", "graphene", "isqrt"], default="diamond")
+    p.add_argument("--workload", choices=["diamond", "graphene", "isqrt", "transport"],
+                   default="diamond")
+    p.add_argument("--tbg-m", type=int, default=31, help="moire index of the TBG cell")
+    p.add_argument("--tbg-tiles", type=int, default=4, help="TBG cells per side")
+    p.add_argument("--transport-moments", type=int, default=2048)
+    p.add_argument("--transport-samples", type=int, default=16, help="samples over all GPUs")
     p.add_argument("--isqrt-n", type=int, default=100_000,
                    help="problems of the batched inverse-sqrt workload")
     p.add_argument("--isqrt-precision", choices=["tf32x3", "tf32", "fp64"], default="tf32x3")
@@ -511,6 +516,98 @@ def bench_isqrt(args, dist):
         print(json.dumps(line), flush=True)
 
 
+def bench_transport(args, dist):
+    """Kubo-Greenwood sigma(E) by FFT-Chebyshev on twisted bilayer graphene
+    (commensurate moire cell m, tiled tiles x tiles; pz, NN intralayer
+    t = -2.7 eV, interlayer 0.48 exp(-(d - 3.35)/0.45) within 6 A), commutator
+    velocities at Gamma, random-phase samples sharded over the GPUs.  One step
+    = one dc_spectrum_fftcheb call over this GPU's samples: FP32 vectors with
+    FP64 transform and contraction; the FP64 path is timed beside it."""
+    import torch
+    import oracle
+    from rsatb_b200 import lattice
+    from rsatb_b200.bounds import estimate_spectral_bounds
+    from rsatb_b200.calc import Chebyshev
+    from rsatb_b200.transport import dc_spectrum_fftcheb
+    from rsatb_b200.vbcsr import BlockSpMat, set_random
+    t0 = time.perf_counter()
+    H, pos, cell, disp = lattice.twisted_bilayer_graphene(m=args.tbg_m,
+                                                         tiles=(args.tbg_tiles, args.tbg_tiles))
+    V = lattice.commutator_velocity(H, disp)
+    gen_s = time.perf_counter() - t0
+    c0 = Chebyshev(BlockSpMat(H.row_ptr, H.col_ind, H.values, 1), -1.0, 1.0)
+    emin, emax = estimate_spectral_bounds(c0)
+    c64 = Chebyshev(c0.H, emin, emax)
+    c32 = c64.astype("f32")
+    V64 = [BlockSpMat(v.row_ptr, v.col_ind, v.values, 1, imaginary=True) for v in V]
+    V32 = [v.astype("f32") for v in V64]
+    R = max(1, args.transport_samples // dist.world)
+    M = args.transport_moments
+    psi64 = torch.empty(H.n_rows, R, dtype=torch.complex128, device="cuda")
+    set_random(psi64, 20240917, normalize=True, orbitals_per_atom=1, kind=0,
+               first_column=dist.rank * R)
+    psi32 = psi64.to(torch.complex64)
+
+    def timed(c, Vs, psi, steps, warmup):
+        for _ in range(warmup):
+            dc_spectrum_fftcheb(c, *Vs, psi, M)
+        torch.cuda.synchronize()
+        dist.barrier()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record()
+        for _ in range(steps):
+            out = dc_spectrum_fftcheb(c, *Vs, psi, M, return_stats=True)
+        ev[1].record()
+        torch.cuda.synchronize()
+        dist.barrier()
+        return dist.max(ev[0].elapsed_time(ev[1]) / steps), out
+
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        ms32, (sig32, energy, st32) = timed(c32, V32, psi32, args.steps, args.warmup)
+    clocks = clk.summary()
+    ms64, (sig64, _, st64) = timed(c64, V64, psi64, 1, 0)
+    sig32 = dist.sum_array(sig32 * R) / (R * dist.world)
+    sig64 = dist.sum_array(sig64 * R) / (R * dist.world)
+    diag = [0, 3, 5]
+    err = float(np.abs(sig32[:, diag] - sig64[:, diag]).max() / np.abs(sig64[:, diag]).max())
+    base = None
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        # Bounded CPU sample: one moire cell (no tiling), 2 samples, 128 moments.
+        Hs, _, _, ds = lattice.twisted_bilayer_graphene(m=args.tbg_m, tiles=(1, 1))
+        Vs = [oracle.Bsr(h.n_block_rows, h.n_block_rows, 1, h.row_ptr, h.col_ind, h.values,
+                         imag=True) for h in lattice.commutator_velocity(Hs, ds)]
+        op = oracle.make_op(oracle.Bsr(Hs.n_block_rows, Hs.n_block_rows, 1, Hs.row_ptr,
+                                       Hs.col_ind, Hs.values), (emax + emin) / 2,
+                            (emax - emin) / 2)
+        ps = np.exp(2j * np.pi * np.random.default_rng(0).random((Hs.n_rows, 2))) / math.sqrt(
+            Hs.n_rows)
+        tc = time.perf_counter()
+        oracle.fftcheb(op, Vs, ps, 128)
+        dt = time.perf_counter() - tc
+        base = {"value": 2 * 128 * Hs.n_rows / dt, "unit": "sample-moment-rows/s",
+                "cores": oracle.num_threads(), "kind": "port", "seconds": round(dt, 3),
+                "sample": f"one moire cell ({Hs.n_rows} atoms), 2 samples, 128 moments, FP64"}
+    units = R * dist.world * M
+    if dist.rank == 0:
+        line = {
+            "metric": "Kubo-Greenwood sigma(E) by FFT-Chebyshev", "value": round(units / (
+                ms32 * 1e-3), 1), "unit": "sample-moments/s", "n_gpus": dist.world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms32, 2),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 vectors, FP64 transform and contraction",
+            "data": "synthetic (seeded TBG generator, random phases)",
+            "config": {"workload": f"transport_tbg: m={args.tbg_m} moire cell tiled "
+                                   f"{args.tbg_tiles}x{args.tbg_tiles}",
+                       "n_rows": H.n_rows, "nnz": int(H.nnz_blocks), "n_moments": M,
+                       "samples_per_gpu": R, "bounds_ev": [round(emin, 4), round(emax, 4)]},
+            "stats_f32": st32, "fp64_path": {"ms_per_step": round(ms64, 2), "stats": st64,
+                                             "mixed_over_fp64": round(ms64 / ms32, 3)},
+            "sigma_err_f32_vs_f64": err, "cpu_baseline": base,
+            "throughput_rows_per_s": round(units * H.n_rows / (ms32 * 1e-3), 1),
+            "clocks": clocks, "generate_seconds": round(gen_s, 1)}
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     if args.spmm_only:
@@ -519,6 +616,10 @@ def main():
     dist = Dist()
     if args.workload == "isqrt" and args.impl == "ours":
         bench_isqrt(args, dist)
+        dist.close()
+        return
+    if args.workload == "transport" and args.impl == "ours":
+        bench_transport(args, dist)
         dist.close()
         return
     if args.impl == "reference":

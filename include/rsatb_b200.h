@@ -225,6 +225,37 @@ RSATB_API int rsatb_evaluate_kpm_density(rsatb_ctx_t ctx, const double* moments,
                                const double* x, int nx, double edge_inset, int kernel,
                                double* rho_out);
 
+/* ------------------------------------------------------------ adjoint KPM */
+
+/* Counters of one rsatb_kpm_moments_vjp call. */
+typedef struct {
+    int checkpoint_stride;    /* moments per recomputed segment */
+    int segments;             /* checkpoint segments */
+    double forward_ms;        /* device time of the forward pass (moments, checkpoints) */
+    double backward_ms;       /* device time of the recompute, adjoint recurrence and SDDMM */
+    int panels_held;          /* N x R panels held at once */
+} rsatb_adjoint_stats;
+
+/* Gradient of f = sum_n dmu[n] mu_n with respect to every stored block value
+ * of H, where mu_n = (1/R) sum_s psi_s^T T_n((H - center)/half_width) psi_s
+ * are the plain KPM moments of Chebyshev::compute_moments
+ * (rsatb/calc/cheby.hpp:479-514) averaged over the R columns.  No
+ * counterpart in the reference, which has no differentiation code: this is
+ * the hand-written adjoint Chebyshev recurrence
+ *     lambda_n = (dmu_n / R) psi + 2 A lambda_{n+1} - lambda_{n+2},
+ *     df/dA = lambda_1 t_0^T + 2 sum_{n>=1} lambda_{n+1} t_n^T,
+ * with t_n = T_n(A) psi recomputed from checkpoints every checkpoint_stride
+ * moments (0: ceil(sqrt(n_moments))), and df/dH = df/dA / half_width
+ * sampled on H's pattern.  Orthogonal form, real H (F64 or F32) and real
+ * psi (device N x n_vectors, the same precision); dmu: host, n_moments.
+ * mu_out (host, may be NULL) receives the moments of the forward pass;
+ * grad_values (device, FP64, nnz_blocks * b * b in the layout of H's
+ * values) is overwritten.  Bounds are held fixed.  Synchronises the stream. */
+RSATB_API int rsatb_kpm_moments_vjp(rsatb_ctx_t ctx, const rsatb_cheb_op* op, const void* psi,
+                                    int n_vectors, rsatb_dtype vec_dtype, int n_moments,
+                                    const double* dmu, int checkpoint_stride, double* mu_out,
+                                    double* grad_values, rsatb_adjoint_stats* stats);
+
 /* ------------------------------------------------ FFT-Chebyshev transport */
 
 /* Counters of one rsatb_dc_spectrum_fftcheb call. */

@@ -315,3 +315,51 @@ def spd_from_spectrum(lam: np.ndarray, seed: int) -> np.ndarray:
     Q, _ = np.linalg.qr(rng.standard_normal((n, n)))
     A = (Q * lam) @ Q.T
     return 0.5 * (A + A.T)
+
+
+# ------------------------------------------------------- adjoint KPM (reference)
+
+def kpm_plain_moments_dense(H: np.ndarray, psi: np.ndarray, center: float, half_width: float,
+                            n_moments: int) -> np.ndarray:
+    """mu_n = (1/R) sum_s psi_s^T T_n(A) psi_s, A = (H - c)/hw, dense FP64
+    (Chebyshev::compute_moments, rsatb/calc/cheby.hpp:479-514, column-averaged)."""
+    A = (H - center * np.eye(H.shape[0])) / half_width
+    R = psi.shape[1]
+    t0, t1 = psi, A @ psi
+    mu = np.zeros(n_moments)
+    for n in range(n_moments):
+        if n == 0:
+            t = t0
+        elif n == 1:
+            t = t1
+        else:
+            t0, t1 = t1, 2.0 * A @ t1 - t0
+            t = t1
+        mu[n] = float(np.sum(psi * t)) / R
+    return mu
+
+
+def kpm_moments_vjp_dense(H: np.ndarray, psi: np.ndarray, center: float, half_width: float,
+                          n_moments: int, dmu: np.ndarray) -> np.ndarray:
+    """Dense FP64 reference gradient d(sum_n dmu_n mu_n)/dH of the plain
+    moments by reverse-mode differentiation of the three-term recurrence
+    (TEST INFRASTRUCTURE; the reference has no differentiation code):
+    lambda_n = (dmu_n/R) psi + 2 A lambda_{n+1} - lambda_{n+2},
+    G = [lambda_1 t_0^T + 2 sum_{n>=1} lambda_{n+1} t_n^T] / hw."""
+    N = H.shape[0]
+    A = (H - center * np.eye(N)) / half_width
+    R = psi.shape[1]
+    M = n_moments
+    t = [psi]
+    if M > 1:
+        t.append(A @ psi)
+    for n in range(2, M):
+        t.append(2.0 * A @ t[-1] - t[-2])
+    lam = [np.zeros_like(psi)] * (M + 2)
+    lam = list(lam)
+    for n in range(M - 1, 0, -1):
+        lam[n] = (dmu[n] / R) * psi + 2.0 * A @ lam[n + 1] - lam[n + 2]
+    G = np.zeros((N, N))
+    for n in range(0, M - 1):
+        G += (1.0 if n == 0 else 2.0) * lam[n + 1] @ t[n].T
+    return G / half_width

@@ -2,7 +2,7 @@
 //
 // One launch computes, for every row of the N x W output panel,
 //
-//     y = s2 * (((s_in * (A in)) - c * x) * s_out) + g_p * p
+//     y = s2 * (((s_in * (A in)) - c * x) * s_out) + g_p * p [+ g_q * q]
 //
 // which covers BlockSpMat::mult_dense (s_in = alpha, no x, no p), the
 // rescaled operator of Chebyshev::apply_form (rsatb/calc/cheby.hpp:555-591:
@@ -42,8 +42,9 @@ struct StepArgs {
     const void* x;     // -c*x term and <y|x> partner (null: none)
     const void* p;     // recurrence predecessor (null: none)
     const void* psi0;  // DOT_PLAIN partner
+    const void* q;     // optional extra term g_q * q (null: none)
     void* y;
-    double s_in, c, s_out, s2, g_p;
+    double s_in, c, s_out, s2, g_p, g_q;
     int imag;          // A = i * vals (real values, complex panel)
     int dot_mode;
     double* partials;  // [gridDim.x][ndots][W]
@@ -142,6 +143,12 @@ __device__ __forceinline__ void finish_row(const StepArgs& a, int64_t row, int g
     } else if (a.s2 != 1.0) {
 #pragma unroll
         for (int v = 0; v < V; ++v) t[v] *= a.s2;
+    }
+    if (a.q) {
+        VT qv[V];
+        load_vals<VT, V>(static_cast<const VT*>(a.q) + off, qv);
+#pragma unroll
+        for (int v = 0; v < V; ++v) t[v] = fma(a.g_q, double(qv[v]), t[v]);
     }
     VT yv[V];
 #pragma unroll

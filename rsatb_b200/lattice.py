@@ -327,3 +327,34 @@ def graphene_displacements(H: BsrArrays, pos: np.ndarray, cell: np.ndarray) -> n
     f -= np.round(f)
     d[:, :2] = f @ C
     return d
+
+
+# ----------------------------------------------------------- silicon sp3s*
+
+# Fixed SK-like mean blocks of an sp3s* basis (s, px, py, pz, s*), eV: the
+# onsite energies and one nearest- and one second-neighbour block.  The
+# means set the spectrum's shape; every element is then perturbed by
+# N(0, sigma) per bond.
+_SI_ONSITE = np.diag([-4.20, 1.715, 1.715, 1.715, 6.685])
+_SI_NN = np.array([[-2.08, 1.43, 1.43, 1.43, 0.00],
+                   [-1.43, 0.43, 1.13, 1.13, -1.36],
+                   [-1.43, 1.13, 0.43, 1.13, -1.36],
+                   [-1.43, 1.13, 1.13, 0.43, -1.36],
+                   [0.00, 1.36, 1.36, 1.36, 0.00]])
+_SI_NNN = 0.1 * _SI_NN
+
+
+def silicon_sp3s(L: int = 8, seed: int = 11, sigma: float = 0.1):
+    """Silicon L^3 conventional cells (8 L^3 atoms, a = 5.431 A), sp3s*
+    (5 orbitals), 5x5 blocks to the 2nd neighbour shell (1 + 4 + 12 = 17 per
+    row); blocks are the fixed means above plus N(0, sigma) eV, symmetric
+    (H_ji = H_ij^T).  Returns H BsrArrays."""
+    row_ptr, col_ind, dist2, _ = diamond_pattern(L, 8)
+    rng = np.random.default_rng(seed)
+    means = {0: _SI_ONSITE, 3: _SI_NN, 8: _SI_NNN}
+
+    def gen(idx, _r, _c):
+        base = np.stack([means[int(d)] for d in dist2[idx]])
+        return base + sigma * rng.standard_normal((idx.size, 5, 5))
+
+    return BsrArrays(row_ptr, col_ind, _symmetric_blocks(row_ptr, col_ind, gen, 5), 5)

@@ -105,17 +105,15 @@ def test_fp32_vectors_against_fp64(torch_cuda):
 def test_sandwich_form_matches_oracle(torch_cuda):
     """Non-orthogonal sandwich Z^H H Z with dressed currents Z^H V Z."""
     from rsatb_b200 import lattice
-    from rsatb_b200.isqrt import graph_inverse_sqrt_host
     H, V = _tbg(m=1, tiles=(3, 3))
-    # S = I + 0.015 |H| on H's pattern plus the diagonal: SPD, non-orthogonal
+    # S = I + 0.015 |H|: SPD and non-orthogonal; Z = S^-1/2 as a dense BSR
     n = H.n_rows
     Sd = np.eye(n) + 0.015 * np.abs(H.to_dense())
-    rows = np.repeat(np.arange(n), np.diff(H.row_ptr))
-    pr, pc = np.r_[rows, np.arange(n)], np.r_[H.col_ind, np.arange(n)]
-    rp, ci, _ = lattice.csr_from_pairs(n, pr, pc)
-    P = lattice.BsrArrays(rp, ci, np.zeros((ci.size, 1, 1)), 1)
-    S = lattice.BsrArrays(*_pattern_from_dense(Sd, P))
-    Z = graph_inverse_sqrt_host(S)
+    w, Q = np.linalg.eigh(Sd)
+    Zfull = (Q / np.sqrt(w)) @ Q.T
+    rp = (np.arange(n + 1) * n).astype(np.int32)
+    ci = np.tile(np.arange(n), n).astype(np.int32)
+    Z = lattice.BsrArrays(rp, ci, Zfull.reshape(-1, 1, 1), 1)
     Zd = Z.to_dense()
     Hs = Zd.T @ H.to_dense() @ Zd
     w = np.linalg.eigvalsh(0.5 * (Hs + Hs.T))
@@ -124,13 +122,6 @@ def test_sandwich_form_matches_oracle(torch_cuda):
     sig, _, _ = _gpu(torch_cuda, H, V, psi, 24, emin, emax, Z=Z)
     sig_o, _ = _oracle(H, V, psi, 24, emin, emax, Z=Z)
     assert rel_err(sig, sig_o) < 1e-10
-
-
-def _pattern_from_dense(D, P):
-    """Values of dense D on the pattern of P (b = 1)."""
-    rows = np.repeat(np.arange(P.n_block_rows), np.diff(P.row_ptr))
-    vals = D[rows, P.col_ind].reshape(-1, 1, 1)
-    return P.row_ptr, P.col_ind, vals, 1
 
 
 def test_graphene_is_isotropic_in_plane(torch_cuda):
