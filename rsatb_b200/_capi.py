@@ -62,6 +62,12 @@ class FftchebStats(C.Structure):
                 ("transform_ms", C.c_double), ("store_bytes", C.c_size_t)]
 
 
+class AdjointStats(C.Structure):
+    _fields_ = [("checkpoint_stride", C.c_int), ("segments", C.c_int),
+                ("forward_ms", C.c_double), ("backward_ms", C.c_double),
+                ("panels_held", C.c_int)]
+
+
 # rsatb_ns_precision
 NS_FP64, NS_TF32X3, NS_TF32 = 0, 1, 2
 
@@ -99,6 +105,8 @@ SIGNATURES = {
                                            _PD]),
     "rsatb_set_random": (_i, [_vp, _u64, _i, _i, _vp, _i, _i, _i64, _i, _i64, _i, _vp]),
     "rsatb_evaluate_kpm_density": (_i, [_vp, _PD, _i, _PD, _i, _d, _i, _PD]),
+    "rsatb_kpm_moments_vjp": (_i, [_vp, C.POINTER(ChebOp), _vp, _i, _i, _i, _PD, _i, _PD, _vp,
+                                   C.POINTER(AdjointStats)]),
     "rsatb_dc_spectrum_fftcheb": (_i, [_vp, C.POINTER(ChebOp), _vp, _vp, _vp, _vp, _i, _i, _i,
                                        _i, _d, _i, _sz, _i, _PD, _PD,
                                        C.POINTER(FftchebStats)]),
