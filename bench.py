@@ -43,8 +43,9 @@ def parse_args():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["diamond", "graphene", "isqrt", "transport"],
+    p.add_argument("--workload", choices=["diamond", "graphene", "isqrt", "transport", "adjoint"],
                    default="diamond")
+    p.add_argument("--si-L", type=int, default=8, help="silicon conventional cells per side")
     p.add_argument("--tbg-m", type=int, default=31, help="moire index of the TBG cell")
     p.add_argument("--tbg-tiles", type=int, default=4, help="TBG cells per side")
     p.add_argument("--transport-moments", type=int, default=2048)
@@ -271,7 +272,9 @@ def roofline(wl, hbm_peak, peak_note, fma_peaks):
     panel width (each of the 3 SpMMs per application is this kernel)."""
     import torch
     from rsatb_b200.workloads import spmm_bytes, spmm_flops
-    Z32 = wl.cheby32.M.Z
+    # The sandwich's SpMMs run on Z, Z^H and H (same pattern); the
+    # orthogonal form on H alone.
+    Z32 = wl.cheby32.M.Z if wl.cheby32.M is not None else wl.cheby32.H
     dt = wl.vec_dtype("f32")
     item = torch.empty(0, dtype=dt).element_size()
     ms = time_spmm(Z32, wl.n_rows, wl.R, dt)
@@ -281,7 +284,8 @@ def roofline(wl, hbm_peak, peak_note, fma_peaks):
     tfs = flops / (ms * 1e-3) / 1e12
     out = {"bound": "hbm", "achieved": round(gbs, 1), "peak": hbm_peak, "unit": "GB/s",
            "frac": round(gbs / hbm_peak, 4), "traffic": None,
-           "kernel": "cheb_step_kernel<float,float,8,4> (Y = A X, FP32, R=%d)" % wl.R,
+           "kernel": "fused BSR Chebyshev step, Y = A X, FP32, R=%d, %dx%d blocks" % (
+               wl.R, wl.H.block_size, wl.H.block_size),
            "algorithmic_bytes_per_launch": nbytes, "ms_per_launch": round(ms, 4),
            "peak_source": peak_note,
            "compute": {"bound": "fp32_fma", "achieved": round(tfs, 2),
@@ -290,7 +294,7 @@ def roofline(wl, hbm_peak, peak_note, fma_peaks):
                        "flops_per_launch": flops,
                        "peak_source": "rsatb_measure_fma_peak (FMA chains, this run)"}}
     # The same SpMM in FP64, and the memory-bound narrow panels.
-    Z64 = wl.cheby64.M.Z
+    Z64 = wl.cheby64.M.Z if wl.cheby64.M is not None else wl.cheby64.H
     dt64 = wl.vec_dtype("f64")
     ms64 = time_spmm(Z64, wl.n_rows, wl.R, dt64)
     out["fp64_same_kernel"] = {
@@ -608,6 +612,122 @@ def bench_transport(args, dist):
         print(json.dumps(line), flush=True)
 
 
+def bench_adjoint(args, dist):
+    """Adjoint KPM on silicon sp3s* (L^3 conventional cells, 5x5 blocks to the
+    2nd shell, N(0, 0.1) eV around fixed SK-like means): loss = L2 between the
+    Jackson DOS (256 moments, 32 Rademacher vectors per GPU, 1001 energies)
+    and the DOS of a second seeded silicon sample; one step = loss forward +
+    gradient with respect to all block values (autograd backward through the
+    checkpointed adjoint recurrence)."""
+    import torch
+    import oracle
+    from rsatb_b200 import lattice
+    from rsatb_b200.adjoint import KpmDosLoss, dos_basis, kpm_moments_vjp
+    from rsatb_b200.bounds import estimate_spectral_bounds
+    from rsatb_b200.calc import Chebyshev, kpm_dos_moments_plain
+    from rsatb_b200.vbcsr import BlockSpMat, set_random
+    M, R = 256, 32
+    H = lattice.silicon_sp3s(L=args.si_L, seed=11)
+    Ht = lattice.silicon_sp3s(L=args.si_L, seed=12)
+    Hd = BlockSpMat(H.row_ptr, H.col_ind, H.values, 5)
+    Htd = BlockSpMat(Ht.row_ptr, Ht.col_ind, Ht.values, 5)
+    e1 = estimate_spectral_bounds(Chebyshev(Hd, -1, 1))
+    e2 = estimate_spectral_bounds(Chebyshev(Htd, -1, 1))
+    emin, emax = min(e1[0], e2[0]), max(e1[1], e2[1])
+    psi = torch.empty(H.n_rows, R, dtype=torch.float64, device="cuda")
+    set_random(psi, 20240917, normalize=True, orbitals_per_atom=5, kind=1,
+               first_column=dist.rank * R)
+    x = np.linspace(-0.98, 0.98, 1001)
+    D = dos_basis(M, x)
+    target = D @ kpm_dos_moments_plain(Chebyshev(Htd, emin, emax), psi, M).real
+    v0 = torch.as_tensor(H.values).cuda()
+
+    def step():
+        v = v0.clone().requires_grad_(True)
+        loss = KpmDosLoss.apply(v, Hd, psi, emin, emax, M, x, target)
+        loss.backward()
+        return float(loss), v.grad
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    dist.barrier()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        ev[0].record()
+        for _ in range(args.steps):
+            loss, g = step()
+        ev[1].record()
+        torch.cuda.synchronize()
+    clocks = clk.summary()
+    ms = dist.max(ev[0].elapsed_time(ev[1]) / args.steps)
+    dist.barrier()
+    # FD checks (h = 1e-6): 6 sampled values and one random direction.
+    h = 1e-6
+    rng = np.random.default_rng(3)
+
+    def L(vals):
+        return float(KpmDosLoss.apply(vals, Hd, psi, emin, emax, M, x, target))
+
+    flat = v0.reshape(-1)
+    fd_err = 0.0
+    gf = g.reshape(-1).cpu().numpy()
+    gscale = float(np.abs(gf).max())
+    for e in rng.choice(flat.numel(), size=6, replace=False):
+        p, m_ = flat.clone(), flat.clone()
+        p[e] += h
+        m_[e] -= h
+        fd = (L(p.view_as(v0)) - L(m_.view_as(v0))) / (2 * h)
+        fd_err = max(fd_err, abs(fd - gf[e]) / gscale)
+    Dv = torch.as_tensor(rng.standard_normal(tuple(v0.shape))).cuda()
+    fd = (L(v0 + h * Dv) - L(v0 - h * Dv)) / (2 * h)
+    an = float((g * Dv).sum())
+    dir_err = abs(fd - an) / max(abs(an), 1e-300)
+    # FP32 vectors against the FP64 gradient (same dmu).
+    Hd.set_values(v0)
+    c64 = Chebyshev(Hd, emin, emax)
+    mu = kpm_dos_moments_plain(c64, psi, M).real
+    dmu = 2.0 * ((D @ mu - target) @ D)
+    g64, _, st64 = kpm_moments_vjp(c64, psi, M, dmu)
+    g32, _, st32 = kpm_moments_vjp(c64.astype("f32"), psi.float(), M, dmu)
+    err32 = float((g32 - g64).abs().max() / g64.abs().max())
+    base = None
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        import scipy.sparse as sp
+        Hcsr = sp.csr_matrix(H.to_dense()) if H.n_rows <= 4000 else None
+        if Hcsr is None:
+            rows = np.repeat(np.arange(H.n_block_rows), np.diff(H.row_ptr))
+            b = 5
+            rr = (rows[:, None, None] * b + np.arange(b)[None, :, None]).repeat(b, 2)
+            cc = (H.col_ind[:, None, None] * b + np.arange(b)[None, None, :]).repeat(b, 1)
+            Hcsr = sp.csr_matrix((H.values.reshape(-1), (rr.reshape(-1), cc.reshape(-1))),
+                                 shape=(H.n_rows, H.n_rows))
+        ms_cpu = 32
+        tc = time.perf_counter()
+        oracle.kpm_moments_vjp_sparse(Hcsr, psi.cpu().numpy(), (emax + emin) / 2,
+                                      (emax - emin) / 2, ms_cpu, dmu[:ms_cpu])
+        dt = time.perf_counter() - tc
+        base = {"value": 1e3 * dt * M / ms_cpu, "unit": "ms per gradient (extrapolated)",
+                "cores": 1, "kind": "port", "seconds": round(dt, 3),
+                "sample": f"{ms_cpu} of {M} moments, same operator and samples, scipy.sparse "
+                          "FP64, extrapolated linearly to 256 moments"}
+    if dist.rank == 0:
+        line = {
+            "metric": "adjoint KPM gradient of a DOS loss", "value": round(ms, 3),
+            "unit": "ms per loss+gradient", "n_gpus": dist.world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded Si sp3s* generator, Rademacher vectors)",
+            "config": {"workload": f"adjoint_si: Si {args.si_L}^3 cells sp3s*, 5x5 blocks to "
+                                   "the 2nd shell", "n_rows": H.n_rows,
+                       "nnz_blocks": int(H.nnz_blocks), "n_moments": M,
+                       "vectors_per_gpu": R, "energies": int(x.size)},
+            "loss": loss, "fd_max_err_rel_to_max_grad": fd_err, "directional_fd_rel_err": dir_err,
+            "grad_f32_vs_f64_rel": err32, "vjp_stats_f64": st64, "vjp_stats_f32": st32,
+            "cpu_baseline": base, "clocks": clocks}
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     if args.spmm_only:
@@ -616,6 +736,10 @@ def main():
     dist = Dist()
     if args.workload == "isqrt" and args.impl == "ours":
         bench_isqrt(args, dist)
+        dist.close()
+        return
+    if args.workload == "adjoint" and args.impl == "ours":
+        bench_adjoint(args, dist)
         dist.close()
         return
     if args.workload == "transport" and args.impl == "ours":

@@ -363,3 +363,35 @@ def kpm_moments_vjp_dense(H: np.ndarray, psi: np.ndarray, center: float, half_wi
     for n in range(0, M - 1):
         G += (1.0 if n == 0 else 2.0) * lam[n + 1] @ t[n].T
     return G / half_width
+
+
+def kpm_moments_vjp_sparse(H, psi: np.ndarray, center: float, half_width: float,
+                           n_moments: int, dmu: np.ndarray):
+    """The same reverse-mode gradient with a scipy.sparse H (CSR, FP64),
+    sampled on H's pattern: returns (mu, grad data aligned with H.data).
+    All t_n are kept (no checkpoints): the CPU baseline of the adjoint."""
+    import scipy.sparse as sp
+    A = (H - center * sp.identity(H.shape[0], format="csr")) / half_width
+    A = A.tocsr()
+    R = psi.shape[1]
+    M = n_moments
+    t = [psi]
+    if M > 1:
+        t.append(A @ psi)
+    for n in range(2, M):
+        t.append(2.0 * (A @ t[-1]) - t[-2])
+    mu = np.array([float(np.sum(psi * tn)) / R for tn in t])
+    lam = [None] * (M + 2)
+    z = np.zeros_like(psi)
+    lam[M] = z
+    lam[M + 1] = z
+    for n in range(M - 1, 0, -1):
+        lam[n] = (dmu[n] / R) * psi + 2.0 * (A @ lam[n + 1]) - lam[n + 2]
+    Hc = H.tocsr()
+    rows = np.repeat(np.arange(Hc.shape[0]), np.diff(Hc.indptr))
+    cols = Hc.indices
+    g = np.zeros(cols.size)
+    for n in range(0, M - 1):
+        w = 1.0 if n == 0 else 2.0
+        g += w * np.einsum("ij,ij->i", lam[n + 1][rows], t[n][cols])
+    return mu, g / half_width

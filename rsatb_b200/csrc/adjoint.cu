@@ -113,17 +113,6 @@ int launch_sddmm(rsatb_context* ctx, const rsatb_bsr_matrix* H, int R, int n0, i
     return RSATB_SUCCESS;
 }
 
-struct DevBuf {
-    void* p = nullptr;
-    ~DevBuf() {
-        if (p) cudaFree(p);
-    }
-    int alloc(size_t bytes) {
-        RSATB_CUDA_TRY(cudaMalloc(&p, bytes ? bytes : 16));
-        return RSATB_SUCCESS;
-    }
-};
-
 StepArgs zero_args(int W) {
     StepArgs a{};
     a.W = W;
@@ -149,26 +138,27 @@ int vjp_impl(rsatb_context* ctx, const rsatb_cheb_op* op, const VT* psi, int R, 
     if (C > M) C = M;
     const int n_seg = (M + C - 1) / C;
 
-    DevBuf bCk, bT, bL, bLam, bZero, bF, bDots, bPart;
-    RSATB_TRY(bCk.alloc(2 * size_t(n_seg) * pbytes));
-    RSATB_TRY(bT.alloc(size_t(C) * pbytes));
-    RSATB_TRY(bL.alloc(size_t(C) * pbytes));
-    RSATB_TRY(bLam.alloc(3 * pbytes));
-    RSATB_TRY(bZero.alloc(pbytes));
-    RSATB_TRY(bF.alloc(3 * pbytes));
-    RSATB_TRY(bDots.alloc(size_t(M) * W * sizeof(double)));
+    // Everything lives in the context's grow-only scratch (no per-call
+    // cudaMalloc / cudaFree): checkpoints, the two segment buffers, three
+    // adjoint panels, a zero panel, three forward panels, dots, partials.
+    const size_t pal = (pbytes + 255) & ~size_t(255);
     const size_t max_ctas = size_t(ctx->sm_count) * 8;
-    RSATB_TRY(bPart.alloc(max_ctas * 2 * W * sizeof(double)));
+    const size_t dots_b = (size_t(M) * W * sizeof(double) + 255) & ~size_t(255);
+    const size_t part_b = (max_ctas * 2 * W * sizeof(double) + 255) & ~size_t(255);
+    const size_t n_pan = 2 * size_t(n_seg) + 2 * size_t(C) + 3 + 1 + 3;
+    void* sp = nullptr;
+    RSATB_TRY(ctx_scratch(ctx, n_pan * pal + dots_b + part_b, &sp));
+    char* base = static_cast<char*>(sp);
     unsigned* counter = nullptr;
     RSATB_TRY(ctx_counters(ctx, 1, &counter));
-    VT* ck = static_cast<VT*>(bCk.p);
-    VT* tseg = static_cast<VT*>(bT.p);
-    VT* lseg = static_cast<VT*>(bL.p);
-    VT* lam = static_cast<VT*>(bLam.p);
-    VT* zero = static_cast<VT*>(bZero.p);
-    VT* f = static_cast<VT*>(bF.p);
-    double* dots = static_cast<double*>(bDots.p);
-    double* partials = static_cast<double*>(bPart.p);
+    VT* ck = reinterpret_cast<VT*>(base);
+    VT* tseg = reinterpret_cast<VT*>(base + 2 * size_t(n_seg) * pal);
+    VT* lseg = reinterpret_cast<VT*>(base + (2 * size_t(n_seg) + C) * pal);
+    VT* lam = reinterpret_cast<VT*>(base + (2 * size_t(n_seg) + 2 * C) * pal);
+    VT* zero = reinterpret_cast<VT*>(base + (2 * size_t(n_seg) + 2 * C + 3) * pal);
+    VT* f = reinterpret_cast<VT*>(base + (2 * size_t(n_seg) + 2 * C + 4) * pal);
+    double* dots = reinterpret_cast<double*>(base + n_pan * pal);
+    double* partials = reinterpret_cast<double*>(base + n_pan * pal + dots_b);
     RSATB_CUDA_TRY(cudaMemsetAsync(zero, 0, pbytes, st));
     RSATB_CUDA_TRY(cudaMemsetAsync(grad, 0, size_t(H->nnz_blocks) * b * b * sizeof(double), st));
 
@@ -195,7 +185,8 @@ int vjp_impl(rsatb_context* ctx, const rsatb_cheb_op* op, const VT* psi, int R, 
         }
         return run_step(ctx, H, vdt, a);
     };
-    auto ckpt = [&](int k, int which) { return ck + (2 * size_t(k) + which) * panel; };
+    const size_t ps = pal / sizeof(VT);  // panel stride in elements
+    auto ckpt = [&](int k, int which) { return ck + (2 * size_t(k) + which) * ps; };
 
     cudaEvent_t e0, e1, e2;
     RSATB_CUDA_TRY(cudaEventCreate(&e0));
@@ -226,7 +217,7 @@ int vjp_impl(rsatb_context* ctx, const rsatb_cheb_op* op, const VT* psi, int R, 
     int fs = 0;
     for (int n = 0; n < M; ++n) {
         if (n > 0) {
-            VT* out = f + size_t(fs) * panel;
+            VT* out = f + size_t(fs) * ps;
             fs = (fs + 1) % 3;
             if (n == 1) RSATB_TRY(step(tc, nullptr, out, 1.0, 0.0, nullptr, 0.0, dots + size_t(n) * W));
             else RSATB_TRY(step(tc, tp, out, 2.0, -1.0, nullptr, 0.0, dots + size_t(n) * W));
@@ -252,24 +243,24 @@ int vjp_impl(rsatb_context* ctx, const rsatb_cheb_op* op, const VT* psi, int R, 
         // recompute t_n, n in [nb0, nb1), into tseg
         RSATB_CUDA_TRY(cudaMemcpyAsync(tseg, ckpt(k, 0), pbytes, cudaMemcpyDeviceToDevice, st));
         for (int n = nb0 + 1; n < nb1; ++n) {
-            VT* out = tseg + size_t(n - nb0) * panel;
-            const VT* cur = tseg + size_t(n - 1 - nb0) * panel;
+            VT* out = tseg + size_t(n - nb0) * ps;
+            const VT* cur = tseg + size_t(n - 1 - nb0) * ps;
             if (n == 1) {
                 RSATB_TRY(step(cur, nullptr, out, 1.0, 0.0, nullptr, 0.0, nullptr));
             } else {
-                const VT* prv = (n - 2 >= nb0) ? tseg + size_t(n - 2 - nb0) * panel : ckpt(k, 1);
+                const VT* prv = (n - 2 >= nb0) ? tseg + size_t(n - 2 - nb0) * ps : ckpt(k, 1);
                 RSATB_TRY(step(cur, prv, out, 2.0, -1.0, nullptr, 0.0, nullptr));
             }
         }
         for (int n = nb1 - 1; n >= nb0; --n) {
             // lambda_{n+1} pairs with t_n in the gradient
-            RSATB_CUDA_TRY(cudaMemcpyAsync(lseg + size_t(n - nb0) * panel, l1, pbytes,
+            RSATB_CUDA_TRY(cudaMemcpyAsync(lseg + size_t(n - nb0) * ps, l1, pbytes,
                                            cudaMemcpyDeviceToDevice, st));
             if (n >= 1) {
-                VT* out = lam + size_t(ls) * panel;
+                VT* out = lam + size_t(ls) * ps;
                 while (out == l1 || out == l2) {
                     ls = (ls + 1) % 3;
-                    out = lam + size_t(ls) * panel;
+                    out = lam + size_t(ls) * ps;
                 }
                 ls = (ls + 1) % 3;
                 RSATB_TRY(step(l1, l2, out, 2.0, -1.0, psi, dmu[n] / double(R), nullptr));
@@ -277,7 +268,7 @@ int vjp_impl(rsatb_context* ctx, const rsatb_cheb_op* op, const VT* psi, int R, 
                 l1 = out;
             }
         }
-        RSATB_TRY(launch_sddmm<VT>(ctx, H, R, nb0, nb1 - nb0, M - 2, inv_hw, lseg, tseg, panel,
+        RSATB_TRY(launch_sddmm<VT>(ctx, H, R, nb0, nb1 - nb0, M - 2, inv_hw, lseg, tseg, int64_t(ps),
                                    grad));
     }
     RSATB_CUDA_TRY(cudaEventRecord(e2, st));

@@ -192,6 +192,69 @@ __device__ __forceinline__ void finish_row(const StepArgs& a, int64_t row, int g
     }
 }
 
+// After every CTA wrote its partial dots: the last CTA to arrive (ticket
+// counter) sums the gridDim.x partials of each of the O = ndots * W outputs
+// and resets the counter for the next launch.  With fewer outputs than
+// threads, T = blockDim / O threads share an output (CTAs b = part, part + T,
+// ...) and their sums are combined in part order; otherwise each thread takes
+// whole outputs with eight independent accumulators, so the L2 loads of one
+// output are in flight together.  The order is fixed for a given grid:
+// deterministic dots.  Needs blockDim.x <= 256.
+__device__ __forceinline__ void finish_partials(const StepArgs& a, int ndots) {
+    __threadfence();
+    __syncthreads();
+    __shared__ unsigned ticket;
+    __shared__ double comb[256];
+    if (threadIdx.x == 0) ticket = atomicAdd(a.counter, 1u);
+    __syncthreads();
+    if (ticket != gridDim.x - 1) return;
+    __threadfence();
+    const int O = ndots * a.W;
+    const int nt = blockDim.x;
+    const unsigned G = gridDim.x;
+    const double* P = a.partials;
+    if (O * 2 > nt) {
+        for (int idx = threadIdx.x; idx < O; idx += nt) {
+            double s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0, s5 = 0, s6 = 0, s7 = 0;
+            unsigned b = 0;
+            for (; b + 8 <= G; b += 8) {
+                s0 += __ldcg(P + size_t(b) * O + idx);
+                s1 += __ldcg(P + size_t(b + 1) * O + idx);
+                s2 += __ldcg(P + size_t(b + 2) * O + idx);
+                s3 += __ldcg(P + size_t(b + 3) * O + idx);
+                s4 += __ldcg(P + size_t(b + 4) * O + idx);
+                s5 += __ldcg(P + size_t(b + 5) * O + idx);
+                s6 += __ldcg(P + size_t(b + 6) * O + idx);
+                s7 += __ldcg(P + size_t(b + 7) * O + idx);
+            }
+            for (; b < G; ++b) s0 += __ldcg(P + size_t(b) * O + idx);
+            a.dots_out[idx] = ((s0 + s1) + (s2 + s3)) + ((s4 + s5) + (s6 + s7));
+        }
+    } else {
+        const int T = nt / O;
+        const int o = threadIdx.x % O, part = threadIdx.x / O;
+        double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+        if (part < T) {
+            unsigned b = part;
+            for (; b + 3 * T < G; b += 4 * T) {
+                s0 += __ldcg(P + size_t(b) * O + o);
+                s1 += __ldcg(P + size_t(b + T) * O + o);
+                s2 += __ldcg(P + size_t(b + 2 * T) * O + o);
+                s3 += __ldcg(P + size_t(b + 3 * T) * O + o);
+            }
+            for (; b < G; b += T) s0 += __ldcg(P + size_t(b) * O + o);
+        }
+        comb[threadIdx.x] = (s0 + s1) + (s2 + s3);
+        __syncthreads();
+        if (threadIdx.x < O) {
+            double t = 0.0;
+            for (int q = 0; q < T; ++q) t += comb[q * O + threadIdx.x];
+            a.dots_out[threadIdx.x] = t;
+        }
+    }
+    if (threadIdx.x == 0) *a.counter = 0u;  // ready for the next launch
+}
+
 // CTA reduction of the per-thread dot partials, then the last-CTA
 // reduction over CTAs.  Deterministic: fixed summation order throughout.
 template <int V>
@@ -215,21 +278,7 @@ __device__ __forceinline__ void reduce_dots(const StepArgs& a, int L, const doub
         for (int t = g; t < nt; t += L) s += red[(d * nt + t) * V + v];
         mine[idx] = s;
     }
-    __threadfence();
-    __syncthreads();
-    __shared__ unsigned ticket;
-    if (threadIdx.x == 0) ticket = atomicAdd(a.counter, 1u);
-    __syncthreads();
-    if (ticket == gridDim.x - 1) {
-        __threadfence();
-        for (int idx = threadIdx.x; idx < ndots * W; idx += nt) {
-            double s = 0.0;
-            for (unsigned b = 0; b < gridDim.x; ++b)
-                s += __ldcg(a.partials + size_t(b) * ndots * W + idx);
-            a.dots_out[idx] = s;
-        }
-        if (threadIdx.x == 0) *a.counter = 0u;  // ready for the next launch
-    }
+    finish_partials(a, ndots);
 }
 
 // Compile-time block size B.  MT: real component type of the matrix values;

@@ -42,21 +42,7 @@ __device__ __forceinline__ void reduce_dots_lanes(const StepArgs& a, int KL, int
         }
         mine[idx] = s;
     }
-    __threadfence();
-    __syncthreads();
-    __shared__ unsigned ticket;
-    if (threadIdx.x == 0) ticket = atomicAdd(a.counter, 1u);
-    __syncthreads();
-    if (ticket == gridDim.x - 1) {
-        __threadfence();
-        for (int idx = threadIdx.x; idx < ndots * W; idx += nt) {
-            double s = 0.0;
-            for (unsigned b = 0; b < gridDim.x; ++b)
-                s += __ldcg(a.partials + size_t(b) * ndots * W + idx);
-            a.dots_out[idx] = s;
-        }
-        if (threadIdx.x == 0) *a.counter = 0u;
-    }
+    finish_partials(a, ndots);
 }
 
 // VT: panel/matrix real type; B: block size; KL: lanes per block row

@@ -119,29 +119,19 @@ __device__ __forceinline__ void reduce_dots_staged(const StepArgs& a, int Lp, in
         const int g = w / V, v = w - g * V;
         const int ch = g / Lp, li = g - ch * Lp;
         double s = 0.0;
-        for (int t = 0; t < nt; ++t) {
-            const int lane = t & 31;
-            if (lane % Lp != li) continue;
-            if ((((t >> 5) * spw + lane / Lp) % n_chunks) != ch) continue;
-            s += red[(d * nt + t) * V + v];
+        if (n_chunks == 1) {
+            for (int t = li; t < nt; t += Lp) s += red[(d * nt + t) * V + v];
+        } else {
+            for (int t = 0; t < nt; ++t) {
+                const int lane = t & 31;
+                if (lane % Lp != li) continue;
+                if ((((t >> 5) * spw + lane / Lp) % n_chunks) != ch) continue;
+                s += red[(d * nt + t) * V + v];
+            }
         }
         mine[idx] = s;
     }
-    __threadfence();
-    __syncthreads();
-    __shared__ unsigned ticket;
-    if (threadIdx.x == 0) ticket = atomicAdd(a.counter, 1u);
-    __syncthreads();
-    if (ticket == gridDim.x - 1) {
-        __threadfence();
-        for (int idx = threadIdx.x; idx < ndots * W; idx += nt) {
-            double s = 0.0;
-            for (unsigned b = 0; b < gridDim.x; ++b)
-                s += __ldcg(a.partials + size_t(b) * ndots * W + idx);
-            a.dots_out[idx] = s;
-        }
-        if (threadIdx.x == 0) *a.counter = 0u;
-    }
+    finish_partials(a, ndots);
 }
 
 template <typename VT, typename MT, int B, int V, bool CM, bool CV, int STAGES>

@@ -65,6 +65,13 @@ struct rsatb_context {
     unsigned* counters = nullptr;
     int n_counters = 0;
     int64_t launches = 0;
+    // The KPM moment recurrence as a captured CUDA graph, replayed while the
+    // call's arguments (key) are unchanged; the key of the last direct run
+    // decides when to capture (the second identical call).
+    cudaGraphExec_t kpm_graph = nullptr;
+    std::string kpm_graph_key;
+    std::string kpm_seen_key;
+    int64_t kpm_graph_launches = 0;
 };
 
 struct rsatb_bsr_matrix {

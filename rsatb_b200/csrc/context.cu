@@ -119,6 +119,7 @@ int rsatb_ctx_destroy(rsatb_ctx_t ctx) {
     cudaStreamSynchronize(ctx->stream);
     if (ctx->scratch) cudaFree(ctx->scratch);
     if (ctx->counters) cudaFree(ctx->counters);
+    if (ctx->kpm_graph) cudaGraphExecDestroy(ctx->kpm_graph);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return RSATB_SUCCESS;

@@ -5,6 +5,8 @@
 
 #include <cmath>
 #include <complex>
+#include <cstdlib>
+#include <string>
 #include <vector>
 
 namespace rsatb_b200 {
@@ -135,6 +137,118 @@ int apply_fused(rsatb_context* ctx, const rsatb_cheb_op* op, const OpShape& sh, 
     return run_step(ctx, op->ZH, vdt, last);   // y = Z^H w, fused epilogue
 }
 
+
+// Key of one recurrence launch sequence: every pointer and scalar its kernel
+// arguments depend on.  A graph captured for a key replays only that key.
+std::string recurrence_key(const rsatb_cheb_op* op, const void* psi, int n_vectors, int vdt,
+                           int n_moments, int doubled, const void* scratch, const void* counter) {
+    std::string k;
+    auto put = [&](const void* p, size_t n) { k.append(static_cast<const char*>(p), n); };
+    auto put_mat = [&](const rsatb_bsr_matrix* A) {
+        put(&A, sizeof(A));
+        if (!A) return;
+        put(&A->values, sizeof(void*));
+        put(&A->row_ptr, sizeof(void*));
+        put(&A->col_ind, sizeof(void*));
+        put(&A->nnz_blocks, sizeof(int64_t));
+        put(&A->n_block_rows, sizeof(int));
+        put(&A->block_size, sizeof(int));
+        put(&A->dtype, sizeof(int));
+        put(&A->flags, sizeof(unsigned));
+    };
+    put(&op->form, sizeof(int));
+    put_mat(op->H);
+    put_mat(op->form == RSATB_FORM_SANDWICH ? op->Z : nullptr);
+    put_mat(op->form == RSATB_FORM_SANDWICH ? op->ZH : nullptr);
+    put(&op->center, sizeof(double));
+    put(&op->half_width, sizeof(double));
+    put(&psi, sizeof(psi));
+    put(&n_vectors, sizeof(int));
+    put(&vdt, sizeof(int));
+    put(&n_moments, sizeof(int));
+    put(&doubled, sizeof(int));
+    put(&scratch, sizeof(scratch));
+    put(&counter, sizeof(counter));
+    return k;
+}
+
+// Runs `issue` (the recurrence's launches) directly, or replays / captures
+// it as a CUDA graph: a key seen on the previous call is captured once and
+// then replayed while it stays the same, so a repeated call costs one graph
+// launch instead of one host launch per step.  Graphs are off when the
+// kernel choice is forced through the environment (its value is not part
+// of the key) or RSATB_NO_GRAPH is set.  On the legacy default stream the
+// graph runs on the context's own stream after the caller's queued work.
+template <typename F>
+int run_recurrence(rsatb_context* ctx, const rsatb_cheb_op* op, const void* psi, int n_vectors,
+                   int vdt, int n_moments, int doubled, const void* scratch,
+                   const void* counter, int n_steps, F&& issue) {
+    const bool graph_ok = n_steps >= 8 && !std::getenv("RSATB_NO_GRAPH") &&
+                          !std::getenv("RSATB_STEP_KERNEL") && !std::getenv("RSATB_STEP_V");
+    if (!graph_ok) return issue();
+    const std::string key =
+        recurrence_key(op, psi, n_vectors, vdt, n_moments, doubled, scratch, counter);
+    const bool replay = ctx->kpm_graph && ctx->kpm_graph_key == key;
+    const bool capture = !replay && ctx->kpm_seen_key == key;
+    if (!replay && !capture) {
+        ctx->kpm_seen_key = key;
+        return issue();
+    }
+    cudaStream_t run = ctx->stream ? ctx->stream : ctx->own_stream;
+    if (run != ctx->stream) {
+        cudaEvent_t e;
+        RSATB_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        const cudaError_t r1 = cudaEventRecord(e, ctx->stream);
+        const cudaError_t r2 = cudaStreamWaitEvent(run, e, 0);
+        cudaEventDestroy(e);
+        RSATB_CUDA_TRY(r1);
+        RSATB_CUDA_TRY(r2);
+    }
+    if (capture) {
+        if (ctx->kpm_graph) {
+            cudaGraphExecDestroy(ctx->kpm_graph);
+            ctx->kpm_graph = nullptr;
+            ctx->kpm_graph_key.clear();
+        }
+        cudaStream_t saved = ctx->stream;
+        ctx->stream = run;
+        const int64_t l0 = ctx->launches;
+        RSATB_CUDA_TRY(cudaStreamBeginCapture(run, cudaStreamCaptureModeThreadLocal));
+        const int st = issue();
+        cudaGraph_t g = nullptr;
+        const cudaError_t ec = cudaStreamEndCapture(run, &g);
+        ctx->stream = saved;
+        if (st != RSATB_SUCCESS) {
+            if (g) cudaGraphDestroy(g);
+            return st;
+        }
+        if (ec != cudaSuccess)
+            return set_error(RSATB_CUDA_ERROR, "recurrence capture: %s", cudaGetErrorString(ec));
+        const cudaError_t ei = cudaGraphInstantiate(&ctx->kpm_graph, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) {
+            ctx->kpm_graph = nullptr;
+            return set_error(RSATB_CUDA_ERROR, "recurrence graph: %s", cudaGetErrorString(ei));
+        }
+        ctx->kpm_graph_key = key;
+        ctx->kpm_graph_launches = ctx->launches - l0;
+        ctx->launches = l0;
+    }
+    RSATB_CUDA_TRY(cudaGraphLaunch(ctx->kpm_graph, run));
+    ctx->launches += ctx->kpm_graph_launches;
+    if (run != ctx->stream) {
+        // later work on the caller's stream sees the moments
+        cudaEvent_t e;
+        RSATB_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        const cudaError_t r1 = cudaEventRecord(e, run);
+        const cudaError_t r2 = cudaStreamWaitEvent(ctx->stream, e, 0);
+        cudaEventDestroy(e);
+        RSATB_CUDA_TRY(r1);
+        RSATB_CUDA_TRY(r2);
+    }
+    return RSATB_SUCCESS;
+}
+
 }  // namespace
 }  // namespace rsatb_b200
 
@@ -231,37 +345,37 @@ int rsatb_kpm_dos_moments(rsatb_ctx_t ctx, const rsatb_cheb_op* op, const void* 
     unsigned* counter = nullptr;
     RSATB_TRY(ctx_counters(ctx, 1, &counter));
 
-    // mu_0 = <psi|psi> per column.
-    {
-        StepArgs a = blank_args(W);
-        a.x = psi;
-        a.in = psi;
-        a.partials = partials;
-        a.dots_out = dots;
-        a.counter = counter;
-        RSATB_TRY(run_coldot(ctx, vec_dtype, sh.n_rows, a));
-    }
+    // The recurrence: mu_0 = <psi|psi> per column, then psi_1 = Op~ psi_0 and
+    // psi_s = 2 Op~ psi_{s-1} - psi_{s-2}, each step with its fused dots.
     const double inv_hw = 1.0 / op->half_width;
-    // Step 1: psi_1 = Op~ psi_0.  Later steps: psi_{s} = 2 Op~ psi_{s-1} - psi_{s-2}.
-    const void* prev = nullptr;   // psi_{s-2}
-    const void* cur = psi;        // psi_{s-1}
-    int slot = 0;
-    for (int sidx = 1; sidx <= n_steps; ++sidx) {
-        void* out = buf[slot];
-        slot = (slot + 1) % 3;
-        double* dslot = dots + size_t(sidx) * 2 * W;
-        if (sidx == 1) {
-            RSATB_TRY(apply_fused(ctx, op, sh, vec_dtype, W, cur, cur, nullptr, out, u, w, inv_hw,
-                                  1.0, 0.0, doubled ? DOT_DOUBLING : DOT_PLAIN, psi, partials,
-                                  dslot, counter));
-        } else {
-            RSATB_TRY(apply_fused(ctx, op, sh, vec_dtype, W, cur, cur, prev, out, u, w, inv_hw,
-                                  2.0, -1.0, doubled ? DOT_DOUBLING : DOT_PLAIN, psi, partials,
-                                  dslot, counter));
+    auto issue = [&]() -> int {
+        {
+            StepArgs a = blank_args(W);
+            a.x = psi;
+            a.in = psi;
+            a.partials = partials;
+            a.dots_out = dots;
+            a.counter = counter;
+            RSATB_TRY(run_coldot(ctx, vec_dtype, sh.n_rows, a));
         }
-        prev = cur;
-        cur = out;
-    }
+        const void* prev = nullptr;   // psi_{s-2}
+        const void* cur = psi;        // psi_{s-1}
+        int slot = 0;
+        for (int sidx = 1; sidx <= n_steps; ++sidx) {
+            void* out = buf[slot];
+            slot = (slot + 1) % 3;
+            double* dslot = dots + size_t(sidx) * 2 * W;
+            RSATB_TRY(apply_fused(ctx, op, sh, vec_dtype, W, cur, cur, sidx == 1 ? nullptr : prev,
+                                  out, u, w, inv_hw, sidx == 1 ? 1.0 : 2.0,
+                                  sidx == 1 ? 0.0 : -1.0, doubled ? DOT_DOUBLING : DOT_PLAIN,
+                                  psi, partials, dslot, counter));
+            prev = cur;
+            cur = out;
+        }
+        return RSATB_SUCCESS;
+    };
+    RSATB_TRY(run_recurrence(ctx, op, psi, n_vectors, vec_dtype, n_moments, doubled, s,
+                             counter, n_steps, issue));
 
     std::vector<double> h(size_t(n_steps + 1) * 2 * W);
     RSATB_CUDA_TRY(cudaMemcpyAsync(h.data(), dots, sizeof(double) * h.size(),

@@ -323,3 +323,26 @@ def test_kernel_variants_match_register_kernel(torch_cuda, case, precision, kern
     tol = (1e-13 if precision == "f64" else 1e-6) * (50 if kernel == "rowsplit" else 1)
     assert rel_err(Y1.cpu().numpy(), Y2.cpu().numpy()) < tol
     assert np.abs(col1 - col2).max() <= tol * np.abs(col2).max() * 10
+
+
+def test_recurrence_graph_replay_matches_direct_run(torch_cuda, monkeypatch):
+    """The second identical call captures the recurrence as a CUDA graph and
+    later ones replay it: same moments bit for bit, same launch count."""
+    torch = torch_cuda
+    from rsatb_b200.calc import kpm_dos_moments
+    from rsatb_b200.vbcsr import set_random
+    H = graphene_case(16, 16)
+    c = build_cheby(H, -9.0, 9.0)
+    psi = torch.empty(H.n_rows, 4, dtype=torch.complex128, device="cuda")
+    set_random(psi, 7)
+    ctx = c.H.ctx
+    mus, counts = [], []
+    for _ in range(4):
+        l0 = ctx.launch_count()
+        mus.append(kpm_dos_moments(c, psi, 96))
+        counts.append(ctx.launch_count() - l0)
+    monkeypatch.setenv("RSATB_NO_GRAPH", "1")
+    direct = kpm_dos_moments(c, psi, 96)
+    for m in mus:
+        assert np.array_equal(m, direct)
+    assert len(set(counts)) == 1 and counts[0] == 1 + 48
