@@ -196,10 +196,10 @@ def dos_grid(emin: float, emax: float, n_moments: int):
 
 def run_moments(wl, cheby, psi, dist):
     from rsatb_b200.calc import kpm_dos_moments
+    from rsatb_b200.shard import combine_average
     mu = kpm_dos_moments(cheby, psi, wl.n_moments)
     if dist.world > 1:
-        s = dist.sum_array(np.concatenate([mu.real, mu.imag]) * wl.R)
-        mu = (s[:wl.n_moments] + 1j * s[wl.n_moments:]) / (wl.R * dist.world)
+        mu = combine_average(mu, wl.R, dist.sum_array, wl.R * dist.world)
     return mu
 
 
