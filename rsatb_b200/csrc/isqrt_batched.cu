@@ -799,7 +799,8 @@ extern "C" int rsatb_isqrt_columns_batched(rsatb_ctx_t ctx, int n_problems, cons
             if (!ch.ids.empty() && chunk_bytes(elems + e, low) > o.workspace) break;
             const int np = npad(p);
             if (ch.buckets.empty() || ch.buckets.back().n_pad != np) {
-                const int tiles = (np + 255) / 256;
+                const int max_nt = low ? tc_max_nt() : 256;
+                const int tiles = (np + max_nt - 1) / max_nt;
                 const int nt = ((np + tiles - 1) / tiles + 15) / 16 * 16;
                 ch.buckets.push_back(Bucket{np, int(ch.ids.size()), 0, elems, nt});
             }

@@ -74,6 +74,8 @@ int launch_tc_gemm(rsatb_context* ctx, const TcMaps& maps, const TcArgs& args);
 // Sets the kernel's shared-memory opt-in and resolves the tensor-map
 // encoder; called on the current device before any capture.
 int prepare_tc_gemm();
+// Widest N tile the selected tensor-core kernel takes (128 or 256).
+int tc_max_nt();
 
 // cuTensorMapEncodeTiled of a bucket: fp32 array `base` (element offset
 // already applied), dims (n_pad, n_pad, count), box (32, box_rows, 1),

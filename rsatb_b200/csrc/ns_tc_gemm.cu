@@ -17,6 +17,7 @@
 #include "umma.cuh"
 
 #include <cudaTypedefs.h>
+#include <cstdlib>
 #include <mutex>
 
 namespace rsatb_b200 {
@@ -207,6 +208,218 @@ __global__ void __launch_bounds__(128, 1)
     }
 }
 
+// ---------------------------------------------------------------------------
+// Warp-specialised variant: warp 0 is the TMA producer, warp 1 the MMA
+// issuer (and TMEM owner), warps 2-5 the epilogue.  A 3-stage ring of
+// 64 KB stages (A hi/lo and B hi/lo, K chunk 32, N tile <= 128) feeds the
+// MMAs; the accumulator is double-buffered in TMEM (2 x 128 columns), so
+// the epilogue of one tile overlaps the main loop of the next.
+constexpr int kWsStages = 3;
+constexpr int kWsTileB = 128 * 128;                 // B tile: up to 128 rows
+constexpr int kWsStageBytes = 2 * kTileA + 2 * kWsTileB;
+constexpr int kWsSmemBytes = kWsStages * kWsStageBytes + 1024;
+constexpr uint32_t kWsTmemCols = 256;               // two 128-column accumulators
+
+__device__ __forceinline__ void ws_epilogue(const TcArgs& args, const TcItem& item,
+                                            const Prob& pr, uint32_t tacc, int quarter,
+                                            int lane) {
+    using namespace umma;
+    const int row = item.m0 + quarter * 32 + lane;
+    const bool in_mat = row < pr.n_pad;
+    const bool vrow = row < pr.n;
+    const int np = pr.n_pad;
+    double r2 = 0.0;
+    for (int c = 0; c < item.nt; c += 16) {
+        float v[16];
+        tmem_ld16(tacc + (uint32_t(quarter * 32) << 16) + uint32_t(c), v);
+        const int col0 = item.n0 + c;
+        if (!in_mat || col0 >= np) continue;
+        const int64_t base = pr.off + int64_t(row) * np + col0;
+        float hi[16], lo[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const int col = col0 + j;
+            const bool valid = vrow && col < pr.n;
+            float x = v[j];
+            if (args.mode == EPI_POLY) {
+                const float xe = args.xe_hi[base + j] + args.xe_lo[base + j];
+                x = fmaf(0.375f, x, fmaf(-1.25f, xe, row == col ? 1.875f : 0.0f));
+            }
+            if (!valid) x = 0.0f;
+            if (args.mode == EPI_RESID && valid) {
+                const double d = double(x) - (row == col ? 1.0 : 0.0);
+                r2 += d * d;
+            }
+            hi[j] = to_tf32(x);
+            lo[j] = x - hi[j];
+        }
+        float4* ch = reinterpret_cast<float4*>(args.c_hi + base);
+        float4* cl = reinterpret_cast<float4*>(args.c_lo + base);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            ch[q] = make_float4(hi[4 * q], hi[4 * q + 1], hi[4 * q + 2], hi[4 * q + 3]);
+            cl[q] = make_float4(lo[4 * q], lo[4 * q + 1], lo[4 * q + 2], lo[4 * q + 3]);
+        }
+        if (args.c64) {
+            double2* cd = reinterpret_cast<double2*>(args.c64 + base);
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+                cd[q] = make_double2(double(hi[2 * q]) + double(lo[2 * q]),
+                                     double(hi[2 * q + 1]) + double(lo[2 * q + 1]));
+        }
+    }
+    if (args.mode == EPI_RESID) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) r2 += __shfl_xor_sync(0xffffffffu, r2, o);
+        if (lane == 0 && r2 != 0.0) atomicAdd(args.res2 + item.p, r2);
+    }
+}
+
+__global__ void __launch_bounds__(192, 1)
+    tc_gemm_ws_kernel(const __grid_constant__ TcMaps maps, const TcArgs args) {
+    using namespace umma;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    __shared__ __align__(8) uint64_t full[kWsStages];
+    __shared__ __align__(8) uint64_t empty[kWsStages];
+    __shared__ __align__(8) uint64_t acc_full[2];
+    __shared__ __align__(8) uint64_t acc_empty[2];
+    __shared__ uint32_t tmem_base;
+    __shared__ volatile int abort_flag;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp == 1) {
+        tmem_alloc(&tmem_base, kWsTmemCols);
+        tmem_relinquish();
+    }
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kWsStages; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&acc_full[b], 1);
+            mbar_init(&acc_empty[b], 4);  // one arrival per epilogue warp
+        }
+        fence_mbarrier_init();
+        abort_flag = 0;
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_base;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---- TMA producer
+            uint32_t g = 0;
+            for (int it = blockIdx.x; it < args.n_items && !abort_flag; it += gridDim.x) {
+                const TcItem item = args.items[it];
+                if (!args.state[item.p].active) continue;
+                const int nk = args.probs[item.p].n_pad / 32;
+                const uint32_t tx = uint32_t(kTileA + item.nt * 128) * (args.split ? 2u : 1u);
+                for (int kc = 0; kc < nk; ++kc, ++g) {
+                    const int s = int(g % kWsStages);
+                    const uint32_t ph = (g / kWsStages) & 1u;
+                    if (!mbar_wait(&empty[s], ph ^ 1u, kWaitLimitNs)) {
+                        record_error(args.error, 1u);
+                        abort_flag = 1;
+                        break;
+                    }
+                    uint8_t* st = smem + s * kWsStageBytes;
+                    mbar_arrive_expect_tx(&full[s], tx);
+                    tma_load_3d(st, &maps.a_hi[item.bucket], &full[s], kc * 32, item.m0, item.z);
+                    tma_load_3d(st + 2 * kTileA, &maps.b_hi[item.bucket], &full[s], kc * 32,
+                                item.n0, item.z);
+                    if (args.split) {
+                        tma_load_3d(st + kTileA, &maps.a_lo[item.bucket], &full[s], kc * 32,
+                                    item.m0, item.z);
+                        tma_load_3d(st + 2 * kTileA + kWsTileB, &maps.b_lo[item.bucket], &full[s],
+                                    kc * 32, item.n0, item.z);
+                    }
+                }
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // ---- MMA issuer
+            uint32_t g = 0, t = 0;
+            for (int it = blockIdx.x; it < args.n_items && !abort_flag; it += gridDim.x) {
+                const TcItem item = args.items[it];
+                if (!args.state[item.p].active) continue;
+                const int nk = args.probs[item.p].n_pad / 32;
+                const uint32_t b = t & 1u, tph = (t >> 1) & 1u;
+                ++t;
+                if (!mbar_wait(&acc_empty[b], tph ^ 1u, kWaitLimitNs)) {
+                    record_error(args.error, 8u);
+                    abort_flag = 1;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t dacc = tmem + b * 128u;
+                const uint32_t idesc = idesc_tf32(128, item.nt);
+                bool ok = true;
+                for (int kc = 0; kc < nk; ++kc, ++g) {
+                    const int s = int(g % kWsStages);
+                    const uint32_t ph = (g / kWsStages) & 1u;
+                    if (!mbar_wait(&full[s], ph, kWaitLimitNs)) {
+                        record_error(args.error, 2u);
+                        abort_flag = 1;
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t a_hi = smem_u32(smem + s * kWsStageBytes);
+                    const uint32_t a_lo = a_hi + kTileA;
+                    const uint32_t b_hi = a_hi + 2 * kTileA;
+                    const uint32_t b_lo = b_hi + kWsTileB;
+#pragma unroll
+                    for (int kk = 0; kk < 4; ++kk) {
+                        const uint32_t ko = kk * 32;
+                        const uint64_t dah = desc_kmajor_sw128(a_hi + ko);
+                        const uint64_t dbh = desc_kmajor_sw128(b_hi + ko);
+                        mma_tf32(dacc, dah, dbh, idesc, (kc | kk) ? 1u : 0u);
+                        if (args.split) {
+                            mma_tf32(dacc, dah, desc_kmajor_sw128(b_lo + ko), idesc, 1u);
+                            mma_tf32(dacc, desc_kmajor_sw128(a_lo + ko), dbh, idesc, 1u);
+                        }
+                    }
+                    mma_commit(&empty[s]);
+                }
+                if (!ok) break;
+                mma_commit(&acc_full[b]);
+            }
+        }
+    } else {
+        // ---- epilogue warps 2..5: TMEM lane quarter = warp % 4
+        const int quarter = warp & 3;
+        uint32_t t = 0;
+        for (int it = blockIdx.x; it < args.n_items && !abort_flag; it += gridDim.x) {
+            const TcItem item = args.items[it];
+            if (!args.state[item.p].active) continue;
+            const Prob pr = args.probs[item.p];
+            const uint32_t b = t & 1u, tph = (t >> 1) & 1u;
+            ++t;
+            if (!mbar_wait(&acc_full[b], tph, kWaitLimitNs)) {
+                if (lane == 0) record_error(args.error, 4u);
+                abort_flag = 1;
+                break;
+            }
+            tc_fence_after();
+            ws_epilogue(args, item, pr, tmem + b * 128u, quarter, lane);
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acc_empty[b]);
+        }
+    }
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(tmem, kWsTmemCols);
+    }
+}
+
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     static std::once_flag once;
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -241,18 +454,31 @@ int encode_bucket_map(CUtensorMap* map, const float* base, int n_pad, int count,
     return RSATB_SUCCESS;
 }
 
+bool use_ws() {
+    const char* s = std::getenv("RSATB_NS_TC");
+    return !(s && s[0] == 's');  // "simple": the single-role kernel
+}
+
 int prepare_tc_gemm() {
     if (!encode_fn()) return set_error(RSATB_CUDA_ERROR, "cuTensorMapEncodeTiled is not available");
     RSATB_CUDA_TRY(cudaFuncSetAttribute(tc_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         kSmemBytes));
+    RSATB_CUDA_TRY(cudaFuncSetAttribute(tc_gemm_ws_kernel,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        kWsSmemBytes));
     return RSATB_SUCCESS;
 }
+
+int tc_max_nt() { return use_ws() ? 128 : 256; }
 
 int launch_tc_gemm(rsatb_context* ctx, const TcMaps& maps, const TcArgs& args) {
     if (args.n_items <= 0) return RSATB_SUCCESS;
     int grid = ctx->sm_count;
     if (args.n_items < grid) grid = args.n_items;
-    tc_gemm_kernel<<<grid, 128, kSmemBytes, ctx->stream>>>(maps, args);
+    if (use_ws())
+        tc_gemm_ws_kernel<<<grid, 192, kWsSmemBytes, ctx->stream>>>(maps, args);
+    else
+        tc_gemm_kernel<<<grid, 128, kSmemBytes, ctx->stream>>>(maps, args);
     RSATB_LAUNCH_CHECK(ctx);
     return RSATB_SUCCESS;
 }
