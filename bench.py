@@ -282,8 +282,14 @@ def roofline(wl, hbm_peak, peak_note, fma_peaks):
     flops = spmm_flops(Z32, wl.R, wl.complex_vectors)
     gbs = nbytes / (ms * 1e-3) / 1e9
     tfs = flops / (ms * 1e-3) / 1e12
+    # DRAM bytes of one launch of this kernel at this shape (diamond 16^3,
+    # 8x8 blocks, R = 128, FP32) from an ncu capture
+    # (profiles/cheb_step_f32_traffic_diamond_L16.md): read + write.
+    traffic = None
+    if wl.n_rows == 262144 and wl.R == 128 and wl.H.block_size == 8 and not wl.complex_vectors:
+        traffic = 394441472 + 115587840
     out = {"bound": "hbm", "achieved": round(gbs, 1), "peak": hbm_peak, "unit": "GB/s",
-           "frac": round(gbs / hbm_peak, 4), "traffic": None,
+           "frac": round(gbs / hbm_peak, 4), "traffic": traffic,
            "kernel": "fused BSR Chebyshev step, Y = A X, FP32, R=%d, %dx%d blocks" % (
                wl.R, wl.H.block_size, wl.H.block_size),
            "algorithmic_bytes_per_launch": nbytes, "ms_per_launch": round(ms, 4),
@@ -508,7 +514,9 @@ def bench_isqrt(args, dist):
             "roofline": {"bound": "tensor", "achieved": round(low_tfs, 1),
                          "peak": round(tf32_peak, 1), "unit": "TFLOP/s",
                          "frac": round(low_tfs / tf32_peak, 4), "traffic": None,
-                         "kernel": "ns tc_gemm_kernel (tcgen05 kind::tf32, executed tile FLOPs)",
+                         "kernel": "tc_gemm_ws_kernel (tcgen05 kind::tf32, executed tile "
+                                   "FLOPs over the whole tensor-core phase, FP64 updates "
+                                   "included in its time)",
                          "peak_source": "MEASURED_PEAKS.json bf16_tflops / 2 (dense TF32 rate)",
                          "fp64_phase": {"achieved": round(f64_tfs, 2),
                                         "peak": round(fma["f64"] / 1e12, 2),

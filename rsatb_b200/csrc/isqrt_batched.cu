@@ -594,6 +594,9 @@ int run_chunk(rsatb_context* ctx, const Opts& o, const Chunk& ch, const int* col
     } guard{ev};
     RSATB_CUDA_TRY(cudaEventRecord(ev[0], s));
 
+    // P is consumed in FP64 only: the tensor-core kernel that can skip its
+    // TF32 hi/lo copy does so.
+    const bool use_ws_tc = tc_max_nt() == 128;
     if (low) {
         RSATB_TRY(prepare_tc_gemm());
         RSATB_TRY(run_phase(ctx, o.graph, [&]() -> int {
@@ -619,8 +622,8 @@ int run_chunk(rsatb_context* ctx, const Opts& o, const Chunk& ch, const int* col
                 // later steps undo, while rounding in the product itself would
                 // add a rotation Q that no step removes.
                 RSATB_TRY(tc_gemm(ctx, ch, d, group_begin, a.x_hi, a.x_lo, a.x_hi, a.x_lo,
-                                  a.p_hi, a.p_lo, a.p64, EPI_POLY, a.x_hi, a.x_lo, split,
-                                  stats));
+                                  use_ws_tc ? nullptr : a.p_hi, use_ws_tc ? nullptr : a.p_lo,
+                                  a.p64, EPI_POLY, a.x_hi, a.x_lo, split, stats));
                 const int st_z = f64_gemm<false, true>(ctx, d, a.p64, a.z64[c], a.z64[c ^ 1],
                                                        EPI_STORE, nullptr, stats, a.z_hi, a.z_lo);
                 RSATB_TRY(st_z);

@@ -210,7 +210,8 @@ __global__ void __launch_bounds__(128, 1)
 
 // ---------------------------------------------------------------------------
 // Warp-specialised variant: warp 0 is the TMA producer, warp 1 the MMA
-// issuer (and TMEM owner), warps 2-5 the epilogue.  A 3-stage ring of
+// issuer (and TMEM owner), warps 2-9 the epilogue (two per TMEM lane
+// quarter).  A 3-stage ring of
 // 64 KB stages (A hi/lo and B hi/lo, K chunk 32, N tile <= 128) feeds the
 // MMAs; the accumulator is double-buffered in TMEM (2 x 128 columns), so
 // the epilogue of one tile overlaps the main loop of the next.
@@ -222,14 +223,15 @@ constexpr uint32_t kWsTmemCols = 256;               // two 128-column accumulato
 
 __device__ __forceinline__ void ws_epilogue(const TcArgs& args, const TcItem& item,
                                             const Prob& pr, uint32_t tacc, int quarter,
-                                            int lane) {
+                                            int half, int lane) {
     using namespace umma;
     const int row = item.m0 + quarter * 32 + lane;
     const bool in_mat = row < pr.n_pad;
     const bool vrow = row < pr.n;
     const int np = pr.n_pad;
     double r2 = 0.0;
-    for (int c = 0; c < item.nt; c += 16) {
+    // two warps share a TMEM lane quarter: they take alternate 16-column chunks
+    for (int c = 16 * half; c < item.nt; c += 32) {
         float v[16];
         tmem_ld16(tacc + (uint32_t(quarter * 32) << 16) + uint32_t(c), v);
         const int col0 = item.n0 + c;
@@ -253,12 +255,14 @@ __device__ __forceinline__ void ws_epilogue(const TcArgs& args, const TcItem& it
             hi[j] = to_tf32(x);
             lo[j] = x - hi[j];
         }
-        float4* ch = reinterpret_cast<float4*>(args.c_hi + base);
-        float4* cl = reinterpret_cast<float4*>(args.c_lo + base);
+        if (args.c_hi) {
+            float4* ch = reinterpret_cast<float4*>(args.c_hi + base);
+            float4* cl = reinterpret_cast<float4*>(args.c_lo + base);
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            ch[q] = make_float4(hi[4 * q], hi[4 * q + 1], hi[4 * q + 2], hi[4 * q + 3]);
-            cl[q] = make_float4(lo[4 * q], lo[4 * q + 1], lo[4 * q + 2], lo[4 * q + 3]);
+            for (int q = 0; q < 4; ++q) {
+                ch[q] = make_float4(hi[4 * q], hi[4 * q + 1], hi[4 * q + 2], hi[4 * q + 3]);
+                cl[q] = make_float4(lo[4 * q], lo[4 * q + 1], lo[4 * q + 2], lo[4 * q + 3]);
+            }
         }
         if (args.c64) {
             double2* cd = reinterpret_cast<double2*>(args.c64 + base);
@@ -275,7 +279,7 @@ __device__ __forceinline__ void ws_epilogue(const TcArgs& args, const TcItem& it
     }
 }
 
-__global__ void __launch_bounds__(192, 1)
+__global__ void __launch_bounds__(320, 1)
     tc_gemm_ws_kernel(const __grid_constant__ TcMaps maps, const TcArgs args) {
     using namespace umma;
     extern __shared__ uint8_t smem_raw[];
@@ -300,7 +304,7 @@ __global__ void __launch_bounds__(192, 1)
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(&acc_full[b], 1);
-            mbar_init(&acc_empty[b], 4);  // one arrival per epilogue warp
+            mbar_init(&acc_empty[b], 8);  // one arrival per epilogue warp
         }
         fence_mbarrier_init();
         abort_flag = 0;
@@ -392,8 +396,10 @@ __global__ void __launch_bounds__(192, 1)
             }
         }
     } else {
-        // ---- epilogue warps 2..5: TMEM lane quarter = warp % 4
+        // ---- epilogue warps 2..9: TMEM lane quarter = warp % 4, two warps
+        // per quarter (alternate column chunks)
         const int quarter = warp & 3;
+        const int half = (warp - 2) >> 2;
         uint32_t t = 0;
         for (int it = blockIdx.x; it < args.n_items && !abort_flag; it += gridDim.x) {
             const TcItem item = args.items[it];
@@ -407,7 +413,7 @@ __global__ void __launch_bounds__(192, 1)
                 break;
             }
             tc_fence_after();
-            ws_epilogue(args, item, pr, tmem + b * 128u, quarter, lane);
+            ws_epilogue(args, item, pr, tmem + b * 128u, quarter, half, lane);
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(&acc_empty[b]);
@@ -476,7 +482,7 @@ int launch_tc_gemm(rsatb_context* ctx, const TcMaps& maps, const TcArgs& args) {
     int grid = ctx->sm_count;
     if (args.n_items < grid) grid = args.n_items;
     if (use_ws())
-        tc_gemm_ws_kernel<<<grid, 192, kWsSmemBytes, ctx->stream>>>(maps, args);
+        tc_gemm_ws_kernel<<<grid, 320, kWsSmemBytes, ctx->stream>>>(maps, args);
     else
         tc_gemm_kernel<<<grid, 128, kSmemBytes, ctx->stream>>>(maps, args);
     RSATB_LAUNCH_CHECK(ctx);
