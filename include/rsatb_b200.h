@@ -363,9 +363,10 @@ RSATB_API int rsatb_isqrt_columns_batched(rsatb_ctx_t ctx, int n_problems, const
 
 /* ------------------------------------------------------------ measurement */
 
-/* FMA-pipe throughput of this device in FLOP/s (FP64 if double_precision,
- * else FP32), from independent FMA chains on every SM timed with CUDA
- * events: the compute roofline of the block SpMM at wide panels. */
+/* FMA-pipe throughput of this device in FLOP/s, from independent FMA chains
+ * on every SM timed with CUDA events: the compute roofline of the block SpMM
+ * at wide panels.  double_precision: 1 FP64, 0 FP32 (scalar FMAs), 2 FP32
+ * issued as packed pairs (fma.rn.f32x2). */
 RSATB_API int rsatb_measure_fma_peak(rsatb_ctx_t ctx, int double_precision, double* flops);
 
 #ifdef __cplusplus

@@ -50,6 +50,7 @@ struct StepArgs {
     double* partials;  // [gridDim.x][ndots][W]
     double* dots_out;  // [ndots][W]
     unsigned* counter;
+    unsigned* fault;   // set non-zero by a kernel whose bounded wait gave up (null: none)
 };
 
 template <typename VT, int V>
@@ -101,6 +102,31 @@ __device__ __forceinline__ void store_vals(VT* __restrict__ p, const VT (&o)[V])
     } else {
 #pragma unroll
         for (int i = 0; i < V; ++i) p[i] = o[i];
+    }
+}
+
+// (d0, d1) += a * (b0, b1): one packed FP32 FMA (fma.rn.f32x2, sm_100),
+// each lane an IEEE fused multiply-add, so the results equal two fmaf.
+__device__ __forceinline__ void fma2(float& d0, float& d1, float a, float b0, float b1) {
+    asm("{\n\t.reg .b64 ra, rb, rd;\n\t"
+        "mov.b64 ra, {%2, %2};\n\t"
+        "mov.b64 rb, {%3, %4};\n\t"
+        "mov.b64 rd, {%0, %1};\n\t"
+        "fma.rn.f32x2 rd, ra, rb, rd;\n\t"
+        "mov.b64 {%0, %1}, rd;\n\t}"
+        : "+f"(d0), "+f"(d1)
+        : "f"(a), "f"(b0), "f"(b1));
+}
+
+// acc[v] += a * x[v] for v < V; FP32 with V even as packed pairs.
+template <typename VT, int V>
+__device__ __forceinline__ void fma_row(VT (&acc)[V], VT a, const VT (&x)[V]) {
+    if constexpr (sizeof(VT) == 4 && V % 2 == 0) {
+#pragma unroll
+        for (int v = 0; v < V; v += 2) fma2(acc[v], acc[v + 1], a, x[v], x[v + 1]);
+    } else {
+#pragma unroll
+        for (int v = 0; v < V; ++v) acc[v] = fma(a, x[v], acc[v]);
     }
 }
 
@@ -333,9 +359,7 @@ __global__ void __launch_bounds__(256) cheb_step_kernel(StepArgs a) {
                             acc[r][v + 1] = fma(ai, xb[c][v], acc[r][v + 1]);
                         }
                     } else {
-                        const VT av = VT(arow[c]);
-#pragma unroll
-                        for (int v = 0; v < V; ++v) acc[r][v] = fma(av, xb[c][v], acc[r][v]);
+                        fma_row<VT, V>(acc[r], VT(arow[c]), xb[c]);
                     }
                 }
             }

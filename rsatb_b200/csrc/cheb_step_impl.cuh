@@ -5,6 +5,7 @@
 #include "cheb_kernels.cuh"
 #include "cheb_staged.cuh"
 #include "cheb_rowsplit.cuh"
+#include "cheb_bulk.cuh"
 
 #include <cstdlib>
 #include <mutex>
@@ -85,7 +86,7 @@ inline int pick_v(int W, bool cv, bool any_b, int block_size, bool dbl) {
 
 constexpr int kNotApplicable = 1000;
 
-// RSATB_STEP_KERNEL=v1|staged|rowsplit forces one kernel family (tuning and
+// RSATB_STEP_KERNEL=v1|staged|rowsplit|bulk forces one kernel family (tuning and
 // A/B tests); unset picks by shape and precision.
 inline int env_kernel() {
     const char* s = std::getenv("RSATB_STEP_KERNEL");
@@ -93,6 +94,7 @@ inline int env_kernel() {
     if (s[0] == 'v' && s[1] == '1') return 1;
     if (s[0] == 's') return 2;
     if (s[0] == 'r') return 3;
+    if (s[0] == 'b') return 4;
     return 0;
 }
 inline bool env_force_v1() { return env_kernel() == 1; }
@@ -222,6 +224,82 @@ inline int pick_v_staged(int W, bool cv, int block_size, bool dbl) {
     return 0;
 }
 
+// Ring depth of the bulk-copy kernel (RSATB_BULK_NS overrides: 2, 3 or 4)
+// and where its X rows come from (RSATB_BULK_X=smem: through the ring too;
+// default: L1-cached global loads).
+inline int bulk_stages() {
+    const char* s = std::getenv("RSATB_BULK_NS");
+    const int n = s ? std::atoi(s) : 0;
+    return (n >= 2 && n <= 4) ? n : 2;
+}
+inline bool bulk_x_global() {
+    const char* s = std::getenv("RSATB_BULK_X");
+    return !(s && s[0] == 's');
+}
+
+template <int W, bool CV, int NS, bool XG>
+int launch_bulk_k(rsatb_context* ctx, StepArgs& a) {
+    using Sh = BulkShape<W, XG>;
+    auto kernel = cheb_step_bulk<W, CV, NS, XG>;
+    const int threads = kBulkWarps * 32;
+    const size_t smem = bulk_smem_bytes<W, XG, NS>();
+    if (smem > 227 * 1024) return kNotApplicable;
+    // Raise the dynamic shared-memory limit of this instantiation once.
+    static bool attr_set = false;
+    if (!attr_set) {
+        if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(smem)) != cudaSuccess) {
+            cudaGetLastError();
+            return kNotApplicable;
+        }
+        attr_set = true;
+    }
+    const int64_t groups = (a.n_block_rows + Sh::S - 1) / Sh::S;
+    const int64_t need = (groups + kBulkWarps - 1) / kBulkWarps;
+    const int per_sm = occupancy(reinterpret_cast<const void*>(kernel), threads, smem);
+    int64_t grid = int64_t(ctx->sm_count) * per_sm;
+    if (grid > int64_t(ctx->sm_count) * 8) grid = int64_t(ctx->sm_count) * 8;
+    if (need < grid) grid = need;
+    if (grid < 1) grid = 1;
+    kernel<<<unsigned(grid), threads, smem, ctx->stream>>>(a);
+    RSATB_LAUNCH_CHECK(ctx);
+    return RSATB_SUCCESS;
+}
+
+template <int W, bool CV, bool XG>
+int launch_bulk_x(rsatb_context* ctx, StepArgs& a) {
+    switch (bulk_stages()) {
+        case 2: return launch_bulk_k<W, CV, 2, XG>(ctx, a);
+        case 3: return launch_bulk_k<W, CV, 3, XG>(ctx, a);
+        default: return launch_bulk_k<W, CV, 4, XG>(ctx, a);
+    }
+}
+
+template <int W, bool CV>
+int launch_bulk_w(rsatb_context* ctx, StepArgs& a) {
+    return bulk_x_global() ? launch_bulk_x<W, CV, true>(ctx, a)
+                           : launch_bulk_x<W, CV, false>(ctx, a);
+}
+
+// FP32 panels, real 8x8 blocks, W in {8, 16, 32, 64, 128, 256}, 16-byte
+// aligned values and operand; kNotApplicable otherwise.
+template <bool CV>
+int launch_bulk(rsatb_context* ctx, StepArgs& a) {
+    if ((reinterpret_cast<uintptr_t>(a.vals) | reinterpret_cast<uintptr_t>(a.in)) & 15u)
+        return kNotApplicable;
+    switch (a.W) {
+        case 8:
+            if constexpr (!CV) return launch_bulk_w<8, CV>(ctx, a);
+            break;
+        case 16: return launch_bulk_w<16, CV>(ctx, a);
+        case 32: return launch_bulk_w<32, CV>(ctx, a);
+        case 64: return launch_bulk_w<64, CV>(ctx, a);
+        case 128: return launch_bulk_w<128, CV>(ctx, a);
+        case 256: return launch_bulk_w<256, CV>(ctx, a);
+    }
+    return kNotApplicable;
+}
+
 template <typename VT, typename MT, int B, bool CM, bool CV>
 int launch_b(rsatb_context* ctx, int V, int64_t rows, StepArgs& a);
 
@@ -254,10 +332,21 @@ int launch_typed(rsatb_context* ctx, int block_size, StepArgs& a) {
         const int st = launch_rowsplit<VT, CM, CV>(ctx, block_size, a);
         if (st != kNotApplicable) return st;
     }
+    if constexpr (sizeof(VT) == 4 && !CM) {
+        // Bulk-copy kernel: FP32, blocks of 8, panels of 32 to 256 values
+        // by default (every width when forced).
+        const bool wide = a.W >= 32;
+        if (block_size == 8 && (forced == 4 || (forced == 0 && wide))) {
+            const int st = launch_bulk<CV>(ctx, a);
+            if (st != kNotApplicable) return st;
+        }
+    }
     // Measured choice (diamond 8x8 blocks, B200): FP64 takes the staged
-    // kernel at every width; FP32 takes it at W = 16 and the register kernel
-    // otherwise.
-    const bool want_staged = forced == 2 || (forced == 0 && (sizeof(VT) == 8 || a.W == 16));
+    // kernel at every width; FP32 takes the bulk-copy kernel from W = 32 up
+    // (above), the staged kernel for complex panels of W = 16 and the
+    // register kernel otherwise.
+    const bool want_staged =
+        forced == 2 || (forced == 0 && (sizeof(VT) == 8 || (a.W == 16 && CV)));
     if (special && want_staged) {
         const int Vs = pick_v_staged(a.W, CV, block_size, sizeof(VT) == 8);
         int st = kNotApplicable;

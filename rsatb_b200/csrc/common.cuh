@@ -110,6 +110,12 @@ inline size_t dtype_real_size(int t) { return dtype_is_double(t) ? 8 : 4; }
 int ctx_scratch(rsatb_context* ctx, size_t bytes, void** out);
 // Pointer to `n` zeroed completion counters.
 int ctx_counters(rsatb_context* ctx, int n, unsigned** out);
+// The context's device fault word (the last of its 64 counters): kernels
+// whose bounded waits give up set it non-zero.
+int ctx_fault_word(rsatb_context* ctx, unsigned** out);
+// After the stream has been synchronised: reads and clears the fault word;
+// RSATB_CUDA_ERROR when a kernel recorded a fault.
+int ctx_check_fault(rsatb_context* ctx);
 
 int check_ctx(rsatb_context* ctx);
 int check_bsr(const rsatb_bsr_matrix* A, const char* name);

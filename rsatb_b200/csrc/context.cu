@@ -65,13 +65,32 @@ int ctx_counters(rsatb_context* ctx, int n, unsigned** out) {
             RSATB_CUDA_TRY(cudaFree(ctx->counters));
             ctx->counters = nullptr;
         }
-        int m = n < 64 ? 64 : n;
+        int m = n < 64 ? 64 : n + 1;
         RSATB_CUDA_TRY(cudaMalloc(&ctx->counters, sizeof(unsigned) * m));
         RSATB_CUDA_TRY(cudaMemsetAsync(ctx->counters, 0, sizeof(unsigned) * m, ctx->stream));
         ctx->n_counters = m;
     }
     *out = ctx->counters;
     return RSATB_SUCCESS;
+}
+
+int ctx_fault_word(rsatb_context* ctx, unsigned** out) {
+    unsigned* c = nullptr;
+    RSATB_TRY(ctx_counters(ctx, 1, &c));
+    *out = c + (ctx->n_counters - 1);
+    return RSATB_SUCCESS;
+}
+
+int ctx_check_fault(rsatb_context* ctx) {
+    if (!ctx->counters) return RSATB_SUCCESS;
+    unsigned* w = ctx->counters + (ctx->n_counters - 1);
+    unsigned h = 0;
+    RSATB_CUDA_TRY(cudaMemcpyAsync(&h, w, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+    RSATB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    if (h == 0) return RSATB_SUCCESS;
+    RSATB_CUDA_TRY(cudaMemsetAsync(w, 0, sizeof(unsigned), ctx->stream));
+    return set_error(RSATB_CUDA_ERROR,
+                     "a step kernel gave up waiting for its bulk copies (bounded wait)");
 }
 
 }  // namespace rsatb_b200

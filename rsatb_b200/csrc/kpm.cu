@@ -12,8 +12,10 @@
 namespace rsatb_b200 {
 
 int run_step(rsatb_context* ctx, const rsatb_bsr_matrix* A, int vdt, const StepArgs& a) {
-    return dtype_is_double(vdt) ? launch_cheb_step_f64(ctx, A, vdt, a)
-                                : launch_cheb_step_f32(ctx, A, vdt, a);
+    StepArgs b = a;
+    if (!b.fault) RSATB_TRY(ctx_fault_word(ctx, &b.fault));
+    return dtype_is_double(vdt) ? launch_cheb_step_f64(ctx, A, vdt, b)
+                                : launch_cheb_step_f32(ctx, A, vdt, b);
 }
 
 int run_coldot(rsatb_context* ctx, int vdt, int64_t n_rows, const StepArgs& a) {
@@ -381,6 +383,7 @@ int rsatb_kpm_dos_moments(rsatb_ctx_t ctx, const rsatb_cheb_op* op, const void* 
     RSATB_CUDA_TRY(cudaMemcpyAsync(h.data(), dots, sizeof(double) * h.size(),
                                    cudaMemcpyDeviceToHost, ctx->stream));
     RSATB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    RSATB_TRY(ctx_check_fault(ctx));
 
     using cd = std::complex<double>;
     // Per-column dot of slot s, dot d, column q.

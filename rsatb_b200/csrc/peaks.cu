@@ -1,7 +1,8 @@
-// Measured FMA-pipe peak (FP64 or FP32), the denominator of the compute
-// roofline of the SpMM at wide panels, where the block SpMM is bound by the
-// CUDA-core FMA rate rather than by HBM.  Every SM runs independent FMA
-// chains; the result is FLOP/s = 2 * FMAs / elapsed time (CUDA events).
+// Measured FMA-pipe peak (FP64, FP32, or FP32 issued as packed f32x2 FMAs),
+// the denominator of the compute roofline of the SpMM at wide panels, where
+// the block SpMM is bound by the CUDA-core FMA rate rather than by HBM.
+// Every SM runs independent FMA chains; the result is FLOP/s = 2 * FMAs /
+// elapsed time (CUDA events).
 #include "common.cuh"
 
 namespace rsatb_b200 {
@@ -22,6 +23,35 @@ __global__ void __launch_bounds__(256) fma_chains(T* out, int iters, T a, T b) {
     if (s == T(-12345.678)) out[threadIdx.x] = s;  // keeps the chains live
 }
 
+// Eight chains of packed pairs: fma.rn.f32x2 (sm_100) does two FP32 FMAs.
+__global__ void __launch_bounds__(256) fma2_chains(float* out, int iters, float a, float b) {
+    unsigned long long x[8];
+    const float base = float(threadIdx.x) * 1e-3f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const float lo = base + float(2 * k), hi = base + float(2 * k + 1);
+        asm("mov.b64 %0, {%1, %2};" : "=l"(x[k]) : "f"(lo), "f"(hi));
+    }
+    unsigned long long av, bv;
+    asm("mov.b64 %0, {%1, %1};" : "=l"(av) : "f"(a));
+    asm("mov.b64 %0, {%1, %1};" : "=l"(bv) : "f"(b));
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                asm volatile("fma.rn.f32x2 %0, %0, %1, %2;" : "+l"(x[k]) : "l"(av), "l"(bv));
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        float lo, hi;
+        asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(x[k]));
+        s += lo + hi;
+    }
+    if (s == -12345.678f) out[threadIdx.x] = s;  // keeps the chains live
+}
+
 }  // namespace
 }  // namespace rsatb_b200
 
@@ -35,14 +65,16 @@ extern "C" int rsatb_measure_fma_peak(rsatb_ctx_t ctx, int double_precision, dou
     RSATB_TRY(ctx_scratch(ctx, 4096, &sink));
     const int threads = 256;
     const int grid = ctx->sm_count * 8;
-    const int iters = double_precision ? 4096 : 8192;
+    const int iters = double_precision == 1 ? 4096 : 8192;
     cudaEvent_t e0, e1;
     RSATB_CUDA_TRY(cudaEventCreate(&e0));
     RSATB_CUDA_TRY(cudaEventCreate(&e1));
     float best_ms = 1e30f;
     for (int rep = 0; rep < 4; ++rep) {
         RSATB_CUDA_TRY(cudaEventRecord(e0, ctx->stream));
-        if (double_precision)
+        if (double_precision == 2)
+            fma2_chains<<<grid, threads, 0, ctx->stream>>>((float*)sink, iters, 0.9999f, 1e-4f);
+        else if (double_precision)
             fma_chains<double><<<grid, threads, 0, ctx->stream>>>((double*)sink, iters,
                                                                    0.999999, 1e-7);
         else
@@ -57,7 +89,8 @@ extern "C" int rsatb_measure_fma_peak(rsatb_ctx_t ctx, int double_precision, dou
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    const double fmas = double(grid) * threads * double(iters) * 4.0 * 8.0;
+    const double fmas = double(grid) * threads * double(iters) * 4.0 * 8.0 *
+                        (double_precision == 2 ? 2.0 : 1.0);
     *flops = 2.0 * fmas / (double(best_ms) * 1e-3);
     return RSATB_SUCCESS;
 }

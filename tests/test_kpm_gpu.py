@@ -290,16 +290,22 @@ def test_lanczos_bounds_contain_spectrum(torch_cuda):
 
 NARROW = [(96, 8, 6, False, False, 8, False), (96, 8, 6, False, False, 4, True),
           (96, 8, 6, False, False, 16, False), (80, 5, 5, False, False, 4, False),
-          (80, 5, 5, False, False, 8, True), (80, 5, 5, False, False, 4, True)]
+          (80, 5, 5, False, False, 8, True), (80, 5, 5, False, False, 4, True),
+          # bulk-copy kernel widths W = 64 and 256 and ragged group counts
+          # (97 block rows: not a multiple of the 2..32 block rows per warp)
+          (97, 8, 7, False, False, 64, False), (97, 8, 7, False, False, 128, True),
+          (97, 8, 7, False, False, 256, False), (97, 8, 7, False, False, 2, True)]
 
 
-@pytest.mark.parametrize("kernel", ["staged", "rowsplit"])
+@pytest.mark.parametrize("kernel", ["staged", "rowsplit", "bulk", "bulk_smem"])
 @pytest.mark.parametrize("case", [c for c in CASES if c[1] in (1, 5, 8)] + NARROW)
 @pytest.mark.parametrize("precision", ["f64", "f32"])
 def test_kernel_variants_match_register_kernel(torch_cuda, case, precision, kernel, monkeypatch):
-    """The cp.async-staged and the narrow-panel row-split step kernels against
-    the register kernel, including the fused epilogue and dots (the row-split
-    kernel sums in another order, hence a relative tolerance)."""
+    """The cp.async-staged, the narrow-panel row-split and the bulk-copy step
+    kernels against the register kernel, including the fused epilogue and
+    dots (the row-split kernel sums in another order, hence a relative
+    tolerance; the bulk-copy kernel keeps the register kernel's order per
+    output and differs only in the FP64 dot reduction order)."""
     torch = torch_cuda
     from rsatb_b200.calc import Chebyshev, _moments
     n, b, deg, cm, imag, R, cv = case
@@ -312,7 +318,9 @@ def test_kernel_variants_match_register_kernel(torch_cuda, case, precision, kern
     dt = {("f64", True): torch.complex128, ("f64", False): torch.float64,
           ("f32", True): torch.complex64, ("f32", False): torch.float32}[(precision, cv)]
     Xd = to_dev(torch, X, dt)
-    monkeypatch.setenv("RSATB_STEP_KERNEL", kernel)
+    monkeypatch.setenv("RSATB_STEP_KERNEL", kernel.split("_")[0])
+    if kernel == "bulk_smem":
+        monkeypatch.setenv("RSATB_BULK_X", "smem")  # X rows through the copy ring too
     Y1 = torch.empty_like(Xd)
     c.H.mult_dense(Xd, Y1)
     mu1, col1 = _moments(c, Xd, 24, True, per_column=True)
