@@ -56,9 +56,9 @@ constexpr size_t bulk_smem_bytes() {
            size_t(kBulkWarps) * 32 * 16 * sizeof(double);
 }
 
-template <int W, bool CV, int NS, bool XG>
-__global__ void __launch_bounds__(kBulkWarps * 32, (NS == 2 || XG) ? 3 : 2)
-    cheb_step_bulk(StepArgs a) {
+// MINB: resident CTAs per SM the register budget is sized for.
+template <int W, bool CV, int NS, bool XG, int MINB>
+__global__ void __launch_bounds__(kBulkWarps * 32, MINB) cheb_step_bulk(StepArgs a) {
     using Sh = BulkShape<W, XG>;
     constexpr int G = Sh::G, S = Sh::S;
     static_assert(W % 8 == 0 && 32 % (W / 8) == 0, "8 values per lane; G must divide 32");

@@ -224,23 +224,27 @@ inline int pick_v_staged(int W, bool cv, int block_size, bool dbl) {
     return 0;
 }
 
-// Ring depth of the bulk-copy kernel (RSATB_BULK_NS overrides: 2, 3 or 4)
-// and where its X rows come from (RSATB_BULK_X=smem: through the ring too;
-// default: L1-cached global loads).
+// Ring depth of the bulk-copy kernel (RSATB_BULK_NS=3 overrides the 2
+// stages), where its X rows come from (RSATB_BULK_X=smem: through the ring
+// too; default: L1-cached global loads) and its register budget
+// (RSATB_BULK_OCC=4: sized for 4 resident CTAs per SM instead of 3).
 inline int bulk_stages() {
     const char* s = std::getenv("RSATB_BULK_NS");
-    const int n = s ? std::atoi(s) : 0;
-    return (n >= 2 && n <= 4) ? n : 2;
+    return (s && std::atoi(s) == 3) ? 3 : 2;
 }
 inline bool bulk_x_global() {
     const char* s = std::getenv("RSATB_BULK_X");
     return !(s && s[0] == 's');
 }
+inline bool bulk_occ4() {
+    const char* s = std::getenv("RSATB_BULK_OCC");
+    return s && std::atoi(s) == 4;
+}
 
-template <int W, bool CV, int NS, bool XG>
+template <int W, bool CV, int NS, bool XG, int MINB>
 int launch_bulk_k(rsatb_context* ctx, StepArgs& a) {
     using Sh = BulkShape<W, XG>;
-    auto kernel = cheb_step_bulk<W, CV, NS, XG>;
+    auto kernel = cheb_step_bulk<W, CV, NS, XG, MINB>;
     const int threads = kBulkWarps * 32;
     const size_t smem = bulk_smem_bytes<W, XG, NS>();
     if (smem > 227 * 1024) return kNotApplicable;
@@ -266,19 +270,14 @@ int launch_bulk_k(rsatb_context* ctx, StepArgs& a) {
     return RSATB_SUCCESS;
 }
 
-template <int W, bool CV, bool XG>
-int launch_bulk_x(rsatb_context* ctx, StepArgs& a) {
-    switch (bulk_stages()) {
-        case 2: return launch_bulk_k<W, CV, 2, XG>(ctx, a);
-        case 3: return launch_bulk_k<W, CV, 3, XG>(ctx, a);
-        default: return launch_bulk_k<W, CV, 4, XG>(ctx, a);
-    }
-}
-
 template <int W, bool CV>
 int launch_bulk_w(rsatb_context* ctx, StepArgs& a) {
-    return bulk_x_global() ? launch_bulk_x<W, CV, true>(ctx, a)
-                           : launch_bulk_x<W, CV, false>(ctx, a);
+    const bool ns3 = bulk_stages() == 3;
+    if (!bulk_x_global())
+        return ns3 ? launch_bulk_k<W, CV, 3, false, 2>(ctx, a)
+                   : launch_bulk_k<W, CV, 2, false, 3>(ctx, a);
+    if (bulk_occ4()) return launch_bulk_k<W, CV, 2, true, 4>(ctx, a);
+    return ns3 ? launch_bulk_k<W, CV, 3, true, 3>(ctx, a) : launch_bulk_k<W, CV, 2, true, 3>(ctx, a);
 }
 
 // FP32 panels, real 8x8 blocks, W in {8, 16, 32, 64, 128, 256}, 16-byte
