@@ -6,6 +6,7 @@
 #include "cheb_staged.cuh"
 #include "cheb_rowsplit.cuh"
 #include "cheb_bulk.cuh"
+#include "cheb_narrow.cuh"
 
 #include <cstdlib>
 #include <mutex>
@@ -86,7 +87,7 @@ inline int pick_v(int W, bool cv, bool any_b, int block_size, bool dbl) {
 
 constexpr int kNotApplicable = 1000;
 
-// RSATB_STEP_KERNEL=v1|staged|rowsplit|bulk forces one kernel family (tuning and
+// RSATB_STEP_KERNEL=v1|staged|rowsplit|bulk|narrow forces one kernel family (tuning and
 // A/B tests); unset picks by shape and precision.
 inline int env_kernel() {
     const char* s = std::getenv("RSATB_STEP_KERNEL");
@@ -95,6 +96,7 @@ inline int env_kernel() {
     if (s[0] == 's') return 2;
     if (s[0] == 'r') return 3;
     if (s[0] == 'b') return 4;
+    if (s[0] == 'n') return 5;
     return 0;
 }
 inline bool env_force_v1() { return env_kernel() == 1; }
@@ -280,6 +282,65 @@ int launch_bulk_w(rsatb_context* ctx, StepArgs& a) {
     return ns3 ? launch_bulk_k<W, CV, 3, true, 3>(ctx, a) : launch_bulk_k<W, CV, 2, true, 3>(ctx, a);
 }
 
+// Ring depth of the narrow-panel kernel (RSATB_NARROW_NS: 2 or 3).
+inline int narrow_stages() {
+    const char* s = std::getenv("RSATB_NARROW_NS");
+    return (s && std::atoi(s) == 3) ? 3 : 2;
+}
+
+template <typename VT, int W, bool CV, int NS>
+int launch_narrow_k(rsatb_context* ctx, StepArgs& a) {
+    using Sh = NarrowShape<VT, W>;
+    auto kernel = cheb_step_narrow<VT, W, CV, NS>;
+    const int threads = kNarrowWarps * 32;
+    // The ring, or the dots reduction that reuses it, whichever is larger.
+    constexpr size_t ring = narrow_smem_bytes<VT, W, NS>();
+    constexpr size_t red_max = 2 * size_t(kNarrowWarps) * 32 * Sh::V * sizeof(double);
+    constexpr size_t smem = ring > red_max ? ring : red_max;
+    if (smem > 200 * 1024) return kNotApplicable;
+    static bool attr_set = false;
+    if (!attr_set) {
+        if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(smem)) != cudaSuccess) {
+            cudaGetLastError();
+            return kNotApplicable;
+        }
+        attr_set = true;
+    }
+    const int64_t groups = (a.n_block_rows + Sh::S - 1) / Sh::S;
+    const int64_t need = (groups + kNarrowWarps - 1) / kNarrowWarps;
+    const int per_sm = occupancy(reinterpret_cast<const void*>(kernel), threads, smem);
+    int64_t grid = int64_t(ctx->sm_count) * per_sm;
+    if (grid > int64_t(ctx->sm_count) * 8) grid = int64_t(ctx->sm_count) * 8;
+    if (need < grid) grid = need;
+    if (grid < 1) grid = 1;
+    kernel<<<unsigned(grid), threads, smem, ctx->stream>>>(a);
+    RSATB_LAUNCH_CHECK(ctx);
+    return RSATB_SUCCESS;
+}
+
+template <typename VT, int W, bool CV>
+int launch_narrow_w(rsatb_context* ctx, StepArgs& a) {
+    return narrow_stages() == 3 ? launch_narrow_k<VT, W, CV, 3>(ctx, a)
+                                : launch_narrow_k<VT, W, CV, 2>(ctx, a);
+}
+
+// Real 8x8 blocks, W in {4, 8, 16}, 16-byte aligned values and operand;
+// kNotApplicable otherwise.
+template <typename VT, bool CV>
+int launch_narrow(rsatb_context* ctx, StepArgs& a) {
+    if ((reinterpret_cast<uintptr_t>(a.vals) | reinterpret_cast<uintptr_t>(a.in)) & 15u)
+        return kNotApplicable;
+    switch (a.W) {
+        case 4:
+            if constexpr (!CV) return launch_narrow_w<VT, 4, CV>(ctx, a);
+            break;
+        case 8: return launch_narrow_w<VT, 8, CV>(ctx, a);
+        case 16: return launch_narrow_w<VT, 16, CV>(ctx, a);
+    }
+    return kNotApplicable;
+}
+
 // FP32 panels, real 8x8 blocks, W in {8, 16, 32, 64, 128, 256}, 16-byte
 // aligned values and operand; kNotApplicable otherwise.
 template <bool CV>
@@ -330,6 +391,13 @@ int launch_typed(rsatb_context* ctx, int block_size, StepArgs& a) {
     if (forced == 3 && (block_size == 5 || block_size == 8)) {
         const int st = launch_rowsplit<VT, CM, CV>(ctx, block_size, a);
         if (st != kNotApplicable) return st;
+    }
+    if constexpr (!CM) {
+        // Narrow-panel lock-step kernel: blocks of 8, W <= 16 (when forced).
+        if (block_size == 8 && forced == 5) {
+            const int st = launch_narrow<VT, CV>(ctx, a);
+            if (st != kNotApplicable) return st;
+        }
     }
     if constexpr (sizeof(VT) == 4 && !CM) {
         // Bulk-copy kernel: FP32, blocks of 8, panels of 32 to 256 values
