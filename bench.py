@@ -61,6 +61,8 @@ def parse_args():
                    help="moments in the bounded CPU baseline sample")
     p.add_argument("--spmm-only", action="store_true",
                    help="time Y = H X alone on a diamond L^3 H (the ncu profiling case)")
+    p.add_argument("--isqrt-no-autotune", action="store_true",
+                   help="batched S^-1/2: built-in tensor-core tiles instead of autotuned ones")
     p.add_argument("--spmm-L", type=int, default=12)
     p.add_argument("--spmm-reps", type=int, default=3)
     return p.parse_args()
@@ -459,9 +461,20 @@ def bench_isqrt(args, dist):
     out = torch.zeros(int((n.astype(np.int64) * ks).sum()), dtype=torch.float64, device="cuda")
     ws = int(args.isqrt_ws_gb * (1 << 30))
 
+    # Tensor-core tiles from the autotuner (seeded samples of every padded
+    # size in the batch), picked before and outside the timed region.
+    tiles, tune_s = None, 0.0
+    if args.isqrt_precision != "fp64" and not args.isqrt_no_autotune:
+        from rsatb_b200.isqrt import autotune_tiles
+        t1 = time.perf_counter()
+        tiles = autotune_tiles(np.unique(n), precision=args.isqrt_precision,
+                               problems_per_size=16)
+        tune_s = time.perf_counter() - t1
+
     def run(prec):
         return inverse_sqrt_columns_batched(batch.flat, n, batch.offset, cs, ks, out_off,
-                                            precision=prec, out=out, workspace_bytes=ws)
+                                            precision=prec, out=out, workspace_bytes=ws,
+                                            tiles=tiles if prec != "fp64" else None)
 
     def timed(prec, steps, warmup):
         for _ in range(warmup):
@@ -528,6 +541,9 @@ def bench_isqrt(args, dist):
             "fp64_only_ms_per_step": round(ms64, 2) if ms64 else None,
             "speedup_vs_fp64_only": round(ms64 / ms, 3) if ms64 else None,
             "clocks": clocks, "generate_seconds": round(gen_s, 1),
+            "autotuned_tiles": None if tiles is None else {
+                "tc_kernel": "warp-specialised" if tiles.tc_kernel == 1 else "single-role",
+                "n_tile_per_n_pad": tiles.nt, "tune_seconds": round(tune_s, 1)},
         }
         print(json.dumps(line), flush=True)
 

@@ -314,6 +314,13 @@ typedef struct {
                                RSATB_NUMERICAL_FAILURE [1e-6] */
     size_t workspace_bytes; /* device workspace per chunk of problems [8 GiB] */
     int no_graph;           /* 0: each chunk's iterations run as one captured CUDA graph */
+    int tc_kernel;          /* tensor-core GEMM: 0 the built-in choice, 1 warp-specialised
+                               (N tile <= 128), 2 single-role (N tile <= 256) */
+    int n_tiles;            /* entries of the N-tile table (0: the built-in rule, the fewest
+                               tiles of at most the kernel's widest N tile) */
+    const int32_t* tile_n_pad; /* host: padded sizes (multiples of 32) of the table */
+    const int32_t* tile_nt;    /* host: the N tile (multiple of 16) for each padded size;
+                                  sizes absent from the table take the built-in rule */
 } rsatb_isqrt_options;
 
 /* Per-call statistics (host). */
@@ -360,6 +367,22 @@ RSATB_API int rsatb_isqrt_columns_batched(rsatb_ctx_t ctx, int n_problems, const
                                           const int64_t* out_offset, double* out,
                                           const rsatb_isqrt_options* options, int32_t* status,
                                           rsatb_isqrt_stats* stats);
+
+/* Autotuner of the tensor-core tiles of rsatb_isqrt_columns_batched.  For
+ * each size in sizes[n_sizes] it builds problems_per_size well-conditioned
+ * SPD matrices of that size on the device, times (CUDA events, best of two
+ * after a warm-up) a fixed-length solve in `precision` (RSATB_NS_TF32X3 or
+ * RSATB_NS_TF32) for each candidate: both tensor-core kernels, and for each
+ * the N tiles that split the padded size into the fewest tiles of at most
+ * 32, 64, 128 (and 256 for the single-role kernel) columns.  It returns the
+ * kernel with the smallest summed time (*tc_kernel_out, 1 or 2) and, for
+ * that kernel, the fastest N tile per size (nt_out[n_sizes]), which go into
+ * rsatb_isqrt_options.tc_kernel / tile_n_pad / tile_nt.  ms_out (optional,
+ * n_sizes x 8) receives every candidate's time: [size][kernel 0..1][tile
+ * 0..3], -1 where the candidate does not exist. */
+RSATB_API int rsatb_isqrt_autotune(rsatb_ctx_t ctx, int precision, int n_sizes,
+                                   const int32_t* sizes, int problems_per_size,
+                                   int* tc_kernel_out, int32_t* nt_out, double* ms_out);
 
 /* ------------------------------------------------------------ measurement */
 

@@ -47,7 +47,8 @@ class ChebOp(C.Structure):
 class IsqrtOptions(C.Structure):
     _fields_ = [("precision", C.c_int), ("max_iter", C.c_int), ("max_fp64_iter", C.c_int),
                 ("tol", C.c_double), ("accept", C.c_double), ("workspace_bytes", C.c_size_t),
-                ("no_graph", C.c_int)]
+                ("no_graph", C.c_int), ("tc_kernel", C.c_int), ("n_tiles", C.c_int),
+                ("tile_n_pad", C.c_void_p), ("tile_nt", C.c_void_p)]
 
 
 class IsqrtStats(C.Structure):
@@ -113,6 +114,7 @@ SIGNATURES = {
     "rsatb_isqrt_columns_batched": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                          C.POINTER(IsqrtOptions), _vp, C.POINTER(IsqrtStats)]),
     "rsatb_measure_fma_peak": (_i, [_vp, _i, _PD]),
+    "rsatb_isqrt_autotune": (_i, [_vp, _i, _i, _vp, _i, _vp, _vp, _vp]),
 }
 
 

@@ -359,6 +359,8 @@ struct Opts {
     double accept;
     size_t workspace;
     bool graph;
+    bool ws;                                // warp-specialised tensor-core kernel
+    std::vector<std::pair<int, int>> tiles; // (n_pad, N tile) overrides
 };
 
 // Device views of one chunk's tables and arrays.
@@ -392,7 +394,7 @@ T* carve(char*& cur, size_t count) {
 int tc_gemm(rsatb_context* ctx, const Chunk& ch, const Dev& d,
             const std::vector<int>& group_item_begin, const float* a_hi, const float* a_lo,
             const float* b_hi, const float* b_lo, float* c_hi, float* c_lo, double* c64,
-            int mode, const float* xe_hi, const float* xe_lo, bool split,
+            int mode, const float* xe_hi, const float* xe_lo, bool split, bool ws,
             rsatb_isqrt_stats* stats) {
     const int nb = int(ch.buckets.size());
     for (int g0 = 0, gi = 0; g0 < nb; g0 += kMaxBuckets, ++gi) {
@@ -419,7 +421,7 @@ int tc_gemm(rsatb_context* ctx, const Chunk& ch, const Dev& d,
         args.mode = mode;
         args.split = split ? 1 : 0;
         args.error = d.error;
-        RSATB_TRY(launch_tc_gemm(ctx, maps, args));
+        RSATB_TRY(launch_tc_gemm(ctx, maps, args, ws));
         if (stats) stats->gemm_launches++;
     }
     return RSATB_SUCCESS;
@@ -596,7 +598,7 @@ int run_chunk(rsatb_context* ctx, const Opts& o, const Chunk& ch, const int* col
 
     // P is consumed in FP64 only: the tensor-core kernel that can skip its
     // TF32 hi/lo copy does so.
-    const bool use_ws_tc = tc_max_nt() == 128;
+    const bool use_ws_tc = o.ws;
     if (low) {
         RSATB_TRY(prepare_tc_gemm());
         RSATB_TRY(run_phase(ctx, o.graph, [&]() -> int {
@@ -604,10 +606,10 @@ int run_chunk(rsatb_context* ctx, const Opts& o, const Chunk& ch, const int* col
                 const int c = k & 1;
                 // W = Z S^T, X = Z W^T (+ residual) on the tensor cores
                 RSATB_TRY(tc_gemm(ctx, ch, d, group_begin, a.z_hi, a.z_lo, a.s_hi, a.s_lo,
-                                  a.w_hi, a.w_lo, nullptr, EPI_STORE, nullptr, nullptr, split,
+                                  a.w_hi, a.w_lo, nullptr, EPI_STORE, nullptr, nullptr, split, o.ws,
                                   stats));
                 RSATB_TRY(tc_gemm(ctx, ch, d, group_begin, a.z_hi, a.z_lo, a.w_hi, a.w_lo,
-                                  a.x_hi, a.x_lo, nullptr, EPI_RESID, nullptr, nullptr, split,
+                                  a.x_hi, a.x_lo, nullptr, EPI_RESID, nullptr, nullptr, split, o.ws,
                                   stats));
                 control_kernel<<<cb, 256, 0, s>>>(P, d.state, d.res2, o.tol, 1);
                 RSATB_LAUNCH_CHECK(ctx);
@@ -623,7 +625,7 @@ int run_chunk(rsatb_context* ctx, const Opts& o, const Chunk& ch, const int* col
                 // add a rotation Q that no step removes.
                 RSATB_TRY(tc_gemm(ctx, ch, d, group_begin, a.x_hi, a.x_lo, a.x_hi, a.x_lo,
                                   use_ws_tc ? nullptr : a.p_hi, use_ws_tc ? nullptr : a.p_lo,
-                                  a.p64, EPI_POLY, a.x_hi, a.x_lo, split, stats));
+                                  a.p64, EPI_POLY, a.x_hi, a.x_lo, split, o.ws, stats));
                 const int st_z = f64_gemm<false, true>(ctx, d, a.p64, a.z64[c], a.z64[c ^ 1],
                                                        EPI_STORE, nullptr, stats, a.z_hi, a.z_lo);
                 RSATB_TRY(st_z);
@@ -748,6 +750,22 @@ extern "C" int rsatb_isqrt_columns_batched(rsatb_ctx_t ctx, int n_problems, cons
     o.workspace = (options && options->workspace_bytes) ? options->workspace_bytes
                                                         : (size_t(8) << 30);
     o.graph = !(options && options->no_graph);
+    const int tck = options ? options->tc_kernel : 0;
+    if (tck < 0 || tck > 2) return set_error(RSATB_INVALID_ARGUMENT, "unknown tc_kernel %d", tck);
+    o.ws = tck == 0 ? default_tc_ws() : tck == 1;
+    if (options && options->n_tiles > 0) {
+        if (!options->tile_n_pad || !options->tile_nt)
+            return set_error(RSATB_INVALID_ARGUMENT, "n_tiles > 0 with a null tile table");
+        for (int t = 0; t < options->n_tiles; ++t) {
+            const int np = options->tile_n_pad[t], nt = options->tile_nt[t];
+            if (np < 32 || np % 32 || nt < 16 || nt % 16 || nt > tc_max_nt(o.ws))
+                return set_error(RSATB_INVALID_ARGUMENT,
+                                 "tile %d: n_pad %d / N tile %d (N tile a multiple of 16 up to "
+                                 "%d, n_pad a multiple of 32)",
+                                 t, np, nt, tc_max_nt(o.ws));
+            o.tiles.emplace_back(np, nt);
+        }
+    }
     for (int p = 0; p < n_problems; ++p) {
         if (n[p] < 1 || n[p] > 1024)
             return set_error(RSATB_INVALID_ARGUMENT, "problem %d: n = %d outside [1, 1024]", p,
@@ -802,9 +820,11 @@ extern "C" int rsatb_isqrt_columns_batched(rsatb_ctx_t ctx, int n_problems, cons
             if (!ch.ids.empty() && chunk_bytes(elems + e, low) > o.workspace) break;
             const int np = npad(p);
             if (ch.buckets.empty() || ch.buckets.back().n_pad != np) {
-                const int max_nt = low ? tc_max_nt() : 256;
+                const int max_nt = low ? tc_max_nt(o.ws) : 256;
                 const int tiles = (np + max_nt - 1) / max_nt;
-                const int nt = ((np + tiles - 1) / tiles + 15) / 16 * 16;
+                int nt = ((np + tiles - 1) / tiles + 15) / 16 * 16;
+                for (const auto& t : o.tiles)
+                    if (t.first == np) nt = t.second;
                 ch.buckets.push_back(Bucket{np, int(ch.ids.size()), 0, elems, nt});
             }
             ch.buckets.back().count++;
@@ -833,5 +853,162 @@ extern "C" int rsatb_isqrt_columns_batched(rsatb_ctx_t ctx, int n_problems, cons
         }
         if (stats) stats->chunks++;
     }
+    return RSATB_SUCCESS;
+}
+
+// ------------------------------------------------------------- autotuner
+
+namespace rsatb_b200 {
+namespace ns {
+namespace {
+
+// count column-major n x n matrices M_p = I + (0.5 / n) H_p with H_p
+// symmetric, zero diagonal, entries uniform in [-1, 1) from a counter hash
+// (splitmix64 finaliser of (seed, p, min(i, j), max(i, j))): by Gershgorin
+// the spectrum lies in [0.5, 1.5], so every sample is SPD.
+__global__ void spd_sample_kernel(double* M, int n, int count, uint64_t seed) {
+    const int64_t nn = int64_t(n) * n;
+    const int64_t total = nn * count;
+    for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total;
+         e += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t p = e / nn;
+        const int rem = int(e - p * nn);
+        const int i = rem % n, j = rem / n;
+        double v = 1.0;
+        if (i != j) {
+            uint64_t x = seed ^ (uint64_t(p) * 0x9E3779B97F4A7C15ull) ^
+                         (uint64_t(min(i, j)) << 32) ^ uint64_t(max(i, j));
+            x ^= x >> 30;
+            x *= 0xBF58476D1CE4E5B9ull;
+            x ^= x >> 27;
+            x *= 0x94D049BB133111EBull;
+            x ^= x >> 31;
+            const double uni = double(x >> 11) * (1.0 / 9007199254740992.0);
+            v = (0.5 / n) * (2.0 * uni - 1.0);
+        }
+        M[e] = v;
+    }
+}
+
+// N tile of candidate `idx` (caps 32, 64, 128, 256 columns) for a padded
+// size, 0 when the kernel does not take it or an earlier cap gives the same.
+int candidate_nt(int np, bool ws, int idx) {
+    static const int caps[4] = {32, 64, 128, 256};
+    auto rule = [&](int cap) {
+        const int tiles = (np + cap - 1) / cap;
+        return ((np + tiles - 1) / tiles + 15) / 16 * 16;
+    };
+    if (caps[idx] > tc_max_nt(ws)) return 0;
+    const int nt = rule(caps[idx]);
+    for (int k = 0; k < idx; ++k)
+        if (rule(caps[k]) == nt) return 0;
+    return nt;
+}
+
+}  // namespace
+}  // namespace ns
+}  // namespace rsatb_b200
+
+extern "C" int rsatb_isqrt_autotune(rsatb_ctx_t ctx, int precision, int n_sizes,
+                                   const int32_t* sizes, int problems_per_size,
+                                   int* tc_kernel_out, int32_t* nt_out, double* ms_out) {
+    using namespace rsatb_b200::ns;
+    clear_error();
+    RSATB_TRY(check_ctx(ctx));
+    if (precision != RSATB_NS_TF32X3 && precision != RSATB_NS_TF32)
+        return set_error(RSATB_INVALID_ARGUMENT,
+                         "autotuning needs a tensor-core precision (RSATB_NS_TF32X3 or TF32)");
+    if (n_sizes < 1 || !sizes || !tc_kernel_out || !nt_out)
+        return set_error(RSATB_INVALID_ARGUMENT, "need at least one size and the outputs");
+    if (problems_per_size < 1 || problems_per_size > 4096)
+        return set_error(RSATB_INVALID_ARGUMENT, "problems_per_size outside [1, 4096]");
+    for (int s = 0; s < n_sizes; ++s)
+        if (sizes[s] < 1 || sizes[s] > 1024)
+            return set_error(RSATB_INVALID_ARGUMENT, "size %d outside [1, 1024]", sizes[s]);
+
+    std::vector<double> ms(size_t(n_sizes) * 8, -1.0);
+    for (int si = 0; si < n_sizes; ++si) {
+        const int n = sizes[si], np = (n + 31) / 32 * 32, count = problems_per_size;
+        const int k = std::min(n, 16);
+        std::vector<int64_t> in_off(count), out_off(count);
+        std::vector<int32_t> nv(count, n), cs(count, 0), kc(count, k);
+        for (int p = 0; p < count; ++p) {
+            in_off[p] = int64_t(p) * n * n;
+            out_off[p] = int64_t(p) * n * k;
+        }
+        double* M = nullptr;
+        double* out = nullptr;
+        RSATB_CUDA_TRY(cudaMalloc(&M, sizeof(double) * size_t(count) * n * n));
+        cudaError_t ae = cudaMalloc(&out, sizeof(double) * size_t(count) * n * k);
+        if (ae != cudaSuccess) {
+            cudaFree(M);
+            RSATB_CUDA_TRY(ae);
+        }
+        struct Free {
+            double *a, *b;
+            ~Free() {
+                cudaFree(a);
+                cudaFree(b);
+            }
+        } guard{M, out};
+        spd_sample_kernel<<<ctx->sm_count * 4, 256, 0, ctx->stream>>>(M, n, count,
+                                                                     0x5EEDull + uint64_t(si));
+        RSATB_LAUNCH_CHECK(ctx);
+        std::vector<int32_t> status(count);
+        for (int kk = 0; kk < 2; ++kk) {
+            const bool ws = kk == 0;
+            for (int idx = 0; idx < 4; ++idx) {
+                int32_t nt = candidate_nt(np, ws, idx);
+                if (!nt) continue;
+                int32_t npad = np;
+                rsatb_isqrt_options o{};
+                o.precision = precision;
+                o.max_iter = 6;        // a fixed-length solve: every candidate does the same work
+                o.max_fp64_iter = 1;
+                o.tol = 1e-300;
+                o.tc_kernel = ws ? 1 : 2;
+                o.n_tiles = 1;
+                o.tile_n_pad = &npad;
+                o.tile_nt = &nt;
+                double best = 1e30;
+                for (int rep = 0; rep < 3; ++rep) {
+                    rsatb_isqrt_stats st{};
+                    RSATB_TRY(rsatb_isqrt_columns_batched(ctx, count, nv.data(), cs.data(),
+                                                          kc.data(), in_off.data(), M,
+                                                          out_off.data(), out, &o, status.data(),
+                                                          &st));
+                    if (rep > 0) best = std::min(best, st.low_ms + st.fp64_ms);
+                }
+                ms[size_t(si) * 8 + kk * 4 + idx] = best;
+            }
+        }
+    }
+    // The kernel with the smaller summed best time, then its best tile per size.
+    double total[2] = {0.0, 0.0};
+    for (int si = 0; si < n_sizes; ++si)
+        for (int kk = 0; kk < 2; ++kk) {
+            double b = 1e30;
+            for (int idx = 0; idx < 4; ++idx) {
+                const double t = ms[size_t(si) * 8 + kk * 4 + idx];
+                if (t >= 0) b = std::min(b, t);
+            }
+            total[kk] += b;
+        }
+    const int kk = total[1] < total[0] ? 1 : 0;
+    *tc_kernel_out = kk + 1;
+    for (int si = 0; si < n_sizes; ++si) {
+        const int np = (sizes[si] + 31) / 32 * 32;
+        double b = 1e30;
+        int best_nt = 0;
+        for (int idx = 0; idx < 4; ++idx) {
+            const double t = ms[size_t(si) * 8 + kk * 4 + idx];
+            if (t >= 0 && t < b) {
+                b = t;
+                best_nt = candidate_nt(np, kk == 0, idx);
+            }
+        }
+        nt_out[si] = best_nt;
+    }
+    if (ms_out) std::copy(ms.begin(), ms.end(), ms_out);
     return RSATB_SUCCESS;
 }

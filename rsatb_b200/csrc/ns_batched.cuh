@@ -70,12 +70,15 @@ struct TcArgs {
 
 // One batched C = A B^T on the tensor cores for the items of up to
 // kMaxBuckets buckets (ns_tc_gemm.cu).  Maps describe A and B per bucket.
-int launch_tc_gemm(rsatb_context* ctx, const TcMaps& maps, const TcArgs& args);
+// ws: the warp-specialised kernel (N tile <= 128), else the single-role one.
+int launch_tc_gemm(rsatb_context* ctx, const TcMaps& maps, const TcArgs& args, bool ws);
 // Sets the kernel's shared-memory opt-in and resolves the tensor-map
 // encoder; called on the current device before any capture.
 int prepare_tc_gemm();
-// Widest N tile the selected tensor-core kernel takes (128 or 256).
-int tc_max_nt();
+// The built-in kernel choice (warp-specialised unless RSATB_NS_TC=simple)
+// and the widest N tile each kernel takes (128 or 256).
+bool default_tc_ws();
+inline int tc_max_nt(bool ws) { return ws ? 128 : 256; }
 
 // cuTensorMapEncodeTiled of a bucket: fp32 array `base` (element offset
 // already applied), dims (n_pad, n_pad, count), box (32, box_rows, 1),

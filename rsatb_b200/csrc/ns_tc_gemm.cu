@@ -460,7 +460,7 @@ int encode_bucket_map(CUtensorMap* map, const float* base, int n_pad, int count,
     return RSATB_SUCCESS;
 }
 
-bool use_ws() {
+bool default_tc_ws() {
     const char* s = std::getenv("RSATB_NS_TC");
     return !(s && s[0] == 's');  // "simple": the single-role kernel
 }
@@ -475,13 +475,11 @@ int prepare_tc_gemm() {
     return RSATB_SUCCESS;
 }
 
-int tc_max_nt() { return use_ws() ? 128 : 256; }
-
-int launch_tc_gemm(rsatb_context* ctx, const TcMaps& maps, const TcArgs& args) {
+int launch_tc_gemm(rsatb_context* ctx, const TcMaps& maps, const TcArgs& args, bool ws) {
     if (args.n_items <= 0) return RSATB_SUCCESS;
     int grid = ctx->sm_count;
     if (args.n_items < grid) grid = args.n_items;
-    if (use_ws())
+    if (ws)
         tc_gemm_ws_kernel<<<grid, 320, kWsSmemBytes, ctx->stream>>>(maps, args);
     else
         tc_gemm_kernel<<<grid, 128, kSmemBytes, ctx->stream>>>(maps, args);

@@ -38,7 +38,8 @@ def inverse_sqrt_columns_batched(M: torch.Tensor, n, in_offset, col_start=None, 
                                  out_offset=None, precision: str = "tf32x3",
                                  max_iter: int = 0, max_fp64_iter: int = 0, tol: float = 0.0,
                                  accept: float = 0.0, workspace_bytes: int = 0,
-                                 graph: bool = True, out: torch.Tensor | None = None):
+                                 graph: bool = True, out: torch.Tensor | None = None,
+                                 tiles: "TileTable | None" = None):
     """Columns [col_start, col_start + k) of M_p^{-1/2} for every problem p
     (isqrt::inverse_sqrt_columns_inplace, rsatb/calc/isqrt_action.hpp:1343,
     for a batch), by the library's batched Newton-Schulz solve.
@@ -48,7 +49,8 @@ def inverse_sqrt_columns_batched(M: torch.Tensor, n, in_offset, col_start=None, 
     Returns (out, status, stats): out a 1-D float64 CUDA tensor with problem
     p's n_p x k_p column-major block at out_offset[p] (packed in problem
     order when out_offset is None), status one rsatb_status per problem,
-    stats a dict of the call's counters.
+    stats a dict of the call's counters.  tiles: the tensor-core kernel and
+    N tiles picked by autotune_tiles (None: the built-in choice).
     """
     if not (M.is_cuda and M.dtype == torch.float64 and M.dim() == 1 and M.is_contiguous()):
         raise ValueError("M must be a contiguous 1-D float64 CUDA tensor")
@@ -72,6 +74,13 @@ def inverse_sqrt_columns_batched(M: torch.Tensor, n, in_offset, col_start=None, 
         out = torch.zeros(max(total, 1), dtype=torch.float64, device=M.device)
     opt = _capi.IsqrtOptions(PRECISIONS[precision], max_iter, max_fp64_iter, tol, accept,
                              workspace_bytes, 0 if graph else 1)
+    if tiles is not None:
+        t_np = np.ascontiguousarray(np.asarray(list(tiles.nt.keys()), dtype=np.int32))
+        t_nt = np.ascontiguousarray(np.asarray(list(tiles.nt.values()), dtype=np.int32))
+        opt.tc_kernel = tiles.tc_kernel
+        opt.n_tiles = int(t_np.size)
+        opt.tile_n_pad = t_np.ctypes.data
+        opt.tile_nt = t_nt.ctypes.data
     stats = _capi.IsqrtStats()
     status = np.zeros(P, dtype=np.int32)
     ctx = context(M.device.index)
@@ -82,6 +91,44 @@ def inverse_sqrt_columns_batched(M: torch.Tensor, n, in_offset, col_start=None, 
         vp(out_offset), C.c_void_p(out.data_ptr()), C.byref(opt), vp(status),
         C.byref(stats)))
     return out, status, {f: getattr(stats, f) for f, _ in stats._fields_}
+
+
+class TileTable:
+    """Tensor-core kernel (1 warp-specialised, 2 single-role) and N tile per
+    padded size for inverse_sqrt_columns_batched, as autotune_tiles picks
+    them; ms holds every candidate's measured time per size."""
+
+    def __init__(self, tc_kernel: int, nt: dict, ms: dict | None = None):
+        self.tc_kernel = int(tc_kernel)
+        self.nt = {int(k): int(v) for k, v in nt.items()}
+        self.ms = ms or {}
+
+    def __repr__(self):
+        kind = "warp-specialised" if self.tc_kernel == 1 else "single-role"
+        return f"TileTable({kind}, nt={self.nt})"
+
+
+def autotune_tiles(sizes, precision: str = "tf32x3", problems_per_size: int = 16,
+                   device: int | None = None) -> TileTable:
+    """Times the tensor-core kernel and N-tile candidates of the batched solve
+    on seeded well-conditioned SPD samples of each size (a fixed-length
+    solve, device time from CUDA events) and returns the fastest choice."""
+    if PRECISIONS.get(precision) not in (_capi.NS_TF32X3, _capi.NS_TF32):
+        raise ValueError("autotuning needs a tensor-core precision ('tf32x3' or 'tf32')")
+    pads = sorted({(int(s) + 31) // 32 * 32 for s in np.asarray(sizes).ravel()})
+    sz = np.ascontiguousarray(np.asarray(pads, dtype=np.int32))
+    nt = np.zeros(sz.size, dtype=np.int32)
+    ms = np.zeros(sz.size * 8, dtype=np.float64)
+    kern = C.c_int(0)
+    ctx = context(device if device is not None else torch.cuda.current_device())
+    ctx.bind_stream()
+    check(lib().rsatb_isqrt_autotune(ctx.handle, PRECISIONS[precision], int(sz.size),
+                                     sz.ctypes.data_as(C.c_void_p), int(problems_per_size),
+                                     C.byref(kern), nt.ctypes.data_as(C.c_void_p),
+                                     ms.ctypes.data_as(C.c_void_p)))
+    table = {int(p): int(t) for p, t in zip(sz, nt)}
+    times = {int(p): ms[8 * i:8 * i + 8].reshape(2, 4).tolist() for i, p in enumerate(sz)}
+    return TileTable(kern.value, table, times)
 
 
 def inverse_sqrt_rows_batched(M: torch.Tensor, rows: torch.Tensor, b: int,

@@ -153,3 +153,49 @@ def test_graph_local_factor_ns_matches_eigen(torch_cuda):
     Ze = graph_inverse_sqrt(S, method="eigen")
     assert _rel(graph_inverse_sqrt(S, method="ns").values, Ze.values) < TOL["fp64"]
     assert _rel(graph_inverse_sqrt(S, method="ns_tf32x3").values, Ze.values) < TOL["tf32x3"]
+
+
+def test_autotuned_tiles_are_valid_and_keep_results(torch_cuda):
+    """The tile autotuner returns a kernel and, per padded size, an N tile the
+    kernel accepts; solving with the tuned table gives the eigen-oracle
+    accuracy and the same result as the built-in tiles up to the split-TF32
+    tolerance (only the tiling of N and the kernel's roles change)."""
+    from rsatb_b200.isqrt import autotune_tiles, inverse_sqrt_columns_batched
+    sizes = [40, 100, 129, 300]
+    table = autotune_tiles(sizes, precision="tf32x3", problems_per_size=4)
+    assert table.tc_kernel in (1, 2)
+    cap = 128 if table.tc_kernel == 1 else 256
+    assert sorted(table.nt) == [64, 128, 160, 320]
+    for n_pad, nt in table.nt.items():
+        assert nt % 16 == 0 and 16 <= nt <= cap
+        times = np.asarray(table.ms[n_pad])
+        assert (times[times >= 0] > 0).all() and (times >= 0).sum() >= 2
+    mats = _batch(sizes, [1e2, 1e3, 1e4, 1e5])
+    M, offs = _pack(torch_cuda, mats)
+    n = np.array(sizes, np.int32)
+    base, st0, _ = inverse_sqrt_columns_batched(M, n, offs, precision="tf32x3")
+    tuned, st1, _ = inverse_sqrt_columns_batched(M, n, offs, precision="tf32x3", tiles=table)
+    assert (st0 == 0).all() and (st1 == 0).all()
+    got = tuned.cpu().numpy()
+    ref = base.cpu().numpy()
+    pos = 0
+    for m in mats:
+        k = m.shape[0]
+        want = oracle.isqrt_columns_eigen(m, 0, k)
+        blk = got[pos:pos + k * k].reshape(k, k).T
+        assert _rel(blk, want) < TOL["tf32x3"]
+        assert _rel(blk, ref[pos:pos + k * k].reshape(k, k).T) < TOL["tf32x3"]
+        pos += k * k
+
+
+def test_tile_table_rejects_bad_tiles(torch_cuda):
+    from rsatb_b200.isqrt import TileTable, inverse_sqrt_columns_batched
+    from rsatb_b200._capi import RsatbError
+    mats = _batch([64], [10.0])
+    M, offs = _pack(torch_cuda, mats)
+    with pytest.raises(RsatbError):
+        inverse_sqrt_columns_batched(M, np.array([64], np.int32), offs, precision="tf32x3",
+                                     tiles=TileTable(1, {64: 24}))  # not a multiple of 16
+    with pytest.raises(RsatbError):
+        inverse_sqrt_columns_batched(M, np.array([64], np.int32), offs, precision="tf32x3",
+                                     tiles=TileTable(1, {64: 256}))  # above the kernel's 128
