@@ -210,22 +210,44 @@ struct F64Item {
     int p, m0, n0;
 };
 
-// FP64 C = A B^T (BT) or C = A B, 64 x 64 tiles, 256 threads of 4 x 4
-// outputs (rows ty + 16 i, columns tx + 16 j), K chunks of 16 through
-// shared memory; same epilogue modes as the tensor-core kernel.  SYM_A
-// multiplies by (A + A^T)/2 instead of A.  c_hi/c_lo (optional) receive the
-// TF32 hi/lo split of C for the next tensor-core GEMMs.
+// D (+)= A B for one m8n8k4 FP64 tile on the tensor cores (mma.sync, the
+// FP64 tensor path of sm_100): A 8x4 row-major, one value per lane at
+// (lane / 4, lane % 4); B 4x8, one value per lane at (lane % 4, lane / 4);
+// D 8x8, two values per lane at (lane / 4, 2 (lane % 4) + {0, 1}).
+__device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d[0]), "+d"(d[1])
+                 : "d"(a), "d"(b));
+}
+
+// FP64 C = A B^T (BT) or C = A B, one 64 x 64 tile per work item, on the
+// FP64 tensor cores: 4 warps, each a 32 x 32 quadrant of 4 x 4 m8n8k4
+// fragments, K chunks of KC through shared memory.  Operands keep the layout
+// their global rows have, so every load is coalesced and every store
+// conflict-free: rows of A (and of B when BT) as [m][k] with stride KC + 4
+// doubles, rows of B (not BT) and of A^T (SYM_A) as [k][n] with stride 68.
+// Both strides are 4 mod 16 doubles, so the 16 lanes of a half-warp fragment
+// load hit 16 different banks.  SYM_A multiplies by (A + A^T)/2 instead of
+// A, summed as the fragment is read.  Same epilogue modes as the tensor-core
+// kernel; c_hi/c_lo (optional) receive the TF32 hi/lo split of C for the
+// next tensor-core GEMMs.
 template <bool BT, bool SYM_A>
-__global__ void __launch_bounds__(256) gemm_f64_kernel(const Prob* probs, const F64Item* items,
+__global__ void __launch_bounds__(128) gemm_f64_kernel(const Prob* probs, const F64Item* items,
                                                        int n_items, const State* st,
                                                        const double* A, const double* B,
                                                        double* C, int mode, const double* Xe,
                                                        double* res2, float* c_hi,
                                                        float* c_lo) {
-    __shared__ double As[16][64 + 1];
-    __shared__ double Bs[16][64 + 1];
-    __shared__ double red[8];
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    constexpr int KC = SYM_A ? 16 : 32;  // K chunk (static shared memory stays under 48 KB)
+    constexpr int LDR = KC + 4;          // [row][k] stride
+    constexpr int LDK = 64 + 4;          // [k][col] stride
+    __shared__ double As[64 * LDR];                    // A rows: [m][k]
+    __shared__ double AsT[SYM_A ? KC * LDK : 1];       // A^T: [k][m]
+    __shared__ double Bs[BT ? 64 * LDR : KC * LDK];    // B rows [n][k] or B [k][n]
+    __shared__ double red[4];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+    const int fr = lane >> 2, fc = lane & 3;
     for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
         const F64Item item = items[it];
         if (!st[item.p].active) continue;
@@ -233,79 +255,99 @@ __global__ void __launch_bounds__(256) gemm_f64_kernel(const Prob* probs, const 
         const int np = pr.n_pad;
         const double* Ap = A + pr.off;
         const double* Bp = B + pr.off;
-        double acc[4][4];
+        double acc[4][4][2];
 #pragma unroll
         for (int i = 0; i < 4; ++i)
 #pragma unroll
-            for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
-        for (int k0 = 0; k0 < np; k0 += 16) {
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int idx = threadIdx.x + 256 * q;
-                const int r = idx >> 4, kk = idx & 15;
+            for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+        for (int k0 = 0; k0 < np; k0 += KC) {
+            // [64 x KC] row chunks: KC consecutive threads read one row.
+#pragma unroll 4
+            for (int q = 0; q < KC / 2; ++q) {
+                const int idx = threadIdx.x + 128 * q;
+                const int r = idx / KC, kk = idx % KC;
                 const int m = item.m0 + r;
-                double av = m < np ? Ap[int64_t(m) * np + k0 + kk] : 0.0;
-                if (SYM_A && m < np) av = 0.5 * (av + Ap[int64_t(k0 + kk) * np + m]);
-                As[kk][r] = av;
+                As[r * LDR + kk] = m < np ? Ap[int64_t(m) * np + k0 + kk] : 0.0;
                 if (BT) {
                     const int nn = item.n0 + r;
-                    Bs[kk][r] = nn < np ? Bp[int64_t(nn) * np + k0 + kk] : 0.0;
-                } else {
+                    Bs[r * LDR + kk] = nn < np ? Bp[int64_t(nn) * np + k0 + kk] : 0.0;
+                }
+            }
+            // [KC x 64] column chunks: 64 consecutive threads read one k row.
+            if (!BT || SYM_A) {
+#pragma unroll 4
+                for (int q = 0; q < KC / 2; ++q) {
+                    const int idx = threadIdx.x + 128 * q;
                     const int kr = idx >> 6, c = idx & 63;
-                    const int nn = item.n0 + c;
-                    Bs[kr][c] = nn < np ? Bp[int64_t(k0 + kr) * np + nn] : 0.0;
+                    if (!BT) {
+                        const int nn = item.n0 + c;
+                        Bs[kr * LDK + c] = nn < np ? Bp[int64_t(k0 + kr) * np + nn] : 0.0;
+                    }
+                    if (SYM_A) {
+                        const int m = item.m0 + c;
+                        AsT[kr * LDK + c] = m < np ? Ap[int64_t(k0 + kr) * np + m] : 0.0;
+                    }
                 }
             }
             __syncthreads();
 #pragma unroll
-            for (int kk = 0; kk < 16; ++kk) {
-                double a[4], b[4];
+            for (int kk = 0; kk < KC; kk += 4) {
+                double af[4], bf[4];
 #pragma unroll
-                for (int i = 0; i < 4; ++i) a[i] = As[kk][ty + 16 * i];
+                for (int i = 0; i < 4; ++i) {
+                    const int m = wm + 8 * i + fr, k = kk + fc;
+                    af[i] = SYM_A ? 0.5 * (As[m * LDR + k] + AsT[k * LDK + m]) : As[m * LDR + k];
+                }
 #pragma unroll
-                for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx + 16 * j];
+                for (int j = 0; j < 4; ++j) {
+                    const int nn = wn + 8 * j + fr, k = kk + fc;
+                    bf[j] = BT ? Bs[nn * LDR + k] : Bs[k * LDK + nn];
+                }
 #pragma unroll
                 for (int i = 0; i < 4; ++i)
 #pragma unroll
-                    for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+                    for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j], af[i], bf[j]);
             }
             __syncthreads();
         }
         double r2 = 0.0;
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-            const int m = item.m0 + ty + 16 * i;
+            const int m = item.m0 + wm + 8 * i + fr;
             if (m >= np) continue;
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
-                const int nn = item.n0 + tx + 16 * j;
-                if (nn >= np) continue;
-                const bool valid = m < pr.n && nn < pr.n;
-                const int64_t e = pr.off + int64_t(m) * np + nn;
-                double x = acc[i][j];
-                if (mode == EPI_POLY) x = fma(0.375, x, fma(-1.25, Xe[e], m == nn ? 1.875 : 0.0));
-                if (!valid) x = 0.0;
-                if (mode == EPI_RESID && valid) {
-                    const double d = x - (m == nn ? 1.0 : 0.0);
-                    r2 += d * d;
-                }
-                C[e] = x;
-                if (c_hi) {
-                    const float f = float(x);
-                    const float h = umma::to_tf32(f);
-                    c_hi[e] = h;
-                    c_lo[e] = f - h;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int nn = item.n0 + wn + 8 * j + 2 * fc + h;
+                    if (nn >= np) continue;
+                    const bool valid = m < pr.n && nn < pr.n;
+                    const int64_t e = pr.off + int64_t(m) * np + nn;
+                    double x = acc[i][j][h];
+                    if (mode == EPI_POLY)
+                        x = fma(0.375, x, fma(-1.25, Xe[e], m == nn ? 1.875 : 0.0));
+                    if (!valid) x = 0.0;
+                    if (mode == EPI_RESID && valid) {
+                        const double d = x - (m == nn ? 1.0 : 0.0);
+                        r2 += d * d;
+                    }
+                    C[e] = x;
+                    if (c_hi) {
+                        const float f = float(x);
+                        const float hv = umma::to_tf32(f);
+                        c_hi[e] = hv;
+                        c_lo[e] = f - hv;
+                    }
                 }
             }
         }
         if (mode == EPI_RESID) {
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) r2 += __shfl_xor_sync(0xffffffffu, r2, o);
-            if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = r2;
+            if (lane == 0) red[warp] = r2;
             __syncthreads();
             if (threadIdx.x == 0) {
-                double s = 0.0;
-                for (int w = 0; w < 8; ++w) s += red[w];
+                const double s = (red[0] + red[1]) + (red[2] + red[3]);
                 if (s != 0.0) atomicAdd(res2 + item.p, s);
             }
             __syncthreads();
@@ -432,9 +474,9 @@ int f64_gemm(rsatb_context* ctx, const Dev& d, const double* A, const double* B,
              int mode, const double* Xe, rsatb_isqrt_stats* stats, float* c_hi = nullptr,
              float* c_lo = nullptr) {
     if (d.n_f64_items == 0) return RSATB_SUCCESS;
-    int grid = ctx->sm_count * 4;
+    int grid = ctx->sm_count * 6;
     if (d.n_f64_items < grid) grid = d.n_f64_items;
-    gemm_f64_kernel<BT, SYM_A><<<grid, 256, 0, ctx->stream>>>(
+    gemm_f64_kernel<BT, SYM_A><<<grid, 128, 0, ctx->stream>>>(
         d.probs, d.f64_items, d.n_f64_items, d.state, A, B, C, mode, Xe, d.res2, c_hi, c_lo);
     RSATB_LAUNCH_CHECK(ctx);
     if (stats) stats->gemm_launches++;
