@@ -220,15 +220,37 @@ __device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
                  : "d"(a), "d"(b));
 }
 
+// 16 bytes global -> shared, zero-filled when !valid (no bytes read then).
+__device__ __forceinline__ void cp16_zfill(void* smem, const void* gmem, bool valid) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem),
+                 "r"(valid ? 16 : 0)
+                 : "memory");
+}
+
+// Shared-memory shape of the FP64 GEMM: K chunk KC, [row][k] stride LDR,
+// [k][col] stride LDK (both 4 mod 16 doubles: the 16 lanes of a half-warp
+// fragment load hit 16 different banks), two stages.
+template <bool BT, bool SYM_A>
+struct F64Shape {
+    static constexpr int KC = SYM_A ? 16 : 32;
+    static constexpr int LDR = KC + 4;
+    static constexpr int LDK = 64 + 4;
+    static constexpr int A_ELEMS = 64 * LDR;
+    static constexpr int AT_ELEMS = SYM_A ? KC * LDK : 0;
+    static constexpr int B_ELEMS = BT ? 64 * LDR : KC * LDK;
+    static constexpr int STAGE = A_ELEMS + AT_ELEMS + B_ELEMS;
+    static constexpr size_t SMEM = 2 * size_t(STAGE) * sizeof(double);
+};
+
 // FP64 C = A B^T (BT) or C = A B, one 64 x 64 tile per work item, on the
 // FP64 tensor cores: 4 warps, each a 32 x 32 quadrant of 4 x 4 m8n8k4
-// fragments, K chunks of KC through shared memory.  Operands keep the layout
-// their global rows have, so every load is coalesced and every store
-// conflict-free: rows of A (and of B when BT) as [m][k] with stride KC + 4
-// doubles, rows of B (not BT) and of A^T (SYM_A) as [k][n] with stride 68.
-// Both strides are 4 mod 16 doubles, so the 16 lanes of a half-warp fragment
-// load hit 16 different banks.  SYM_A multiplies by (A + A^T)/2 instead of
-// A, summed as the fragment is read.  Same epilogue modes as the tensor-core
+// fragments, K chunks of KC double-buffered in shared memory by cp.async
+// (the next chunk is in flight while the current one is multiplied).
+// Operands keep the layout their global rows have, so every copy is
+// coalesced: rows of A (and of B when BT) as [m][k], rows of B (not BT) and
+// of A^T (SYM_A) as [k][n].  SYM_A multiplies by (A + A^T)/2 instead of A,
+// summed as the fragment is read.  Same epilogue modes as the tensor-core
 // kernel; c_hi/c_lo (optional) receive the TF32 hi/lo split of C for the
 // next tensor-core GEMMs.
 template <bool BT, bool SYM_A>
@@ -238,12 +260,9 @@ __global__ void __launch_bounds__(128) gemm_f64_kernel(const Prob* probs, const 
                                                        double* C, int mode, const double* Xe,
                                                        double* res2, float* c_hi,
                                                        float* c_lo) {
-    constexpr int KC = SYM_A ? 16 : 32;  // K chunk (static shared memory stays under 48 KB)
-    constexpr int LDR = KC + 4;          // [row][k] stride
-    constexpr int LDK = 64 + 4;          // [k][col] stride
-    __shared__ double As[64 * LDR];                    // A rows: [m][k]
-    __shared__ double AsT[SYM_A ? KC * LDK : 1];       // A^T: [k][m]
-    __shared__ double Bs[BT ? 64 * LDR : KC * LDK];    // B rows [n][k] or B [k][n]
+    using Sh = F64Shape<BT, SYM_A>;
+    constexpr int KC = Sh::KC, LDR = Sh::LDR, LDK = Sh::LDK;
+    extern __shared__ __align__(16) double f64_smem[];
     __shared__ double red[4];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
@@ -255,41 +274,61 @@ __global__ void __launch_bounds__(128) gemm_f64_kernel(const Prob* probs, const 
         const int np = pr.n_pad;
         const double* Ap = A + pr.off;
         const double* Bp = B + pr.off;
+        // Copies of chunk k0 into stage s: [64 x KC] row chunks as KC / 2
+        // 16-byte units per row, [KC x 64] column chunks as 32 units per k row.
+        auto issue = [&](int k0, int s) {
+            double* As = f64_smem + s * Sh::STAGE;
+            double* AsT = As + Sh::A_ELEMS;
+            double* Bs = AsT + Sh::AT_ELEMS;
+#pragma unroll
+            for (int q = 0; q < KC / 4; ++q) {
+                const int idx = threadIdx.x + 128 * q;
+                const int r = idx / (KC / 2), u = idx % (KC / 2);
+                const int m = item.m0 + r;
+                cp16_zfill(As + r * LDR + 2 * u, Ap + (m < np ? int64_t(m) * np + k0 + 2 * u : 0),
+                           m < np);
+                if (BT) {
+                    const int nn = item.n0 + r;
+                    cp16_zfill(Bs + r * LDR + 2 * u,
+                               Bp + (nn < np ? int64_t(nn) * np + k0 + 2 * u : 0), nn < np);
+                }
+            }
+            if (!BT || SYM_A) {
+#pragma unroll
+                for (int q = 0; q < KC / 4; ++q) {
+                    const int idx = threadIdx.x + 128 * q;
+                    const int kr = idx >> 5, u = idx & 31;
+                    if (!BT) {
+                        const int nn = item.n0 + 2 * u;
+                        cp16_zfill(Bs + kr * LDK + 2 * u,
+                                   Bp + (nn < np ? int64_t(k0 + kr) * np + nn : 0), nn < np);
+                    }
+                    if (SYM_A) {
+                        const int m = item.m0 + 2 * u;
+                        cp16_zfill(AsT + kr * LDK + 2 * u,
+                                   Ap + (m < np ? int64_t(k0 + kr) * np + m : 0), m < np);
+                    }
+                }
+            }
+            asm volatile("cp.async.commit_group;\n" ::: "memory");
+        };
         double acc[4][4][2];
 #pragma unroll
         for (int i = 0; i < 4; ++i)
 #pragma unroll
             for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-        for (int k0 = 0; k0 < np; k0 += KC) {
-            // [64 x KC] row chunks: KC consecutive threads read one row.
-#pragma unroll 4
-            for (int q = 0; q < KC / 2; ++q) {
-                const int idx = threadIdx.x + 128 * q;
-                const int r = idx / KC, kk = idx % KC;
-                const int m = item.m0 + r;
-                As[r * LDR + kk] = m < np ? Ap[int64_t(m) * np + k0 + kk] : 0.0;
-                if (BT) {
-                    const int nn = item.n0 + r;
-                    Bs[r * LDR + kk] = nn < np ? Bp[int64_t(nn) * np + k0 + kk] : 0.0;
-                }
-            }
-            // [KC x 64] column chunks: 64 consecutive threads read one k row.
-            if (!BT || SYM_A) {
-#pragma unroll 4
-                for (int q = 0; q < KC / 2; ++q) {
-                    const int idx = threadIdx.x + 128 * q;
-                    const int kr = idx >> 6, c = idx & 63;
-                    if (!BT) {
-                        const int nn = item.n0 + c;
-                        Bs[kr * LDK + c] = nn < np ? Bp[int64_t(k0 + kr) * np + nn] : 0.0;
-                    }
-                    if (SYM_A) {
-                        const int m = item.m0 + c;
-                        AsT[kr * LDK + c] = m < np ? Ap[int64_t(k0 + kr) * np + m] : 0.0;
-                    }
-                }
+        issue(0, 0);
+        for (int k0 = 0, s = 0; k0 < np; k0 += KC, s ^= 1) {
+            if (k0 + KC < np) {
+                issue(k0 + KC, s ^ 1);
+                asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+            } else {
+                asm volatile("cp.async.wait_group 0;\n" ::: "memory");
             }
             __syncthreads();
+            const double* As = f64_smem + s * Sh::STAGE;
+            const double* AsT = As + Sh::A_ELEMS;
+            const double* Bs = AsT + Sh::AT_ELEMS;
 #pragma unroll
             for (int kk = 0; kk < KC; kk += 4) {
                 double af[4], bf[4];
@@ -308,7 +347,7 @@ __global__ void __launch_bounds__(128) gemm_f64_kernel(const Prob* probs, const 
 #pragma unroll
                     for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j], af[i], bf[j]);
             }
-            __syncthreads();
+            __syncthreads();  // stage s is refilled by the next iteration's copies
         }
         double r2 = 0.0;
 #pragma unroll
@@ -476,7 +515,7 @@ int f64_gemm(rsatb_context* ctx, const Dev& d, const double* A, const double* B,
     if (d.n_f64_items == 0) return RSATB_SUCCESS;
     int grid = ctx->sm_count * 6;
     if (d.n_f64_items < grid) grid = d.n_f64_items;
-    gemm_f64_kernel<BT, SYM_A><<<grid, 128, 0, ctx->stream>>>(
+    gemm_f64_kernel<BT, SYM_A><<<grid, 128, F64Shape<BT, SYM_A>::SMEM, ctx->stream>>>(
         d.probs, d.f64_items, d.n_f64_items, d.state, A, B, C, mode, Xe, d.res2, c_hi, c_lo);
     RSATB_LAUNCH_CHECK(ctx);
     if (stats) stats->gemm_launches++;
@@ -521,6 +560,13 @@ int run_chunk(rsatb_context* ctx, const Opts& o, const Chunk& ch, const int* col
     const int P = int(ch.probs.size());
     const bool low = o.precision != RSATB_NS_FP64;
     const bool split = o.precision == RSATB_NS_TF32X3;
+    // Dynamic shared-memory opt-in of the FP64 GEMMs, before any capture.
+    RSATB_CUDA_TRY(cudaFuncSetAttribute(gemm_f64_kernel<true, false>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        int(F64Shape<true, false>::SMEM)));
+    RSATB_CUDA_TRY(cudaFuncSetAttribute(gemm_f64_kernel<false, true>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        int(F64Shape<false, true>::SMEM)));
 
     // Work items, ordered by bucket (the buckets of a launch group are
     // contiguous), largest problems first.
