@@ -389,7 +389,8 @@ RSATB_API int rsatb_isqrt_autotune(rsatb_ctx_t ctx, int precision, int n_sizes,
 /* FMA-pipe throughput of this device in FLOP/s, from independent FMA chains
  * on every SM timed with CUDA events: the compute roofline of the block SpMM
  * at wide panels.  double_precision: 1 FP64, 0 FP32 (scalar FMAs), 2 FP32
- * issued as packed pairs (fma.rn.f32x2). */
+ * issued as packed pairs (fma.rn.f32x2), 3 FP64 on the tensor cores
+ * (mma.sync m8n8k4 f64 tiles). */
 RSATB_API int rsatb_measure_fma_peak(rsatb_ctx_t ctx, int double_precision, double* flops);
 
 #ifdef __cplusplus

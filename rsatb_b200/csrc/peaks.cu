@@ -1,4 +1,5 @@
-// Measured FMA-pipe peak (FP64, FP32, or FP32 issued as packed f32x2 FMAs),
+// Measured FMA-pipe peak (FP64, FP32, FP32 issued as packed f32x2 FMAs, or
+// FP64 on the tensor cores as m8n8k4 tiles),
 // the denominator of the compute roofline of the SpMM at wide panels, where
 // the block SpMM is bound by the CUDA-core FMA rate rather than by HBM.
 // Every SM runs independent FMA chains; the result is FLOP/s = 2 * FMAs /
@@ -52,6 +53,29 @@ __global__ void __launch_bounds__(256) fma2_chains(float* out, int iters, float 
     if (s == -12345.678f) out[threadIdx.x] = s;  // keeps the chains live
 }
 
+// Eight independent chains of FP64 tensor-core tiles (mma.sync m8n8k4 f64:
+// 256 FMAs per warp per instruction).
+__global__ void __launch_bounds__(256) dmma_chains(double* out, int iters, double a, double b) {
+    double d[8][2];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) d[k][0] = d[k][1] = double(threadIdx.x) * 1e-3 + k;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                asm volatile(
+                    "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, "
+                    "{%0, %1};"
+                    : "+d"(d[k][0]), "+d"(d[k][1])
+                    : "d"(a), "d"(b));
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s += d[k][0] + d[k][1];
+    if (s == -12345.678) out[threadIdx.x] = s;  // keeps the chains live
+}
+
 }  // namespace
 }  // namespace rsatb_b200
 
@@ -65,14 +89,16 @@ extern "C" int rsatb_measure_fma_peak(rsatb_ctx_t ctx, int double_precision, dou
     RSATB_TRY(ctx_scratch(ctx, 4096, &sink));
     const int threads = 256;
     const int grid = ctx->sm_count * 8;
-    const int iters = double_precision == 1 ? 4096 : 8192;
+    const int iters = double_precision == 1 ? 4096 : (double_precision == 3 ? 64 : 8192);
     cudaEvent_t e0, e1;
     RSATB_CUDA_TRY(cudaEventCreate(&e0));
     RSATB_CUDA_TRY(cudaEventCreate(&e1));
     float best_ms = 1e30f;
     for (int rep = 0; rep < 4; ++rep) {
         RSATB_CUDA_TRY(cudaEventRecord(e0, ctx->stream));
-        if (double_precision == 2)
+        if (double_precision == 3)
+            dmma_chains<<<grid, threads, 0, ctx->stream>>>((double*)sink, iters, 0.999999, 1e-7);
+        else if (double_precision == 2)
             fma2_chains<<<grid, threads, 0, ctx->stream>>>((float*)sink, iters, 0.9999f, 1e-4f);
         else if (double_precision)
             fma_chains<double><<<grid, threads, 0, ctx->stream>>>((double*)sink, iters,
@@ -89,8 +115,10 @@ extern "C" int rsatb_measure_fma_peak(rsatb_ctx_t ctx, int double_precision, dou
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    const double fmas = double(grid) * threads * double(iters) * 4.0 * 8.0 *
-                        (double_precision == 2 ? 2.0 : 1.0);
+    // Per thread and inner step: 1 FMA (scalar), 2 (f32x2) or 256 / 32 = 8
+    // (one m8n8k4 tile per warp).
+    const double per = double_precision == 2 ? 2.0 : (double_precision == 3 ? 8.0 : 1.0);
+    const double fmas = double(grid) * threads * double(iters) * 4.0 * 8.0 * per;
     *flops = 2.0 * fmas / (double(best_ms) * 1e-3);
     return RSATB_SUCCESS;
 }
