@@ -1,0 +1,127 @@
+// Fused Chebyshev step on the FP64 tensor cores: real 8x8 blocks, panels of
+// W = 8 to 256 real values per row (W a multiple of 8), stored in FP64 or
+// FP32 (VT).  FP32 operands are widened to FP64 as they are loaded, so an
+// FP32 panel is multiplied with FP64 products and FP64 accumulation (its
+// result is rounded to FP32 once, at the store).
+//
+// An 8x8 block times 8 panel columns is exactly two mma.sync m8n8k4 f64
+// tiles (K = 8 split in two halves of 4): the block is the A operand (one
+// value per lane at row lane / 4, column lane % 4 + 4h) and 8 columns of the
+// gathered X_j rows the B operand (one value per lane at row lane % 4 + 4h,
+// column lane / 4).  A warp owns one block row and all W / 8 column groups,
+// so each of its fragment loads reads 256 contiguous-ish bytes (8 rows x 32
+// bytes of A, or 4 rows x 64 bytes of X_j) and each MMA instruction carries
+// 256 FMAs.  For narrow panels U blocks of the row are loaded together, so
+// several blocks are in flight per warp.
+//
+// The accumulator leaves each lane two consecutive columns of one output
+// row per column group, which is the layout finish_row expects with V = 2
+// (the (re, im) pairs of a complex panel stay together).  The FP64 column
+// dots of the epilogue are summed over the block row's 8 rows by shuffles
+// and accumulated per warp in shared memory; the CTA then sums its warps in
+// a fixed order and finish_partials sums the CTAs (deterministic).
+#pragma once
+
+#include "cheb_kernels.cuh"
+
+namespace rsatb_b200 {
+
+constexpr int kDmmaWarps = 4;
+
+__device__ __forceinline__ void dmma_884(double (&d)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d[0]), "+d"(d[1])
+                 : "d"(a), "d"(b));
+}
+
+// Blocks of a row loaded together: enough loads in flight at narrow panels,
+// registers bounded at wide ones.
+template <int W>
+struct DmmaShape {
+    static constexpr int NG = W / 8;
+    static constexpr int U = W <= 16 ? 4 : (W <= 32 ? 2 : 1);
+};
+
+template <typename VT, int W, bool CV>
+__global__ void __launch_bounds__(kDmmaWarps * 32) cheb_step_dmma(StepArgs a) {
+    static_assert(W % 8 == 0 && W <= 256, "8-column groups");
+    constexpr int NG = DmmaShape<W>::NG, U = DmmaShape<W>::U;
+    __shared__ double dsm[kDmmaWarps][2][W];  // per warp: dots d0, d1 per column
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int fr = lane >> 2, fc = lane & 3;
+    const VT* __restrict__ vals = static_cast<const VT*>(a.vals);
+    const VT* __restrict__ in = static_cast<const VT*>(a.in);
+    const int ndots = a.dot_mode == DOT_DOUBLING ? 2 : (a.dot_mode == DOT_PLAIN ? 1 : 0);
+    for (int c = lane; c < 2 * W; c += 32) dsm[warp][c / W][c % W] = 0.0;
+    __syncwarp();
+
+    for (int64_t i = int64_t(blockIdx.x) * kDmmaWarps + warp; i < a.n_block_rows;
+         i += int64_t(gridDim.x) * kDmmaWarps) {
+        const int k0 = __ldg(a.row_ptr + i), k1 = __ldg(a.row_ptr + i + 1);
+        double acc[NG][2];
+#pragma unroll
+        for (int g = 0; g < NG; ++g) acc[g][0] = acc[g][1] = 0.0;
+        for (int k = k0; k < k1; k += U) {
+            double af[U][2], bf[U][NG][2];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int kk = k + u;
+                const bool valid = kk < k1;
+                const int64_t j = valid ? __ldg(a.col_ind + kk) : 0;
+                const VT* blk = vals + int64_t(valid ? kk : k0) * 64 + fr * 8 + fc;
+                const VT* xr = in + (j * 8 + fc) * W + fr;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    af[u][h] = valid ? double(__ldg(blk + 4 * h)) : 0.0;
+#pragma unroll
+                    for (int g = 0; g < NG; ++g)
+                        bf[u][g][h] = valid ? double(__ldg(xr + 4 * h * W + 8 * g)) : 0.0;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+#pragma unroll
+                for (int h = 0; h < 2; ++h)
+#pragma unroll
+                    for (int g = 0; g < NG; ++g) dmma_884(acc[g], af[u][h], bf[u][g][h]);
+        }
+        // Epilogue: lane holds output row i*8 + fr, columns 8g + 2fc + {0, 1}.
+#pragma unroll
+        for (int g = 0; g < NG; ++g) {
+            double e0[2] = {0.0, 0.0}, e1[2] = {0.0, 0.0};
+            const VT out2[2] = {VT(acc[g][0]), VT(acc[g][1])};
+            finish_row<VT, 2, CV>(a, i * 8 + fr, 4 * g + fc, out2, e0, e1);
+            if (ndots) {
+#pragma unroll
+                for (int o = 4; o < 32; o <<= 1) {
+                    e0[0] += __shfl_xor_sync(0xffffffffu, e0[0], o);
+                    e0[1] += __shfl_xor_sync(0xffffffffu, e0[1], o);
+                    if (ndots == 2) {
+                        e1[0] += __shfl_xor_sync(0xffffffffu, e1[0], o);
+                        e1[1] += __shfl_xor_sync(0xffffffffu, e1[1], o);
+                    }
+                }
+                if (fr == 0) {
+                    dsm[warp][0][8 * g + 2 * fc] += e0[0];
+                    dsm[warp][0][8 * g + 2 * fc + 1] += e0[1];
+                    dsm[warp][1][8 * g + 2 * fc] += e1[0];
+                    dsm[warp][1][8 * g + 2 * fc + 1] += e1[1];
+                }
+            }
+        }
+    }
+    if (ndots) {
+        __syncthreads();
+        double* mine = a.partials + size_t(blockIdx.x) * ndots * W;
+        for (int idx = threadIdx.x; idx < ndots * W; idx += blockDim.x) {
+            const int d = idx / W, col = idx - d * W;
+            double s = 0.0;
+#pragma unroll
+            for (int w = 0; w < kDmmaWarps; ++w) s += dsm[w][d][col];
+            mine[idx] = s;
+        }
+        finish_partials(a, ndots);
+    }
+}
+
+}  // namespace rsatb_b200

@@ -7,6 +7,7 @@
 #include "cheb_rowsplit.cuh"
 #include "cheb_bulk.cuh"
 #include "cheb_narrow.cuh"
+#include "cheb_dmma.cuh"
 
 #include <cstdlib>
 #include <mutex>
@@ -87,7 +88,7 @@ inline int pick_v(int W, bool cv, bool any_b, int block_size, bool dbl) {
 
 constexpr int kNotApplicable = 1000;
 
-// RSATB_STEP_KERNEL=v1|staged|rowsplit|bulk|narrow forces one kernel family (tuning and
+// RSATB_STEP_KERNEL=v1|staged|rowsplit|bulk|narrow|dmma forces one kernel family (tuning and
 // A/B tests); unset picks by shape and precision.
 inline int env_kernel() {
     const char* s = std::getenv("RSATB_STEP_KERNEL");
@@ -97,6 +98,7 @@ inline int env_kernel() {
     if (s[0] == 'r') return 3;
     if (s[0] == 'b') return 4;
     if (s[0] == 'n') return 5;
+    if (s[0] == 'd') return 6;
     return 0;
 }
 inline bool env_force_v1() { return env_kernel() == 1; }
@@ -325,6 +327,45 @@ int launch_narrow_w(rsatb_context* ctx, StepArgs& a) {
                                 : launch_narrow_k<VT, W, CV, 2>(ctx, a);
 }
 
+template <typename VT, int W, bool CV>
+int launch_dmma_k(rsatb_context* ctx, StepArgs& a) {
+    auto kernel = cheb_step_dmma<VT, W, CV>;
+    const int threads = kDmmaWarps * 32;
+    const int64_t need = (a.n_block_rows + kDmmaWarps - 1) / kDmmaWarps;
+    const int per_sm = occupancy(reinterpret_cast<const void*>(kernel), threads, 0);
+    int64_t grid = int64_t(ctx->sm_count) * per_sm;
+    if (grid > int64_t(ctx->sm_count) * 8) grid = int64_t(ctx->sm_count) * 8;
+    if (need < grid) grid = need;
+    if (grid < 1) grid = 1;
+    kernel<<<unsigned(grid), threads, 0, ctx->stream>>>(a);
+    RSATB_LAUNCH_CHECK(ctx);
+    return RSATB_SUCCESS;
+}
+
+// Panels on the FP64 tensor cores: real 8x8 blocks, W a multiple of 8 up
+// to 256 (complex panels: W = 2R); FP32 panels at W <= 32 only (wider ones
+// are compute-bound, where the FP32 FMA kernels are faster); kNotApplicable
+// otherwise.
+template <typename VT, bool CV>
+int launch_dmma(rsatb_context* ctx, StepArgs& a) {
+    if (sizeof(VT) == 4 && a.W > 32) return kNotApplicable;
+    switch (a.W) {
+        case 8: return launch_dmma_k<VT, 8, CV>(ctx, a);
+        case 16: return launch_dmma_k<VT, 16, CV>(ctx, a);
+        case 32: return launch_dmma_k<VT, 32, CV>(ctx, a);
+        case 64:
+            if constexpr (sizeof(VT) == 8) return launch_dmma_k<VT, 64, CV>(ctx, a);
+            break;
+        case 128:
+            if constexpr (sizeof(VT) == 8) return launch_dmma_k<VT, 128, CV>(ctx, a);
+            break;
+        case 256:
+            if constexpr (sizeof(VT) == 8) return launch_dmma_k<VT, 256, CV>(ctx, a);
+            break;
+    }
+    return kNotApplicable;
+}
+
 // Real 8x8 blocks, W in {4, 8, 16}, 16-byte aligned values and operand;
 // kNotApplicable otherwise.
 template <typename VT, bool CV>
@@ -393,6 +434,19 @@ int launch_typed(rsatb_context* ctx, int block_size, StepArgs& a) {
         if (st != kNotApplicable) return st;
     }
     if constexpr (!CM) {
+        // FP64 tensor-core kernel, blocks of 8: the default for FP64 panels
+        // and for FP32 panels of W <= 16 (measured on the diamond 8x8 BSR,
+        // B200: FP64 R = 8 / 16 / 32 / 128 take 0.093 / 0.158 / 0.267 /
+        // 1.01 ms against 0.226 / 0.213 / 0.349 / 1.22 for the staged
+        // kernel; FP32 R = 8 / 16 take 0.078 / 0.109 ms against 0.103 /
+        // 0.119 for the register kernel).
+        const bool want = forced == 6 || (forced == 0 && (sizeof(VT) == 8 || a.W <= 16));
+        if (block_size == 8 && want) {
+            const int st = launch_dmma<VT, CV>(ctx, a);
+            if (st != kNotApplicable) return st;
+        }
+    }
+    if constexpr (!CM) {
         // Narrow-panel lock-step kernel: blocks of 8, W <= 16 (when forced).
         if (block_size == 8 && forced == 5) {
             const int st = launch_narrow<VT, CV>(ctx, a);
@@ -408,9 +462,9 @@ int launch_typed(rsatb_context* ctx, int block_size, StepArgs& a) {
             if (st != kNotApplicable) return st;
         }
     }
-    // Measured choice (diamond 8x8 blocks, B200): FP64 takes the staged
-    // kernel at every width; FP32 takes the bulk-copy kernel from W = 32 up
-    // (above), the staged kernel for complex panels of W = 16 and the
+    // Measured choice (diamond 8x8 blocks, B200), after the tensor-core and
+    // bulk-copy kernels above: FP64 takes the staged kernel (other block
+    // sizes), FP32 the staged kernel for complex panels of W = 16 and the
     // register kernel otherwise.
     const bool want_staged =
         forced == 2 || (forced == 0 && (sizeof(VT) == 8 || (a.W == 16 && CV)));

@@ -297,12 +297,13 @@ NARROW = [(96, 8, 6, False, False, 8, False), (96, 8, 6, False, False, 4, True),
           (97, 8, 7, False, False, 256, False), (97, 8, 7, False, False, 2, True)]
 
 
-@pytest.mark.parametrize("kernel", ["staged", "rowsplit", "bulk", "bulk_smem", "narrow"])
+@pytest.mark.parametrize("kernel", ["staged", "rowsplit", "bulk", "bulk_smem", "narrow", "dmma"])
 @pytest.mark.parametrize("case", [c for c in CASES if c[1] in (1, 5, 8)] + NARROW)
 @pytest.mark.parametrize("precision", ["f64", "f32"])
 def test_kernel_variants_match_register_kernel(torch_cuda, case, precision, kernel, monkeypatch):
-    """The cp.async-staged, the row-split, the bulk-copy and the lock-step
-    narrow-panel step kernels against the register kernel, including the fused epilogue and
+    """The cp.async-staged, the row-split, the bulk-copy, the lock-step
+    narrow-panel and the FP64 tensor-core step kernels against the register
+    kernel, including the fused epilogue and
     dots (the row-split kernel sums in another order, hence a relative
     tolerance; the bulk-copy kernel keeps the register kernel's order per
     output and differs only in the FP64 dot reduction order)."""
