@@ -84,6 +84,15 @@ __global__ void __launch_bounds__(kBulkWarps * 32, MINB) cheb_step_bulk(StepArgs
         umma::fence_mbarrier_init();
     }
     __syncwarp();
+    if (a.wait_check) {
+        // Arm stage 0 for 16 bytes that no copy delivers: the bounded wait
+        // runs out, records the fault and the kernel leaves (no copy issued).
+        if (lane == 0) umma::mbar_arrive_expect_tx(&bars[warp][0], 16u);
+        __syncwarp();
+        const bool got = umma::mbar_wait(&bars[warp][0], 0u, 5000000ull);
+        if (!__all_sync(0xffffffffu, got) && lane == 0 && a.fault) atomicOr(a.fault, 1u);
+        return;
+    }
 
     // Producer: the item sequence (group, step) NS items ahead of the
     // consumer; pj holds the column block of the current producer item.

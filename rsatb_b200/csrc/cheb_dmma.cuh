@@ -34,18 +34,18 @@ __device__ __forceinline__ void dmma_884(double (&d)[2], double a, double b) {
                  : "d"(a), "d"(b));
 }
 
-// Blocks of a row loaded together: enough loads in flight at narrow panels,
-// registers bounded at wide ones.
-template <int W>
+// Blocks of a row loaded together (UU, 0: by width): enough loads in flight
+// at narrow panels, registers bounded at wide ones.
+template <int W, int UU = 0>
 struct DmmaShape {
     static constexpr int NG = W / 8;
-    static constexpr int U = W <= 16 ? 4 : (W <= 32 ? 2 : 1);
+    static constexpr int U = UU ? UU : (W <= 16 ? 4 : (W <= 32 ? 2 : 1));
 };
 
-template <typename VT, int W, bool CV>
+template <typename VT, int W, bool CV, int UU>
 __global__ void __launch_bounds__(kDmmaWarps * 32) cheb_step_dmma(StepArgs a) {
     static_assert(W % 8 == 0 && W <= 256, "8-column groups");
-    constexpr int NG = DmmaShape<W>::NG, U = DmmaShape<W>::U;
+    constexpr int NG = DmmaShape<W, UU>::NG, U = DmmaShape<W, UU>::U;
     __shared__ double dsm[kDmmaWarps][2][W];  // per warp: dots d0, d1 per column
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int fr = lane >> 2, fc = lane & 3;

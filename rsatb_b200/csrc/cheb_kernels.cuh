@@ -51,6 +51,8 @@ struct StepArgs {
     double* dots_out;  // [ndots][W]
     unsigned* counter;
     unsigned* fault;   // set non-zero by a kernel whose bounded wait gave up (null: none)
+    int wait_check;    // non-zero: the bulk-copy kernel only runs a wait that cannot
+                       // complete (a 5 ms limit), to check the fault report
 };
 
 template <typename VT, int V>

@@ -276,6 +276,10 @@ int launch_bulk_k(rsatb_context* ctx, StepArgs& a) {
 
 template <int W, bool CV>
 int launch_bulk_w(rsatb_context* ctx, StepArgs& a) {
+    // RSATB_TEST_BULK_WAIT=1: run only the wait that cannot complete (tests
+    // of the bounded-wait fault report).
+    const char* wc = std::getenv("RSATB_TEST_BULK_WAIT");
+    a.wait_check = (wc && wc[0] == '1') ? 1 : 0;
     const bool ns3 = bulk_stages() == 3;
     if (!bulk_x_global())
         return ns3 ? launch_bulk_k<W, CV, 3, false, 2>(ctx, a)
@@ -327,9 +331,17 @@ int launch_narrow_w(rsatb_context* ctx, StepArgs& a) {
                                 : launch_narrow_k<VT, W, CV, 2>(ctx, a);
 }
 
-template <typename VT, int W, bool CV>
-int launch_dmma_k(rsatb_context* ctx, StepArgs& a) {
-    auto kernel = cheb_step_dmma<VT, W, CV>;
+// Blocks of a row loaded together by the tensor-core kernel at W <= 32
+// (RSATB_DMMA_U: 2, 4 or 8; unset: by width).
+inline int dmma_u() {
+    const char* s = std::getenv("RSATB_DMMA_U");
+    const int u = s ? std::atoi(s) : 0;
+    return (u == 2 || u == 4 || u == 8) ? u : 0;
+}
+
+template <typename VT, int W, bool CV, int UU>
+int launch_dmma_u(rsatb_context* ctx, StepArgs& a) {
+    auto kernel = cheb_step_dmma<VT, W, CV, UU>;
     const int threads = kDmmaWarps * 32;
     const int64_t need = (a.n_block_rows + kDmmaWarps - 1) / kDmmaWarps;
     const int per_sm = occupancy(reinterpret_cast<const void*>(kernel), threads, 0);
@@ -340,6 +352,18 @@ int launch_dmma_k(rsatb_context* ctx, StepArgs& a) {
     kernel<<<unsigned(grid), threads, 0, ctx->stream>>>(a);
     RSATB_LAUNCH_CHECK(ctx);
     return RSATB_SUCCESS;
+}
+
+template <typename VT, int W, bool CV>
+int launch_dmma_k(rsatb_context* ctx, StepArgs& a) {
+    if constexpr (W <= 32) {
+        switch (dmma_u()) {
+            case 2: return launch_dmma_u<VT, W, CV, 2>(ctx, a);
+            case 4: return launch_dmma_u<VT, W, CV, 4>(ctx, a);
+            case 8: return launch_dmma_u<VT, W, CV, 8>(ctx, a);
+        }
+    }
+    return launch_dmma_u<VT, W, CV, 0>(ctx, a);
 }
 
 // Panels on the FP64 tensor cores: real 8x8 blocks, W a multiple of 8 up

@@ -355,3 +355,28 @@ def test_recurrence_graph_replay_matches_direct_run(torch_cuda, monkeypatch):
     for m in mus:
         assert np.array_equal(m, direct)
     assert len(set(counts)) == 1 and counts[0] == 1 + 48
+
+
+def test_bulk_kernel_bounded_wait_reports_fault(torch_cuda, monkeypatch):
+    """A bounded mbarrier wait that runs out (armed for bytes no copy
+    delivers) sets the context's fault word; rsatb_kpm_dos_moments then
+    fails with RSATB_CUDA_ERROR instead of hanging, and the context stays
+    usable: the next call returns the oracle's moments."""
+    torch = torch_cuda
+    from rsatb_b200._capi import RsatbError
+    from rsatb_b200.calc import kpm_dos_moments
+    A = random_hermitian_bsr(40, 8, 5, seed=3, complex_values=False, scale=0.2)
+    bound = np.abs(np.linalg.eigvalsh(A.to_dense())).max() + 0.5
+    c = build_cheby(A, -bound, bound, precision="f32")
+    X = np.random.default_rng(5).standard_normal((40 * 8, 16))
+    Xd = to_dev(torch, X, torch.float32)
+    monkeypatch.setenv("RSATB_STEP_KERNEL", "bulk")
+    monkeypatch.setenv("RSATB_TEST_BULK_WAIT", "1")
+    with pytest.raises(RsatbError, match="bounded wait"):
+        kpm_dos_moments(c, Xd, 8)
+    monkeypatch.delenv("RSATB_TEST_BULK_WAIT")
+    mu = kpm_dos_moments(c, Xd, 8)
+    monkeypatch.setenv("RSATB_STEP_KERNEL", "v1")
+    ref = kpm_dos_moments(c, Xd, 8)
+    assert np.all(np.isfinite(mu))
+    assert np.abs(mu - ref).max() <= 1e-6 * np.abs(ref).max()
