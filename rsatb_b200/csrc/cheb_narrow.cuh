@@ -55,7 +55,7 @@ __global__ void __launch_bounds__(kNarrowWarps * 32) cheb_step_narrow(StepArgs a
     using Sh = NarrowShape<VT, W>;
     constexpr int V = Sh::V, G = Sh::G, S = Sh::S;
     static_assert(!CV || V % 2 == 0, "complex panels need (re, im) pairs per lane");
-    extern __shared__ __align__(16) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned char* ring = smem + size_t(warp) * NS * Sh::STAGE;
     int2* table = reinterpret_cast<int2*>(smem + size_t(kNarrowWarps) * NS * Sh::STAGE) +
