@@ -55,19 +55,28 @@ struct StepArgs {
                        // complete (a 5 ms limit), to check the fault report
 };
 
-template <typename VT, int V>
+// Loads of V consecutive values.  CG = false: the read-only data path
+// (__ldg), for data no thread of the launch writes; CG = true: L2-coherent
+// loads (__ldcg), for data written earlier in the same launch.
+template <typename T, bool CG>
+__device__ __forceinline__ T ld_path(const T* p) {
+    if constexpr (CG) return __ldcg(p);
+    else return __ldg(p);
+}
+
+template <typename VT, int V, bool CG = false>
 __device__ __forceinline__ void load_vals(const VT* __restrict__ p, VT (&o)[V]) {
     if constexpr (sizeof(VT) == 8 && V % 2 == 0) {
 #pragma unroll
         for (int i = 0; i < V / 2; ++i) {
-            const double2 t = __ldg(reinterpret_cast<const double2*>(p) + i);
+            const double2 t = ld_path<double2, CG>(reinterpret_cast<const double2*>(p) + i);
             o[2 * i] = t.x;
             o[2 * i + 1] = t.y;
         }
     } else if constexpr (sizeof(VT) == 4 && V % 4 == 0) {
 #pragma unroll
         for (int i = 0; i < V / 4; ++i) {
-            const float4 t = __ldg(reinterpret_cast<const float4*>(p) + i);
+            const float4 t = ld_path<float4, CG>(reinterpret_cast<const float4*>(p) + i);
             o[4 * i] = t.x;
             o[4 * i + 1] = t.y;
             o[4 * i + 2] = t.z;
@@ -76,13 +85,13 @@ __device__ __forceinline__ void load_vals(const VT* __restrict__ p, VT (&o)[V]) 
     } else if constexpr (sizeof(VT) == 4 && V % 2 == 0) {
 #pragma unroll
         for (int i = 0; i < V / 2; ++i) {
-            const float2 t = __ldg(reinterpret_cast<const float2*>(p) + i);
+            const float2 t = ld_path<float2, CG>(reinterpret_cast<const float2*>(p) + i);
             o[2 * i] = t.x;
             o[2 * i + 1] = t.y;
         }
     } else {
 #pragma unroll
-        for (int i = 0; i < V; ++i) o[i] = __ldg(p + i);
+        for (int i = 0; i < V; ++i) o[i] = ld_path<VT, CG>(p + i);
     }
 }
 
@@ -132,8 +141,10 @@ __device__ __forceinline__ void fma_row(VT (&acc)[V], VT a, const VT (&x)[V]) {
     }
 }
 
-// Epilogue for one output row: rescale, recurrence, store, dots.
-template <typename VT, int V, bool CV>
+// Epilogue for one output row: rescale, recurrence, store, dots.  CG: the
+// x, p, q and psi0 panels are read through L2 (written earlier in the same
+// launch).
+template <typename VT, int V, bool CV, bool CG = false>
 __device__ __forceinline__ void finish_row(const StepArgs& a, int64_t row, int g,
                                            const VT (&acc)[V], double (&d0)[V],
                                            double (&d1)[V]) {
@@ -152,7 +163,7 @@ __device__ __forceinline__ void finish_row(const StepArgs& a, int64_t row, int g
     }
     VT xv[V];
     if (a.x) {
-        load_vals<VT, V>(static_cast<const VT*>(a.x) + off, xv);
+        load_vals<VT, V, CG>(static_cast<const VT*>(a.x) + off, xv);
     } else {
 #pragma unroll
         for (int v = 0; v < V; ++v) xv[v] = VT(0);
@@ -165,7 +176,7 @@ __device__ __forceinline__ void finish_row(const StepArgs& a, int64_t row, int g
     }
     if (a.p) {
         VT pv[V];
-        load_vals<VT, V>(static_cast<const VT*>(a.p) + off, pv);
+        load_vals<VT, V, CG>(static_cast<const VT*>(a.p) + off, pv);
 #pragma unroll
         for (int v = 0; v < V; ++v) t[v] = fma(a.s2, t[v], a.g_p * double(pv[v]));
     } else if (a.s2 != 1.0) {
@@ -174,7 +185,7 @@ __device__ __forceinline__ void finish_row(const StepArgs& a, int64_t row, int g
     }
     if (a.q) {
         VT qv[V];
-        load_vals<VT, V>(static_cast<const VT*>(a.q) + off, qv);
+        load_vals<VT, V, CG>(static_cast<const VT*>(a.q) + off, qv);
 #pragma unroll
         for (int v = 0; v < V; ++v) t[v] = fma(a.g_q, double(qv[v]), t[v]);
     }
@@ -204,7 +215,7 @@ __device__ __forceinline__ void finish_row(const StepArgs& a, int64_t row, int g
         }
     } else if (a.dot_mode == DOT_PLAIN) {
         VT qv[V];
-        load_vals<VT, V>(static_cast<const VT*>(a.psi0) + off, qv);
+        load_vals<VT, V, CG>(static_cast<const VT*>(a.psi0) + off, qv);
         if constexpr (CV) {
 #pragma unroll
             for (int v = 0; v < V; v += 2) {

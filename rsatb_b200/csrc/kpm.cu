@@ -3,6 +3,7 @@
 // driven from the host, computed on the device.
 #include "cheb_kernels.cuh"
 
+#include <algorithm>
 #include <cmath>
 #include <complex>
 #include <cstdlib>
@@ -17,6 +18,11 @@ int run_step(rsatb_context* ctx, const rsatb_bsr_matrix* A, int vdt, const StepA
     return dtype_is_double(vdt) ? launch_cheb_step_f64(ctx, A, vdt, b)
                                 : launch_cheb_step_f32(ctx, A, vdt, b);
 }
+
+int run_persistent_recurrence(rsatb_context* ctx, const rsatb_bsr_matrix* H, int vdt, int W,
+                              double center, double inv_hw, int doubled, const void* psi,
+                              void* const buf[3], int n_steps, double* part, size_t part_capacity,
+                              double* dots, unsigned* bar, unsigned* fault, bool* done);
 
 int run_coldot(rsatb_context* ctx, int vdt, int64_t n_rows, const StepArgs& a) {
     return dtype_is_double(vdt) ? launch_coldot_f64(ctx, vdt, n_rows, a)
@@ -335,7 +341,15 @@ int rsatb_kpm_dos_moments(rsatb_ctx_t ctx, const rsatb_cheb_op* op, const void* 
     const size_t part_bytes = round256(max_ctas * 2 * W * sizeof(double));
     const size_t dots_bytes = round256(size_t(n_steps + 1) * 2 * W * sizeof(double));
     const int n_panels = 3 + (sh.sandwich ? 2 : 0);
-    const size_t total = n_panels * vbytes + part_bytes + dots_bytes;
+    // Per-step, per-CTA dot slots of the persistent recurrence (small
+    // scalar-block operators; at most one CTA of 256 threads per 64 rows).
+    const bool small_csr = !sh.sandwich && op->H->block_size == 1 && n_steps > 0 &&
+                           int64_t(sh.n_rows) * W <= (int64_t(1) << 22);
+    const size_t persist_grid =
+        std::min<size_t>(size_t(ctx->sm_count) * 8, size_t(sh.n_rows) * W / 256 + 1);
+    const size_t persist_elems = small_csr ? size_t(n_steps + 1) * persist_grid * 2 * W : 0;
+    const size_t persist_bytes = round256(persist_elems * sizeof(double));
+    const size_t total = n_panels * vbytes + part_bytes + dots_bytes + persist_bytes;
     void* s = nullptr;
     RSATB_TRY(ctx_scratch(ctx, total, &s));
     char* base = static_cast<char*>(s);
@@ -344,8 +358,18 @@ int rsatb_kpm_dos_moments(rsatb_ctx_t ctx, const rsatb_cheb_op* op, const void* 
     void* w = sh.sandwich ? base + 4 * vbytes : nullptr;
     double* partials = reinterpret_cast<double*>(base + n_panels * vbytes);
     double* dots = reinterpret_cast<double*>(base + n_panels * vbytes + part_bytes);
+    double* persist_part =
+        reinterpret_cast<double*>(base + n_panels * vbytes + part_bytes + dots_bytes);
     unsigned* counter = nullptr;
-    RSATB_TRY(ctx_counters(ctx, 1, &counter));
+    RSATB_TRY(ctx_counters(ctx, 2, &counter));
+    unsigned* fault_word = nullptr;
+    RSATB_TRY(ctx_fault_word(ctx, &fault_word));
+    bool persistent = false;
+    if (small_csr)
+        RSATB_TRY(run_persistent_recurrence(ctx, op->H, vec_dtype, W, op->center,
+                                            1.0 / op->half_width, doubled, psi, buf, n_steps,
+                                            persist_part, persist_elems, dots, counter + 1,
+                                            fault_word, &persistent));
 
     // The recurrence: mu_0 = <psi|psi> per column, then psi_1 = Op~ psi_0 and
     // psi_s = 2 Op~ psi_{s-1} - psi_{s-2}, each step with its fused dots.
@@ -376,8 +400,9 @@ int rsatb_kpm_dos_moments(rsatb_ctx_t ctx, const rsatb_cheb_op* op, const void* 
         }
         return RSATB_SUCCESS;
     };
-    RSATB_TRY(run_recurrence(ctx, op, psi, n_vectors, vec_dtype, n_moments, doubled, s,
-                             counter, n_steps, issue));
+    if (!persistent)
+        RSATB_TRY(run_recurrence(ctx, op, psi, n_vectors, vec_dtype, n_moments, doubled, s,
+                                 counter, n_steps, issue));
 
     std::vector<double> h(size_t(n_steps + 1) * 2 * W);
     RSATB_CUDA_TRY(cudaMemcpyAsync(h.data(), dots, sizeof(double) * h.size(),

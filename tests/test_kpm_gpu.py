@@ -338,6 +338,7 @@ def test_recurrence_graph_replay_matches_direct_run(torch_cuda, monkeypatch):
     """The second identical call captures the recurrence as a CUDA graph and
     later ones replay it: same moments bit for bit, same launch count."""
     torch = torch_cuda
+    monkeypatch.setenv("RSATB_NO_PERSIST", "1")  # the small-operator path is one launch
     from rsatb_b200.calc import kpm_dos_moments
     from rsatb_b200.vbcsr import set_random
     H = graphene_case(16, 16)
@@ -380,3 +381,32 @@ def test_bulk_kernel_bounded_wait_reports_fault(torch_cuda, monkeypatch):
     ref = kpm_dos_moments(c, Xd, 8)
     assert np.all(np.isfinite(mu))
     assert np.abs(mu - ref).max() <= 1e-6 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("precision,doubled", [("f64", True), ("f64", False), ("f32", True)])
+def test_persistent_recurrence_matches_graph_path(torch_cuda, monkeypatch, precision, doubled):
+    """Small scalar-block operators run the whole recurrence as one
+    cooperative launch (grid barriers between steps); its moments match the
+    per-step path to rounding (only the order of the FP64 dot sums differs)
+    and the oracle, in two launches per call."""
+    torch = torch_cuda
+    from rsatb_b200.calc import kpm_dos_moments, kpm_dos_moments_plain
+    from rsatb_b200.vbcsr import set_random
+    H = graphene_case(12, 10)
+    c = build_cheby(H, -9.0, 9.0, precision=precision)
+    dt = torch.complex128 if precision == "f64" else torch.complex64
+    psi = torch.empty(H.n_rows, 8, dtype=dt, device="cuda")
+    set_random(psi, 11)
+    run = kpm_dos_moments if doubled else kpm_dos_moments_plain
+    ctx = c.H.ctx
+    l0 = ctx.launch_count()
+    mu_p = run(c, psi, 64)
+    assert ctx.launch_count() - l0 == 2
+    monkeypatch.setenv("RSATB_NO_PERSIST", "1")
+    mu_g = run(c, psi, 64)
+    tol = 1e-12 if precision == "f64" else 1e-6
+    assert np.abs(mu_p - mu_g).max() <= tol * np.abs(mu_g).max()
+    if precision == "f64":
+        want = oracle.kpm_moments(oracle_op(H, -9.0, 9.0), psi.cpu().numpy(), 64,
+                                  doubled=doubled)
+        assert _moment_err(mu_p, want) < 1e-10
