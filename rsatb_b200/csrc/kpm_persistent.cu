@@ -118,6 +118,27 @@ __global__ void __launch_bounds__(256) kpm_persistent_kernel(PersistArgs pa) {
         cta_partials<V>(W, L, 1, d0, d1, red, pa.part + size_t(blockIdx.x) * 2 * W);
     }
 
+    // When every thread owns one row of at most kCache nonzeros (the grid
+    // covers all rows), its column indices and values stay in registers for
+    // the whole recurrence.
+    constexpr int kCache = 8;
+    const bool one_row = total <= stride;
+    int nk = -1;
+    int64_t cj[kCache];
+    VT cv[kCache];
+    if (one_row && t0 < total) {
+        const int64_t i = t0 / L;
+        const int k0 = __ldg(b.row_ptr + i), k1 = __ldg(b.row_ptr + i + 1);
+        if (k1 - k0 <= kCache) {
+            nk = k1 - k0;
+#pragma unroll
+            for (int q = 0; q < kCache; ++q) {
+                cj[q] = q < nk ? __ldg(b.col_ind + k0 + q) : 0;
+                cv[q] = q < nk ? __ldg(vals + k0 + q) : VT(0);
+            }
+        }
+    }
+
     const VT* prev = nullptr;
     const VT* cur = static_cast<const VT*>(pa.psi);
     int bi = 0;
@@ -134,20 +155,35 @@ __global__ void __launch_bounds__(256) kpm_persistent_kernel(PersistArgs pa) {
         double d0[V], d1[V];
 #pragma unroll
         for (int v = 0; v < V; ++v) d0[v] = d1[v] = 0.0;
-        for (int64_t t = t0; t < total; t += stride) {
-            const int64_t i = t / L;
+        if (nk >= 0) {
+            const int64_t i = t0 / L;
             VT acc[V];
 #pragma unroll
             for (int v = 0; v < V; ++v) acc[v] = VT(0);
-            const int k0 = __ldg(b.row_ptr + i), k1 = __ldg(b.row_ptr + i + 1);
-            for (int k = k0; k < k1; ++k) {
-                const int64_t j = __ldg(b.col_ind + k);
-                const VT av = __ldg(vals + k);
-                VT xv[V];
-                load_vals<VT, V, true>(cur + j * W + int64_t(g) * V, xv);
-                fma_row<VT, V>(acc, av, xv);
-            }
+            VT xv[kCache][V];
+#pragma unroll
+            for (int q = 0; q < kCache; ++q)
+                if (q < nk) load_vals<VT, V, true>(cur + cj[q] * W + int64_t(g) * V, xv[q]);
+#pragma unroll
+            for (int q = 0; q < kCache; ++q)
+                if (q < nk) fma_row<VT, V>(acc, cv[q], xv[q]);
             finish_row<VT, V, CV, true>(a, i, g, acc, d0, d1);
+        } else {
+            for (int64_t t = t0; t < total; t += stride) {
+                const int64_t i = t / L;
+                VT acc[V];
+#pragma unroll
+                for (int v = 0; v < V; ++v) acc[v] = VT(0);
+                const int k0 = __ldg(b.row_ptr + i), k1 = __ldg(b.row_ptr + i + 1);
+                for (int k = k0; k < k1; ++k) {
+                    const int64_t j = __ldg(b.col_ind + k);
+                    const VT av = __ldg(vals + k);
+                    VT xv[V];
+                    load_vals<VT, V, true>(cur + j * W + int64_t(g) * V, xv);
+                    fma_row<VT, V>(acc, av, xv);
+                }
+                finish_row<VT, V, CV, true>(a, i, g, acc, d0, d1);
+            }
         }
         cta_partials<V>(W, L, ndots, d0, d1, red,
                         pa.part + size_t(s) * slot + size_t(blockIdx.x) * 2 * W);
@@ -186,6 +222,12 @@ int launch_persistent(rsatb_context* ctx, PersistArgs pa, int64_t n_rows, double
     int64_t grid = int64_t(ctx->sm_count) * per_sm;
     const int64_t need = (n_rows * L + threads - 1) / threads;
     if (need < grid) grid = need;
+    // RSATB_PERSIST_CTAS caps the CTA count (fewer CTAs: cheaper barriers,
+    // more rows per thread).
+    if (const char* cap = std::getenv("RSATB_PERSIST_CTAS")) {
+        const int64_t c = std::atoll(cap);
+        if (c > 0 && c < grid) grid = c;
+    }
     if (grid < 1) grid = 1;
     if (size_t(pa.n_steps + 1) * size_t(grid) * 2 * pa.base.W > part_capacity)
         return kPersistSkipped;  // the caller's slots were sized for fewer CTAs
