@@ -29,7 +29,13 @@
 
 namespace rsatb_b200 {
 
-constexpr int kDmmaWarps = 4;
+// Warps per CTA: 8 for FP32 panels (neighbouring block rows of one CTA
+// share their gathered X_j lines in L1: FP32 R = 8 0.080 -> 0.062 ms on the
+// diamond 8x8 BSR), 4 for FP64 (more warps measured slower at R = 128).
+template <typename VT>
+constexpr int dmma_warps() {
+    return sizeof(VT) == 4 ? 8 : 4;
+}
 
 __device__ __forceinline__ void dmma_884(double (&d)[2], double a, double b) {
     asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
@@ -46,7 +52,8 @@ struct DmmaShape {
 };
 
 template <typename VT, int W, bool CV, int UU>
-__global__ void __launch_bounds__(kDmmaWarps * 32) cheb_step_dmma(StepArgs a) {
+__global__ void __launch_bounds__(dmma_warps<VT>() * 32) cheb_step_dmma(StepArgs a) {
+    constexpr int kDmmaWarps = dmma_warps<VT>();
     static_assert(W % 8 == 0 && W <= 256, "8-column groups");
     constexpr int NG = DmmaShape<W, UU>::NG, U = DmmaShape<W, UU>::U;
     // 16-column spans with 2-value X loads: FP64 panels (measured at FP32

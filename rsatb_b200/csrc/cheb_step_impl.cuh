@@ -342,8 +342,9 @@ inline int dmma_u() {
 template <typename VT, int W, bool CV, int UU>
 int launch_dmma_u(rsatb_context* ctx, StepArgs& a) {
     auto kernel = cheb_step_dmma<VT, W, CV, UU>;
-    const int threads = kDmmaWarps * 32;
-    const int64_t need = (a.n_block_rows + kDmmaWarps - 1) / kDmmaWarps;
+    constexpr int kWarps = dmma_warps<VT>();
+    const int threads = kWarps * 32;
+    const int64_t need = (a.n_block_rows + kWarps - 1) / kWarps;
     const int per_sm = occupancy(reinterpret_cast<const void*>(kernel), threads, 0);
     int64_t grid = int64_t(ctx->sm_count) * per_sm;
     if (grid > int64_t(ctx->sm_count) * 8) grid = int64_t(ctx->sm_count) * 8;
