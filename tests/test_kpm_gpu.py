@@ -71,6 +71,11 @@ CASES = [
     (200, 1, 8, False, True, 48, True),
     (50, 5, 4, True, False, 2, True),
     (40, 8, 5, True, False, 8, True),
+    # imaginary-unit 8x8 blocks on complex panels: W = 16 and 32 (the
+    # tensor-core and bulk-copy kernels), W = 256 (paired tensor-core loads)
+    (40, 8, 5, False, True, 8, True),
+    (40, 8, 5, False, True, 16, True),
+    (33, 8, 4, False, True, 128, True),
 ]
 
 
