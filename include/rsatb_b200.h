@@ -278,8 +278,13 @@ typedef struct {
  * samples.  Vx, Vy, Vz: velocity matrices (RSATB_BSR_IMAGINARY_UNIT for the
  * i*W of a real k-point, or complex), H's shape and precision.  psi: device
  * N x n_vectors complex (C128, or C64 for FP32 vectors; the transform and
- * the contraction are FP64 either way).  formulation 0 (Greenwood) only;
- * partition_sections > 0 asks for at least that many row sections,
+ * the contraction are FP64 either way).  formulation 0 Greenwood, 1
+ * Bastin: beside phi3 the zero-padded 2M-point inverse FFTs phi1, phi2 of
+ * the moments times the complex phase weights (:443-461), all six (a, b)
+ * components of eps (conj(L3_a) R1_b + conj(L1_a) R3_b) + i sqrt(1 - eps^2)
+ * (conj(L2_a) R3_b - conj(L3_a) R2_b) (:496-519), then the cumulative
+ * trapezoid of Re(i zeta) over the ascending grid: sigma(mu, T = 0)
+ * (:635-659).  partition_sections > 0 asks for at least that many row sections,
  * max_workspace_bytes bounds the device memory (0: 80 % of what is free).
  * sigma_out (host) receives n_moments x 6 (xx xy xz yy yz zz; Greenwood
  * fills xx, yy, zz) scaled by prefactor, energy_out (host) the ascending

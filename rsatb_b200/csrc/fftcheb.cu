@@ -1,6 +1,6 @@
 // FFT-Chebyshev Kubo-Greenwood transport on the device: the
 // dc_spectrum_fftcheb / accumulate_fftcheb_block path of
-// rsatb/calc/fftcheb_transport.hpp:270-660 with the Greenwood formulation.
+// rsatb/calc/fftcheb_transport.hpp:270-660, Greenwood and Bastin formulations.
 //
 // Per sample block (all R samples at once) and per section of rows:
 //   left chain   l_m = T_m(Op~) psi,          stored as J_a l_m for a = x, y, z
@@ -104,6 +104,81 @@ __global__ void extend_kernel(int M, int64_t nq, int chunk_rows, int R, int64_t 
             E[int64_t(2 * M - m) * nq + q] = make_double2(xr * c + xi * sn, -xr * sn + xi * c);
         }
     }
+}
+
+// Bastin phi1 / phi2 inputs (fftcheb_transport.hpp:453-461, fft.hpp:156-174):
+// the weighted moments w[m] S_m (complex w) in the first M points of a
+// 2M-point sequence, zeros in the last M.  Layout as extend_kernel.
+template <typename T>
+__global__ void pad_kernel(int M, int64_t nq, int chunk_rows, int R, int64_t sec_rows,
+                           int64_t row_off, int64_t slot_elems, const T* S, const double2* w,
+                           double2* E) {
+    const int m = blockIdx.y;
+    const double2 wm = w[m];
+    for (int64_t q = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; q < nq;
+         q += int64_t(gridDim.x) * blockDim.x) {
+        const int s = int(q % R);
+        const int64_t row = (q / R) % chunk_rows;
+        const int a = int(q / (int64_t(chunk_rows) * R));
+        const int64_t src = int64_t(m) * slot_elems + (a * sec_rows + row_off + row) * R + s;
+        const double xr = double(S[2 * src]), xi = double(S[2 * src + 1]);
+        E[int64_t(m) * nq + q] = make_double2(wm.x * xr - wm.y * xi, wm.x * xi + wm.y * xr);
+        E[int64_t(M + m) * nq + q] = make_double2(0.0, 0.0);
+    }
+}
+
+// Bastin kernel accumulation (fftcheb_transport.hpp:496-519): for energy k
+// (one CTA) and every component (a, b), a <= b,
+//   K[k][ab] += sum over rows, samples of
+//     eps_k (conj(L3_a) R1_b + conj(L1_a) R3_b)
+//     + i sqrt(1 - eps_k^2) (conj(L2_a) R3_b - conj(L3_a) R2_b),
+// summed per thread, then in a fixed tree order (deterministic).
+__global__ void __launch_bounds__(256) bastin_contract_kernel(int M, int64_t nq, int64_t per_axis,
+                                                              const double2* L3, const double2* R3,
+                                                              const double2* L1, const double2* R1,
+                                                              const double2* L2, const double2* R2,
+                                                              double* K) {
+    const int k = blockIdx.x;
+    const double th = M_PI * (double(k) + 0.5) / double(M);
+    const double eps = cos(th), root = sin(th);
+    __shared__ double red[12][256];
+    double acc[6][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}, {0, 0}, {0, 0}};
+    const int64_t o = int64_t(k) * nq;
+    // conj(x) y, accumulated into (re, im)
+    auto cmac = [](double (&d)[2], double2 x, double2 y, double f_re, double f_im) {
+        const double re = x.x * y.x + x.y * y.y, im = x.x * y.y - x.y * y.x;
+        d[0] += f_re * re - f_im * im;
+        d[1] += f_re * im + f_im * re;
+    };
+    for (int64_t q = threadIdx.x; q < per_axis; q += blockDim.x) {
+        int comp = 0;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const double2 l3 = L3[o + a * per_axis + q], l1 = L1[o + a * per_axis + q],
+                          l2 = L2[o + a * per_axis + q];
+#pragma unroll
+            for (int b = a; b < 3; ++b, ++comp) {
+                const double2 r3 = R3[o + b * per_axis + q], r1 = R1[o + b * per_axis + q],
+                              r2 = R2[o + b * per_axis + q];
+                cmac(acc[comp], l3, r1, eps, 0.0);
+                cmac(acc[comp], l1, r3, eps, 0.0);
+                cmac(acc[comp], l2, r3, 0.0, root);
+                cmac(acc[comp], l3, r2, 0.0, -root);
+            }
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+        red[2 * c][threadIdx.x] = acc[c][0];
+        red[2 * c + 1][threadIdx.x] = acc[c][1];
+    }
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w)
+            for (int c = 0; c < 12; ++c) red[c][threadIdx.x] += red[c][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x < 12) K[int64_t(k) * 12 + threadIdx.x] += red[threadIdx.x][0];
 }
 
 // K[k][a] += sum over the chunk's (row, s) of conj(L3[k][q]) R3[k][q] /
@@ -264,8 +339,10 @@ unsigned grid_for(int64_t n, int sm) {
 
 template <typename T>
 int fftcheb_impl(const Ctx& c, const rsatb_bsr_matrix* const* V, const T* psi, int R, int M,
-                 double prefactor, int sections, size_t workspace, int kernel, double* sigma_out,
-                 double* energy_out, rsatb_fftcheb_stats* stats) {
+                 int formulation, double prefactor, int sections, size_t workspace, int kernel,
+                 double* sigma_out, double* energy_out, rsatb_fftcheb_stats* stats) {
+    const bool bastin = formulation == 1;
+    const int n_tf = bastin ? 3 : 1;  // transforms per side and row: phi3 (+ phi1, phi2)
     rsatb_context* ctx = c.ctx;
     cudaStream_t st = ctx->stream;
     const int b = c.op->H->block_size;
@@ -291,7 +368,8 @@ int fftcheb_impl(const Ctx& c, const rsatb_bsr_matrix* const* V, const T* psi, i
     // quarter of what remains after the fixed buffers.
     const size_t avail = workspace - fixed;
     const size_t fft_budget = avail / 4;
-    const size_t fft_per_row = 2 * 2 * size_t(M) * 3 * R * sizeof(double2) * 2;  // + cuFFT work
+    const size_t fft_per_row =
+        size_t(n_tf) * 2 * 2 * size_t(M) * 3 * R * sizeof(double2) * 2;  // + cuFFT work
     int64_t chunk_rows = int64_t(fft_budget / fft_per_row);
     if (chunk_rows < 1) chunk_rows = 1;
     int64_t sec_brows = int64_t((avail - fft_budget) / store_per_brow);
@@ -319,9 +397,11 @@ int fftcheb_impl(const Ctx& c, const rsatb_bsr_matrix* const* V, const T* psi, i
     const int64_t slot = 3 * sec_rows_max * R;  // complex entries per moment slot
     RSATB_TRY(bS.alloc(2 * size_t(M) * slot * cplx));
     const int64_t nq_max = 3 * chunk_rows * R;
-    RSATB_TRY(bE.alloc(2 * 2 * size_t(M) * nq_max * sizeof(double2)));
+    RSATB_TRY(bE.alloc(size_t(n_tf) * 2 * 2 * size_t(M) * nq_max * sizeof(double2)));
     RSATB_TRY(bK.alloc(size_t(M) * 12 * sizeof(double)));
     RSATB_TRY(bWts.alloc(size_t(M) * sizeof(double)));
+    DevBuf bPw;
+    if (bastin) RSATB_TRY(bPw.alloc(2 * size_t(M) * sizeof(double2)));
     T* J[3];
     for (int a = 0; a < 3; ++a) J[a] = bJ.as<T>() + size_t(a) * N * 2 * R;
     T* rinit = bRinit.as<T>();
@@ -335,6 +415,11 @@ int fftcheb_impl(const Ctx& c, const rsatb_bsr_matrix* const* V, const T* psi, i
     T* SR = SL + 2 * size_t(M) * slot;
     double2* EL = bE.as<double2>();
     double2* ER = EL + 2 * size_t(M) * nq_max;
+    // Bastin: phi1 and phi2 of both sides follow.
+    double2* EL1 = bastin ? ER + 2 * size_t(M) * nq_max : nullptr;
+    double2* ER1 = bastin ? EL1 + 2 * size_t(M) * nq_max : nullptr;
+    double2* EL2 = bastin ? ER1 + 2 * size_t(M) * nq_max : nullptr;
+    double2* ER2 = bastin ? EL2 + 2 * size_t(M) * nq_max : nullptr;
     double* K = bK.as<double>();
 
     std::vector<double> g(M), wts(M);
@@ -342,6 +427,20 @@ int fftcheb_impl(const Ctx& c, const rsatb_bsr_matrix* const* V, const T* psi, i
     for (int m = 0; m < M; ++m) wts[m] = g[m] / M_PI;  // phi3_weight (fftcheb_transport.hpp)
     RSATB_CUDA_TRY(cudaMemcpyAsync(bWts.p, wts.data(), M * sizeof(double),
                                    cudaMemcpyHostToDevice, st));
+    // Bastin phase weights (fftcheb_transport.hpp:302-310): phase_weight[m] =
+    // 2 g_m / (pi (1 + [m == 0])) e^{i pi m / 2M}, phase_weight_m = m times it.
+    std::vector<double2> pw;
+    if (bastin) {
+        pw.resize(2 * size_t(M));
+        for (int m = 0; m < M; ++m) {
+            const double coeff = 2.0 * g[m] / (M_PI * (1.0 + (m == 0 ? 1.0 : 0.0)));
+            const double th = M_PI * double(m) / (2.0 * double(M));
+            pw[m] = make_double2(coeff * std::cos(th), coeff * std::sin(th));
+            pw[M + m] = make_double2(pw[m].x * double(m), pw[m].y * double(m));
+        }
+        RSATB_CUDA_TRY(cudaMemcpyAsync(bPw.p, pw.data(), pw.size() * sizeof(double2),
+                                       cudaMemcpyHostToDevice, st));
+    }
     RSATB_CUDA_TRY(cudaMemsetAsync(K, 0, size_t(M) * 12 * sizeof(double), st));
 
     // cuFFT plans: full chunks and the last, shorter chunk of a section.
@@ -464,8 +563,27 @@ int fftcheb_impl(const Ctx& c, const rsatb_bsr_matrix* const* V, const T* psi, i
             RSATB_CUFFT_TRY(cufftExecZ2Z(plan, reinterpret_cast<cufftDoubleComplex*>(ER),
                                          reinterpret_cast<cufftDoubleComplex*>(ER),
                                          CUFFT_INVERSE));
-            greenwood_contract_kernel<<<M, 256, 0, st>>>(M, nq, cr * R, EL, ER, K);
-            RSATB_LAUNCH_CHECK(ctx);
+            if (!bastin) {
+                greenwood_contract_kernel<<<M, 256, 0, st>>>(M, nq, cr * R, EL, ER, K);
+                RSATB_LAUNCH_CHECK(ctx);
+            } else {
+                const double2* w1 = bPw.as<double2>();
+                const double2* w2 = w1 + M;
+                double2* dst[4] = {EL1, ER1, EL2, ER2};
+                const T* src[4] = {SL, SR, SL, SR};
+                const double2* wt[4] = {w1, w1, w2, w2};
+                for (int t = 0; t < 4; ++t) {
+                    pad_kernel<T><<<grid, 256, 0, st>>>(M, nq, int(cr), R, rows, c0, sslot,
+                                                        src[t], wt[t], dst[t]);
+                    RSATB_LAUNCH_CHECK(ctx);
+                    RSATB_CUFFT_TRY(cufftExecZ2Z(plan, reinterpret_cast<cufftDoubleComplex*>(dst[t]),
+                                                 reinterpret_cast<cufftDoubleComplex*>(dst[t]),
+                                                 CUFFT_INVERSE));
+                }
+                bastin_contract_kernel<<<M, 256, 0, st>>>(M, nq, cr * R, EL, ER, EL1, ER1, EL2,
+                                                          ER2, K);
+                RSATB_LAUNCH_CHECK(ctx);
+            }
             ++chunks;
         }
         RSATB_CUDA_TRY(cudaEventRecord(ev1, st));
@@ -484,8 +602,27 @@ int fftcheb_impl(const Ctx& c, const rsatb_bsr_matrix* const* V, const T* psi, i
         const int src = M - 1 - k;
         energy_out[k] = c.op->center +
                         c.op->half_width * std::cos(M_PI * (double(src) + 0.5) / double(M));
-        for (int comp = 0; comp < 6; ++comp)
-            sigma_out[k * 6 + comp] = prefactor * Kh[2 * (size_t(src) * 6 + comp)] / double(R);
+        if (!bastin)
+            for (int comp = 0; comp < 6; ++comp)
+                sigma_out[k * 6 + comp] = prefactor * Kh[2 * (size_t(src) * 6 + comp)] / double(R);
+    }
+    if (bastin) {
+        // sigma(mu, T = 0): cumulative trapezoid of Re(i zeta(eps)) over the
+        // ascending Chebyshev grid (fftcheb_transport.hpp:635-659), zeta the
+        // sample-averaged kernel.
+        double running[6] = {0, 0, 0, 0, 0, 0}, prev[6] = {0, 0, 0, 0, 0, 0};
+        double eps_prev = 0.0;
+        for (int k = 0; k < M; ++k) {
+            const int src = M - 1 - k;
+            const double eps = std::cos(M_PI * (double(src) + 0.5) / double(M));
+            for (int comp = 0; comp < 6; ++comp) {
+                const double integrand = -Kh[2 * (size_t(src) * 6 + comp) + 1] / double(R);
+                if (k > 0) running[comp] += 0.5 * (prev[comp] + integrand) * (eps - eps_prev);
+                sigma_out[k * 6 + comp] = prefactor * running[comp];
+                prev[comp] = integrand;
+            }
+            eps_prev = eps;
+        }
     }
     if (stats) {
         stats->sections = n_sections;
@@ -539,18 +676,18 @@ extern "C" int rsatb_dc_spectrum_fftcheb(rsatb_ctx_t ctx, const rsatb_cheb_op* o
     if (6 * n_vectors > 1536)
         return set_error(RSATB_NOT_SUPPORTED, "%d samples exceed one block (256 at most)",
                          n_vectors);
-    if (formulation != 0)
-        return set_error(RSATB_NOT_SUPPORTED,
-                         "formulation %d: only Greenwood (0) runs on the device", formulation);
+    if (formulation != 0 && formulation != 1)
+        return set_error(RSATB_INVALID_ARGUMENT,
+                         "formulation %d: 0 (Greenwood) or 1 (Bastin)", formulation);
     if (!aligned16(psi)) return set_error(RSATB_INVALID_ARGUMENT, "psi must be 16-byte aligned");
     if (stats) *stats = rsatb_fftcheb_stats{};
     const rsatb_bsr_matrix* V[3] = {Vx, Vy, Vz};
     Ctx c{ctx, op, sandwich, int(vec_dtype)};
     if (dtype_is_double(vec_dtype))
         return fftcheb_impl<double>(c, V, static_cast<const double*>(psi), n_vectors, n_moments,
-                                    prefactor, partition_sections, max_workspace_bytes, kernel,
-                                    sigma_out, energy_out, stats);
+                                    formulation, prefactor, partition_sections,
+                                    max_workspace_bytes, kernel, sigma_out, energy_out, stats);
     return fftcheb_impl<float>(c, V, static_cast<const float*>(psi), n_vectors, n_moments,
-                               prefactor, partition_sections, max_workspace_bytes, kernel,
-                               sigma_out, energy_out, stats);
+                               formulation, prefactor, partition_sections, max_workspace_bytes,
+                               kernel, sigma_out, energy_out, stats);
 }

@@ -30,7 +30,9 @@ def dc_spectrum_fftcheb(cheby: Chebyshev, Vx: BlockSpMat, Vy: BlockSpMat, Vz: Bl
                         max_workspace_mb: float = 0.0, kernel: KpmKernel = KpmKernel.Jackson,
                         return_stats: bool = False):
     """Returns (sigma[n_moments, 6], energy[n_moments]) and, with
-    return_stats, the call's counters.  psi: (N, R) complex CUDA tensor
+    return_stats, the call's counters.  Greenwood: the zero-temperature
+    sigma(E) (diagonal components); Bastin: sigma(mu, T = 0), the cumulative
+    energy integral of the six-component zeta kernel.  psi: (N, R) complex CUDA tensor
     (complex128, or complex64 for FP32 vectors)."""
     if n_moments <= 0:
         raise ValueError("n_moments must be positive")
@@ -38,8 +40,8 @@ def dc_spectrum_fftcheb(cheby: Chebyshev, Vx: BlockSpMat, Vy: BlockSpMat, Vz: Bl
         raise ValueError("psi must be a contiguous (N, R) complex CUDA tensor")
     if psi.shape[0] != cheby.n_rows:
         raise ValueError("psi rows differ from the operator size")
-    if formulation != GREENWOOD:
-        raise NotImplementedError("only the Greenwood formulation runs on the GPU")
+    if formulation not in (GREENWOOD, BASTIN):
+        raise ValueError("formulation must be GREENWOOD (0) or BASTIN (1)")
     ctx = cheby.H.ctx
     ctx.bind_stream()
     op = cheby.c_op()

@@ -59,14 +59,15 @@ def _gpu(torch, H, V, psi, M, emin, emax, precision="f64", Z=None, **kw):
     return dc_spectrum_fftcheb(c, *Vd, p, M, return_stats=True, **kw)
 
 
-def _oracle(H, V, psi, M, emin, emax, Z=None, sections=1):
+def _oracle(H, V, psi, M, emin, emax, Z=None, sections=1, formulation=0):
     c, hw = (emax + emin) / 2, (emax - emin) / 2
     if Z is None:
         op = oracle.make_op(to_oracle(H), c, hw)
     else:
         op = oracle.make_op(to_oracle(H), c, hw, to_oracle(Z), to_oracle(adjoint_arrays(Z)))
     Vo = [to_oracle(v, imag=True) for v in V]
-    return oracle.fftcheb(op, Vo, psi, M, formulation=0, prefactor=1.0, sections=sections)
+    return oracle.fftcheb(op, Vo, psi, M, formulation=formulation, prefactor=1.0,
+                          sections=sections)
 
 
 @pytest.mark.parametrize("M", [1, 2, 17, 64])
@@ -137,7 +138,34 @@ def test_graphene_is_isotropic_in_plane(torch_cuda):
     assert rel_err(yy, xx) < 0.3   # stochastic trace with 8 samples
 
 
-def test_bastin_and_bad_arguments_refused(torch_cuda):
+@pytest.mark.parametrize("M", [1, 2, 17, 48])
+def test_bastin_matches_oracle_tbg(torch_cuda, M):
+    """Bastin: phi1, phi2 (zero-padded inverse FFTs with the complex phase
+    weights) beside phi3, all six tensor components, then the cumulative
+    energy integral (fftcheb_transport.hpp:443-519, 635-659)."""
+    H, V = _tbg()
+    emin, emax = _bounds(H)
+    psi = _phases(H.n_rows, 3, seed=7)
+    sig, en, _ = _gpu(torch_cuda, H, V, psi, M, emin, emax, formulation=1)
+    sig_o, en_o = _oracle(H, V, psi, M, emin, emax, formulation=1)
+    assert np.allclose(en, en_o, rtol=0, atol=1e-13)
+    assert rel_err(sig, sig_o) < 1e-10
+
+
+def test_bastin_sections_and_fp32(torch_cuda):
+    H, V = _tbg()
+    emin, emax = _bounds(H)
+    psi = _phases(H.n_rows, 2, seed=2)
+    s1, _, _ = _gpu(torch_cuda, H, V, psi, 32, emin, emax, formulation=1)
+    s3, _, st3 = _gpu(torch_cuda, H, V, psi, 32, emin, emax, formulation=1,
+                      partition_sections=3, max_workspace_mb=6.0)
+    s32, _, _ = _gpu(torch_cuda, H, V, psi, 32, emin, emax, formulation=1, precision="f32")
+    assert st3["sections"] >= 3
+    assert rel_err(s3, s1) < 1e-12
+    assert rel_err(s32, s1) < 1e-4
+
+
+def test_bad_arguments_refused(torch_cuda):
     from rsatb_b200._capi import RsatbError
     from rsatb_b200.calc import Chebyshev
     from rsatb_b200.transport import dc_spectrum_fftcheb
@@ -145,7 +173,7 @@ def test_bastin_and_bad_arguments_refused(torch_cuda):
     c = Chebyshev(_dev(H), -10, 10)
     Vd = [_dev(v, imaginary=True) for v in V]
     p = torch_cuda.as_tensor(_phases(H.n_rows, 1)).cuda()
-    with pytest.raises(NotImplementedError):
-        dc_spectrum_fftcheb(c, *Vd, p, 8, formulation=1)
+    with pytest.raises(ValueError):
+        dc_spectrum_fftcheb(c, *Vd, p, 8, formulation=2)
     with pytest.raises(RsatbError):   # FP32 vectors with FP64 matrices
         dc_spectrum_fftcheb(c, *Vd, p.to(torch_cuda.complex64), 8)
