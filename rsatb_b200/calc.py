@@ -141,6 +141,33 @@ class Chebyshev:
                                         dtype_code(X.dtype)))
         return Y
 
+    def apply_dual(self, V: BlockSpMat, X: torch.Tensor, Y: torch.Tensor,
+                   mode: ChebyMode = ChebyMode.NORMAL, scale: float = 1.0) -> torch.Tensor:
+        """Y = scale * (V dressed by the form) X: V X (Orthogonal) or Z^H V Z X
+        (Sandwich) (cheby.hpp:249-291); mode is immaterial for these forms."""
+        ctx = self.H.ctx
+        ctx.bind_stream()
+        op = self.c_op()
+        check(lib().rsatb_cheb_apply_dual(ctx.handle, C.byref(op), V.handle,
+                                          C.c_void_p(X.data_ptr()), C.c_void_p(Y.data_ptr()),
+                                          X.shape[1], dtype_code(X.dtype), float(scale)))
+        return Y
+
+    def propagate(self, V_in: torch.Tensor, V_out: torch.Tensor, coeffs,
+                  mode: ChebyMode = ChebyMode.NORMAL) -> torch.Tensor:
+        """V_out = sum_n c_n T_n(Op~) V_in (cheby.hpp:367-441); coeffs complex
+        (a real panel takes their real parts)."""
+        c = np.ascontiguousarray(np.asarray(coeffs, dtype=np.complex128))
+        flat = np.ascontiguousarray(np.stack([c.real, c.imag], axis=-1).reshape(-1))
+        ctx = self.H.ctx
+        ctx.bind_stream()
+        op = self.c_op()
+        check(lib().rsatb_cheb_propagate(ctx.handle, C.byref(op), C.c_void_p(V_in.data_ptr()),
+                                         C.c_void_p(V_out.data_ptr()), V_in.shape[1],
+                                         dtype_code(V_in.dtype),
+                                         flat.ctypes.data_as(C.POINTER(C.c_double)), int(c.size)))
+        return V_out
+
     def compute_moments(self, V: torch.Tensor, N: int) -> np.ndarray:
         """Per-column plain moments <v|T_n|v>, shape (N, R) (cheby.hpp:479-514)."""
         _, col = _moments(self, V, N, doubled=False, per_column=True)

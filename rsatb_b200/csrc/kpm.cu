@@ -257,6 +257,41 @@ int run_recurrence(rsatb_context* ctx, const rsatb_cheb_op* op, const void* psi,
     return RSATB_SUCCESS;
 }
 
+// Y += c X over n complex (cv) or real values, c = (c_re, c_im); a real
+// panel takes Re(c), as Chebyshev's CoeffCast does for a real scalar type
+// (rsatb/calc/cheby.hpp:113-121).
+template <typename T>
+__global__ void axpy_coeff_kernel(int64_t n, bool cv, double c_re, double c_im, const T* X, T* Y) {
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    if (cv) {
+        for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += stride) {
+            const double xr = double(X[2 * i]), xi = double(X[2 * i + 1]);
+            Y[2 * i] = T(double(Y[2 * i]) + c_re * xr - c_im * xi);
+            Y[2 * i + 1] = T(double(Y[2 * i + 1]) + c_re * xi + c_im * xr);
+        }
+    } else {
+        for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += stride)
+            Y[i] = T(double(Y[i]) + c_re * double(X[i]));
+    }
+}
+
+int axpy_coeff(rsatb_context* ctx, int vdt, int64_t n_values, double c_re, double c_im,
+               const void* X, void* Y) {
+    const bool cv = dtype_is_complex(vdt);
+    const int64_t n = cv ? n_values / 2 : n_values;
+    int64_t grid = (n + 255) / 256;
+    if (grid > int64_t(ctx->sm_count) * 8) grid = int64_t(ctx->sm_count) * 8;
+    if (grid < 1) grid = 1;
+    if (dtype_is_double(vdt))
+        axpy_coeff_kernel<double><<<unsigned(grid), 256, 0, ctx->stream>>>(
+            n, cv, c_re, c_im, static_cast<const double*>(X), static_cast<double*>(Y));
+    else
+        axpy_coeff_kernel<float><<<unsigned(grid), 256, 0, ctx->stream>>>(
+            n, cv, c_re, c_im, static_cast<const float*>(X), static_cast<float*>(Y));
+    RSATB_LAUNCH_CHECK(ctx);
+    return RSATB_SUCCESS;
+}
+
 }  // namespace
 }  // namespace rsatb_b200
 
@@ -469,6 +504,93 @@ int rsatb_kpm_dos_moments(rsatb_ctx_t ctx, const rsatb_cheb_op* op, const void* 
             col_mu_out[2 * i] = colmu[i].real();
             col_mu_out[2 * i + 1] = colmu[i].imag();
         }
+    }
+    return RSATB_SUCCESS;
+}
+
+int rsatb_cheb_apply_dual(rsatb_ctx_t ctx, const rsatb_cheb_op* op, rsatb_bsr_t V,
+                          const void* X, void* Y, int n_vectors, rsatb_dtype vec_dtype,
+                          double scale) {
+    clear_error();
+    RSATB_TRY(check_ctx(ctx));
+    OpShape sh{};
+    RSATB_TRY(check_op(op, vec_dtype, &sh));
+    RSATB_TRY(check_matrix_square(V, "V"));
+    RSATB_TRY(check_vec_dtype(V, vec_dtype, "V"));
+    if (int64_t(V->n_block_rows) * V->block_size != sh.n_rows)
+        return set_error(RSATB_INVALID_ARGUMENT, "V and H sizes differ");
+    int W = 0;
+    RSATB_TRY(panel_width(n_vectors, vec_dtype, &W));
+    if (!X || !Y) return set_error(RSATB_INVALID_ARGUMENT, "null multivector");
+    if (!aligned16(X) || !aligned16(Y))
+        return set_error(RSATB_INVALID_ARGUMENT, "multivectors must be 16-byte aligned");
+    if (X == Y) return set_error(RSATB_INVALID_ARGUMENT, "apply_dual cannot run in place");
+    StepArgs a = blank_args(W);
+    if (!sh.sandwich) {
+        a.in = X;
+        a.y = Y;
+        a.s_in = scale;
+        return run_step(ctx, V, vec_dtype, a);
+    }
+    const size_t vbytes = round256(size_t(sh.n_rows) * W * dtype_real_size(vec_dtype));
+    void* s = nullptr;
+    RSATB_TRY(ctx_scratch(ctx, 2 * vbytes, &s));
+    void* u = s;
+    void* w = static_cast<char*>(s) + vbytes;
+    a.in = X;
+    a.y = u;
+    RSATB_TRY(run_step(ctx, op->Z, vec_dtype, a));   // u = Z x
+    a.in = u;
+    a.y = w;
+    RSATB_TRY(run_step(ctx, V, vec_dtype, a));       // w = V Z x
+    a.in = w;
+    a.y = Y;
+    a.s_in = scale;
+    return run_step(ctx, op->ZH, vec_dtype, a);      // y = scale Z^H V Z x
+}
+
+int rsatb_cheb_propagate(rsatb_ctx_t ctx, const rsatb_cheb_op* op, const void* X, void* Y,
+                         int n_vectors, rsatb_dtype vec_dtype, const double* coeffs,
+                         int n_coeffs) {
+    clear_error();
+    RSATB_TRY(check_ctx(ctx));
+    OpShape sh{};
+    RSATB_TRY(check_op(op, vec_dtype, &sh));
+    int W = 0;
+    RSATB_TRY(panel_width(n_vectors, vec_dtype, &W));
+    if (n_coeffs < 0) return set_error(RSATB_INVALID_ARGUMENT, "n_coeffs < 0");
+    if (n_coeffs == 0) return RSATB_SUCCESS;  // Y unchanged, as the reference returns early
+    if (!X || !Y || !coeffs) return set_error(RSATB_INVALID_ARGUMENT, "null argument");
+    if (!aligned16(X) || !aligned16(Y))
+        return set_error(RSATB_INVALID_ARGUMENT, "multivectors must be 16-byte aligned");
+    if (X == Y) return set_error(RSATB_INVALID_ARGUMENT, "propagate cannot run in place");
+    const int64_t n_values = sh.n_rows * W;
+    const size_t vbytes = round256(size_t(n_values) * dtype_real_size(vec_dtype));
+    const int n_panels = 3 + (sh.sandwich ? 2 : 0);
+    void* s = nullptr;
+    RSATB_TRY(ctx_scratch(ctx, n_panels * vbytes, &s));
+    char* base = static_cast<char*>(s);
+    void* buf[3] = {base, base + vbytes, base + 2 * vbytes};
+    void* u = sh.sandwich ? base + 3 * vbytes : nullptr;
+    void* w = sh.sandwich ? base + 4 * vbytes : nullptr;
+    // Y = c_0 T_0 X = c_0 X (cheby.hpp:399-441): zero, then add.
+    RSATB_CUDA_TRY(cudaMemsetAsync(Y, 0, size_t(n_values) * dtype_real_size(vec_dtype),
+                                   ctx->stream));
+    RSATB_TRY(axpy_coeff(ctx, vec_dtype, n_values, coeffs[0], coeffs[1], X, Y));
+    const double inv_hw = 1.0 / op->half_width;
+    const void* prev = nullptr;  // T_{n-2} X
+    const void* cur = X;         // T_{n-1} X
+    int slot = 0;
+    for (int n = 1; n < n_coeffs; ++n) {
+        void* out = buf[slot];
+        slot = (slot + 1) % 3;
+        // T_1 = Op~ X; T_n = 2 Op~ T_{n-1} - T_{n-2}
+        RSATB_TRY(apply_fused(ctx, op, sh, vec_dtype, W, cur, cur, n == 1 ? nullptr : prev, out, u,
+                              w, inv_hw, n == 1 ? 1.0 : 2.0, n == 1 ? 0.0 : -1.0, DOT_NONE,
+                              nullptr, nullptr, nullptr, nullptr));
+        RSATB_TRY(axpy_coeff(ctx, vec_dtype, n_values, coeffs[2 * n], coeffs[2 * n + 1], out, Y));
+        prev = cur;
+        cur = out;
     }
     return RSATB_SUCCESS;
 }

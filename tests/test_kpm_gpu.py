@@ -415,3 +415,78 @@ def test_persistent_recurrence_matches_graph_path(torch_cuda, monkeypatch, preci
         want = oracle.kpm_moments(oracle_op(H, -9.0, 9.0), psi.cpu().numpy(), 64,
                                   doubled=doubled)
         assert _moment_err(mu_p, want) < 1e-10
+
+
+def _dense_op(H, emin, emax, Z=None):
+    c, hw = (emax + emin) / 2, (emax - emin) / 2
+    Hd = H.to_dense()
+    if Z is not None:
+        Zd = Z.to_dense()
+        Hd = Zd.conj().T @ Hd @ Zd
+    return (Hd - c * np.eye(Hd.shape[0])) / hw
+
+
+def _propagate_ref(Op, X, coeffs):
+    """sum_n c_n T_n(Op) X by the three-term recurrence (cheby.hpp:399-441)."""
+    t0, out = X.copy(), coeffs[0] * X
+    if len(coeffs) > 1:
+        t1 = Op @ X
+        out = out + coeffs[1] * t1
+        for c in coeffs[2:]:
+            t0, t1 = t1, 2 * (Op @ t1) - t0
+            out = out + c * t1
+    return out
+
+
+@pytest.mark.parametrize("case", ["graphene_c128", "diamond_sandwich_f64", "bsr8_f32"])
+def test_propagate_matches_dense(torch_cuda, case):
+    """Chebyshev::propagate: V_out = sum c_n T_n(Op~) V_in with complex
+    coefficients (a real panel takes their real parts)."""
+    torch = torch_cuda
+    rng = np.random.default_rng(8)
+    coeffs = rng.standard_normal(13) + 1j * rng.standard_normal(13)
+    if case == "graphene_c128":
+        H, Z, emin, emax, prec, cv, R = graphene_case(8, 8), None, -8.7, 8.9, "f64", True, 4
+    elif case == "diamond_sandwich_f64":
+        H, S, Z = diamond_case()
+        emin, emax, prec, cv, R = -15.0, 15.0, "f64", False, 16
+    else:
+        H = random_hermitian_bsr(30, 8, 5, seed=4, complex_values=False, scale=0.2)
+        Z, prec, cv, R = None, "f32", True, 8
+        b = np.abs(np.linalg.eigvalsh(H.to_dense())).max() + 0.5
+        emin, emax = -b, b
+    X = _panel(rng, H.n_rows, R, cv)
+    dt = {("f64", True): torch.complex128, ("f64", False): torch.float64,
+          ("f32", True): torch.complex64, ("f32", False): torch.float32}[(prec, cv)]
+    c = build_cheby(H, emin, emax, Z, precision=prec)
+    Xd = to_dev(torch, X, dt)
+    Yd = torch.empty_like(Xd)
+    c.propagate(Xd, Yd, coeffs)
+    want = _propagate_ref(_dense_op(H, emin, emax, Z), X, coeffs if cv else coeffs.real)
+    tol = 1e-12 if prec == "f64" else 2e-5
+    assert rel_err(Yd.cpu().numpy(), want) < tol
+    # no coefficients: the output is left as it was
+    Yd.fill_(3.0)
+    c.propagate(Xd, Yd, [])
+    assert (Yd.cpu().numpy() == 3.0).all()
+
+
+def test_apply_dual_orthogonal_and_sandwich(torch_cuda):
+    """Chebyshev::apply_dual: scale * V X (orthogonal) and scale * Z^H V Z X
+    (sandwich) with an imaginary-unit velocity matrix."""
+    torch = torch_cuda
+    rng = np.random.default_rng(12)
+    H, S, Z = diamond_case()
+    W = random_hermitian_bsr(H.n_block_rows, 8, 4, seed=21, complex_values=False)
+    Vd = dev_bsr(W, imaginary=True)
+    X = _panel(rng, H.n_rows, 6, True)
+    Xd = to_dev(torch, X)
+    Yd = torch.empty_like(Xd)
+    Vdense = 1j * W.to_dense()
+    c = build_cheby(H, -15.0, 15.0)
+    c.apply_dual(Vd, Xd, Yd, scale=-0.25)
+    assert rel_err(Yd.cpu().numpy(), -0.25 * (Vdense @ X)) < 1e-13
+    cs = build_cheby(H, -15.0, 15.0, Z)
+    cs.apply_dual(Vd, Xd, Yd, scale=0.5)
+    Zd = Z.to_dense()
+    assert rel_err(Yd.cpu().numpy(), 0.5 * (Zd.conj().T @ Vdense @ Zd @ X)) < 1e-12
