@@ -180,6 +180,7 @@ class BlockSpMat:
         self.ctx.bind_stream()
         check(lib().rsatb_bsr_set_values(self.ctx.handle, self.handle, C.c_void_p(v.data_ptr()),
                                          _capi.BSR_DEVICE_POINTERS))
+        self._adj = None
 
     def mult_dense(self, X: torch.Tensor, Y: torch.Tensor, alpha: float = 1.0) -> torch.Tensor:
         """Y = alpha * A X (vbcsr BlockSpMat::mult_dense)."""
@@ -192,6 +193,44 @@ class BlockSpMat:
                                          C.c_void_p(Y.data_ptr()), X.shape[1],
                                          dtype_code(X.dtype), float(alpha)))
         return Y
+
+    def mult(self, x: torch.Tensor, y: torch.Tensor, alpha: float = 1.0) -> torch.Tensor:
+        """y = alpha * A x for one vector (N,) (vbcsr BlockSpMat::mult)."""
+        self.mult_dense(x.reshape(-1, 1), y.reshape(-1, 1), alpha)
+        return y
+
+    def mult_optimized(self, X: torch.Tensor, Y: torch.Tensor) -> torch.Tensor:
+        """Y = A X; the device path is the same fused kernel as mult_dense."""
+        return self.mult_dense(X, Y)
+
+    def _adjoint_cached(self) -> "BlockSpMat":
+        adj = getattr(self, "_adj", None)
+        if adj is None:
+            adj = self.adjoint()
+            self._adj = adj
+        return adj
+
+    def mult_dense_adjoint(self, X: torch.Tensor, Y: torch.Tensor,
+                           alpha: float = 1.0) -> torch.Tensor:
+        """Y = alpha * A^H X (vbcsr BlockSpMat::mult_dense_adjoint); A^H is built
+        once and kept (invalidated by set_values)."""
+        return self._adjoint_cached().mult_dense(X, Y, alpha)
+
+    def mult_adjoint(self, x: torch.Tensor, y: torch.Tensor, alpha: float = 1.0) -> torch.Tensor:
+        """y = alpha * A^H x for one vector."""
+        self._adjoint_cached().mult_dense(x.reshape(-1, 1), y.reshape(-1, 1), alpha)
+        return y
+
+    def duplicate(self) -> "BlockSpMat":
+        """An independent copy (same precision)."""
+        return self.astype("f64" if self.is_double else "f32")
+
+    def get_block_density(self) -> float:
+        """Stored blocks over all block positions."""
+        return self.nnz_blocks / float(max(1, self.n_block_rows * self.n_block_cols))
+
+    def block_size_elements(self) -> int:
+        return self.block_size * self.block_size
 
     def __del__(self):
         h = getattr(self, "handle", None)
@@ -255,6 +294,37 @@ class DistMultiVector:
 
     def scale(self, s) -> None:
         self.data.mul_(s)
+
+    def axpy(self, a, x: "DistMultiVector") -> None:
+        """self += a * x."""
+        self.data.add_(x.data, alpha=a)
+
+    def bdot(self, other: "DistMultiVector") -> np.ndarray:
+        """Per-column bilinear sum_i self_i other_i (no conjugation), FP64."""
+        a = self.data.to(torch.complex128)
+        b = other.data.to(torch.complex128)
+        return (a * b).sum(0).cpu().numpy()
+
+    def swap(self, other: "DistMultiVector") -> None:
+        """Exchanges the two panels (no copy)."""
+        self.data, other.data = other.data, self.data
+
+    def set_constant(self, value) -> None:
+        self.data.fill_(value)
+
+    def get_col(self, j: int) -> torch.Tensor:
+        """Column j as a new (N,) device tensor."""
+        return self.data[:, j].clone()
+
+    def set_col(self, j: int, v: torch.Tensor) -> None:
+        self.data[:, j].copy_(v)
+
+    def row_data(self, row: int) -> torch.Tensor:
+        """Row `row` of the panel (a view)."""
+        return self.data[row]
+
+    def __call__(self, row: int, col: int):
+        return self.data[row, col].item()
 
 
 def set_random(out: torch.Tensor, seed: int, normalize: bool = True, atom_index=None,

@@ -490,3 +490,38 @@ def test_apply_dual_orthogonal_and_sandwich(torch_cuda):
     cs.apply_dual(Vd, Xd, Yd, scale=0.5)
     Zd = Z.to_dense()
     assert rel_err(Yd.cpu().numpy(), 0.5 * (Zd.conj().T @ Vdense @ Zd @ X)) < 1e-12
+
+
+def test_vbcsr_subset(torch_cuda):
+    """The vbcsr pieces the calc layer calls (DistMultiVector algebra,
+    BlockSpMat mult / mult_dense_adjoint / duplicate) against numpy."""
+    torch = torch_cuda
+    from rsatb_b200.vbcsr import DistMultiVector
+    rng = np.random.default_rng(31)
+    A = random_hermitian_bsr(20, 5, 4, seed=6, complex_values=True)
+    Ad = dev_bsr(A)
+    n = A.n_rows
+    X = _panel(rng, n, 3, True)
+    Y = torch.empty(n, 3, dtype=torch.complex128, device="cuda")
+    Ad.mult_dense_adjoint(to_dev(torch, X), Y, alpha=0.5)
+    assert rel_err(Y.cpu().numpy(), 0.5 * A.to_dense().conj().T @ X) < 1e-13
+    x = to_dev(torch, X[:, 0].copy())
+    y = torch.empty(n, dtype=torch.complex128, device="cuda")
+    Ad.mult(x, y)
+    assert rel_err(y.cpu().numpy(), A.to_dense() @ X[:, 0]) < 1e-13
+    D = Ad.duplicate()
+    D.mult_dense(to_dev(torch, X), Y)
+    assert rel_err(Y.cpu().numpy(), A.to_dense() @ X) < 1e-13
+    assert Ad.get_block_density() == A.nnz_blocks / (20 * 20)
+    a = DistMultiVector(n, 3, data=to_dev(torch, X))
+    b = DistMultiVector(n, 3, data=to_dev(torch, _panel(rng, n, 3, True)))
+    Bh = b.data.cpu().numpy()
+    assert np.allclose(a.bdot(b), (X * Bh).sum(0)) and np.allclose(a.dot(b), (X.conj() * Bh).sum(0))
+    a.axpy(2.0, b)
+    assert np.allclose(a.data.cpu().numpy(), X + 2.0 * Bh)
+    a.swap(b)
+    assert np.allclose(a.data.cpu().numpy(), Bh)
+    b.set_constant(1.5)
+    assert (b.data.cpu().numpy() == 1.5).all()
+    a.set_col(1, b.get_col(0))
+    assert np.allclose(a.data[:, 1].cpu().numpy(), 1.5) and a(0, 1) == 1.5
