@@ -89,7 +89,7 @@ __global__ void __launch_bounds__(256) kpm_persistent_kernel(PersistArgs pa) {
     __shared__ double red[2 * 256 * V];
     const StepArgs& b = pa.base;
     const int W = b.W, L = W / V;
-    const int g = threadIdx.x % L;
+    const int g = threadIdx.x % L;  // blockDim.x is a multiple of L
     const int64_t total = b.n_block_rows * L;  // scalar rows x lanes per row
     const int64_t stride = int64_t(gridDim.x) * blockDim.x;
     const int64_t t0 = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -214,11 +214,15 @@ template <typename VT, int V, bool CV>
 int launch_persistent(rsatb_context* ctx, PersistArgs pa, int64_t n_rows, double* dots,
                       size_t part_capacity) {
     auto kernel = kpm_persistent_kernel<VT, V, CV>;
-    const int threads = 256;
+    // The CTA size is a multiple of the L lanes of a row (W = 6: L = 3, 255
+    // threads), so a thread's column group is threadIdx.x % L in every CTA
+    // and at every grid stride, as the kernel and cta_partials assume.
+    const int L = pa.base.W / V;
+    if (L > 256) return kPersistSkipped;
+    const int threads = 256 - 256 % L;
     int per_sm = 0;
     RSATB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0));
     if (per_sm < 1) return kPersistSkipped;
-    const int L = pa.base.W / V;
     int64_t grid = int64_t(ctx->sm_count) * per_sm;
     const int64_t need = (n_rows * L + threads - 1) / threads;
     if (need < grid) grid = need;

@@ -1,0 +1,183 @@
+"""The DOS and transport surface of RSATB's Python object (rsatb/pybind_rsatb.cpp:
+549-603, 813-825; rsatb/calc/observables.hpp:311-441, 691-780) over operators
+the caller has already built.
+
+Model construction (structures, Slater-Koster / LCAO models) is outside this
+package, so ``RSATB`` is constructed from the operators themselves: H, the
+optional graph-local factor Z of the overlap, the velocity matrices and the
+cell.  ``SetupOptions`` keeps the reference's field names.  Everything below
+runs on the device through the C ABI; no result is computed on the host
+except the small grids and the final scalings.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import lattice
+from .bounds import estimate_spectral_bounds
+from .calc import (Chebyshev, ISQRTMPreconditioner, dos_energy_grid, dos_moment_count,
+                   evaluate_kpm_density, kpm_dos_moments, parse_kpm_kernel)
+from .transport import BASTIN, GREENWOOD, dc_spectrum_fftcheb
+from ._capi import RANDOM_PHASE
+from .vbcsr import BlockSpMat, set_random
+
+
+@dataclass
+class SetupOptions:
+    """rsatb::model::SetupOptions (pybind_rsatb.cpp:263-341): sampling and
+    spectral bounds.  Only the Gamma point is served (real operators);
+    ``precision`` ('f64' or 'mixed': FP32 vectors and operators, FP64 dots)
+    is this package's addition."""
+    kpoints: list = field(default_factory=lambda: [[0.0, 0.0, 0.0]])
+    nsamples: int = 1
+    sample_seed: int = 20240917
+    compute_bounds: bool = True
+    energy_bounds: tuple | None = None
+    bounds_zero_tol: float = 1e-12
+    bounds_max_matvecs: int = 10000
+    precision: str = "f64"
+
+
+def _as_device(A) -> BlockSpMat:
+    if isinstance(A, BlockSpMat):
+        return A
+    if isinstance(A, lattice.BsrArrays):
+        return BlockSpMat(A.row_ptr, A.col_ind, A.values, A.block_size, A.n_block_cols)
+    raise TypeError("operators are BlockSpMat or lattice.BsrArrays")
+
+
+def _volume(cell: np.ndarray, axis: str) -> float:
+    """TransportNormalizationVolume (observables.hpp:277-285): the cell vector
+    length for one axis, the area for two, the volume for three."""
+    idx = ["abc".index(a) for a in axis]
+    vecs = [np.asarray(cell[i], dtype=np.float64) for i in idx]
+    if len(vecs) == 1:
+        return float(np.linalg.norm(vecs[0]))
+    if len(vecs) == 2:
+        return float(np.linalg.norm(np.cross(vecs[0], vecs[1])))
+    return float(abs(np.dot(vecs[0], np.cross(vecs[1], vecs[2]))))
+
+
+class RSATB:
+    """``_rsatb.RSATB`` for prebuilt operators.
+
+    H: Hamiltonian (BlockSpMat or lattice.BsrArrays, real, Gamma point).
+    Z: graph-local factor of the overlap (non-orthogonal basis: the sandwich
+    form Z^H H Z), or None.  velocities: (Vx, Vy, Vz) real matrices W_a of the
+    velocities i W_a (for compute_dc_spectrum).  cell: 3 x 3 lattice vectors
+    in Angstrom (rows a, b, c).  orbitals_per_atom / atom_index key the
+    seeded sample vectors by atom, as SampleVectors::initialize does.
+    """
+
+    def __init__(self, H, options: SetupOptions | None = None, Z=None, velocities=None,
+                 cell=None, orbitals_per_atom: int = 1, atom_index=None,
+                 spin_degeneracy: float = 2.0):
+        self.options = options or SetupOptions()
+        if any(np.any(np.asarray(k) != 0.0) for k in self.options.kpoints):
+            raise NotImplementedError("only the Gamma point is served (real operators)")
+        if self.options.precision not in ("f64", "mixed"):
+            raise ValueError("precision must be 'f64' or 'mixed'")
+        self.H = _as_device(H)
+        self.Z = _as_device(Z) if Z is not None else None
+        self.V = None
+        if velocities is not None:
+            self.V = [v if isinstance(v, BlockSpMat) else
+                      BlockSpMat(v.row_ptr, v.col_ind, v.values, v.block_size, v.n_block_cols,
+                                 imaginary=True)
+                      for v in velocities]
+        self.cell = None if cell is None else np.asarray(cell, dtype=np.float64)
+        self.orbitals_per_atom = int(orbitals_per_atom)
+        self.atom_index = atom_index
+        self.spin_degeneracy = float(spin_degeneracy)
+        self._bounds = None
+        if self.options.energy_bounds is not None:
+            lo, hi = self.options.energy_bounds
+            self._bounds = (float(lo), float(hi))
+        elif self.options.compute_bounds:
+            self._bounds = self._estimate_bounds()
+
+    # -- operators --------------------------------------------------------
+
+    def _cheby(self, emin: float, emax: float, mixed: bool) -> Chebyshev:
+        pre = ISQRTMPreconditioner(self.Z) if self.Z is not None else None
+        c = Chebyshev(self.H, emin, emax, preconditioner=pre)
+        return c.astype("f32") if mixed else c
+
+    def _estimate_bounds(self):
+        c = self._cheby(-1.0, 1.0, False)
+        return estimate_spectral_bounds(c)
+
+    def energy_bounds(self):
+        """(emin, emax) of the operator, padded as the reference pads its
+        Lanczos estimate (spectral_bounds.hpp:75)."""
+        if self._bounds is None:
+            raise RuntimeError("Spectral bound is not computed yet. Set it true during Setup "
+                               "stage for random state method support.")
+        return self._bounds
+
+    def _samples(self, dtype) -> torch.Tensor:
+        n = self.H.shape[0]
+        psi = torch.empty(n, self.options.nsamples, dtype=dtype,
+                          device=f"cuda:{self.H.ctx.device}")
+        set_random(psi, int(self.options.sample_seed), normalize=True,
+                   atom_index=self.atom_index, orbitals_per_atom=self.orbitals_per_atom,
+                   kind=RANDOM_PHASE)
+        return psi
+
+    # -- observables ------------------------------------------------------
+
+    def compute_dos(self, dE: float, method: str = "kpm"):
+        """ComputeDos (observables.hpp:311-441), method 'kpm': the Jackson
+        moment count for a FWHM of dE, the KPM density on the 2 nt grid,
+        scaled by 2.  Returns (dos, omega)."""
+        if method == "corr":
+            raise NotImplementedError("dos method 'corr' is not served on the device")
+        if method != "kpm":
+            raise ValueError(f"dos method must be 'kpm' or 'corr', got '{method}'")
+        if not dE > 0.0:
+            raise ValueError("dos dE must be a positive energy resolution in eV")
+        emin, emax = self.energy_bounds()
+        N = dos_moment_count((emax - emin) / 2.0, dE)
+        mixed = self.options.precision == "mixed"
+        c = self._cheby(emin, emax, mixed)
+        psi = self._samples(torch.complex64 if mixed else torch.complex128)
+        mu = kpm_dos_moments(c, psi, N)
+        x, omega, nt = dos_energy_grid(emin, emax, dE)
+        rho = evaluate_kpm_density(mu, x, 0.5 / nt, device=self.H.ctx.device)
+        return 2.0 * rho, omega
+
+    def compute_dc_spectrum(self, n_moments: int, formulation: str = "greenwood",
+                            axis: str = "abc", partition_sections: int = 0,
+                            max_workspace_mb: float = 0, kernel: str = "jackson",
+                            method: str = "fftcheb"):
+        """ComputeDcSpectrum (observables.hpp:691-780) with the fftcheb method:
+        prefactor pi g_s (4 Greenwood, 8 Bastin) norb / volume(axis).
+        Returns (sigma[n_moments * 6], energy[n_moments])."""
+        if method != "fftcheb":
+            raise NotImplementedError(f"dc method '{method}': only 'fftcheb' is served")
+        if self.V is None:
+            raise ValueError("compute_dc_spectrum needs the velocity matrices")
+        if self.cell is None:
+            raise ValueError("compute_dc_spectrum needs the cell for its normalisation")
+        forms = {"greenwood": GREENWOOD, "bastin": BASTIN}
+        if formulation not in forms:
+            raise ValueError(f"Unknown dc formulation: {formulation}")
+        if not axis or any(a not in "abc" for a in axis) or len(set(axis)) != len(axis):
+            raise ValueError(f"axis must be a subset of 'abc', got '{axis}'")
+        emin, emax = self.energy_bounds()
+        mixed = self.options.precision == "mixed"
+        c = self._cheby(emin, emax, mixed)
+        V = [v.astype("f32") for v in self.V] if mixed else self.V
+        psi = self._samples(torch.complex64 if mixed else torch.complex128)
+        norb = self.H.shape[0]
+        trace_prefactor = norb / _volume(self.cell, axis)
+        prefactor = (math.pi * self.spin_degeneracy *
+                     (4.0 if formulation == "greenwood" else 8.0) * trace_prefactor)
+        sigma, energy = dc_spectrum_fftcheb(
+            c, *V, psi, int(n_moments), forms[formulation], prefactor,
+            int(partition_sections), float(max_workspace_mb), parse_kpm_kernel(kernel))
+        return sigma.reshape(-1), energy

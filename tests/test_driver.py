@@ -1,0 +1,115 @@
+"""The RSATB facade (rsatb_b200.driver): ComputeDos and ComputeDcSpectrum
+(rsatb/calc/observables.hpp:311-441, 691-780) over prebuilt operators,
+checked against the oracle's moments, density and fftcheb on the same
+seeded sample vectors."""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+from _util import rel_err, to_oracle
+
+
+def test_normalisation_volume():
+    from rsatb_b200.driver import _volume
+    cell = np.array([[2.0, 0.0, 0.0], [1.0, 3.0, 0.0], [0.0, 0.0, 5.0]])
+    assert _volume(cell, "a") == pytest.approx(2.0)
+    assert _volume(cell, "b") == pytest.approx(math.sqrt(10.0))
+    assert _volume(cell, "ab") == pytest.approx(6.0)
+    assert _volume(cell, "abc") == pytest.approx(30.0)
+    assert _volume(cell, "ac") == pytest.approx(10.0)
+
+
+def test_setup_options_defaults():
+    from rsatb_b200.driver import SetupOptions
+    o = SetupOptions()
+    assert o.nsamples == 1 and o.sample_seed == 20240917 and o.compute_bounds
+    assert o.kpoints == [[0.0, 0.0, 0.0]]
+
+
+def _oracle_samples(n, nsamples, seed):
+    return oracle.set_random(seed, 0, True, np.arange(n), 1, n, nsamples, True)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["f64", "mixed"])
+def test_compute_dos_matches_oracle(precision):
+    import torch
+    from rsatb_b200 import lattice
+    from rsatb_b200.calc import dos_energy_grid, dos_moment_count
+    from rsatb_b200.driver import RSATB, SetupOptions
+    torch.cuda.set_device(0)
+    H, _, _ = lattice.graphene(12, 12)
+    emin, emax = -8.6, 8.7
+    opts = SetupOptions(nsamples=3, sample_seed=77, energy_bounds=(emin, emax),
+                        precision=precision)
+    calc = RSATB(H, opts)
+    assert calc.energy_bounds() == (emin, emax)
+    dE = 0.25
+    dos, omega = calc.compute_dos(dE)
+    N = dos_moment_count((emax - emin) / 2, dE)
+    x, omega_o, nt = dos_energy_grid(emin, emax, dE)
+    psi = _oracle_samples(H.n_rows, 3, 77)
+    op = oracle.make_op(to_oracle(H), (emax + emin) / 2, (emax - emin) / 2)
+    mu = oracle.kpm_moments(op, psi, N)
+    want = 2.0 * oracle.density(mu, x, 0.5 / nt)
+    assert dos.shape == (2 * nt,) and np.array_equal(omega, omega_o)
+    assert rel_err(dos, want) < (1e-10 if precision == "f64" else 1e-5)
+    # ComputeDos returns 2 rho(x) per unit of the rescaled energy x (grid
+    # step 1 / nt): it integrates to 2 (spin) over [-1, 1].
+    assert abs(np.sum(dos) / nt - 2.0) < 0.05
+
+
+@pytest.mark.gpu
+def test_compute_dos_bounds_and_errors():
+    import torch
+    from rsatb_b200 import lattice
+    from rsatb_b200.driver import RSATB, SetupOptions
+    torch.cuda.set_device(0)
+    H, _, _ = lattice.graphene(8, 8)
+    calc = RSATB(H, SetupOptions())
+    lo, hi = calc.energy_bounds()
+    w = np.linalg.eigvalsh(H.to_dense())
+    assert lo < w[0] and hi > w[-1]
+    with pytest.raises(ValueError):
+        calc.compute_dos(0.0)
+    with pytest.raises(ValueError):
+        calc.compute_dos(0.1, method="lanczos")
+    none = RSATB(H, SetupOptions(compute_bounds=False))
+    with pytest.raises(RuntimeError):
+        none.energy_bounds()
+    with pytest.raises(ValueError):
+        calc.compute_dc_spectrum(16)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("formulation", ["greenwood", "bastin"])
+def test_compute_dc_spectrum_matches_oracle(formulation):
+    import torch
+    from rsatb_b200 import lattice
+    from rsatb_b200.driver import RSATB, SetupOptions, _volume
+    torch.cuda.set_device(0)
+    H, pos, cell, disp = lattice.twisted_bilayer_graphene(m=1, tiles=(4, 4))
+    V = lattice.commutator_velocity(H, disp)
+    w = np.linalg.eigvalsh(H.to_dense())
+    emin, emax = w[0] - 0.5, w[-1] + 0.5
+    opts = SetupOptions(nsamples=2, sample_seed=9, energy_bounds=(emin, emax))
+    calc = RSATB(H, opts, velocities=V, cell=cell)
+    M = 48
+    sigma, energy = calc.compute_dc_spectrum(M, formulation=formulation, axis="ab")
+    psi = _oracle_samples(H.n_rows, 2, 9)
+    op = oracle.make_op(to_oracle(H), (emax + emin) / 2, (emax - emin) / 2)
+    Vo = [to_oracle(v, imag=True) for v in V]
+    pref = math.pi * 2.0 * (4.0 if formulation == "greenwood" else 8.0) * H.n_rows / _volume(cell, "ab")
+    sig_o, en_o = oracle.fftcheb(op, Vo, psi, M, formulation=0 if formulation == "greenwood" else 1,
+                                 prefactor=pref)
+    assert sigma.shape == (6 * M,)
+    assert np.allclose(energy, en_o, rtol=0, atol=1e-13)
+    assert rel_err(sigma, sig_o.reshape(-1)) < 1e-10
+    with pytest.raises(ValueError):
+        calc.compute_dc_spectrum(M, formulation="kubo")
+    with pytest.raises(ValueError):
+        calc.compute_dc_spectrum(M, axis="xy")

@@ -388,19 +388,23 @@ def test_bulk_kernel_bounded_wait_reports_fault(torch_cuda, monkeypatch):
     assert np.abs(mu - ref).max() <= 1e-6 * np.abs(ref).max()
 
 
-@pytest.mark.parametrize("precision,doubled", [("f64", True), ("f64", False), ("f32", True)])
-def test_persistent_recurrence_matches_graph_path(torch_cuda, monkeypatch, precision, doubled):
+@pytest.mark.parametrize("precision,doubled,R", [("f64", True, 8), ("f64", False, 8),
+                                                 ("f32", True, 8), ("f64", True, 3),
+                                                 ("f64", True, 5), ("f32", True, 6),
+                                                 ("f64", False, 1)])
+def test_persistent_recurrence_matches_graph_path(torch_cuda, monkeypatch, precision, doubled, R):
     """Small scalar-block operators run the whole recurrence as one
     cooperative launch (grid barriers between steps); its moments match the
     per-step path to rounding (only the order of the FP64 dot sums differs)
-    and the oracle, in two launches per call."""
+    and the oracle, in two launches per call.  R = 3, 5, 6 give rows of 3, 5
+    and 3 lanes, which do not divide 256 threads."""
     torch = torch_cuda
     from rsatb_b200.calc import kpm_dos_moments, kpm_dos_moments_plain
     from rsatb_b200.vbcsr import set_random
     H = graphene_case(12, 10)
     c = build_cheby(H, -9.0, 9.0, precision=precision)
     dt = torch.complex128 if precision == "f64" else torch.complex64
-    psi = torch.empty(H.n_rows, 8, dtype=dt, device="cuda")
+    psi = torch.empty(H.n_rows, R, dtype=dt, device="cuda")
     set_random(psi, 11)
     run = kpm_dos_moments if doubled else kpm_dos_moments_plain
     ctx = c.H.ctx
