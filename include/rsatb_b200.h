@@ -243,6 +243,30 @@ RSATB_API int rsatb_evaluate_kpm_density(rsatb_ctx_t ctx, const double* moments,
                                const double* x, int nx, double edge_inset, int kernel,
                                double* rho_out);
 
+/* Chebyshev coefficients of e^{-i x t} (forward != 0) or e^{+i x t}:
+ * c_n = (2 - delta_n0) (-+i)^n J_n(t), truncated before the first n with
+ * |J_n(t)| <= precision and |J_{n+1}(t)| <= precision.
+ * rsatb::calc::timeprop_coeff (rsatb/calc/cheby.hpp:85-106) with
+ * build_bessel_vector (rsatb/calc/bessel.hpp:9-52).  The Bessel values are
+ * computed on the device (Miller's backward recurrence).  *n_coeffs gets the
+ * full length; the first min(length, capacity) coefficients are written to
+ * coeffs (host, (re, im) pairs).  t must be positive and below about 64,000
+ * (the reference's order limit 65536), else RSATB_INVALID_ARGUMENT. */
+RSATB_API int rsatb_timeprop_coeff(rsatb_ctx_t ctx, double time_step, double precision,
+                                   int forward, int capacity, double* coeffs, int* n_coeffs);
+
+/* The correlation-series DOS of ComputeDos(method = "corr")
+ * (rsatb/calc/observables.hpp:393-428): C(j pi) = sum_n c_n(j pi) mu_n for
+ * j = 1..nt with the coefficients above (corr_from_moments,
+ * rsatb/calc/dos.hpp:30-46; C(0) = mu_0), a Hann window, the mirror
+ * C(-t) = conj C(t), an unnormalised inverse FFT of 2 nt points (cuFFT) and
+ * the reorder to energies (i - nt)/nt, i/nt.  moments: host, (re, im) x
+ * n_moments (at least rsatb_timeprop_coeff(nt pi) terms for the full
+ * expansion).  cdos_out (host, (re, im) x (nt + 1)) and dos_out (host,
+ * 2 nt) may each be NULL. */
+RSATB_API int rsatb_corr_dos(rsatb_ctx_t ctx, const double* moments, int n_moments, int nt,
+                             double precision, double* cdos_out, double* dos_out);
+
 /* ------------------------------------------------------------ adjoint KPM */
 
 /* Counters of one rsatb_kpm_moments_vjp call. */

@@ -256,6 +256,57 @@ def fftcheb(op: OrcOp, V, psi: np.ndarray, n_moments: int, formulation: int = 0,
     return sigma.reshape(n_moments, 6), energy
 
 
+# ------------------------------------------------------ correlation-series DOS
+
+def timeprop_coeff(time_step: float, precision: float = 1e-14, forward: bool = True) -> np.ndarray:
+    """rsatb/calc/cheby.hpp:85-106 with build_bessel_vector
+    (rsatb/calc/bessel.hpp:9-52): J_n(t) for ascending n from scipy's Bessel
+    function (the reference uses the bessel-library's cyl_j), kept while
+    |J_n| > eps or |J_{n+1}| > eps; c_n = (2 - delta_n0) (-+i)^n J_n."""
+    from scipy.special import jv
+    n_max = 65536
+    chunk = int(time_step + 64 * max(1.0, time_step) ** (1.0 / 3.0) + 64)
+    vals = jv(np.arange(min(chunk + 1, n_max + 1)), time_step)
+    n_terms = None
+    for n in range(vals.size - 1):
+        if abs(vals[n]) <= precision and abs(vals[n + 1]) <= precision:
+            n_terms = n
+            break
+    if n_terms is None:
+        raise RuntimeError("bessel: series not converged")
+    J = vals[:n_terms]
+    phase = (-1j if forward else 1j) ** np.arange(n_terms)
+    c = 2.0 * phase * J
+    c[0] *= 0.5
+    return c
+
+
+def corr_from_moments(mu: np.ndarray, nt: int, precision: float = 1e-14) -> np.ndarray:
+    """rsatb/calc/dos.hpp:30-46: C(j pi) = sum_n c_n(j pi) mu_n, C(0) = mu_0."""
+    mu = np.asarray(mu, dtype=np.complex128)
+    out = np.zeros(nt + 1, dtype=np.complex128)
+    out[0] = mu[0]
+    for j in range(1, nt + 1):
+        c = timeprop_coeff(j * np.pi, precision, True)
+        m = min(c.size, mu.size)
+        out[j] = np.sum(c[:m] * mu[:m])
+    return out
+
+
+def corr_dos(mu: np.ndarray, nt: int, precision: float = 1e-14) -> np.ndarray:
+    """ComputeDos "corr" (rsatb/calc/observables.hpp:393-428): Hann window,
+    mirrored series, unnormalised inverse FFT of 2 nt points, reordered."""
+    cd = corr_from_moments(mu, nt, precision)
+    full = np.zeros(2 * nt + 1, dtype=np.complex128)
+    full[0] = cd[0]
+    for i in range(1, nt + 1):
+        f = 0.5 * (1 + np.cos(np.pi * (i - 1) / nt))
+        full[i] = cd[i] * f
+        full[2 * nt - i] = np.conj(cd[i]) * f
+    F = np.fft.ifft(full[:2 * nt]) * (2 * nt)   # FFTW_BACKWARD is unnormalised
+    return np.concatenate([F[nt:].real, F[:nt].real]), cd
+
+
 # ----------------------------------------------------- dense inverse square root
 
 EIGEN_CLAMP = 1.0e-12

@@ -259,6 +259,47 @@ def dos_moment_count(half_width: float, de_ev: float) -> int:
     return max(1, int(math.ceil(jackson_fwhm * half_width / de_ev)))
 
 
+def timeprop_coeff(time_step: float, precision: float = 1e-14, forward: bool = True,
+                   device=None) -> np.ndarray:
+    """Chebyshev coefficients of exp(-+i x t) (cheby.hpp:85-106, truncated as
+    bessel.hpp:9-52), computed on the GPU."""
+    ctx = context(device)
+    n = C.c_int(0)
+    check(lib().rsatb_timeprop_coeff(ctx.handle, float(time_step), float(precision),
+                                     int(bool(forward)), 0, None, C.byref(n)))
+    out = np.zeros(n.value, dtype=np.complex128)
+    P = C.POINTER(C.c_double)
+    check(lib().rsatb_timeprop_coeff(ctx.handle, float(time_step), float(precision),
+                                     int(bool(forward)), n.value,
+                                     out.view(np.float64).ctypes.data_as(P), C.byref(n)))
+    return out
+
+
+def corr_moment_count(nt: int, precision: float = 1e-14, device=None) -> int:
+    """Moments the correlation DOS needs: the expansion length of the longest
+    time nt*pi (observables.hpp:354-357)."""
+    return timeprop_coeff(nt * math.pi, precision, True, device).size
+
+
+def corr_dos(moments, nt: int, precision: float = 1e-14, device=None):
+    """corr_from_moments (dos.hpp:30-46) and the windowed inverse FFT of
+    ComputeDos "corr" (observables.hpp:393-428) on the GPU.  Returns
+    (dos[2 nt], cdos[nt + 1])."""
+    if nt < 1:
+        raise ValueError("nt must be positive")
+    mu = np.ascontiguousarray(np.asarray(moments, dtype=np.complex128))
+    if mu.size < 1:
+        raise ValueError("corr_dos needs at least one moment")
+    cdos = np.zeros(nt + 1, dtype=np.complex128)
+    dos = np.zeros(2 * nt)
+    ctx = context(device)
+    P = C.POINTER(C.c_double)
+    check(lib().rsatb_corr_dos(ctx.handle, mu.view(np.float64).ctypes.data_as(P), mu.size,
+                               int(nt), float(precision),
+                               cdos.view(np.float64).ctypes.data_as(P), dos.ctypes.data_as(P)))
+    return dos, cdos
+
+
 def dos_energy_grid(emin: float, emax: float, de_ev: float):
     """The uniform 2*nt grid of ComputeDos (observables.hpp:336, 370-375,
     438-443): returns (x_grid, omega, nt)."""

@@ -19,8 +19,9 @@ import torch
 
 from . import lattice
 from .bounds import estimate_spectral_bounds
-from .calc import (Chebyshev, ISQRTMPreconditioner, dos_energy_grid, dos_moment_count,
-                   evaluate_kpm_density, kpm_dos_moments, parse_kpm_kernel)
+from .calc import (Chebyshev, ISQRTMPreconditioner, corr_dos, corr_moment_count,
+                   dos_energy_grid, dos_moment_count, evaluate_kpm_density, kpm_dos_moments,
+                   parse_kpm_kernel)
 from .transport import BASTIN, GREENWOOD, dc_spectrum_fftcheb
 from ._capi import RANDOM_PHASE
 from .vbcsr import BlockSpMat, set_random
@@ -131,23 +132,29 @@ class RSATB:
     # -- observables ------------------------------------------------------
 
     def compute_dos(self, dE: float, method: str = "kpm"):
-        """ComputeDos (observables.hpp:311-441), method 'kpm': the Jackson
-        moment count for a FWHM of dE, the KPM density on the 2 nt grid,
-        scaled by 2.  Returns (dos, omega)."""
-        if method == "corr":
-            raise NotImplementedError("dos method 'corr' is not served on the device")
-        if method != "kpm":
+        """ComputeDos (observables.hpp:311-441).  'kpm': the Jackson moment
+        count for a FWHM of dE, the KPM density on the 2 nt grid, scaled by
+        2.  'corr': the moments of the longest time nt*pi, the correlation
+        series, Hann window and inverse FFT.  Returns (dos, omega)."""
+        if method != "kpm" and method != "corr":
             raise ValueError(f"dos method must be 'kpm' or 'corr', got '{method}'")
         if not dE > 0.0:
             raise ValueError("dos dE must be a positive energy resolution in eV")
         emin, emax = self.energy_bounds()
-        N = dos_moment_count((emax - emin) / 2.0, dE)
+        x, omega, nt = dos_energy_grid(emin, emax, dE)
+        dev = self.H.ctx.device
+        if method == "kpm":
+            N = dos_moment_count((emax - emin) / 2.0, dE)
+        else:
+            N = corr_moment_count(nt, device=dev)
         mixed = self.options.precision == "mixed"
         c = self._cheby(emin, emax, mixed)
         psi = self._samples(torch.complex64 if mixed else torch.complex128)
         mu = kpm_dos_moments(c, psi, N)
-        x, omega, nt = dos_energy_grid(emin, emax, dE)
-        rho = evaluate_kpm_density(mu, x, 0.5 / nt, device=self.H.ctx.device)
+        if method == "corr":
+            dos, _ = corr_dos(mu, nt, device=dev)
+            return dos, omega
+        rho = evaluate_kpm_density(mu, x, 0.5 / nt, device=dev)
         return 2.0 * rho, omega
 
     def compute_dc_spectrum(self, n_moments: int, formulation: str = "greenwood",

@@ -78,6 +78,14 @@ def test_compute_dos_bounds_and_errors():
         calc.compute_dos(0.0)
     with pytest.raises(ValueError):
         calc.compute_dos(0.1, method="lanczos")
+    # Both estimators share the grid and integrate to 2 per unit of x (grid
+    # step 1 / nt); their integrated DOS curves agree to the broadening.
+    d_kpm, w_kpm = calc.compute_dos(0.3)
+    d_corr, w_corr = calc.compute_dos(0.3, method="corr")
+    nt = d_kpm.size // 2
+    assert np.array_equal(w_kpm, w_corr)
+    assert abs(d_kpm.sum() / nt - 2.0) < 0.05 and abs(d_corr.sum() / nt - 2.0) < 1e-9
+    assert np.abs(np.cumsum(d_kpm) - np.cumsum(d_corr)).max() / nt < 0.25
     none = RSATB(H, SetupOptions(compute_bounds=False))
     with pytest.raises(RuntimeError):
         none.energy_bounds()
@@ -113,3 +121,26 @@ def test_compute_dc_spectrum_matches_oracle(formulation):
         calc.compute_dc_spectrum(M, formulation="kubo")
     with pytest.raises(ValueError):
         calc.compute_dc_spectrum(M, axis="xy")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["f64", "mixed"])
+def test_compute_dos_corr_matches_oracle(precision):
+    import torch
+    from rsatb_b200 import lattice
+    from rsatb_b200.calc import dos_energy_grid
+    from rsatb_b200.driver import RSATB, SetupOptions
+    torch.cuda.set_device(0)
+    H, _, _ = lattice.graphene(12, 12)
+    emin, emax = -8.6, 8.7
+    calc = RSATB(H, SetupOptions(nsamples=2, sample_seed=5, energy_bounds=(emin, emax),
+                                 precision=precision))
+    dE = 0.4
+    dos, omega = calc.compute_dos(dE, method="corr")
+    x, omega_o, nt = dos_energy_grid(emin, emax, dE)
+    N = oracle.timeprop_coeff(nt * np.pi).size
+    psi = _oracle_samples(H.n_rows, 2, 5)
+    op = oracle.make_op(to_oracle(H), (emax + emin) / 2, (emax - emin) / 2)
+    want, _ = oracle.corr_dos(oracle.kpm_moments(op, psi, N), nt)
+    assert dos.shape == (2 * nt,) and np.array_equal(omega, omega_o)
+    assert np.abs(dos - want).max() < (1e-10 if precision == "f64" else 1e-5) * np.abs(want).max()

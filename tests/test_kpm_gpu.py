@@ -529,3 +529,68 @@ def test_vbcsr_subset(torch_cuda):
     assert (b.data.cpu().numpy() == 1.5).all()
     a.set_col(1, b.get_col(0))
     assert np.allclose(a.data[:, 1].cpu().numpy(), 1.5) and a(0, 1) == 1.5
+
+
+# ------------------------------------------------ time propagation, corr DOS
+
+@pytest.mark.parametrize("t", [np.pi, 5 * np.pi, 70 * np.pi, 700 * np.pi, 2000 * np.pi])
+def test_timeprop_coeff_matches_oracle(torch_cuda, t):
+    """timeprop_coeff (cheby.hpp:85-106): the same truncation length as the
+    ascending Bessel evaluation of bessel.hpp, coefficients to 1e-12."""
+    from rsatb_b200.calc import timeprop_coeff
+    got = timeprop_coeff(t)
+    want = oracle.timeprop_coeff(t)
+    assert got.size == want.size
+    assert np.abs(got - want).max() < 1e-12
+    back = timeprop_coeff(t, forward=False)
+    assert np.abs(back - np.conj(want)).max() < 1e-12
+
+
+def test_timeprop_coeff_length_at_production_time(torch_cuda):
+    """test_dos.cpp:235-248: at t = 2000 pi the expansion is finite and has
+    between 6283 and 7000 terms."""
+    from rsatb_b200.calc import timeprop_coeff
+    c = timeprop_coeff(2000 * np.pi)
+    assert np.all(np.isfinite(c)) and 6283 < c.size < 7000
+
+
+def test_corr_series_analytic(torch_cuda):
+    """test_dos.cpp:150-170: with mu_n = cos(n pi / 3) for even n and 0 for
+    odd n, the correlation series is C(t) = cos(t / 2) exactly."""
+    from rsatb_b200.calc import corr_dos, corr_moment_count
+    nt = 40
+    N = corr_moment_count(nt)
+    n = np.arange(N)
+    mu = np.where(n % 2 == 0, np.cos(n * np.pi / 3), 0.0).astype(np.complex128)
+    dos, cdos = corr_dos(mu, nt)
+    assert np.abs(cdos - np.cos(0.5 * np.pi * np.arange(nt + 1))).max() < 1e-10
+    want, want_c = oracle.corr_dos(mu, nt)
+    assert np.abs(cdos - want_c).max() < 1e-12
+    assert np.abs(dos - want).max() < 1e-10 * np.abs(want).max()
+    with pytest.raises(Exception):
+        corr_dos(mu, 0)
+
+
+def test_corr_series_matches_stepwise_propagation(torch_cuda):
+    """test_dos.cpp:171-232: the moment route equals stepwise propagation
+    psi_j = e^{-i Op pi} psi_{j-1} (Chebyshev::propagate) with overlaps
+    <psi_0|psi_j>, to expansion truncation."""
+    torch = torch_cuda
+    from rsatb_b200.calc import corr_dos, corr_moment_count, kpm_dos_moments, timeprop_coeff
+    from rsatb_b200.vbcsr import set_random
+    H = graphene_case(6, 6)
+    c = build_cheby(H, -8.7, 8.9)
+    R, nt = 3, 24
+    psi = torch.empty(H.n_rows, R, dtype=torch.complex128, device="cuda")
+    set_random(psi, 31)
+    mu = kpm_dos_moments(c, psi, corr_moment_count(nt))
+    _, cdos = corr_dos(mu, nt)
+    step = timeprop_coeff(np.pi)
+    cur = psi.clone()
+    nxt = torch.empty_like(psi)
+    stepwise = [complex((psi.conj() * psi).sum().item()) / R]
+    for _ in range(nt):
+        c.propagate(cur, nxt, step)
+        cur, nxt = nxt, cur
+        stepwise.append(complex((psi.conj() * cur).sum().item()) / R)
+    assert np.abs(cdos - np.array(stepwise)).max() < 1e-12

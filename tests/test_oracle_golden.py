@@ -299,3 +299,23 @@ def test_dense_ns_and_eigen_route_agree_on_exact_construction():
         Z, r = oracle.ns_inverse_sqrt_dense(A)
         assert r["converged"]
         assert np.linalg.norm(Z - exact) / ref < 1e-10
+
+
+def test_oracle_corr_series_analytic():
+    """test_dos.cpp:150-170 pins the correlation route: mu_n = cos(n pi / 3)
+    (even n), 0 (odd n) gives C(t) = cos(t / 2) at t = j pi."""
+    nt = 30
+    N = oracle.timeprop_coeff(nt * np.pi).size
+    n = np.arange(N)
+    mu = np.where(n % 2 == 0, np.cos(n * np.pi / 3), 0.0)
+    cd = oracle.corr_from_moments(mu, nt)
+    assert np.abs(cd - np.cos(0.5 * np.pi * np.arange(nt + 1))).max() < 1e-10
+
+
+def test_oracle_timeprop_length():
+    """test_dos.cpp:235-248: 6283 < terms(2000 pi) < 7000, all finite; the
+    forward and backward expansions are conjugate."""
+    c = oracle.timeprop_coeff(2000 * np.pi)
+    assert 6283 < c.size < 7000 and np.all(np.isfinite(c))
+    b = oracle.timeprop_coeff(3.0, forward=False)
+    assert np.allclose(b, np.conj(oracle.timeprop_coeff(3.0)), rtol=0, atol=1e-16)
