@@ -142,6 +142,21 @@ RSATB_API void* rsatb_bsr_values(rsatb_bsr_t A);
 /* Overwrites the values from host (or device with RSATB_BSR_DEVICE_POINTERS). */
 RSATB_API int rsatb_bsr_set_values(rsatb_ctx_t ctx, rsatb_bsr_t A, const void* values, unsigned flags);
 
+/* Bloch sum of real-space images into the values of `out` (C128, its
+ * pattern already set): block s = sum over the bonds e of slot s of
+ * w_e (i if imag_unit) exp(-2 pi i k . R_e) V_e, summed in bond order.
+ * BlochPhase / AddLocalBlock (rsatb/operator/block_assembly.hpp:31-100);
+ * with w_e = (R + r_j - r_i)_a and imag_unit the commutator velocity
+ * (rsatb/operator/commutator_velocity.hpp:114-255).  Device arrays: slot_ptr
+ * (nnz_blocks + 1, int64: bonds slot_ptr[s] .. slot_ptr[s+1]-1 belong to
+ * block s), shifts (3 doubles per bond, in the units k is given against),
+ * image_values (b*b per bond, F64 or C128, row-major), weights (one per
+ * bond, or NULL).  k: host, 3 doubles.  Stream-ordered, no sync. */
+RSATB_API int rsatb_bloch_sum(rsatb_ctx_t ctx, rsatb_bsr_t out, const int64_t* slot_ptr,
+                              const double* shifts, const void* image_values,
+                              rsatb_dtype image_dtype, const double* weights, const double* k,
+                              int imag_unit);
+
 /* Y = alpha * A X.  BlockSpMat::mult_dense (vbcsr), called by
  * Chebyshev::mult_by (rsatb/calc/cheby.hpp:599-606).  X, Y device, N x R of
  * vec_dtype; a real matrix may multiply a complex multivector. */

@@ -256,6 +256,28 @@ def fftcheb(op: OrcOp, V, psi: np.ndarray, n_moments: int, formulation: int = 0,
     return sigma.reshape(n_moments, 6), energy
 
 
+# ------------------------------------------------------------ Bloch sums
+
+def bloch_dense(rows, cols, shifts, blocks, n_block_rows: int, k, weights=None,
+                imag_unit: bool = False, n_block_cols: int | None = None) -> np.ndarray:
+    """Dense H(k) = sum_e w_e (i) exp(-2 pi i k . R_e) H_e at blocks
+    (rows[e], cols[e]) (BlochPhase and AddLocalBlock,
+    rsatb/operator/block_assembly.hpp:31-100)."""
+    blocks = np.asarray(blocks)
+    b = blocks.shape[1]
+    nbc = n_block_cols or n_block_rows
+    out = np.zeros((n_block_rows * b, nbc * b), dtype=np.complex128)
+    ph = np.exp(-2j * np.pi * (np.asarray(shifts, dtype=np.float64) @ np.asarray(k, dtype=np.float64)))
+    if weights is not None:
+        ph = ph * np.asarray(weights)
+    if imag_unit:
+        ph = 1j * ph
+    for e in range(len(rows)):
+        i, j = int(rows[e]), int(cols[e])
+        out[i * b:(i + 1) * b, j * b:(j + 1) * b] += ph[e] * blocks[e]
+    return out
+
+
 # ------------------------------------------------------ correlation-series DOS
 
 def timeprop_coeff(time_step: float, precision: float = 1e-14, forward: bool = True) -> np.ndarray:

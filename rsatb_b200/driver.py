@@ -18,6 +18,7 @@ import numpy as np
 import torch
 
 from . import lattice
+from .bloch import ImageOperator
 from .bounds import estimate_spectral_bounds
 from .calc import (Chebyshev, ISQRTMPreconditioner, corr_dos, corr_moment_count,
                    dos_energy_grid, dos_moment_count, evaluate_kpm_density, kpm_dos_moments,
@@ -66,23 +67,36 @@ def _volume(cell: np.ndarray, axis: str) -> float:
 class RSATB:
     """``_rsatb.RSATB`` for prebuilt operators.
 
-    H: Hamiltonian (BlockSpMat or lattice.BsrArrays, real, Gamma point).
-    Z: graph-local factor of the overlap (non-orthogonal basis: the sandwich
-    form Z^H H Z), or None.  velocities: (Vx, Vy, Vz) real matrices W_a of the
-    velocities i W_a (for compute_dc_spectrum).  cell: 3 x 3 lattice vectors
-    in Angstrom (rows a, b, c).  orbitals_per_atom / atom_index key the
-    seeded sample vectors by atom, as SampleVectors::initialize does.
+    H: Hamiltonian, either one matrix (BlockSpMat or lattice.BsrArrays: the
+    Gamma point) or a ``bloch.ImageOperator`` of real-space images, summed on
+    the device at every k-point of ``options.kpoints`` (fractional, against
+    the image shifts).  Z: graph-local factor of the overlap (non-orthogonal
+    basis: the sandwich form Z^H H Z; one matrix only), or None.  velocities:
+    (Vx, Vy, Vz) real matrices W_a of the velocities i W_a (for
+    compute_dc_spectrum, Gamma only).  cell: 3 x 3 lattice vectors in
+    Angstrom (rows a, b, c).  orbitals_per_atom / atom_index key the seeded
+    sample vectors by atom, as SampleVectors::initialize does.
     """
 
     def __init__(self, H, options: SetupOptions | None = None, Z=None, velocities=None,
                  cell=None, orbitals_per_atom: int = 1, atom_index=None,
                  spin_degeneracy: float = 2.0):
         self.options = options or SetupOptions()
-        if any(np.any(np.asarray(k) != 0.0) for k in self.options.kpoints):
-            raise NotImplementedError("only the Gamma point is served (real operators)")
         if self.options.precision not in ("f64", "mixed"):
             raise ValueError("precision must be 'f64' or 'mixed'")
-        self.H = _as_device(H)
+        self.kpoints = [np.asarray(k, dtype=np.float64).reshape(3) for k in self.options.kpoints]
+        if not self.kpoints:
+            raise ValueError("kpoints must hold at least one k-point")
+        self.images = H if isinstance(H, ImageOperator) else None
+        if self.images is None:
+            if any(np.any(k != 0.0) for k in self.kpoints):
+                raise ValueError("k-points other than Gamma need the operator's images "
+                                 "(bloch.ImageOperator)")
+            self.H = _as_device(H)
+        else:
+            if Z is not None:
+                raise NotImplementedError("the sandwich form takes one matrix, not images")
+            self.H = self.images.at_k(self.kpoints[0])
         self.Z = _as_device(Z) if Z is not None else None
         self.V = None
         if velocities is not None:
@@ -103,14 +117,24 @@ class RSATB:
 
     # -- operators --------------------------------------------------------
 
-    def _cheby(self, emin: float, emax: float, mixed: bool) -> Chebyshev:
+    def _operator(self, kidx: int) -> BlockSpMat:
+        if self.images is None or kidx == 0:
+            return self.H
+        return self.images.at_k(self.kpoints[kidx])
+
+    def _cheby(self, emin: float, emax: float, mixed: bool, kidx: int = 0) -> Chebyshev:
         pre = ISQRTMPreconditioner(self.Z) if self.Z is not None else None
-        c = Chebyshev(self.H, emin, emax, preconditioner=pre)
+        c = Chebyshev(self._operator(kidx), emin, emax, preconditioner=pre)
         return c.astype("f32") if mixed else c
 
     def _estimate_bounds(self):
-        c = self._cheby(-1.0, 1.0, False)
-        return estimate_spectral_bounds(c)
+        """The widest padded Lanczos window over the k-points (the reference
+        keeps one window for all of them, OperatorSet::emin/emax)."""
+        lo, hi = np.inf, -np.inf
+        for kidx in range(len(self.kpoints)):
+            a, b = estimate_spectral_bounds(self._cheby(-1.0, 1.0, False, kidx))
+            lo, hi = min(lo, a), max(hi, b)
+        return lo, hi
 
     def energy_bounds(self):
         """(emin, emax) of the operator, padded as the reference pads its
@@ -148,14 +172,17 @@ class RSATB:
         else:
             N = corr_moment_count(nt, device=dev)
         mixed = self.options.precision == "mixed"
-        c = self._cheby(emin, emax, mixed)
         psi = self._samples(torch.complex64 if mixed else torch.complex128)
-        mu = kpm_dos_moments(c, psi, N)
-        if method == "corr":
-            dos, _ = corr_dos(mu, nt, device=dev)
-            return dos, omega
-        rho = evaluate_kpm_density(mu, x, 0.5 / nt, device=dev)
-        return 2.0 * rho, omega
+        out = []
+        for kidx in range(len(self.kpoints)):
+            # One DOS of 2 nt points per k-point, in k-point order
+            # (observables.hpp:368, 383-386: offset k_idx * 2 nt).
+            mu = kpm_dos_moments(self._cheby(emin, emax, mixed, kidx), psi, N)
+            if method == "corr":
+                out.append(corr_dos(mu, nt, device=dev)[0])
+            else:
+                out.append(2.0 * evaluate_kpm_density(mu, x, 0.5 / nt, device=dev))
+        return np.concatenate(out), omega
 
     def compute_dc_spectrum(self, n_moments: int, formulation: str = "greenwood",
                             axis: str = "abc", partition_sections: int = 0,
@@ -170,6 +197,8 @@ class RSATB:
             raise ValueError("compute_dc_spectrum needs the velocity matrices")
         if self.cell is None:
             raise ValueError("compute_dc_spectrum needs the cell for its normalisation")
+        if self.images is not None or len(self.kpoints) != 1:
+            raise NotImplementedError("compute_dc_spectrum: one real operator at Gamma only")
         forms = {"greenwood": GREENWOOD, "bastin": BASTIN}
         if formulation not in forms:
             raise ValueError(f"Unknown dc formulation: {formulation}")

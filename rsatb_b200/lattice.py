@@ -103,6 +103,41 @@ def graphene(n1: int = 60, n2: int = 60, t: float = -2.7, a_cc: float = 1.42):
     return BsrArrays(row_ptr, col_ind, vals, 1), pos, cell
 
 
+def graphene_images(n1: int = 60, n2: int = 60, t: float = -2.7, a_cc: float = 1.42):
+    """The bonds of graphene()'s n1 x n2 supercell as real-space images: for
+    every A atom the three bonds to B at cells (i, j), (i - 1, j), (i, j - 1),
+    and their reverses, each with its supercell image shift R (integer, in
+    units of the supercell vectors) and bond vector r_j + R - r_i.  Any
+    n1, n2 >= 1 (a 1 x 1 cell has three images of the one A-B pair).
+    Returns (rows, cols, shifts[n, 3], blocks[n, 1, 1], bond_vectors[n, 3],
+    n_atoms, cell[3, 3])."""
+    a = math.sqrt(3.0) * a_cc
+    a1 = np.array([a, 0.0, 0.0])
+    a2 = np.array([a / 2, a * math.sqrt(3.0) / 2, 0.0])
+    delta = (a1 + a2) / 3.0
+    i, j = np.meshgrid(np.arange(n1), np.arange(n2), indexing="ij")
+    i = i.ravel(order="F")
+    j = j.ravel(order="F")
+    A = 2 * (i + n1 * j)
+    rows, cols, shifts, vecs = [], [], [], []
+    for di, dj in ((0, 0), (-1, 0), (0, -1)):
+        ii, jj = i + di, j + dj
+        B = 2 * ((ii % n1) + n1 * (jj % n2)) + 1
+        R = np.stack([np.floor_divide(ii, n1), np.floor_divide(jj, n2), np.zeros_like(ii)], 1)
+        d = delta + di * a1 + dj * a2
+        rows += [A, B]
+        cols += [B, A]
+        shifts += [R, -R]
+        vecs += [np.tile(d, (A.size, 1)), np.tile(-d, (A.size, 1))]
+    rows = np.concatenate(rows)
+    cols = np.concatenate(cols)
+    shifts = np.concatenate(shifts).astype(np.float64)
+    vecs = np.concatenate(vecs)
+    blocks = np.full((rows.size, 1, 1), float(t))
+    cell = np.array([n1 * a1, n2 * a2, [0.0, 0.0, 20.0]])
+    return rows, cols, shifts, blocks, vecs, 2 * n1 * n2, cell
+
+
 # ------------------------------------------------------------------- diamond
 
 _DIAMOND_BASIS4 = np.array([[0, 0, 0], [0, 2, 2], [2, 0, 2], [2, 2, 0],

@@ -144,3 +144,45 @@ def test_compute_dos_corr_matches_oracle(precision):
     want, _ = oracle.corr_dos(oracle.kpm_moments(op, psi, N), nt)
     assert dos.shape == (2 * nt,) and np.array_equal(omega, omega_o)
     assert np.abs(dos - want).max() < (1e-10 if precision == "f64" else 1e-5) * np.abs(want).max()
+
+
+@pytest.mark.gpu
+def test_compute_dos_kpoints_matches_oracle():
+    """k-points from real-space images: one DOS of 2 nt points per k-point,
+    in k-point order (observables.hpp:368-386), each equal to the oracle's
+    KPM density of the oracle's dense Bloch sum; the estimated window holds
+    every band of every k-point."""
+    import torch
+    from rsatb_b200 import lattice
+    from rsatb_b200.bloch import ImageOperator
+    from rsatb_b200.calc import dos_energy_grid, dos_moment_count
+    from rsatb_b200.driver import RSATB, SetupOptions
+    from rsatb_b200.lattice import BsrArrays
+    torch.cuda.set_device(0)
+    r, c, sh, bl, bv, n, cell = lattice.graphene_images(6, 6)
+    op = ImageOperator(r, c, sh, bl, 1, n, bond_vectors=bv)
+    kpts = [[0.0, 0.0, 0.0], [0.25, 0.1, 0.0], [0.5, 0.5, 0.0]]
+    emin, emax = -8.6, 8.7
+    calc = RSATB(op, SetupOptions(kpoints=kpts, nsamples=2, sample_seed=3,
+                                  energy_bounds=(emin, emax)))
+    dE = 0.3
+    dos, omega = calc.compute_dos(dE)
+    x, _, nt = dos_energy_grid(emin, emax, dE)
+    N = dos_moment_count((emax - emin) / 2, dE)
+    psi = _oracle_samples(n, 2, 3)
+    assert dos.shape == (3 * 2 * nt,)
+    rows = np.repeat(np.arange(n), np.diff(op.row_ptr))
+    for q, k in enumerate(kpts):
+        Hd = oracle.bloch_dense(r, c, sh, bl, n, k)
+        A = BsrArrays(op.row_ptr, op.col_ind, Hd[rows, op.col_ind].reshape(-1, 1, 1), 1)
+        mu = oracle.kpm_moments(oracle.make_op(to_oracle(A), (emax + emin) / 2,
+                                               (emax - emin) / 2), psi, N)
+        want = 2.0 * oracle.density(mu, x, 0.5 / nt)
+        assert rel_err(dos[q * 2 * nt:(q + 1) * 2 * nt], want) < 1e-10
+    est = RSATB(op, SetupOptions(kpoints=kpts))
+    lo, hi = est.energy_bounds()
+    for k in kpts:
+        w = np.linalg.eigvalsh(oracle.bloch_dense(r, c, sh, bl, n, k))
+        assert lo < w[0] and hi > w[-1]
+    with pytest.raises(ValueError):
+        RSATB(lattice.graphene(6, 6)[0], SetupOptions(kpoints=kpts))
