@@ -388,9 +388,6 @@ int launch_dmma_k(rsatb_context* ctx, StepArgs& a) {
             case 16: return launch_dmma_c<VT, W, CV, 16>(ctx, a);
         }
         if (dmma_chunk_env()) return launch_dmma_u<VT, W, CV, 0, dmma_warps<VT>(), true>(ctx, a);
-        // FP32 W = 8: 16-warp CTAs (diamond 16^3, 8x8 blocks: 0.0784 ->
-        // 0.0723 ms; other narrow shapes within 3 % of their defaults).
-        if constexpr (sizeof(VT) == 4 && W == 8) return launch_dmma_u<VT, W, CV, 0, 16>(ctx, a);
     }
     return launch_dmma_u<VT, W, CV, 0>(ctx, a);
 }
