@@ -73,7 +73,8 @@ class RSATB:
     the image shifts).  Z: graph-local factor of the overlap (non-orthogonal
     basis: the sandwich form Z^H H Z; one matrix only), or None.  velocities:
     (Vx, Vy, Vz) real matrices W_a of the velocities i W_a (for
-    compute_dc_spectrum, Gamma only).  cell: 3 x 3 lattice vectors in
+    compute_dc_spectrum with one matrix H; with images they are summed from
+    the bond vectors).  cell: 3 x 3 lattice vectors in
     Angstrom (rows a, b, c).  orbitals_per_atom / atom_index key the seeded
     sample vectors by atom, as SampleVectors::initialize does.
     """
@@ -99,6 +100,8 @@ class RSATB:
             self.H = self.images.at_k(self.kpoints[0])
         self.Z = _as_device(Z) if Z is not None else None
         self.V = None
+        if velocities is not None and self.images is not None:
+            raise ValueError("with images the velocities come from the bond vectors")
         if velocities is not None:
             self.V = [v if isinstance(v, BlockSpMat) else
                       BlockSpMat(v.row_ptr, v.col_ind, v.values, v.block_size, v.n_block_cols,
@@ -189,16 +192,16 @@ class RSATB:
                             max_workspace_mb: float = 0, kernel: str = "jackson",
                             method: str = "fftcheb"):
         """ComputeDcSpectrum (observables.hpp:691-780) with the fftcheb method:
-        prefactor pi g_s (4 Greenwood, 8 Bastin) norb / volume(axis).
-        Returns (sigma[n_moments * 6], energy[n_moments])."""
+        prefactor pi g_s (4 Greenwood, 8 Bastin) norb / volume(axis).  With
+        images, H(k) and the commutator velocities V_a(k) are summed on the
+        device for every k-point.  Returns (sigma[n_k * n_moments * 6],
+        energy[n_moments]), one block of sigma per k-point in k-point order."""
         if method != "fftcheb":
             raise NotImplementedError(f"dc method '{method}': only 'fftcheb' is served")
-        if self.V is None:
+        if self.V is None and self.images is None:
             raise ValueError("compute_dc_spectrum needs the velocity matrices")
         if self.cell is None:
             raise ValueError("compute_dc_spectrum needs the cell for its normalisation")
-        if self.images is not None or len(self.kpoints) != 1:
-            raise NotImplementedError("compute_dc_spectrum: one real operator at Gamma only")
         forms = {"greenwood": GREENWOOD, "bastin": BASTIN}
         if formulation not in forms:
             raise ValueError(f"Unknown dc formulation: {formulation}")
@@ -206,14 +209,24 @@ class RSATB:
             raise ValueError(f"axis must be a subset of 'abc', got '{axis}'")
         emin, emax = self.energy_bounds()
         mixed = self.options.precision == "mixed"
-        c = self._cheby(emin, emax, mixed)
-        V = [v.astype("f32") for v in self.V] if mixed else self.V
         psi = self._samples(torch.complex64 if mixed else torch.complex128)
         norb = self.H.shape[0]
         trace_prefactor = norb / _volume(self.cell, axis)
         prefactor = (math.pi * self.spin_degeneracy *
                      (4.0 if formulation == "greenwood" else 8.0) * trace_prefactor)
-        sigma, energy = dc_spectrum_fftcheb(
-            c, *V, psi, int(n_moments), forms[formulation], prefactor,
-            int(partition_sections), float(max_workspace_mb), parse_kpm_kernel(kernel))
-        return sigma.reshape(-1), energy
+        sigmas, energy = [], None
+        for kidx, k in enumerate(self.kpoints):
+            c = self._cheby(emin, emax, mixed, kidx)
+            if self.images is not None:
+                V = [self.images.velocity_at_k(k, a) for a in range(3)]
+            else:
+                V = self.V
+            if mixed:
+                V = [v.astype("f32") for v in V]
+            sigma, en = dc_spectrum_fftcheb(
+                c, *V, psi, int(n_moments), forms[formulation], prefactor,
+                int(partition_sections), float(max_workspace_mb), parse_kpm_kernel(kernel))
+            sigmas.append(sigma.reshape(-1))
+            if energy is None:
+                energy = en
+        return np.concatenate(sigmas), energy

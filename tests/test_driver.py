@@ -186,3 +186,47 @@ def test_compute_dos_kpoints_matches_oracle():
         assert lo < w[0] and hi > w[-1]
     with pytest.raises(ValueError):
         RSATB(lattice.graphene(6, 6)[0], SetupOptions(kpoints=kpts))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("formulation", ["greenwood", "bastin"])
+def test_compute_dc_spectrum_kpoints_matches_oracle(formulation):
+    """Transport at k-points from images: H(k) and V_a(k) (complex, summed
+    on the device) per k-point, one sigma block each (observables.hpp:
+    741-772), against the oracle's fftcheb on its own dense Bloch sums."""
+    import torch
+    from rsatb_b200 import lattice
+    from rsatb_b200.bloch import ImageOperator
+    from rsatb_b200.driver import RSATB, SetupOptions, _volume
+    from rsatb_b200.lattice import BsrArrays
+    torch.cuda.set_device(0)
+    r, c, sh, bl, bv, n, cell = lattice.graphene_images(6, 5)
+    op = ImageOperator(r, c, sh, bl, 1, n, bond_vectors=bv)
+    kpts = [[0.0, 0.0, 0.0], [0.2, 0.35, 0.0]]
+    emin, emax = -8.7, 8.8
+    calc = RSATB(op, SetupOptions(kpoints=kpts, nsamples=2, sample_seed=21,
+                                  energy_bounds=(emin, emax)), cell=cell)
+    M = 40
+    sigma, energy = calc.compute_dc_spectrum(M, formulation=formulation, axis="ab")
+    assert sigma.shape == (2 * M * 6,)
+    psi = _oracle_samples(n, 2, 21)
+    rows = np.repeat(np.arange(n), np.diff(op.row_ptr))
+
+    def at(dense, imag=False):
+        vals = dense[rows, op.col_ind].reshape(-1, 1, 1)
+        return to_oracle(BsrArrays(op.row_ptr, op.col_ind, vals, 1))
+
+    pref = np.pi * 2.0 * (4.0 if formulation == "greenwood" else 8.0) * n / _volume(cell, "ab")
+    for q, k in enumerate(kpts):
+        Ho = at(oracle.bloch_dense(r, c, sh, bl, n, k))
+        Vo = [at(oracle.bloch_dense(r, c, sh, bl, n, k, weights=bv[:, a], imag_unit=True))
+              for a in range(3)]
+        oop = oracle.make_op(Ho, (emax + emin) / 2, (emax - emin) / 2)
+        sig_o, en_o = oracle.fftcheb(oop, Vo, psi, M,
+                                     formulation=0 if formulation == "greenwood" else 1,
+                                     prefactor=pref)
+        assert rel_err(sigma[q * M * 6:(q + 1) * M * 6], sig_o.reshape(-1)) < 1e-10
+        assert np.allclose(energy, en_o, rtol=0, atol=1e-13)
+    with pytest.raises(ValueError):
+        RSATB(op, SetupOptions(kpoints=kpts, energy_bounds=(emin, emax)), cell=cell,
+              velocities=(None, None, None))
