@@ -62,10 +62,12 @@ typedef enum {
 } rsatb_dtype;
 
 /* Operator forms, rsatb::calc::ChebyOpForm (rsatb/calc/cheby.hpp:78-82).
- * The Solve form (CG per matvec) is not implemented on the device. */
+ * The Solve form runs one batched CG with S per application; it is served
+ * by rsatb_cheb_apply_op and (plain recurrence) rsatb_kpm_dos_moments. */
 typedef enum {
     RSATB_FORM_ORTHOGONAL = 0,
-    RSATB_FORM_SANDWICH = 1
+    RSATB_FORM_SANDWICH = 1,
+    RSATB_FORM_SOLVE = 2
 } rsatb_form;
 
 /* Summation kernels, rsatb::calc::KpmKernel (rsatb/calc/kpm.hpp:49). */
@@ -157,6 +159,18 @@ RSATB_API int rsatb_bloch_sum(rsatb_ctx_t ctx, rsatb_bsr_t out, const int64_t* s
                               rsatb_dtype image_dtype, const double* weights, const double* k,
                               int imag_unit);
 
+/* Solves S X = B for every column (rsatb::calc::LinearSolver::solve for a
+ * multivector, rsatb/calc/solver.hpp:216-312): batched CG from X's
+ * contents, per-column step lengths, a column below tol or at breakdown
+ * frozen, stopping when the largest column residual |r| < tol or after
+ * max_iter iterations.  S square SPD (Hermitian), B and X device panels of
+ * n_vectors (1..256) columns, distinct, 16-byte aligned.  iterations and
+ * max_residual (host, may be NULL) receive the count and the final
+ * residual.  Reads the residuals back every iteration (synchronises). */
+RSATB_API int rsatb_cg_solve(rsatb_ctx_t ctx, rsatb_bsr_t S, const void* B, void* X,
+                             int n_vectors, rsatb_dtype vec_dtype, double tol, int max_iter,
+                             int* iterations, double* max_residual);
+
 /* Y = alpha * A X.  BlockSpMat::mult_dense (vbcsr), called by
  * Chebyshev::mult_by (rsatb/calc/cheby.hpp:599-606).  X, Y device, N x R of
  * vec_dtype; a real matrix may multiply a complex multivector. */
@@ -166,7 +180,10 @@ RSATB_API int rsatb_bsr_mult_dense(rsatb_ctx_t ctx, rsatb_bsr_t A, const void* X
 /* ----------------------------------------------------- rescaled operator */
 
 /* The operator a Chebyshev<T> iterates (rsatb/calc/cheby.hpp:147-201):
- * Orthogonal: H;  Sandwich: Z^H H Z with Z and its adjoint ZH.
+ * Orthogonal: H;  Sandwich: Z^H H Z with Z and its adjoint ZH;  Solve:
+ * S^-1 H with the overlap S, one unpreconditioned batched CG per
+ * application (LinearSolver(1e-8, 1000), cheby.hpp:188-192; cg_tol and
+ * cg_max_iter 0 select those defaults).
  * Every matrix must share one precision; the multivectors passed with the
  * operator must have that precision too (F64/C128 or F32/C64). */
 typedef struct {
@@ -176,6 +193,9 @@ typedef struct {
     rsatb_bsr_t ZH;      /* sandwich only: Z^H (rsatb_bsr_adjoint) */
     double center;       /* (emax + emin)/2 */
     double half_width;   /* (emax - emin)/2 */
+    rsatb_bsr_t S;       /* solve only: the overlap, SPD */
+    double cg_tol;       /* solve only: largest column residual |r| at exit */
+    int cg_max_iter;     /* solve only: CG iterations per application at most */
 } rsatb_cheb_op;
 
 /* Y = ((Op) X - center X) / half_width.  Chebyshev::apply_op NORMAL

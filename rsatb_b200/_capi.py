@@ -22,7 +22,7 @@ STATUS_NAMES = {
 # rsatb_dtype
 F64, F32, C128, C64 = 0, 1, 2, 3
 # rsatb_form
-FORM_ORTHOGONAL, FORM_SANDWICH = 0, 1
+FORM_ORTHOGONAL, FORM_SANDWICH, FORM_SOLVE = 0, 1, 2
 # rsatb_kpm_kernel
 KPM_NONE, KPM_JACKSON, KPM_COSTAPER, KPM_VPTAPER = 0, 1, 2, 3
 # rsatb_random_kind
@@ -41,7 +41,8 @@ class RsatbError(RuntimeError):
 
 class ChebOp(C.Structure):
     _fields_ = [("form", C.c_int), ("H", C.c_void_p), ("Z", C.c_void_p), ("ZH", C.c_void_p),
-                ("center", C.c_double), ("half_width", C.c_double)]
+                ("center", C.c_double), ("half_width", C.c_double), ("S", C.c_void_p),
+                ("cg_tol", C.c_double), ("cg_max_iter", C.c_int)]
 
 
 class IsqrtOptions(C.Structure):
@@ -111,6 +112,7 @@ SIGNATURES = {
     "rsatb_timeprop_coeff": (_i, [_vp, _d, _d, _i, _i, _PD, C.POINTER(_i)]),
     "rsatb_corr_dos": (_i, [_vp, _PD, _i, _i, _d, _PD, _PD]),
     "rsatb_bloch_sum": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _vp, _PD, _i]),
+    "rsatb_cg_solve": (_i, [_vp, _vp, _vp, _vp, _i, _i, _d, _i, C.POINTER(_i), _PD]),
     "rsatb_kpm_moments_vjp": (_i, [_vp, C.POINTER(ChebOp), _vp, _i, _i, _i, _PD, _i, _PD, _vp,
                                    C.POINTER(AdjointStats)]),
     "rsatb_dc_spectrum_fftcheb": (_i, [_vp, C.POINTER(ChebOp), _vp, _vp, _vp, _vp, _i, _i, _i,

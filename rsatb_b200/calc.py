@@ -83,16 +83,31 @@ class Chebyshev:
 
     ``Chebyshev(H, emin, emax)`` is the Orthogonal form;
     ``Chebyshev(H, emin, emax, preconditioner=pre)`` the Sandwich form
-    Z^H H Z.  The Solve form (a CG per matvec) is not provided.
+    Z^H H Z;  ``Chebyshev(H, emin, emax, overlap=S)`` the Solve form S^-1 H,
+    one batched CG with S per application (cheby.hpp:188-192; tolerance
+    ``cg_tol`` 1e-8 and at most ``cg_max_iter`` 1000 iterations, as
+    LinearSolver's defaults).  The Solve form serves ``apply_op`` and the
+    plain moment recurrence.
     """
 
     def __init__(self, H: BlockSpMat, emin: float, emax: float,
-                 preconditioner: ISQRTMPreconditioner | None = None, verbose: bool = False):
+                 preconditioner: ISQRTMPreconditioner | None = None, verbose: bool = False,
+                 overlap: BlockSpMat | None = None, cg_tol: float = 1e-8,
+                 cg_max_iter: int = 1000):
         if H.shape[0] != H.shape[1]:
             raise ValueError("H must be square")
+        if overlap is not None and preconditioner is not None:
+            raise ValueError("the Solve form takes S, the Sandwich form a preconditioner: not both")
+        if overlap is not None and overlap.shape != H.shape:
+            raise ValueError("S and H shapes differ")
         self.H = H
         self.M = preconditioner
-        self.form = ChebyOpForm.Sandwich if preconditioner is not None else ChebyOpForm.Orthogonal
+        self.S = overlap
+        self.cg_tol, self.cg_max_iter = float(cg_tol), int(cg_max_iter)
+        if overlap is not None:
+            self.form = ChebyOpForm.Solve
+        else:
+            self.form = ChebyOpForm.Sandwich if preconditioner is not None else ChebyOpForm.Orthogonal
         self.verbose = verbose
         self.set_window(emin, emax)
 
@@ -110,29 +125,39 @@ class Chebyshev:
         return self.H.is_double
 
     def op_is_hermitian(self) -> bool:
-        """cheby.hpp:222: every form here is Hermitian."""
+        """cheby.hpp:222: Orthogonal and Sandwich are Hermitian, Solve is not."""
         return self.form != ChebyOpForm.Solve
 
     def astype(self, precision: str) -> "Chebyshev":
         """A copy whose matrices are stored in 'f64' or 'f32'."""
         pre = self.M.astype(precision) if self.M is not None else None
+        S = self.S.astype(precision) if self.S is not None else None
         c = Chebyshev(self.H.astype(precision), self.center - self.half_width,
-                      self.center + self.half_width, preconditioner=pre)
+                      self.center + self.half_width, preconditioner=pre, overlap=S,
+                      cg_tol=self.cg_tol, cg_max_iter=self.cg_max_iter)
         return c
 
     def c_op(self) -> _capi.ChebOp:
         op = _capi.ChebOp()
-        op.form = _capi.FORM_SANDWICH if self.form == ChebyOpForm.Sandwich else _capi.FORM_ORTHOGONAL
+        op.form = {ChebyOpForm.Sandwich: _capi.FORM_SANDWICH, ChebyOpForm.Solve: _capi.FORM_SOLVE,
+                   ChebyOpForm.Orthogonal: _capi.FORM_ORTHOGONAL}[self.form]
         op.H = self.H.handle
         if self.M is not None:
             op.Z = self.M.Z.handle
             op.ZH = self.M.ZH.handle
+        if self.S is not None:
+            op.S = self.S.handle
+            op.cg_tol = self.cg_tol
+            op.cg_max_iter = self.cg_max_iter
         op.center = self.center
         op.half_width = self.half_width
         return op
 
     def apply_op(self, X: torch.Tensor, Y: torch.Tensor, mode: ChebyMode = ChebyMode.NORMAL):
-        """Y = Op~ X (cheby.hpp:232-235); ADJOINT equals NORMAL for these forms."""
+        """Y = Op~ X (cheby.hpp:232-235); ADJOINT equals NORMAL for the
+        Hermitian forms.  Solve form: Y's contents start the CG."""
+        if self.form == ChebyOpForm.Solve and mode == ChebyMode.ADJOINT:
+            raise NotImplementedError("the Solve form serves NORMAL applications only")
         ctx = self.H.ctx
         ctx.bind_stream()
         op = self.c_op()
@@ -298,6 +323,25 @@ def corr_dos(moments, nt: int, precision: float = 1e-14, device=None):
                                int(nt), float(precision),
                                cdos.view(np.float64).ctypes.data_as(P), dos.ctypes.data_as(P)))
     return dos, cdos
+
+
+def cg_solve(S: BlockSpMat, B: torch.Tensor, X: torch.Tensor, tol: float = 1e-8,
+             max_iter: int = 1000):
+    """X = S^-1 B column by column by batched CG from X's contents
+    (LinearSolver::solve, solver.hpp:216-312).  Returns (iterations,
+    largest column residual)."""
+    for T in (B, X):
+        if not T.is_cuda or T.dim() != 2 or not T.is_contiguous():
+            raise ValueError("B and X must be contiguous (N, R) CUDA tensors")
+    if B.shape != X.shape or B.dtype != X.dtype:
+        raise ValueError("B and X must have one shape and dtype")
+    ctx = S.ctx
+    ctx.bind_stream()
+    it, res = C.c_int(0), C.c_double(0.0)
+    check(lib().rsatb_cg_solve(ctx.handle, S.handle, C.c_void_p(B.data_ptr()),
+                               C.c_void_p(X.data_ptr()), B.shape[1], dtype_code(B.dtype),
+                               float(tol), int(max_iter), C.byref(it), C.byref(res)))
+    return it.value, res.value
 
 
 def dos_energy_grid(emin: float, emax: float, de_ev: float):

@@ -24,6 +24,12 @@ int run_persistent_recurrence(rsatb_context* ctx, const rsatb_bsr_matrix* H, int
                               void* const buf[3], int n_steps, double* part, size_t part_capacity,
                               double* dots, unsigned* bar, unsigned* fault, bool* done);
 
+int solve_form_apply(rsatb_context* ctx, const rsatb_cheb_op* op, const void* X, void* Y,
+                     int n_vectors, int vdt);
+int solve_form_moments(rsatb_context* ctx, const rsatb_cheb_op* op, const void* psi,
+                       int n_vectors, int vdt, int n_moments, double* mu_out,
+                       double* col_mu_out);
+
 int run_coldot(rsatb_context* ctx, int vdt, int64_t n_rows, const StepArgs& a) {
     return dtype_is_double(vdt) ? launch_coldot_f64(ctx, vdt, n_rows, a)
                                 : launch_coldot_f32(ctx, vdt, n_rows, a);
@@ -322,6 +328,13 @@ int rsatb_cheb_apply_op(rsatb_ctx_t ctx, const rsatb_cheb_op* op, const void* X,
                         int n_vectors, rsatb_dtype vec_dtype) {
     clear_error();
     RSATB_TRY(check_ctx(ctx));
+    if (op && op->form == RSATB_FORM_SOLVE) {
+        if (!X || !Y) return set_error(RSATB_INVALID_ARGUMENT, "null multivector");
+        if (!aligned16(X) || !aligned16(Y))
+            return set_error(RSATB_INVALID_ARGUMENT, "multivectors must be 16-byte aligned");
+        if (X == Y) return set_error(RSATB_INVALID_ARGUMENT, "apply_op cannot run in place");
+        return solve_form_apply(ctx, op, X, Y, n_vectors, vec_dtype);
+    }
     OpShape sh{};
     RSATB_TRY(check_op(op, vec_dtype, &sh));
     int W = 0;
@@ -348,6 +361,17 @@ int rsatb_kpm_dos_moments(rsatb_ctx_t ctx, const rsatb_cheb_op* op, const void* 
                           double* mu_out, double* col_mu_out) {
     clear_error();
     RSATB_TRY(check_ctx(ctx));
+    if (op && op->form == RSATB_FORM_SOLVE) {
+        if (n_moments <= 0) return set_error(RSATB_INVALID_ARGUMENT, "n_moments must be positive");
+        if (!psi || !mu_out) return set_error(RSATB_INVALID_ARGUMENT, "null psi or mu_out");
+        if (!aligned16(psi)) return set_error(RSATB_INVALID_ARGUMENT, "psi must be 16-byte aligned");
+        if (doubled)
+            return set_error(RSATB_INVALID_ARGUMENT,
+                             "the Solve form S^-1 H is not Hermitian: use the plain recurrence "
+                             "(doubled = 0)");
+        return solve_form_moments(ctx, op, psi, n_vectors, vec_dtype, n_moments, mu_out,
+                                  col_mu_out);
+    }
     OpShape sh{};
     RSATB_TRY(check_op(op, vec_dtype, &sh));
     int W = 0;

@@ -1,0 +1,115 @@
+"""The Solve operator form S^-1 H: the batched CG (rsatb_cg_solve,
+LinearSolver::solve for a multivector, rsatb/calc/solver.hpp:216-312), the
+operator application (Chebyshev::apply_form's Solve branch,
+rsatb/calc/cheby.hpp:569-590) and the plain KPM recurrence over it
+(dos.hpp:172-187), against dense FP64 solves and the oracle's dense
+recurrence."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle
+from _util import rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    torch.cuda.set_device(0)
+    return torch
+
+
+@pytest.fixture(scope="module")
+def diamond():
+    from rsatb_b200 import lattice
+    H, S = lattice.diamond_lcao(L=2, seed=3)
+    Hd, Sd = H.to_dense(), S.to_dense()
+    assert np.linalg.eigvalsh(Sd)[0] > 0.05
+    w = np.linalg.eigvals(np.linalg.solve(Sd, Hd)).real
+    return H, S, Hd, Sd, w.min() - 0.5, w.max() + 0.5
+
+
+def _dev(A, precision="f64"):
+    from rsatb_b200.vbcsr import BlockSpMat
+    M = BlockSpMat(A.row_ptr, A.col_ind, A.values, A.block_size)
+    return M.astype("f32") if precision == "f32" else M
+
+
+@pytest.mark.parametrize("cplx,precision", [(False, "f64"), (True, "f64"), (False, "f32")])
+def test_cg_solve_matches_dense(torch_cuda, diamond, cplx, precision):
+    torch = torch_cuda
+    from rsatb_b200.calc import cg_solve
+    H, S, Hd, Sd, _, _ = diamond
+    rng = np.random.default_rng(5)
+    n, R = Sd.shape[0], (3 if cplx else 5)
+    B = rng.standard_normal((n, R))
+    if cplx:
+        B = B + 1j * rng.standard_normal((n, R))
+    B[:, 1] = 0.0   # a zero right-hand side freezes at once (no 0/0)
+    dt = {(False, "f64"): torch.float64, (True, "f64"): torch.complex128,
+          (False, "f32"): torch.float32}[(cplx, precision)]
+    Bd = torch.as_tensor(B).to(dt).cuda().contiguous()
+    Xd = torch.zeros_like(Bd)
+    tol = 1e-12 if precision == "f64" else 1e-4
+    it, res = cg_solve(_dev(S, precision), Bd, Xd, tol=tol, max_iter=500)
+    want = np.linalg.solve(Sd, B)
+    got = Xd.cpu().numpy()
+    assert res < tol and 0 < it < 500
+    assert rel_err(got, want) < (1e-10 if precision == "f64" else 1e-4)
+    assert np.all(got[:, 1] == 0)
+    # started from the solution, the CG stops after one iteration
+    it2, res2 = cg_solve(_dev(S, precision), Bd, Xd, tol=max(tol, 10 * res), max_iter=500)
+    assert it2 == 1
+
+
+def test_solve_form_apply_matches_dense(torch_cuda, diamond):
+    torch = torch_cuda
+    from rsatb_b200.calc import Chebyshev
+    H, S, Hd, Sd, emin, emax = diamond
+    c = Chebyshev(_dev(H), emin, emax, overlap=_dev(S), cg_tol=1e-12)
+    rng = np.random.default_rng(2)
+    X = rng.standard_normal((Hd.shape[0], 4)) + 1j * rng.standard_normal((Hd.shape[0], 4))
+    Xd = torch.as_tensor(X).cuda().contiguous()
+    Yd = torch.zeros_like(Xd)
+    c.apply_op(Xd, Yd)
+    cen, hw = (emax + emin) / 2, (emax - emin) / 2
+    want = (np.linalg.solve(Sd, Hd @ X) - cen * X) / hw
+    assert rel_err(Yd.cpu().numpy(), want) < 1e-10
+
+
+@pytest.mark.parametrize("cg_tol,tol", [(1e-12, 1e-9), (1e-8, 1e-5)])
+def test_solve_form_moments_match_oracle(torch_cuda, diamond, cg_tol, tol):
+    """Plain moments of S^-1 H (op_is_hermitian() is false for this form)
+    against the oracle's dense recurrence on S^-1 H."""
+    torch = torch_cuda
+    from rsatb_b200.calc import Chebyshev, kpm_dos_moments
+    from rsatb_b200.vbcsr import set_random
+    H, S, Hd, Sd, emin, emax = diamond
+    c = Chebyshev(_dev(H), emin, emax, overlap=_dev(S), cg_tol=cg_tol)
+    assert not c.op_is_hermitian()
+    psi = torch.empty(Hd.shape[0], 4, dtype=torch.float64, device="cuda")
+    set_random(psi, 9)
+    mu = kpm_dos_moments(c, psi, 40)
+    want = oracle.kpm_plain_moments_dense(np.linalg.solve(Sd, Hd), psi.cpu().numpy(),
+                                          (emax + emin) / 2, (emax - emin) / 2, 40)
+    assert np.abs(mu.real - want).max() < tol * abs(want[0])
+    assert np.abs(mu.imag).max() == 0.0
+
+
+def test_solve_form_refuses_doubling_and_other_entries(torch_cuda, diamond):
+    torch = torch_cuda
+    from rsatb_b200._capi import RsatbError
+    from rsatb_b200.calc import Chebyshev, _moments
+    H, S, Hd, Sd, emin, emax = diamond
+    c = Chebyshev(_dev(H), emin, emax, overlap=_dev(S))
+    psi = torch.ones(Hd.shape[0], 2, dtype=torch.float64, device="cuda")
+    with pytest.raises(RsatbError):
+        _moments(c, psi, 8, doubled=True)
+    Y = torch.empty_like(psi)
+    with pytest.raises(RsatbError):
+        c.propagate(psi, Y, [1.0, 0.5])
+    with pytest.raises(ValueError):
+        Chebyshev(_dev(H), emin, emax, overlap=_dev(S), preconditioner=object())
