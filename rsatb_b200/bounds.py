@@ -21,8 +21,14 @@ PADDING = 0.5  # eV, spectral_bounds.hpp:75
 
 def lanczos_extremes(cheby: Chebyshev, steps: int = 20, seed: int = 2):
     """(theta_min, theta_max, res_min, res_max) of the operator cheby iterates
-    (its window is ignored: the operator is applied unscaled)."""
-    unit = Chebyshev(cheby.H, -1.0, 1.0, preconditioner=cheby.M)  # center 0, half_width 1
+    (its window is ignored: the operator is applied unscaled).  For the
+    Solve form S^-1 H the Lanczos basis is S-orthonormal (S^-1 H is
+    self-adjoint in the S inner product), the generalised problem
+    H x = lambda S x that the reference hands to PRIMME."""
+    S = getattr(cheby, "S", None)
+    unit = Chebyshev(cheby.H, -1.0, 1.0, preconditioner=cheby.M, overlap=S,
+                     cg_tol=getattr(cheby, "cg_tol", 1e-8),
+                     cg_max_iter=getattr(cheby, "cg_max_iter", 1000))  # center 0, half_width 1
     n = cheby.n_rows
     dt = torch.complex128 if cheby.H.is_complex or cheby.H.imaginary else torch.float64
     if not cheby.H.is_double:
@@ -33,30 +39,41 @@ def lanczos_extremes(cheby: Chebyshev, steps: int = 20, seed: int = 2):
     v = torch.empty(n, 1, dtype=dt, device=dev)
     set_random(v, seed, normalize=True)
     v = v.to(wdt)
-    v = v / torch.linalg.vector_norm(v)
     m = min(steps, n)
+
+    def metric(x):  # S x for the Solve form, x otherwise
+        if S is None:
+            return x
+        out = torch.empty_like(x.to(dt).contiguous())
+        S.mult_dense(x.to(dt).contiguous(), out)
+        return out.to(wdt)
+
+    v = v / torch.sqrt(torch.vdot(v[:, 0], metric(v)[:, 0]).real)
     Q = torch.zeros(n, m, dtype=wdt, device=dev)
+    SQ = torch.zeros(n, m, dtype=wdt, device=dev)
     alpha = np.zeros(m)
     beta = np.zeros(m)
-    w = torch.empty_like(v)
+    w = torch.zeros_like(v.to(dt))
     q = v
     for j in range(m):
         Q[:, j] = q[:, 0]
+        SQ[:, j] = metric(q)[:, 0]
+        w.zero_()
         unit.apply_op(q.to(dt).contiguous(), w)
         wc = w.to(wdt)
-        a = torch.vdot(q[:, 0], wc[:, 0]).real.item()
+        a = torch.vdot(SQ[:, j], wc[:, 0]).real.item()
         alpha[j] = a
-        wc = wc - Q[:, :j + 1] @ (Q[:, :j + 1].conj().T @ wc)   # full reorthogonalisation
-        wc = wc - Q[:, :j + 1] @ (Q[:, :j + 1].conj().T @ wc)
-        b = torch.linalg.vector_norm(wc).item()
+        for _ in range(2):  # full reorthogonalisation in the (S) inner product
+            wc = wc - Q[:, :j + 1] @ (SQ[:, :j + 1].conj().T @ wc)
+        b = torch.sqrt(torch.vdot(wc[:, 0], metric(wc)[:, 0]).real.clamp(min=0.0)).item()
         beta[j] = b
         if b < 1e-12 * max(1.0, abs(a)):
             m = j + 1
             break
         q = wc / b
     T = np.diag(alpha[:m]) + np.diag(beta[:m - 1], 1) + np.diag(beta[:m - 1], -1)
-    theta, S = np.linalg.eigh(T)
-    res = np.abs(beta[m - 1] * S[-1, :])
+    theta, Y = np.linalg.eigh(T)
+    res = np.abs(beta[m - 1] * Y[-1, :])
     return float(theta[0]), float(theta[-1]), float(res[0]), float(res[-1])
 
 

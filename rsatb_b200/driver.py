@@ -29,6 +29,22 @@ from .vbcsr import BlockSpMat, set_random
 
 
 @dataclass
+class PreconditionerOptions:
+    """rsatb::model::PreconditionerOptions (rsatb/model/setup.hpp:33-51):
+    operator_form 'solve' (S^-1 H, a CG with S per application) or
+    'sandwich' (Z^H H Z).  tol, sptol and maxiter configure the reference's
+    construction of Z, which happens outside this package (Z is passed in);
+    cg_tol and cg_max_iter are the Solve form's CG settings (LinearSolver's
+    1e-8 and 1000)."""
+    operator_form: str = "solve"
+    tol: float = 1e-7
+    sptol: float = 1e-5
+    maxiter: int = 0
+    cg_tol: float = 1e-8
+    cg_max_iter: int = 1000
+
+
+@dataclass
 class SetupOptions:
     """rsatb::model::SetupOptions (pybind_rsatb.cpp:263-341): sampling and
     spectral bounds.  Only the Gamma point is served (real operators);
@@ -41,6 +57,7 @@ class SetupOptions:
     energy_bounds: tuple | None = None
     bounds_zero_tol: float = 1e-12
     bounds_max_matvecs: int = 10000
+    preconditioner: PreconditionerOptions = field(default_factory=PreconditionerOptions)
     precision: str = "f64"
 
 
@@ -81,7 +98,7 @@ class RSATB:
 
     def __init__(self, H, options: SetupOptions | None = None, Z=None, velocities=None,
                  cell=None, orbitals_per_atom: int = 1, atom_index=None,
-                 spin_degeneracy: float = 2.0):
+                 spin_degeneracy: float = 2.0, S=None):
         self.options = options or SetupOptions()
         if self.options.precision not in ("f64", "mixed"):
             raise ValueError("precision must be 'f64' or 'mixed'")
@@ -99,6 +116,20 @@ class RSATB:
                 raise NotImplementedError("the sandwich form takes one matrix, not images")
             self.H = self.images.at_k(self.kpoints[0])
         self.Z = _as_device(Z) if Z is not None else None
+        self.S = _as_device(S) if S is not None else None
+        form = self.options.preconditioner.operator_form.strip().lower()
+        if form not in ("solve", "sandwich"):
+            raise ValueError(f"Unknown operator form '{form}' (expected solve or sandwich)")
+        # An orthogonal basis passes neither matrix; otherwise the form picks
+        # which of S and Z the operator uses (ParseOperatorForm, setup.hpp:54).
+        if self.S is not None and self.Z is not None:
+            raise ValueError("pass S for the solve form or Z for the sandwich form, not both")
+        if self.S is not None and form != "solve":
+            raise ValueError("S was given but operator_form is 'sandwich' (pass Z)")
+        if self.Z is not None and form != "sandwich":
+            raise ValueError("Z was given but operator_form is 'solve' (pass S)")
+        if self.S is not None and self.images is not None:
+            raise NotImplementedError("the solve form takes one matrix, not images")
         self.V = None
         if velocities is not None and self.images is not None:
             raise ValueError("with images the velocities come from the bond vectors")
@@ -127,7 +158,9 @@ class RSATB:
 
     def _cheby(self, emin: float, emax: float, mixed: bool, kidx: int = 0) -> Chebyshev:
         pre = ISQRTMPreconditioner(self.Z) if self.Z is not None else None
-        c = Chebyshev(self._operator(kidx), emin, emax, preconditioner=pre)
+        po = self.options.preconditioner
+        c = Chebyshev(self._operator(kidx), emin, emax, preconditioner=pre, overlap=self.S,
+                      cg_tol=po.cg_tol, cg_max_iter=po.cg_max_iter)
         return c.astype("f32") if mixed else c
 
     def _estimate_bounds(self):
@@ -202,6 +235,9 @@ class RSATB:
             raise ValueError("compute_dc_spectrum needs the velocity matrices")
         if self.cell is None:
             raise ValueError("compute_dc_spectrum needs the cell for its normalisation")
+        if self.S is not None:
+            raise NotImplementedError("compute_dc_spectrum: the solve form is not served; use "
+                                      "operator_form 'sandwich' with Z")
         forms = {"greenwood": GREENWOOD, "bastin": BASTIN}
         if formulation not in forms:
             raise ValueError(f"Unknown dc formulation: {formulation}")

@@ -230,3 +230,49 @@ def test_compute_dc_spectrum_kpoints_matches_oracle(formulation):
     with pytest.raises(ValueError):
         RSATB(op, SetupOptions(kpoints=kpts, energy_bounds=(emin, emax)), cell=cell,
               velocities=(None, None, None))
+
+
+@pytest.mark.gpu
+def test_compute_dos_solve_form():
+    """PreconditionerOptions(operator_form='solve'): the DOS of S^-1 H by the
+    plain recurrence with a CG per application, against a dense FP64
+    recurrence on S^-1 H with the same samples; the estimated window (an
+    S-orthonormal Lanczos) holds the generalised spectrum."""
+    import torch
+    from rsatb_b200 import lattice
+    from rsatb_b200.calc import dos_energy_grid, dos_moment_count
+    from rsatb_b200.driver import PreconditionerOptions, RSATB, SetupOptions
+    torch.cuda.set_device(0)
+    H, S = lattice.diamond_lcao(L=2, seed=3)
+    Hd, Sd = H.to_dense(), S.to_dense()
+    A = np.linalg.solve(Sd, Hd)
+    w = np.sort(np.linalg.eigvals(A).real)
+    est = RSATB(H, SetupOptions(preconditioner=PreconditionerOptions(cg_tol=1e-12)), S=S)
+    lo, hi = est.energy_bounds()
+    assert lo < w[0] and hi > w[-1]
+    emin, emax = w[0] - 0.5, w[-1] + 0.5
+    calc = RSATB(H, SetupOptions(nsamples=2, sample_seed=4, energy_bounds=(emin, emax),
+                                 preconditioner=PreconditionerOptions(cg_tol=1e-12)), S=S)
+    dE = 0.6
+    dos, omega = calc.compute_dos(dE)
+    x, _, nt = dos_energy_grid(emin, emax, dE)
+    N = dos_moment_count((emax - emin) / 2, dE)
+    psi = _oracle_samples(H.n_rows, 2, 4)
+    c, hw = (emax + emin) / 2, (emax - emin) / 2
+    At = (A - c * np.eye(A.shape[0])) / hw
+    t0, t1 = psi, At @ psi
+    mu = np.zeros(N, dtype=np.complex128)
+    mu[0] = np.sum(psi.conj() * t0) / 2
+    mu[1] = np.sum(psi.conj() * t1) / 2
+    for n in range(2, N):
+        t0, t1 = t1, 2 * At @ t1 - t0
+        mu[n] = np.sum(psi.conj() * t1) / 2
+    want = 2.0 * oracle.density(mu, x, 0.5 / nt)
+    assert rel_err(dos, want) < 1e-8
+    with pytest.raises(ValueError):
+        RSATB(H, SetupOptions(preconditioner=PreconditionerOptions(operator_form="sandwich")),
+              S=S)
+    with pytest.raises(ValueError):
+        PreconditionerOptions(operator_form="cg") and RSATB(
+            H, SetupOptions(preconditioner=PreconditionerOptions(operator_form="cg"),
+                            energy_bounds=(emin, emax)))
