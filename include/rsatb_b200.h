@@ -163,13 +163,16 @@ RSATB_API int rsatb_bloch_sum(rsatb_ctx_t ctx, rsatb_bsr_t out, const int64_t* s
  * multivector, rsatb/calc/solver.hpp:216-312): batched CG from X's
  * contents, per-column step lengths, a column below tol or at breakdown
  * frozen, stopping when the largest column residual |r| < tol or after
- * max_iter iterations.  S square SPD (Hermitian), B and X device panels of
+ * max_iter iterations.  With Z and ZH = Z^H (both or neither): symmetric
+ * preconditioning by the graph-local factor (solver.hpp:329-338), the CG on
+ * Z^H S Z Y = Z^H B from Y = 0 and X = Z Y, tol then bounding that
+ * system's residual.  S square SPD (Hermitian), B and X device panels of
  * n_vectors (1..256) columns, distinct, 16-byte aligned.  iterations and
  * max_residual (host, may be NULL) receive the count and the final
  * residual.  Reads the residuals back every iteration (synchronises). */
-RSATB_API int rsatb_cg_solve(rsatb_ctx_t ctx, rsatb_bsr_t S, const void* B, void* X,
-                             int n_vectors, rsatb_dtype vec_dtype, double tol, int max_iter,
-                             int* iterations, double* max_residual);
+RSATB_API int rsatb_cg_solve(rsatb_ctx_t ctx, rsatb_bsr_t S, rsatb_bsr_t Z, rsatb_bsr_t ZH,
+                             const void* B, void* X, int n_vectors, rsatb_dtype vec_dtype,
+                             double tol, int max_iter, int* iterations, double* max_residual);
 
 /* Y = alpha * A X.  BlockSpMat::mult_dense (vbcsr), called by
  * Chebyshev::mult_by (rsatb/calc/cheby.hpp:599-606).  X, Y device, N x R of
@@ -181,9 +184,11 @@ RSATB_API int rsatb_bsr_mult_dense(rsatb_ctx_t ctx, rsatb_bsr_t A, const void* X
 
 /* The operator a Chebyshev<T> iterates (rsatb/calc/cheby.hpp:147-201):
  * Orthogonal: H;  Sandwich: Z^H H Z with Z and its adjoint ZH;  Solve:
- * S^-1 H with the overlap S, one unpreconditioned batched CG per
- * application (LinearSolver(1e-8, 1000), cheby.hpp:188-192; cg_tol and
- * cg_max_iter 0 select those defaults).
+ * S^-1 H with the overlap S, one batched CG per application
+ * (LinearSolver(1e-8, 1000), cheby.hpp:188-199; cg_tol and cg_max_iter 0
+ * select those defaults), preconditioned symmetrically by Z when Z and ZH
+ * are set (the reference's default route: the graph-local seed
+ * preconditions an exact solve).
  * Every matrix must share one precision; the multivectors passed with the
  * operator must have that precision too (F64/C128 or F32/C64). */
 typedef struct {

@@ -86,8 +86,9 @@ class Chebyshev:
     Z^H H Z;  ``Chebyshev(H, emin, emax, overlap=S)`` the Solve form S^-1 H,
     one batched CG with S per application (cheby.hpp:188-192; tolerance
     ``cg_tol`` 1e-8 and at most ``cg_max_iter`` 1000 iterations, as
-    LinearSolver's defaults).  The Solve form serves ``apply_op`` and the
-    plain moment recurrence.
+    LinearSolver's defaults), preconditioned by the factor of
+    ``preconditioner`` when one is given as well.  The Solve form serves
+    ``apply_op`` and the plain moment recurrence.
     """
 
     def __init__(self, H: BlockSpMat, emin: float, emax: float,
@@ -96,8 +97,6 @@ class Chebyshev:
                  cg_max_iter: int = 1000):
         if H.shape[0] != H.shape[1]:
             raise ValueError("H must be square")
-        if overlap is not None and preconditioner is not None:
-            raise ValueError("the Solve form takes S, the Sandwich form a preconditioner: not both")
         if overlap is not None and overlap.shape != H.shape:
             raise ValueError("S and H shapes differ")
         self.H = H
@@ -105,6 +104,8 @@ class Chebyshev:
         self.S = overlap
         self.cg_tol, self.cg_max_iter = float(cg_tol), int(cg_max_iter)
         if overlap is not None:
+            # With a preconditioner too: its factor preconditions the CG
+            # symmetrically (cheby.hpp:195-199), the operator stays S^-1 H.
             self.form = ChebyOpForm.Solve
         else:
             self.form = ChebyOpForm.Sandwich if preconditioner is not None else ChebyOpForm.Orthogonal
@@ -326,10 +327,11 @@ def corr_dos(moments, nt: int, precision: float = 1e-14, device=None):
 
 
 def cg_solve(S: BlockSpMat, B: torch.Tensor, X: torch.Tensor, tol: float = 1e-8,
-             max_iter: int = 1000):
+             max_iter: int = 1000, preconditioner: "ISQRTMPreconditioner | None" = None):
     """X = S^-1 B column by column by batched CG from X's contents
-    (LinearSolver::solve, solver.hpp:216-312).  Returns (iterations,
-    largest column residual)."""
+    (LinearSolver::solve, solver.hpp:216-312), or with the graph-local
+    factor as symmetric preconditioner (solver.hpp:329-338).  Returns
+    (iterations, largest column residual)."""
     for T in (B, X):
         if not T.is_cuda or T.dim() != 2 or not T.is_contiguous():
             raise ValueError("B and X must be contiguous (N, R) CUDA tensors")
@@ -338,7 +340,9 @@ def cg_solve(S: BlockSpMat, B: torch.Tensor, X: torch.Tensor, tol: float = 1e-8,
     ctx = S.ctx
     ctx.bind_stream()
     it, res = C.c_int(0), C.c_double(0.0)
-    check(lib().rsatb_cg_solve(ctx.handle, S.handle, C.c_void_p(B.data_ptr()),
+    Z = preconditioner.Z.handle if preconditioner is not None else None
+    ZH = preconditioner.ZH.handle if preconditioner is not None else None
+    check(lib().rsatb_cg_solve(ctx.handle, S.handle, Z, ZH, C.c_void_p(B.data_ptr()),
                                C.c_void_p(X.data_ptr()), B.shape[1], dtype_code(B.dtype),
                                float(tol), int(max_iter), C.byref(it), C.byref(res)))
     return it.value, res.value

@@ -15,7 +15,8 @@
 // epilogue; the per-column dots are FP64 and deterministic (fixed-order
 // partial sums per CTA, then over CTAs); alpha and beta are formed on the
 // device; the host reads the column residuals once per iteration for the
-// stopping test.
+// stopping test.  With the graph-local factor Z (ISQRTMPreconditioner, whose
+// type is Symmetric) the CG runs on Z^H S Z Y = Z^H B and X = Z Y.
 #include "cheb_kernels.cuh"
 
 #include <algorithm>
@@ -158,6 +159,10 @@ struct SolveWork {
     void* P;
     void* AP;
     void* tmp;
+    void* u1;   // Z p (preconditioned operator)
+    void* u2;   // S Z p
+    void* Yp;   // solution of the preconditioned system
+    void* Bp;   // its right-hand side Z^H b
     double2* part;
     double2* d_rr;
     double2* d_rr2;
@@ -258,11 +263,23 @@ StepArgs plain_args(int W, const void* in, void* y) {
     return a;
 }
 
-// Batched CG for S X = B from X's contents (solver.hpp:216-312).
-int cg_solve(const SolveCall& s, const SolveWork& w, const rsatb_bsr_matrix* S, const void* B,
-             void* X, double tol, int max_iter, int* iters_out, double* resid_out) {
-    // R = B - S X, P = R
-    RSATB_TRY(run_step(s.ctx, S, s.vdt, plain_args(s.W, X, w.AP)));
+// out = S in, or Z^H S Z in when a symmetric preconditioner Z is given
+// (SymPrecondMat::mult_dense, rsatb/calc/preconditioner.hpp:249-262).
+int apply_A(const SolveCall& s, const SolveWork& w, const rsatb_bsr_matrix* S,
+            const rsatb_bsr_matrix* Z, const rsatb_bsr_matrix* ZH, const void* in, void* out) {
+    if (!Z) return run_step(s.ctx, S, s.vdt, plain_args(s.W, in, out));
+    RSATB_TRY(run_step(s.ctx, Z, s.vdt, plain_args(s.W, in, w.u1)));
+    RSATB_TRY(run_step(s.ctx, S, s.vdt, plain_args(s.W, w.u1, w.u2)));
+    return run_step(s.ctx, ZH, s.vdt, plain_args(s.W, w.u2, out));
+}
+
+// Batched CG for A X = B from X's contents (solver.hpp:216-312), A = S or
+// Z^H S Z.
+int cg_core(const SolveCall& s, const SolveWork& w, const rsatb_bsr_matrix* S,
+            const rsatb_bsr_matrix* Z, const rsatb_bsr_matrix* ZH, const void* B, void* X,
+            double tol, int max_iter, int* iters_out, double* resid_out) {
+    // R = B - A X, P = R
+    RSATB_TRY(apply_A(s, w, S, Z, ZH, X, w.AP));
     RSATB_CUDA_TRY(cudaMemcpyAsync(w.R, B, s.vbytes, cudaMemcpyDeviceToDevice, s.ctx->stream));
     RSATB_TRY(axpby(s, -1.0, w.AP, 1.0, w.R));
     RSATB_CUDA_TRY(cudaMemcpyAsync(w.P, w.R, s.vbytes, cudaMemcpyDeviceToDevice, s.ctx->stream));
@@ -273,7 +290,7 @@ int cg_solve(const SolveCall& s, const SolveWork& w, const rsatb_bsr_matrix* S, 
     int it = 0;
     double max_err = 0.0;
     for (int k = 0; k < max_iter; ++k) {
-        RSATB_TRY(run_step(s.ctx, S, s.vdt, plain_args(s.W, w.P, w.AP)));
+        RSATB_TRY(apply_A(s, w, S, Z, ZH, w.P, w.AP));
         RSATB_TRY(dots(s, w, w.P, w.AP, w.d_pap));
         cg_alpha_kernel<<<(s.ncols + 127) / 128, 128, 0, s.ctx->stream>>>(rr, w.d_pap, s.ncols,
                                                                          tol * tol, w.d_alpha);
@@ -295,6 +312,19 @@ int cg_solve(const SolveCall& s, const SolveWork& w, const rsatb_bsr_matrix* S, 
     if (!std::isfinite(max_err))
         return set_error(RSATB_NUMERICAL_FAILURE, "cg: residual is not finite");
     return RSATB_SUCCESS;
+}
+
+// S X = B.  With Z: the explicitly symmetric-preconditioned system
+// Z^H S Z Y = Z^H B from Y = 0, then X = Z Y (solver.hpp:329-338); X's
+// contents are not used then.  Without: CG from X's contents.
+int cg_solve(const SolveCall& s, const SolveWork& w, const rsatb_bsr_matrix* S,
+             const rsatb_bsr_matrix* Z, const rsatb_bsr_matrix* ZH, const void* B, void* X,
+             double tol, int max_iter, int* iters_out, double* resid_out) {
+    if (!Z) return cg_core(s, w, S, nullptr, nullptr, B, X, tol, max_iter, iters_out, resid_out);
+    RSATB_TRY(run_step(s.ctx, ZH, s.vdt, plain_args(s.W, B, w.Bp)));
+    RSATB_CUDA_TRY(cudaMemsetAsync(w.Yp, 0, s.vbytes, s.ctx->stream));
+    RSATB_TRY(cg_core(s, w, S, Z, ZH, w.Bp, w.Yp, tol, max_iter, iters_out, resid_out));
+    return run_step(s.ctx, Z, s.vdt, plain_args(s.W, w.Yp, X));
 }
 
 int solve_setup(rsatb_context* ctx, const rsatb_bsr_matrix* S, int vdt, int n_vectors,
@@ -322,7 +352,7 @@ int solve_setup(rsatb_context* ctx, const rsatb_bsr_matrix* S, int vdt, int n_ve
                                                          int64_t(ctx->sm_count) * 4)));
     const size_t part_b = ((sizeof(double2) * size_t(w->grid) * n_vectors) + 255) & ~size_t(255);
     const size_t col_b = ((sizeof(double2) * n_vectors) + 255) & ~size_t(255);
-    const int n_panels = 4 + extra_panels;
+    const int n_panels = 8 + extra_panels;
     void* base = nullptr;
     RSATB_TRY(ctx_scratch(ctx, n_panels * vb + part_b + 5 * col_b, &base));
     char* p = static_cast<char*>(base);
@@ -330,7 +360,11 @@ int solve_setup(rsatb_context* ctx, const rsatb_bsr_matrix* S, int vdt, int n_ve
     w->P = p + vb;
     w->AP = p + 2 * vb;
     w->tmp = p + 3 * vb;
-    for (int i = 0; i < extra_panels; ++i) panels[i] = p + (4 + i) * vb;
+    w->u1 = p + 4 * vb;
+    w->u2 = p + 5 * vb;
+    w->Yp = p + 6 * vb;
+    w->Bp = p + 7 * vb;
+    for (int i = 0; i < extra_panels; ++i) panels[i] = p + (8 + i) * vb;
     char* q = p + n_panels * vb;
     w->part = reinterpret_cast<double2*>(q);
     q += part_b;
@@ -355,6 +389,17 @@ int check_solve_op(const rsatb_cheb_op* op, int vdt) {
         return set_error(RSATB_INVALID_ARGUMENT, "H and the multivector types do not match");
     if (!(op->half_width > 0.0) || !std::isfinite(op->center))
         return set_error(RSATB_INVALID_ARGUMENT, "spectral window needs half_width > 0");
+    if ((op->Z == nullptr) != (op->ZH == nullptr))
+        return set_error(RSATB_INVALID_ARGUMENT, "a preconditioned Solve form needs Z and ZH");
+    if (op->Z) {
+        RSATB_TRY(check_bsr(op->Z, "Z"));
+        RSATB_TRY(check_bsr(op->ZH, "ZH"));
+        if (op->Z->n_block_rows != op->H->n_block_rows || op->Z->block_size != op->H->block_size ||
+            op->ZH->n_block_rows != op->H->n_block_rows || op->ZH->block_size != op->H->block_size ||
+            dtype_is_double(op->Z->dtype) != dtype_is_double(vdt) ||
+            dtype_is_double(op->ZH->dtype) != dtype_is_double(vdt))
+            return set_error(RSATB_INVALID_ARGUMENT, "Z, ZH and H shapes or precisions differ");
+    }
     if (op->cg_tol < 0.0 || op->cg_max_iter < 0)
         return set_error(RSATB_INVALID_ARGUMENT, "cg_tol and cg_max_iter must not be negative");
     return RSATB_SUCCESS;
@@ -368,7 +413,8 @@ int op_iters(const rsatb_cheb_op* op) { return op->cg_max_iter > 0 ? op->cg_max_
 int apply_solve(const SolveCall& s, const SolveWork& w, const rsatb_cheb_op* op, const void* x,
                 void* y, int* iters, double* resid) {
     RSATB_TRY(run_step(s.ctx, op->H, s.vdt, plain_args(s.W, x, w.tmp)));
-    RSATB_TRY(cg_solve(s, w, op->S, w.tmp, y, op_tol(op), op_iters(op), iters, resid));
+    RSATB_TRY(cg_solve(s, w, op->S, op->Z, op->ZH, w.tmp, y, op_tol(op), op_iters(op), iters,
+                       resid));
     return axpby(s, -op->center / op->half_width, x, 1.0 / op->half_width, y);
 }
 
@@ -443,9 +489,9 @@ int solve_form_moments(rsatb_context* ctx, const rsatb_cheb_op* op, const void* 
 
 using namespace rsatb_b200;
 
-extern "C" int rsatb_cg_solve(rsatb_ctx_t ctx, rsatb_bsr_t S, const void* B, void* X,
-                              int n_vectors, rsatb_dtype vec_dtype, double tol, int max_iter,
-                              int* iterations, double* max_residual) {
+extern "C" int rsatb_cg_solve(rsatb_ctx_t ctx, rsatb_bsr_t S, rsatb_bsr_t Z, rsatb_bsr_t ZH,
+                              const void* B, void* X, int n_vectors, rsatb_dtype vec_dtype,
+                              double tol, int max_iter, int* iterations, double* max_residual) {
     clear_error();
     RSATB_TRY(check_ctx(ctx));
     if (!B || !X) return set_error(RSATB_INVALID_ARGUMENT, "null multivector");
@@ -454,12 +500,22 @@ extern "C" int rsatb_cg_solve(rsatb_ctx_t ctx, rsatb_bsr_t S, const void* B, voi
         return set_error(RSATB_INVALID_ARGUMENT, "multivectors must be 16-byte aligned");
     if (!(tol > 0.0) || max_iter < 1)
         return set_error(RSATB_INVALID_ARGUMENT, "cg needs tol > 0 and max_iter >= 1");
+    if ((Z == nullptr) != (ZH == nullptr))
+        return set_error(RSATB_INVALID_ARGUMENT, "the preconditioner needs Z and ZH");
     SolveCall s{};
     SolveWork w{};
     RSATB_TRY(solve_setup(ctx, S, vec_dtype, n_vectors, 0, &s, &w, nullptr));
+    if (Z) {
+        RSATB_TRY(check_bsr(Z, "Z"));
+        RSATB_TRY(check_bsr(ZH, "ZH"));
+        if (Z->n_block_rows != S->n_block_rows || Z->block_size != S->block_size ||
+            ZH->n_block_rows != S->n_block_rows || ZH->block_size != S->block_size ||
+            Z->dtype != S->dtype || ZH->dtype != S->dtype)
+            return set_error(RSATB_INVALID_ARGUMENT, "Z, ZH and S shapes or types differ");
+    }
     int it = 0;
     double res = 0.0;
-    RSATB_TRY(cg_solve(s, w, S, B, X, tol, max_iter, &it, &res));
+    RSATB_TRY(cg_solve(s, w, S, Z, ZH, B, X, tol, max_iter, &it, &res));
     if (iterations) *iterations = it;
     if (max_residual) *max_residual = res;
     return RSATB_SUCCESS;

@@ -122,12 +122,12 @@ class RSATB:
             raise ValueError(f"Unknown operator form '{form}' (expected solve or sandwich)")
         # An orthogonal basis passes neither matrix; otherwise the form picks
         # which of S and Z the operator uses (ParseOperatorForm, setup.hpp:54).
-        if self.S is not None and self.Z is not None:
-            raise ValueError("pass S for the solve form or Z for the sandwich form, not both")
+        # 'solve' takes S (and Z, if given, preconditions its CG, the
+        # reference's default route); 'sandwich' takes Z alone.
         if self.S is not None and form != "solve":
-            raise ValueError("S was given but operator_form is 'sandwich' (pass Z)")
-        if self.Z is not None and form != "sandwich":
-            raise ValueError("Z was given but operator_form is 'solve' (pass S)")
+            raise ValueError("S was given but operator_form is 'sandwich' (pass Z alone)")
+        if self.Z is not None and self.S is None and form != "sandwich":
+            raise ValueError("operator_form 'solve' needs S (Z alone gives the sandwich form)")
         if self.S is not None and self.images is not None:
             raise NotImplementedError("the solve form takes one matrix, not images")
         self.V = None

@@ -111,5 +111,43 @@ def test_solve_form_refuses_doubling_and_other_entries(torch_cuda, diamond):
     Y = torch.empty_like(psi)
     with pytest.raises(RsatbError):
         c.propagate(psi, Y, [1.0, 0.5])
-    with pytest.raises(ValueError):
-        Chebyshev(_dev(H), emin, emax, overlap=_dev(S), preconditioner=object())
+
+
+def _factor(S):
+    from rsatb_b200.calc import ISQRTMPreconditioner
+    from rsatb_b200.isqrt import graph_inverse_sqrt_host
+    return ISQRTMPreconditioner(_dev(graph_inverse_sqrt_host(S)))
+
+
+def test_preconditioned_cg_matches_dense(torch_cuda, diamond):
+    """Symmetric preconditioning by the graph-local factor Z
+    (solver.hpp:329-338): Z^H S Z Y = Z^H B from Y = 0, X = Z Y; the same
+    solution as the dense solve in fewer iterations than the plain CG."""
+    torch = torch_cuda
+    from rsatb_b200.calc import cg_solve
+    H, S, Hd, Sd, _, _ = diamond
+    rng = np.random.default_rng(8)
+    B = rng.standard_normal((Sd.shape[0], 6))
+    Bd = torch.as_tensor(B).cuda().contiguous()
+    X0 = torch.zeros_like(Bd)
+    it0, _ = cg_solve(_dev(S), Bd, X0, tol=1e-12, max_iter=500)
+    X1 = torch.full_like(Bd, 7.0)   # ignored: the preconditioned solve starts from Y = 0
+    it1, res1 = cg_solve(_dev(S), Bd, X1, tol=1e-12, max_iter=500, preconditioner=_factor(S))
+    want = np.linalg.solve(Sd, B)
+    assert res1 < 1e-12 and it1 < it0
+    assert rel_err(X1.cpu().numpy(), want) < 1e-10
+
+
+def test_preconditioned_solve_form_moments(torch_cuda, diamond):
+    torch = torch_cuda
+    from rsatb_b200.calc import Chebyshev, kpm_dos_moments
+    from rsatb_b200.vbcsr import set_random
+    H, S, Hd, Sd, emin, emax = diamond
+    c = Chebyshev(_dev(H), emin, emax, overlap=_dev(S), preconditioner=_factor(S), cg_tol=1e-12)
+    assert c.form.name == "Solve"
+    psi = torch.empty(Hd.shape[0], 3, dtype=torch.float64, device="cuda")
+    set_random(psi, 12)
+    mu = kpm_dos_moments(c, psi, 32)
+    want = oracle.kpm_plain_moments_dense(np.linalg.solve(Sd, Hd), psi.cpu().numpy(),
+                                          (emax + emin) / 2, (emax - emin) / 2, 32)
+    assert np.abs(mu.real - want).max() < 1e-9 * abs(want[0])
