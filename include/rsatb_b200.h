@@ -307,6 +307,18 @@ RSATB_API int rsatb_timeprop_coeff(rsatb_ctx_t ctx, double time_step, double pre
 RSATB_API int rsatb_corr_dos(rsatb_ctx_t ctx, const double* moments, int n_moments, int nt,
                              double precision, double* cdos_out, double* dos_out);
 
+/* sigma(mu, T) of the six tensor components from a zero-temperature
+ * spectrum, rsatb::calc::integrate_dc_spectrum
+ * (rsatb/calc/fftcheb_transport.hpp:950-1040): T <= 0 interpolates linearly
+ * at mu (clamped to the grid's ends); T > 0 (kelvin) integrates the
+ * piecewise-linear spectrum exactly against -df/dE.  sigma: host,
+ * n_energy x 6; energy: host, n_energy values, strictly ascending when
+ * T > 0 (else RSATB_INVALID_ARGUMENT); sigma_out: host, 6 values.
+ * Computed on the device (one thread per component, energy order). */
+RSATB_API int rsatb_integrate_dc_spectrum(rsatb_ctx_t ctx, const double* sigma,
+                                          const double* energy, int n_energy, double mu,
+                                          double temp, double* sigma_out);
+
 /* ------------------------------------------------------------ adjoint KPM */
 
 /* Counters of one rsatb_kpm_moments_vjp call. */

@@ -278,6 +278,47 @@ def bloch_dense(rows, cols, shifts, blocks, n_block_rows: int, k, weights=None,
     return out
 
 
+# ------------------------------------------------- finite-temperature sigma
+
+def integrate_dc_spectrum(sigma: np.ndarray, energy: np.ndarray, mu: float,
+                          temp: float) -> np.ndarray:
+    """rsatb/calc/fftcheb_transport.hpp:950-1040 (with fermi_dirac_energy
+    :67-82): interpolation at T <= 0, the exact integral of the
+    piecewise-linear spectrum against -df/dE at T > 0."""
+    import math
+    s = np.asarray(sigma, dtype=np.float64).reshape(-1, 6)
+    e = np.asarray(energy, dtype=np.float64)
+    out = np.zeros(6)
+    if e.size == 0:
+        return out
+    if temp <= 0.0:
+        for c in range(6):
+            out[c] = np.interp(mu, e, s[:, c])
+        return out
+    kb = 8.617333262e-5
+    kt = kb * temp
+
+    def f(x):
+        beta = 1.0 / kt
+        if x >= mu:
+            t = math.exp(beta * (mu - x))
+            return t / (1.0 + t)
+        t = math.exp(beta * (x - mu))
+        return 1.0 / (1.0 + t)
+
+    def F(x):
+        y = (x - mu) / kt
+        return x - kt * (max(y, 0.0) + math.log1p(math.exp(-abs(y))))
+
+    for i in range(1, e.size):
+        e0, e1 = e[i - 1], e[i]
+        de = e1 - e0
+        w = f(e0) - f(e1)
+        m = F(e1) - F(e0) - f(e1) * de
+        out += s[i - 1] * w + (s[i] - s[i - 1]) / de * m
+    return out
+
+
 # ------------------------------------------------------ correlation-series DOS
 
 def timeprop_coeff(time_step: float, precision: float = 1e-14, forward: bool = True) -> np.ndarray:

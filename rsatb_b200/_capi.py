@@ -111,6 +111,7 @@ SIGNATURES = {
     "rsatb_evaluate_kpm_density": (_i, [_vp, _PD, _i, _PD, _i, _d, _i, _PD]),
     "rsatb_timeprop_coeff": (_i, [_vp, _d, _d, _i, _i, _PD, C.POINTER(_i)]),
     "rsatb_corr_dos": (_i, [_vp, _PD, _i, _i, _d, _PD, _PD]),
+    "rsatb_integrate_dc_spectrum": (_i, [_vp, _PD, _PD, _i, _d, _d, _PD]),
     "rsatb_bloch_sum": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _vp, _PD, _i]),
     "rsatb_cg_solve": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _d, _i, C.POINTER(_i), _PD]),
     "rsatb_kpm_moments_vjp": (_i, [_vp, C.POINTER(ChebOp), _vp, _i, _i, _i, _PD, _i, _PD, _vp,

@@ -261,3 +261,101 @@ extern "C" int rsatb_corr_dos(rsatb_ctx_t ctx, const double* moments, int n_mome
     if (bad) return set_error(RSATB_NUMERICAL_FAILURE, "corr_dos: short Miller start");
     return RSATB_SUCCESS;
 }
+
+// ---------------------------------------------------------------------------
+// sigma(mu, T) from a zero-temperature spectrum, integrate_dc_spectrum
+// (rsatb/calc/fftcheb_transport.hpp:950-1040): at T <= 0 linear
+// interpolation at mu (clamped to the ends); at T > 0 the piecewise-linear
+// spectrum integrated exactly against -df/dE, interval by interval, with
+// the antiderivative E - kT softplus((E - mu)/kT) of f.  One thread per
+// tensor component sums its intervals in energy order.
+
+namespace rsatb_b200 {
+namespace {
+
+constexpr double kBoltzmannEv = 8.617333262e-5;  // eV / K
+
+__device__ double fermi_dirac_dev(double e, double mu, double temp) {
+    if (temp <= 0.0) return e <= mu ? 1.0 : 0.0;
+    const double beta = 1.0 / (temp * kBoltzmannEv);
+    if (e >= mu) {
+        const double t = exp(beta * (mu - e));
+        return t / (1.0 + t);
+    }
+    const double t = exp(beta * (e - mu));
+    return 1.0 / (1.0 + t);
+}
+
+__global__ void integrate_dc_kernel(const double* __restrict__ sigma,
+                                    const double* __restrict__ energy, int n, double mu,
+                                    double temp, double* __restrict__ out) {
+    const int comp = threadIdx.x;
+    if (comp >= 6) return;
+    if (temp <= 0.0) {
+        double v;
+        if (mu <= energy[0]) {
+            v = sigma[comp];
+        } else if (mu >= energy[n - 1]) {
+            v = sigma[(n - 1) * 6 + comp];
+        } else {
+            int hi = 1;  // first energy >= mu
+            while (energy[hi] < mu) ++hi;
+            const int lo = hi - 1;
+            const double t = (mu - energy[lo]) / (energy[hi] - energy[lo]);
+            v = (1.0 - t) * sigma[lo * 6 + comp] + t * sigma[hi * 6 + comp];
+        }
+        out[comp] = v;
+        return;
+    }
+    const double kt = kBoltzmannEv * temp;
+    auto F = [&](double e) {
+        const double x = (e - mu) / kt;
+        return e - kt * (fmax(x, 0.0) + log1p(exp(-fabs(x))));
+    };
+    double acc = 0.0;
+    for (int i = 1; i < n; ++i) {
+        const double e0 = energy[i - 1], e1 = energy[i], de = e1 - e0;
+        const double f0 = fermi_dirac_dev(e0, mu, temp), f1 = fermi_dirac_dev(e1, mu, temp);
+        const double weight = f0 - f1;
+        const double moment = F(e1) - F(e0) - f1 * de;
+        const double s0 = sigma[(i - 1) * 6 + comp], s1 = sigma[i * 6 + comp];
+        acc += s0 * weight + (s1 - s0) / de * moment;
+    }
+    out[comp] = acc;
+}
+
+}  // namespace
+}  // namespace rsatb_b200
+
+extern "C" int rsatb_integrate_dc_spectrum(rsatb_ctx_t ctx, const double* sigma,
+                                           const double* energy, int n_energy, double mu,
+                                           double temp, double* sigma_out) {
+    clear_error();
+    RSATB_TRY(check_ctx(ctx));
+    if (!sigma_out || n_energy < 0 || (n_energy > 0 && (!sigma || !energy)))
+        return set_error(RSATB_INVALID_ARGUMENT, "integrate_dc_spectrum: bad arguments");
+    for (int c = 0; c < 6; ++c) sigma_out[c] = 0.0;
+    if (n_energy == 0) return RSATB_SUCCESS;
+    if (temp > 0.0)
+        for (int i = 1; i < n_energy; ++i)
+            if (!(energy[i] - energy[i - 1] > 0.0))
+                return set_error(RSATB_INVALID_ARGUMENT,
+                                 "integrate_dc_spectrum: energies must be strictly ascending");
+    double *d_s = nullptr, *d_e = nullptr, *d_o = nullptr;
+    RSATB_CUDA_TRY(cudaMallocAsync(&d_s, sizeof(double) * 6 * n_energy, ctx->stream));
+    RSATB_CUDA_TRY(cudaMallocAsync(&d_e, sizeof(double) * n_energy, ctx->stream));
+    RSATB_CUDA_TRY(cudaMallocAsync(&d_o, sizeof(double) * 6, ctx->stream));
+    RSATB_CUDA_TRY(cudaMemcpyAsync(d_s, sigma, sizeof(double) * 6 * n_energy,
+                                   cudaMemcpyHostToDevice, ctx->stream));
+    RSATB_CUDA_TRY(cudaMemcpyAsync(d_e, energy, sizeof(double) * n_energy,
+                                   cudaMemcpyHostToDevice, ctx->stream));
+    integrate_dc_kernel<<<1, 32, 0, ctx->stream>>>(d_s, d_e, n_energy, mu, temp, d_o);
+    RSATB_LAUNCH_CHECK(ctx);
+    RSATB_CUDA_TRY(cudaMemcpyAsync(sigma_out, d_o, sizeof(double) * 6, cudaMemcpyDeviceToHost,
+                                   ctx->stream));
+    cudaFreeAsync(d_s, ctx->stream);
+    cudaFreeAsync(d_e, ctx->stream);
+    cudaFreeAsync(d_o, ctx->stream);
+    RSATB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return RSATB_SUCCESS;
+}

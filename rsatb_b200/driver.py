@@ -23,7 +23,7 @@ from .bounds import estimate_spectral_bounds
 from .calc import (Chebyshev, ISQRTMPreconditioner, corr_dos, corr_moment_count,
                    dos_energy_grid, dos_moment_count, evaluate_kpm_density, kpm_dos_moments,
                    parse_kpm_kernel)
-from .transport import BASTIN, GREENWOOD, dc_spectrum_fftcheb
+from .transport import BASTIN, GREENWOOD, dc_spectrum_fftcheb, integrate_dc_spectrum
 from ._capi import RANDOM_PHASE
 from .vbcsr import BlockSpMat, set_random
 
@@ -266,3 +266,16 @@ class RSATB:
             if energy is None:
                 energy = en
         return np.concatenate(sigmas), energy
+
+    def compute_dc(self, n_moments: int, mu: float, temp: float, formulation: str = "greenwood",
+                   axis: str = "abc", partition_sections: int = 0, max_workspace_mb: float = 0,
+                   kernel: str = "jackson", method: str = "fftcheb"):
+        """ComputeDc (observables.hpp:791-850): the spectrum of
+        compute_dc_spectrum integrated against -df/dE at (mu, temp) per
+        k-point.  Returns 6 values per k-point."""
+        sigma, energy = self.compute_dc_spectrum(n_moments, formulation, axis, partition_sections,
+                                                 max_workspace_mb, kernel, method)
+        dev = self.H.ctx.device
+        per_k = sigma.reshape(len(self.kpoints), n_moments, 6)
+        return np.concatenate([integrate_dc_spectrum(sk, energy, mu, temp, device=dev)
+                               for sk in per_k])

@@ -58,3 +58,21 @@ def dc_spectrum_fftcheb(cheby: Chebyshev, Vx: BlockSpMat, Vy: BlockSpMat, Vz: Bl
     if return_stats:
         return out + ({f: getattr(stats, f) for f, _ in stats._fields_},)
     return out
+
+
+def integrate_dc_spectrum(sigma, energy, mu: float, temp: float, device=None) -> np.ndarray:
+    """sigma(mu, T) (6 components) from a zero-temperature spectrum
+    sigma[n_energy, 6] on `energy` (fftcheb_transport.hpp:950-1040), on the
+    GPU: linear interpolation at T <= 0, the exact integral of the
+    piecewise-linear spectrum against -df/dE at T > 0 (kelvin)."""
+    from .vbcsr import context
+    s = np.ascontiguousarray(np.asarray(sigma, dtype=np.float64).reshape(-1, 6))
+    e = np.ascontiguousarray(np.asarray(energy, dtype=np.float64).reshape(-1))
+    if s.shape[0] != e.size:
+        raise ValueError("sigma must hold 6 values per energy")
+    out = np.zeros(6)
+    P = C.POINTER(C.c_double)
+    check(lib().rsatb_integrate_dc_spectrum(context(device).handle, s.ctypes.data_as(P),
+                                            e.ctypes.data_as(P), e.size, float(mu), float(temp),
+                                            out.ctypes.data_as(P)))
+    return out

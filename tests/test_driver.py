@@ -209,6 +209,10 @@ def test_compute_dc_spectrum_kpoints_matches_oracle(formulation):
     M = 40
     sigma, energy = calc.compute_dc_spectrum(M, formulation=formulation, axis="ab")
     assert sigma.shape == (2 * M * 6,)
+    dc = calc.compute_dc(M, 0.3, 300.0, formulation=formulation, axis="ab")
+    want_dc = np.concatenate([oracle.integrate_dc_spectrum(sigma[q * M * 6:(q + 1) * M * 6],
+                                                           energy, 0.3, 300.0) for q in range(2)])
+    assert dc.shape == (12,) and np.abs(dc - want_dc).max() <= 1e-10 * np.abs(want_dc).max()
     psi = _oracle_samples(n, 2, 21)
     rows = np.repeat(np.arange(n), np.diff(op.row_ptr))
 

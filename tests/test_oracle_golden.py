@@ -319,3 +319,16 @@ def test_oracle_timeprop_length():
     assert 6283 < c.size < 7000 and np.all(np.isfinite(c))
     b = oracle.timeprop_coeff(3.0, forward=False)
     assert np.allclose(b, np.conj(oracle.timeprop_coeff(3.0)), rtol=0, atol=1e-16)
+
+
+def test_oracle_integrate_dc_linear_spectrum():
+    """integrate_dc_spectrum is exact for a piecewise-linear spectrum: a
+    linear sigma(E) = a + b E gives a + b mu at any T once the grid covers
+    the -df/dE window; T = 0 interpolates."""
+    e = np.linspace(-12.0, 12.0, 961)   # -df/dE below 1e-16 at the ends up to 3000 K
+    a = np.arange(1.0, 7.0)
+    b = np.linspace(-0.5, 0.5, 6)
+    s = a[None, :] + e[:, None] * b[None, :]
+    for T in (0.0, 30.0, 300.0, 3000.0):
+        got = oracle.integrate_dc_spectrum(s, e, 0.37, T)
+        assert np.abs(got - (a + 0.37 * b)).max() < 1e-10

@@ -177,3 +177,24 @@ def test_bad_arguments_refused(torch_cuda):
         dc_spectrum_fftcheb(c, *Vd, p, 8, formulation=2)
     with pytest.raises(RsatbError):   # FP32 vectors with FP64 matrices
         dc_spectrum_fftcheb(c, *Vd, p.to(torch_cuda.complex64), 8)
+
+
+@pytest.mark.parametrize("temp", [0.0, 1e-3, 77.0, 300.0, 5000.0])
+def test_integrate_dc_spectrum_matches_oracle(torch_cuda, temp):
+    """sigma(mu, T) from a spectrum (fftcheb_transport.hpp:950-1040) on the
+    device against the oracle's restatement, for mu inside, between and
+    outside the grid."""
+    from rsatb_b200.transport import integrate_dc_spectrum
+    rng = np.random.default_rng(3)
+    e = np.sort(rng.uniform(-6.0, 6.0, 300))
+    s = rng.standard_normal((300, 6))
+    for mu in (-7.0, e[10], 0.123, 6.5):
+        got = integrate_dc_spectrum(s, e, mu, temp)
+        want = oracle.integrate_dc_spectrum(s, e, mu, temp)
+        # The interval moment F(e1) - F(e0) - f(e1) de cancels to a small
+        # difference of O(|E|) terms, and random spectra (no smoothness)
+        # divide it by de: 1e-10 of the O(1) spectrum values.
+        assert np.abs(got - want).max() <= 1e-10 * np.abs(s).max()
+    if temp > 0:
+        with pytest.raises(Exception):
+            integrate_dc_spectrum(s, e[::-1].copy(), 0.0, temp)
