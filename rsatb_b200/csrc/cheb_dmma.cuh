@@ -51,13 +51,9 @@ struct DmmaShape {
     static constexpr int U = UU ? UU : (W <= 16 ? 4 : (W <= 32 ? 2 : 1));
 };
 
-// KW warps per CTA.  CHUNK: each CTA walks one contiguous run of block rows
-// (its warps on neighbouring rows, then the next ones), so the gathered X_j
-// rows of one neighbourhood stay in that SM's L1; otherwise warps stride
-// over the whole matrix.
-template <typename VT, int W, bool CV, int UU, int KW = dmma_warps<VT>(), bool CHUNK = false>
-__global__ void __launch_bounds__(KW * 32) cheb_step_dmma(StepArgs a) {
-    constexpr int kDmmaWarps = KW;
+template <typename VT, int W, bool CV, int UU>
+__global__ void __launch_bounds__(dmma_warps<VT>() * 32) cheb_step_dmma(StepArgs a) {
+    constexpr int kDmmaWarps = dmma_warps<VT>();
     static_assert(W % 8 == 0 && W <= 256, "8-column groups");
     constexpr int NG = DmmaShape<W, UU>::NG, U = DmmaShape<W, UU>::U;
     // 16-column spans with 2-value X loads: FP64 panels (measured at FP32
@@ -72,14 +68,8 @@ __global__ void __launch_bounds__(KW * 32) cheb_step_dmma(StepArgs a) {
     for (int c = lane; c < 2 * W; c += 32) dsm[warp][c / W][c % W] = 0.0;
     __syncwarp();
 
-    const int64_t chunk = CHUNK ? (a.n_block_rows + gridDim.x - 1) / gridDim.x : 0;
-    const int64_t row_end =
-        CHUNK ? (int64_t(blockIdx.x) + 1) * chunk < a.n_block_rows ? (int64_t(blockIdx.x) + 1) * chunk
-                                                                    : a.n_block_rows
-              : a.n_block_rows;
-    const int64_t row_step = CHUNK ? kDmmaWarps : int64_t(gridDim.x) * kDmmaWarps;
-    for (int64_t i = (CHUNK ? int64_t(blockIdx.x) * chunk : int64_t(blockIdx.x) * kDmmaWarps) + warp;
-         i < row_end; i += row_step) {
+    for (int64_t i = int64_t(blockIdx.x) * kDmmaWarps + warp; i < a.n_block_rows;
+         i += int64_t(gridDim.x) * kDmmaWarps) {
         const int k0 = __ldg(a.row_ptr + i), k1 = __ldg(a.row_ptr + i + 1);
         double acc[NG][2];
 #pragma unroll

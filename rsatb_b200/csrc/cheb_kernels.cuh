@@ -239,6 +239,7 @@ __device__ __forceinline__ void finish_row(const StepArgs& a, int64_t row, int g
 // whole outputs with eight independent accumulators, so the L2 loads of one
 // output are in flight together.  The order is fixed for a given grid:
 // deterministic dots.  Needs blockDim.x <= 256.
+// CTAs of at most 256 threads (comb below), which every step kernel uses.
 __device__ __forceinline__ void finish_partials(const StepArgs& a, int ndots) {
     __threadfence();
     __syncthreads();
@@ -249,12 +250,11 @@ __device__ __forceinline__ void finish_partials(const StepArgs& a, int ndots) {
     if (ticket != gridDim.x - 1) return;
     __threadfence();
     const int O = ndots * a.W;
-    // comb holds 256 values: CTAs of more threads combine with their first 256.
-    const int nt = blockDim.x < 256 ? int(blockDim.x) : 256;
+    const int nt = blockDim.x;
     const unsigned G = gridDim.x;
     const double* P = a.partials;
     if (O * 2 > nt) {
-        for (int idx = threadIdx.x; idx < O; idx += blockDim.x) {
+        for (int idx = threadIdx.x; idx < O; idx += nt) {
             double s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0, s5 = 0, s6 = 0, s7 = 0;
             unsigned b = 0;
             for (; b + 8 <= G; b += 8) {
@@ -284,7 +284,7 @@ __device__ __forceinline__ void finish_partials(const StepArgs& a, int ndots) {
             }
             for (; b < G; b += T) s0 += __ldcg(P + size_t(b) * O + o);
         }
-        if (threadIdx.x < nt) comb[threadIdx.x] = (s0 + s1) + (s2 + s3);
+        comb[threadIdx.x] = (s0 + s1) + (s2 + s3);
         __syncthreads();
         if (threadIdx.x < O) {
             double t = 0.0;

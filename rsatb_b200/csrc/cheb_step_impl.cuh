@@ -339,23 +339,10 @@ inline int dmma_u() {
     return (u == 2 || u == 4 || u == 8) ? u : 0;
 }
 
-// Narrow-panel CTA shape of the tensor-core kernel (tuning):
-// RSATB_DMMA_WARPS = 4, 8 or 16 warps per CTA, RSATB_DMMA_CHUNK=1 for
-// contiguous row runs per CTA.  Unset: dmma_warps<VT>(), strided rows.
-inline int dmma_warps_env() {
-    const char* s = std::getenv("RSATB_DMMA_WARPS");
-    const int w = s ? std::atoi(s) : 0;
-    return (w == 4 || w == 8 || w == 16) ? w : 0;
-}
-inline bool dmma_chunk_env() {
-    const char* s = std::getenv("RSATB_DMMA_CHUNK");
-    return s && std::atoi(s) == 1;
-}
-
-template <typename VT, int W, bool CV, int UU, int KW = dmma_warps<VT>(), bool CHUNK = false>
+template <typename VT, int W, bool CV, int UU>
 int launch_dmma_u(rsatb_context* ctx, StepArgs& a) {
-    auto kernel = cheb_step_dmma<VT, W, CV, UU, KW, CHUNK>;
-    constexpr int kWarps = KW;
+    auto kernel = cheb_step_dmma<VT, W, CV, UU>;
+    constexpr int kWarps = dmma_warps<VT>();
     const int threads = kWarps * 32;
     const int64_t need = (a.n_block_rows + kWarps - 1) / kWarps;
     const int per_sm = occupancy(reinterpret_cast<const void*>(kernel), threads, 0);
@@ -368,12 +355,6 @@ int launch_dmma_u(rsatb_context* ctx, StepArgs& a) {
     return RSATB_SUCCESS;
 }
 
-template <typename VT, int W, bool CV, int KW>
-int launch_dmma_c(rsatb_context* ctx, StepArgs& a) {
-    return dmma_chunk_env() ? launch_dmma_u<VT, W, CV, 0, KW, true>(ctx, a)
-                            : launch_dmma_u<VT, W, CV, 0, KW, false>(ctx, a);
-}
-
 template <typename VT, int W, bool CV>
 int launch_dmma_k(rsatb_context* ctx, StepArgs& a) {
     if constexpr (W <= 32) {
@@ -382,12 +363,6 @@ int launch_dmma_k(rsatb_context* ctx, StepArgs& a) {
             case 4: return launch_dmma_u<VT, W, CV, 4>(ctx, a);
             case 8: return launch_dmma_u<VT, W, CV, 8>(ctx, a);
         }
-        switch (dmma_warps_env()) {
-            case 4: return launch_dmma_c<VT, W, CV, 4>(ctx, a);
-            case 8: return launch_dmma_c<VT, W, CV, 8>(ctx, a);
-            case 16: return launch_dmma_c<VT, W, CV, 16>(ctx, a);
-        }
-        if (dmma_chunk_env()) return launch_dmma_u<VT, W, CV, 0, dmma_warps<VT>(), true>(ctx, a);
     }
     return launch_dmma_u<VT, W, CV, 0>(ctx, a);
 }
