@@ -23,6 +23,7 @@ from .bounds import estimate_spectral_bounds
 from .calc import (Chebyshev, ISQRTMPreconditioner, corr_dos, corr_moment_count,
                    dos_energy_grid, dos_moment_count, evaluate_kpm_density, kpm_dos_moments,
                    parse_kpm_kernel)
+from .shard import gather_kpoint_results, partition_kpoints, torch_all_reduce_sum
 from .transport import BASTIN, GREENWOOD, dc_spectrum_fftcheb, integrate_dc_spectrum
 from ._capi import RANDOM_PHASE
 from .vbcsr import BlockSpMat, set_random
@@ -98,8 +99,9 @@ class RSATB:
 
     def __init__(self, H, options: SetupOptions | None = None, Z=None, velocities=None,
                  cell=None, orbitals_per_atom: int = 1, atom_index=None,
-                 spin_degeneracy: float = 2.0, S=None):
+                 spin_degeneracy: float = 2.0, S=None, npar: int | None = None):
         self.options = options or SetupOptions()
+        self.npar = npar
         if self.options.precision not in ("f64", "mixed"):
             raise ValueError("precision must be 'f64' or 'mixed'")
         self.kpoints = [np.asarray(k, dtype=np.float64).reshape(3) for k in self.options.kpoints]
@@ -163,13 +165,46 @@ class RSATB:
                       cg_tol=po.cg_tol, cg_max_iter=po.cg_max_iter)
         return c.astype("f32") if mixed else c
 
+    # -- k-point distribution over ranks ------------------------------------
+    # Under torch.distributed the k-points are spread over npar colours
+    # (default: one per rank) as PartitionKPoints does; every rank computes
+    # its own k-points with all samples, and the per-k-point results are
+    # gathered as GatherKPointResults does.  One process: everything local.
+
+    def _dist(self):
+        import torch.distributed as dist
+        if dist.is_available() and dist.is_initialized():
+            return dist.get_rank(), dist.get_world_size()
+        return 0, 1
+
+    def _local_kidx(self):
+        rank, world = self._dist()
+        return [i for i, _ in partition_kpoints(self.kpoints, self.npar or world, rank, world)]
+
+    def _all_reduce(self):
+        import torch.distributed as dist
+        dev = f"cuda:{self.H.ctx.device}" if dist.get_backend() == "nccl" else None
+        return torch_all_reduce_sum(device=dev)
+
+    def _gather(self, per_k: np.ndarray) -> np.ndarray:
+        rank, world = self._dist()
+        if world == 1:
+            return per_k
+        return gather_kpoint_results(per_k, self.npar or world, rank, world, self._all_reduce())
+
     def _estimate_bounds(self):
         """The widest padded Lanczos window over the k-points (the reference
         keeps one window for all of them, OperatorSet::emin/emax)."""
         lo, hi = np.inf, -np.inf
-        for kidx in range(len(self.kpoints)):
+        for kidx in self._local_kidx():
             a, b = estimate_spectral_bounds(self._cheby(-1.0, 1.0, False, kidx))
             lo, hi = min(lo, a), max(hi, b)
+        if self._dist()[1] > 1:
+            import torch.distributed as dist
+            dev = f"cuda:{self.H.ctx.device}" if dist.get_backend() == "nccl" else "cpu"
+            t = torch.tensor([-lo, hi], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            lo, hi = -float(t[0]), float(t[1])
         return lo, hi
 
     def energy_bounds(self):
@@ -209,16 +244,16 @@ class RSATB:
             N = corr_moment_count(nt, device=dev)
         mixed = self.options.precision == "mixed"
         psi = self._samples(torch.complex64 if mixed else torch.complex128)
-        out = []
-        for kidx in range(len(self.kpoints)):
-            # One DOS of 2 nt points per k-point, in k-point order
-            # (observables.hpp:368, 383-386: offset k_idx * 2 nt).
+        # One DOS of 2 nt points per k-point, in k-point order
+        # (observables.hpp:368, 383-386: offset k_idx * 2 nt).
+        out = np.zeros((len(self.kpoints), 2 * nt))
+        for kidx in self._local_kidx():
             mu = kpm_dos_moments(self._cheby(emin, emax, mixed, kidx), psi, N)
             if method == "corr":
-                out.append(corr_dos(mu, nt, device=dev)[0])
+                out[kidx] = corr_dos(mu, nt, device=dev)[0]
             else:
-                out.append(2.0 * evaluate_kpm_density(mu, x, 0.5 / nt, device=dev))
-        return np.concatenate(out), omega
+                out[kidx] = 2.0 * evaluate_kpm_density(mu, x, 0.5 / nt, device=dev)
+        return self._gather(out).reshape(-1), omega
 
     def compute_dc_spectrum(self, n_moments: int, formulation: str = "greenwood",
                             axis: str = "abc", partition_sections: int = 0,
@@ -250,8 +285,10 @@ class RSATB:
         trace_prefactor = norb / _volume(self.cell, axis)
         prefactor = (math.pi * self.spin_degeneracy *
                      (4.0 if formulation == "greenwood" else 8.0) * trace_prefactor)
-        sigmas, energy = [], None
-        for kidx, k in enumerate(self.kpoints):
+        sigmas = np.zeros((len(self.kpoints), int(n_moments) * 6))
+        energy = None
+        for kidx in self._local_kidx():
+            k = self.kpoints[kidx]
             c = self._cheby(emin, emax, mixed, kidx)
             if self.images is not None:
                 V = [self.images.velocity_at_k(k, a) for a in range(3)]
@@ -262,10 +299,16 @@ class RSATB:
             sigma, en = dc_spectrum_fftcheb(
                 c, *V, psi, int(n_moments), forms[formulation], prefactor,
                 int(partition_sections), float(max_workspace_mb), parse_kpm_kernel(kernel))
-            sigmas.append(sigma.reshape(-1))
+            sigmas[kidx] = sigma.reshape(-1)
             if energy is None:
                 energy = en
-        return np.concatenate(sigmas), energy
+        rank, world = self._dist()
+        if world > 1:
+            # The grid is the same for every k-point; rank 0 owns k-point 0
+            # (BroadcastSharedGrid, observables.hpp:156-175).
+            mine = energy if rank == 0 else np.zeros(int(n_moments))
+            energy = self._all_reduce()(np.asarray(mine, dtype=np.float64))
+        return self._gather(sigmas).reshape(-1), energy
 
     def compute_dc(self, n_moments: int, mu: float, temp: float, formulation: str = "greenwood",
                    axis: str = "abc", partition_sections: int = 0, max_workspace_mb: float = 0,

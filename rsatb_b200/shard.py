@@ -50,3 +50,38 @@ def torch_all_reduce_sum(device=None):
         dist.all_reduce(t)
         return t.cpu().numpy()
     return f
+
+
+# ------------------------------------------------------------- k-points
+
+def kpoint_colour(npar: int, world_rank: int, world_size: int) -> int:
+    """The sub-communicator ("colour") of a rank when the k-points are
+    spread over npar of them (clamped to [1, world_size])."""
+    npar = max(1, min(int(npar), int(world_size)))
+    return (int(world_rank) * npar) // int(world_size)
+
+
+def partition_kpoints(kpoints, npar: int, world_rank: int, world_size: int):
+    """PartitionKPoints (rsatb/setup/kpoint_partition.hpp:56-80): k-point i
+    belongs to colour i mod npar; every rank of a colour owns the same
+    k-points.  Returns [(global index, k-point), ...] in ascending index."""
+    if world_size < 1:
+        raise ValueError("world_size must be at least 1")
+    if not 0 <= world_rank < world_size:
+        raise ValueError("world_rank is outside the communicator")
+    npar_c = max(1, min(int(npar), int(world_size)))
+    colour = kpoint_colour(npar, world_rank, world_size)
+    return [(i, k) for i, k in enumerate(kpoints) if i % npar_c == colour]
+
+
+def gather_kpoint_results(values: np.ndarray, npar: int, world_rank: int, world_size: int,
+                          all_reduce_sum) -> np.ndarray:
+    """GatherKPointResults (rsatb/calc/observables.hpp:137-148): the global
+    per-k-point array, zero where this rank owns nothing, summed over the
+    first rank of every colour (the reference's master communicator) and
+    shared with every rank (its broadcast within the colour).  One
+    all-reduce in which only colour leaders contribute does both."""
+    colour = kpoint_colour(npar, world_rank, world_size)
+    leader = world_rank == 0 or kpoint_colour(npar, world_rank - 1, world_size) != colour
+    v = np.asarray(values, dtype=np.float64)
+    return all_reduce_sum(v.ravel() if leader else np.zeros(v.size)).reshape(v.shape)

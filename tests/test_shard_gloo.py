@@ -103,3 +103,58 @@ def test_two_gloo_ranks_equal_single_process_transport(tmp_path):
                                    H.values), -1.0, 10.0)
     sig_all, _ = oracle.fftcheb(op, V, _samples(H, 0, 4), 16)
     assert np.abs(np.load(out) - sig_all).max() <= 1e-12 * np.abs(sig_all).max()
+
+
+def test_partition_kpoints_matches_reference_rules():
+    """kpoint_partition.hpp's tests (test_setup_stages.cpp:40-93): one rank
+    owns everything; every k-point has exactly one colour and ranks of a
+    colour agree; npar above the world size is clamped; a rank outside the
+    communicator is refused."""
+    from rsatb_b200.shard import kpoint_colour, partition_kpoints
+    ks = [[0.1 * i, 0.0, 0.0] for i in range(7)]
+    assert [i for i, _ in partition_kpoints(ks[:5], 1, 0, 1)] == [0, 1, 2, 3, 4]
+    for ws in (1, 2, 3, 4, 8):
+        for npar in range(1, ws + 1):
+            per_colour, covered = {}, set()
+            for r in range(ws):
+                idx = [i for i, _ in partition_kpoints(ks, npar, r, ws)]
+                c = kpoint_colour(npar, r, ws)
+                per_colour.setdefault(c, idx)
+                assert per_colour[c] == idx
+                covered.update(idx)
+            assert covered == set(range(7))
+    assert {i for r in range(2) for i, _ in partition_kpoints(ks[:4], 16, r, 2)} == set(range(4))
+    with pytest.raises(ValueError):
+        partition_kpoints(ks[:2], 1, 4, 4)
+    with pytest.raises(ValueError):
+        partition_kpoints(ks[:2], 1, 0, 0)
+
+
+def _kpoint_rank(rank, port, world, npar, out):
+    import torch.distributed as dist
+    from rsatb_b200.shard import gather_kpoint_results, partition_kpoints, torch_all_reduce_sum
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        ks = [[0.05 * i, 0.02 * i, 0.0] for i in range(5)]
+        local = np.zeros((5, 3))
+        for i, k in partition_kpoints(ks, npar, rank, world):
+            local[i] = [i, k[0], k[1]]     # any per-k-point result
+        full = gather_kpoint_results(local, npar, rank, world, torch_all_reduce_sum())
+        np.save(out + f".{rank}.npy", full)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,npar", [(2, 2), (3, 3), (3, 2), (2, 1)])
+def test_gather_kpoint_results_gloo(tmp_path, world, npar):
+    """Every rank receives the full per-k-point array, each k-point counted
+    once although several ranks of a colour computed it."""
+    import torch.multiprocessing as mp
+    out = str(tmp_path / "k")
+    mp.start_processes(_kpoint_rank, args=(_free_port(), world, npar, out), nprocs=world,
+                       start_method="spawn")
+    want = np.array([[i, 0.05 * i, 0.02 * i] for i in range(5)])
+    for r in range(world):
+        assert np.abs(np.load(out + f".{r}.npy") - want).max() < 1e-15
