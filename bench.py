@@ -63,6 +63,9 @@ def parse_args():
                    help="time Y = H X alone on a diamond L^3 H (the ncu profiling case)")
     p.add_argument("--isqrt-no-autotune", action="store_true",
                    help="batched S^-1/2: built-in tensor-core tiles instead of autotuned ones")
+    p.add_argument("--forms-only", action="store_true",
+                   help="time one application of the sandwich and the solve forms")
+    p.add_argument("--forms-L", type=int, default=8)
     p.add_argument("--spmm-L", type=int, default=12)
     p.add_argument("--spmm-reps", type=int, default=3)
     return p.parse_args()
@@ -440,6 +443,57 @@ def spmm_only(args):
     print(json.dumps(out), flush=True)
 
 
+def forms_only(args):
+    """Cost of one operator application in the Sandwich form Z^H H Z and in
+    the Solve form S^-1 H (CG with S, plain and preconditioned by the
+    graph-local Z), the comparison the reference quotes for diamond
+    (rsatb/model/setup.hpp:44-47: the sandwich 5.9x faster per matvec).
+    Diamond LCAO L^3 cells, 8x8 blocks, R = 16 real vectors, FP64; each
+    application starts its CG from zero."""
+    import torch
+    from rsatb_b200 import lattice
+    from rsatb_b200.bounds import estimate_spectral_bounds
+    from rsatb_b200.calc import Chebyshev, ISQRTMPreconditioner, cg_solve
+    from rsatb_b200.isqrt import graph_inverse_sqrt
+    from rsatb_b200.vbcsr import BlockSpMat, set_random
+    H, S = lattice.diamond_lcao(L=args.forms_L, seed=7)
+    Z = graph_inverse_sqrt(S, method="ns")
+    dev = lambda A: BlockSpMat(A.row_ptr, A.col_ind, A.values, A.block_size)
+    Hd, Sd = dev(H), dev(S)
+    pre = ISQRTMPreconditioner(dev(Z))
+    emin, emax = estimate_spectral_bounds(Chebyshev(Hd, -1.0, 1.0, preconditioner=pre))
+    forms = {"sandwich": Chebyshev(Hd, emin, emax, preconditioner=pre),
+             "solve_cg": Chebyshev(Hd, emin, emax, overlap=Sd),
+             "solve_pcg_z": Chebyshev(Hd, emin, emax, overlap=Sd, preconditioner=pre)}
+    R = 16
+    X = torch.empty(H.n_rows, R, dtype=torch.float64, device="cuda")
+    set_random(X, 3)
+    Y = torch.empty_like(X)
+    out = {"n_rows": H.n_rows, "R": R, "nnz_blocks": int(H.nnz_blocks)}
+    for name, c in forms.items():
+        for _ in range(2):
+            Y.zero_()
+            c.apply_op(X, Y)
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        for _ in range(args.spmm_reps):
+            Y.zero_()
+            c.apply_op(X, Y)
+        e.record()
+        torch.cuda.synchronize()
+        out[f"{name}_ms"] = round(s.elapsed_time(e) / args.spmm_reps, 4)
+    B = torch.empty_like(X)
+    Hd.mult_dense(X, B)
+    for name, p in (("cg", None), ("pcg_z", pre)):
+        Xs = torch.zeros_like(X)
+        it, res = cg_solve(Sd, B, Xs, tol=1e-8, max_iter=1000, preconditioner=p)
+        out[f"{name}_iterations"] = it
+    out["solve_cg_over_sandwich"] = round(out["solve_cg_ms"] / out["sandwich_ms"], 2)
+    out["solve_pcg_z_over_sandwich"] = round(out["solve_pcg_z_ms"] / out["sandwich_ms"], 2)
+    print(json.dumps(out), flush=True)
+
+
 def bench_isqrt(args, dist):
     """Batched graph-local S^-1/2: args.isqrt_n SPD problems per GPU, sizes
     uniform in [40, 400], condition numbers log-uniform in [1e2, 1e5]; each
@@ -768,6 +822,9 @@ def main():
     args = parse_args()
     if args.spmm_only:
         spmm_only(args)
+        return
+    if args.forms_only:
+        forms_only(args)
         return
     dist = Dist()
     if args.workload == "isqrt" and args.impl == "ours":
