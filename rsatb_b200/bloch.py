@@ -21,6 +21,29 @@ from ._capi import check, lib
 from .vbcsr import BlockSpMat, context
 
 
+def image_pattern(rows, cols, n_block_rows: int, n_block_cols: int):
+    """The pattern of H(k) from the bonds (rows[e], cols[e]): returns
+    (order, slot_ptr, row_ptr, col_ind) with the bonds in `order` sorted by
+    output block (row, col), bonds of one block kept in input order;
+    bonds order[slot_ptr[s]:slot_ptr[s + 1]] sum into block s, whose column
+    is col_ind[s]; row_ptr is the CSR row pointer over the blocks."""
+    rows = np.asarray(rows, dtype=np.int64)
+    cols = np.asarray(cols, dtype=np.int64)
+    n = rows.size
+    order = np.lexsort((cols, rows))
+    key = rows[order] * int(n_block_cols) + cols[order]
+    first = np.ones(n, dtype=bool)
+    first[1:] = key[1:] != key[:-1]
+    slot_start = np.flatnonzero(first)
+    slot_ptr = np.append(slot_start, n).astype(np.int64)
+    prow = rows[order][slot_start]
+    col_ind = cols[order][slot_start].astype(np.int32)
+    row_ptr = np.zeros(int(n_block_rows) + 1, dtype=np.int32)
+    np.add.at(row_ptr, prow + 1, 1)
+    row_ptr = np.cumsum(row_ptr).astype(np.int32)
+    return order, slot_ptr, row_ptr, col_ind
+
+
 class ImageOperator:
     """Bonds (rows[e], cols[e], shifts[e]) with blocks[e] (b x b, real or
     complex); shifts in the units k is given against (fractional for integer
@@ -43,18 +66,9 @@ class ImageOperator:
             raise ValueError("bond index outside the matrix")
         self.block_size, self.n_block_rows, self.n_block_cols = b, int(n_block_rows), nbc
         # Bonds sorted by output block (row, col); equal blocks keep input order.
-        order = np.lexsort((cols, rows))
-        key = rows[order] * nbc + cols[order]
-        first = np.ones(n, dtype=bool)
-        first[1:] = key[1:] != key[:-1]
-        slot_start = np.flatnonzero(first)
-        self.nnz_blocks = slot_start.size
-        slot_ptr = np.append(slot_start, n).astype(np.int64)
-        prow = rows[order][slot_start]
-        self.col_ind = cols[order][slot_start].astype(np.int32)
-        self.row_ptr = np.zeros(self.n_block_rows + 1, dtype=np.int32)
-        np.add.at(self.row_ptr, prow + 1, 1)
-        self.row_ptr = np.cumsum(self.row_ptr).astype(np.int32)
+        order, slot_ptr, self.row_ptr, self.col_ind = image_pattern(rows, cols,
+                                                                    self.n_block_rows, nbc)
+        self.nnz_blocks = self.col_ind.size
         self.ctx = context(device)
         dev = f"cuda:{self.ctx.device}"
         cplx = np.iscomplexobj(blocks)
