@@ -234,6 +234,28 @@ def kpm_dos_moments(cheby: Chebyshev, psi_in: torch.Tensor, n_moments: int) -> n
     return m
 
 
+def kpm_ldos_moments(cheby: Chebyshev, orbitals, n_moments: int) -> np.ndarray:
+    """Local moments mu_n(i) = <e_i|T_n(Op~)|e_i> of the orbitals i, one
+    unit column each (KPM local density of states; Weisse et al., Rev. Mod.
+    Phys. 78, 275, sec. II.C), through the same recurrence as
+    kpm_dos_moments (doubled for the Hermitian forms).  Returns
+    (n_moments, len(orbitals)), real."""
+    idx = np.asarray(orbitals, dtype=np.int64).reshape(-1)
+    if idx.size == 0:
+        raise ValueError("no orbitals given")
+    if idx.min() < 0 or idx.max() >= cheby.n_rows:
+        raise ValueError("orbital index outside the operator")
+    cplx = cheby.H.is_complex or cheby.H.imaginary
+    if cheby.is_double:
+        dt = torch.complex128 if cplx else torch.float64
+    else:
+        dt = torch.complex64 if cplx else torch.float32
+    psi = torch.zeros(cheby.n_rows, idx.size, dtype=dt, device=f"cuda:{cheby.H.ctx.device}")
+    psi[torch.as_tensor(idx, device=psi.device), torch.arange(idx.size, device=psi.device)] = 1.0
+    _, col = _moments(cheby, psi, n_moments, doubled=cheby.op_is_hermitian(), per_column=True)
+    return col.real.copy()
+
+
 def kpm_dos_moments_plain(cheby: Chebyshev, psi_in: torch.Tensor, n_moments: int) -> np.ndarray:
     m, _ = _moments(cheby, psi_in, n_moments, doubled=False)
     return m

@@ -22,7 +22,7 @@ from .bloch import ImageOperator
 from .bounds import estimate_spectral_bounds
 from .calc import (Chebyshev, ISQRTMPreconditioner, corr_dos, corr_moment_count,
                    dos_energy_grid, dos_moment_count, evaluate_kpm_density, kpm_dos_moments,
-                   parse_kpm_kernel)
+                   kpm_ldos_moments, parse_kpm_kernel)
 from .shard import gather_kpoint_results, partition_kpoints, torch_all_reduce_sum
 from .transport import BASTIN, GREENWOOD, dc_spectrum_fftcheb, integrate_dc_spectrum
 from ._capi import RANDOM_PHASE
@@ -254,6 +254,27 @@ class RSATB:
             else:
                 out[kidx] = 2.0 * evaluate_kpm_density(mu, x, 0.5 / nt, device=dev)
         return self._gather(out).reshape(-1), omega
+
+    def compute_ldos(self, orbitals, dE: float):
+        """Orbital-resolved KPM local DOS on ComputeDos's grid: for every
+        orbital i, 2 rho_i(x) with rho_i from the moments <e_i|T_n|e_i> and
+        the Jackson moment count of compute_dos (the same factor 2 and the
+        same per-unit-x convention as compute_dos).  Returns
+        (ldos[n_k, n_orbitals, 2 nt], omega)."""
+        if not dE > 0.0:
+            raise ValueError("dE must be a positive energy resolution in eV")
+        emin, emax = self.energy_bounds()
+        x, omega, nt = dos_energy_grid(emin, emax, dE)
+        N = dos_moment_count((emax - emin) / 2.0, dE)
+        idx = np.asarray(orbitals, dtype=np.int64).reshape(-1)
+        mixed = self.options.precision == "mixed"
+        dev = self.H.ctx.device
+        out = np.zeros((len(self.kpoints), idx.size, 2 * nt))
+        for kidx in self._local_kidx():
+            mu = kpm_ldos_moments(self._cheby(emin, emax, mixed, kidx), idx, N)
+            for j in range(idx.size):
+                out[kidx, j] = 2.0 * evaluate_kpm_density(mu[:, j], x, 0.5 / nt, device=dev)
+        return self._gather(out), omega
 
     def compute_dc_spectrum(self, n_moments: int, formulation: str = "greenwood",
                             axis: str = "abc", partition_sections: int = 0,
