@@ -281,42 +281,3 @@ def test_compute_dos_solve_form():
             H, SetupOptions(preconditioner=PreconditionerOptions(operator_form="cg"),
                             energy_bounds=(emin, emax)))
 
-
-@pytest.mark.gpu
-@pytest.mark.parametrize("precision,tol", [("f64", 1e-10), ("mixed", 1e-4)])
-def test_compute_ldos_matches_exact_diagonalisation(precision, tol):
-    """Orbital LDOS: the local moments <e_i|T_n|e_i> against the FP64
-    exact-diagonalisation oracle sum_n |U_in|^2 T_m(x_n), and the LDOS
-    against the oracle's density of those moments (error peak-normalised,
-    as for the DOS)."""
-    import torch
-    from rsatb_b200 import lattice
-    from rsatb_b200.calc import Chebyshev, dos_energy_grid, dos_moment_count, kpm_ldos_moments
-    from rsatb_b200.driver import RSATB, SetupOptions
-    from rsatb_b200.vbcsr import BlockSpMat
-    torch.cuda.set_device(0)
-    H, _, _ = lattice.graphene(8, 7)
-    emin, emax = -8.6, 8.7
-    c, hw = (emax + emin) / 2, (emax - emin) / 2
-    w, U = np.linalg.eigh(H.to_dense())
-    theta = np.arccos((w - c) / hw)
-    orbs = [0, 5, 17, 111]
-    M = 64
-    mu_ed = np.array([[np.sum(U[i] ** 2 * np.cos(m * theta)) for i in orbs] for m in range(M)])
-    cheb = Chebyshev(BlockSpMat(H.row_ptr, H.col_ind, H.values, 1), emin, emax)
-    if precision == "mixed":
-        cheb = cheb.astype("f32")
-    mu = kpm_ldos_moments(cheb, orbs, M)
-    assert mu.shape == (M, len(orbs))
-    # A single unit column does not average the FP32 rounding away as the
-    # stochastic DOS does: mixed-mode local moments to 5e-5, LDOS to 1e-4.
-    assert np.abs(mu - mu_ed).max() < (1e-10 if precision == "f64" else 5e-5)
-    calc = RSATB(H, SetupOptions(energy_bounds=(emin, emax), precision=precision))
-    dE = 0.4
-    ldos, omega = calc.compute_ldos(orbs, dE)
-    x, _, nt = dos_energy_grid(emin, emax, dE)
-    N = dos_moment_count(hw, dE)
-    for j, i in enumerate(orbs):
-        mu_i = np.array([np.sum(U[i] ** 2 * np.cos(m * theta)) for m in range(N)])
-        want = 2.0 * oracle.density(mu_i.astype(np.complex128), x, 0.5 / nt)
-        assert np.abs(ldos[0, j] - want).max() < tol * want.max()

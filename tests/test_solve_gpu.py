@@ -152,35 +152,3 @@ def test_preconditioned_solve_form_moments(torch_cuda, diamond):
                                           (emax + emin) / 2, (emax - emin) / 2, 32)
     assert np.abs(mu.real - want).max() < 1e-9 * abs(want[0])
 
-
-def _csr_dev(A):
-    """A dense matrix as a device BSR of 1x1 blocks (its nonzero pattern)."""
-    from rsatb_b200.vbcsr import BlockSpMat
-    rows, cols = np.nonzero(A)
-    row_ptr = np.zeros(A.shape[0] + 1, dtype=np.int32)
-    np.add.at(row_ptr, rows + 1, 1)
-    return BlockSpMat(np.cumsum(row_ptr), cols, A[rows, cols].reshape(-1, 1, 1), 1)
-
-
-def test_cg_reference_cases(torch_cuda):
-    """The cases of the reference's test_solver.cpp: S = 2 I gives X = B / 2;
-    a 1-D Laplacian with a varying diagonal is solved to the residual
-    tolerance, plainly and with a diagonal symmetric preconditioner."""
-    torch = torch_cuda
-    from rsatb_b200.calc import ISQRTMPreconditioner, cg_solve
-    rng = np.random.default_rng(4)
-    n = 40
-    B = rng.standard_normal((n, 3))
-    Bd = torch.as_tensor(B).cuda().contiguous()
-    X = torch.zeros_like(Bd)
-    it, _ = cg_solve(_csr_dev(2.0 * np.eye(n)), Bd, X, tol=1e-8, max_iter=100)
-    assert it == 1 and np.abs(X.cpu().numpy() - B / 2).max() < 1e-13
-    A = np.diag(2.0 + 0.1 * (np.arange(n) % 3)) - np.eye(n, k=1) - np.eye(n, k=-1)
-    X = torch.zeros_like(Bd)
-    it, res = cg_solve(_csr_dev(A), Bd, X, tol=1e-8, max_iter=1000)
-    assert res < 1e-8 and np.abs(A @ X.cpu().numpy() - B).max() < 1e-7
-    D = np.diag(1.0 / np.sqrt(np.diag(A)))
-    X = torch.zeros_like(Bd)
-    it2, res2 = cg_solve(_csr_dev(A), Bd, X, tol=1e-10, max_iter=1000,
-                         preconditioner=ISQRTMPreconditioner(_csr_dev(D)))
-    assert res2 < 1e-10 and np.abs(A @ X.cpu().numpy() - B).max() < 1e-8
