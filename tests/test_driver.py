@@ -24,10 +24,16 @@ def test_normalisation_volume():
 
 
 def test_setup_options_defaults():
+    """SetupOptions and PreconditionerOptions defaults of the reference
+    (pybind_rsatb.cpp:292-299, rsatb/model/setup.hpp:33-51)."""
     from rsatb_b200.driver import SetupOptions
     o = SetupOptions()
     assert o.nsamples == 1 and o.sample_seed == 20240917 and o.compute_bounds
-    assert o.kpoints == [[0.0, 0.0, 0.0]]
+    assert o.kpoints == [[0.0, 0.0, 0.0]] and o.energy_bounds is None
+    assert o.bounds_zero_tol == 1e-12 and o.bounds_max_matvecs == 10000
+    p = o.preconditioner
+    assert (p.operator_form, p.tol, p.sptol, p.maxiter) == ("solve", 1e-7, 1e-5, 0)
+    assert (p.cg_tol, p.cg_max_iter) == (1e-8, 1000)
 
 
 def _oracle_samples(n, nsamples, seed):
