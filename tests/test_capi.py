@@ -82,3 +82,30 @@ def test_invalid_arguments_are_status_codes():
                                    _capi.F64, 4, 1,
                                    mu.ctypes.data_as(C.POINTER(C.c_double)), None)
     assert st == 18  # NotSupported
+
+
+def _ctx_first_functions() -> list[str]:
+    """Entry points returning a status whose first parameter is the context."""
+    text = "".join(h.read_text() for h in sorted((ROOT / "include").glob("*.h")))
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\bint\s+(rsatb_\w+)\s*\(\s*rsatb_ctx_t\s+ctx\b", text)))
+
+
+def test_null_context_is_a_status_code_everywhere():
+    """Every entry point taking a context refuses a null one with
+    RSATB_INVALID_ARGUMENT and a message, before touching any other argument
+    (no GPU involved); destroying a null context is a no-op."""
+    from rsatb_b200 import _capi
+    lib = _capi.lib()
+    names = [n for n in _ctx_first_functions() if n != "rsatb_ctx_destroy"]
+    assert len(names) >= 25
+    for name in names:
+        fn = getattr(lib, name)
+        args = [None]
+        for t in fn.argtypes[1:]:
+            is_pointer = (t is C.c_void_p or t is C.c_char_p
+                          or (isinstance(t, type) and issubclass(t, C._Pointer)))
+            args.append(None if is_pointer else t(0))
+        assert fn(*args) == 1, name   # RSATB_INVALID_ARGUMENT
+        assert b"null context" in lib.rsatb_last_error(), name
+    assert lib.rsatb_ctx_destroy(None) == 0
