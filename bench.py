@@ -364,7 +364,7 @@ def fma_peaks() -> dict:
     from rsatb_b200.vbcsr import context
     ctx = context()
     out = {}
-    for name, dp in (("f64", 1), ("f32", 0), ("f32x2", 2), ("f64_dmma", 3)):
+    for name, dp in (("f64", 1), ("f32", 0), ("f32x2", 2), ("f64_dmma", 3), ("tf32_mma", 4)):
         v = C.c_double()
         _capi.check(_capi.lib().rsatb_measure_fma_peak(ctx.handle, dp, C.byref(v)))
         out[name] = v.value

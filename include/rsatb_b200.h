@@ -110,6 +110,14 @@ RSATB_API int rsatb_ctx_destroy(rsatb_ctx_t ctx);
 RSATB_API int rsatb_ctx_set_stream(rsatb_ctx_t ctx, void* stream);
 /* The stream the context launches on (a cudaStream_t). */
 RSATB_API void* rsatb_ctx_stream(rsatb_ctx_t ctx);
+/* Waits for the work queued on the context's stream.  Returns
+ * RSATB_CUDA_ERROR ("... bounded wait ...") when a step kernel of an
+ * asynchronous call queued since the last check gave up on a bounded wait
+ * (rsatb_bsr_mult_dense, rsatb_cheb_apply_op, rsatb_cheb_apply_dual and
+ * rsatb_cheb_propagate return before their kernels run, so they cannot
+ * report it themselves); the report clears the context's fault word.  Every
+ * entry point that synchronises (moments, transport, CG, the adjoint)
+ * reports such a give-up the same way, its own or an earlier call's. */
 RSATB_API int rsatb_ctx_synchronize(rsatb_ctx_t ctx);
 /* Number of kernels the context has launched so far (all entry points). */
 RSATB_API int64_t rsatb_ctx_launch_count(rsatb_ctx_t ctx);
@@ -246,7 +254,12 @@ RSATB_API int rsatb_kpm_dos_moments(rsatb_ctx_t ctx, const rsatb_cheb_op* op, co
  * arithmetic and results as rsatb_kpm_dos_moments; it allocates nothing:
  * all its temporaries live in one fixed 32 MiB static device array that
  * every GPU loading the library holds until exit.  The first call on a
- * device looks up that array's address (make it before any stream capture).
+ * device looks up that array's address (make it before any stream capture);
+ * with lazy module loading (the CUDA 12.2+ default) that first call is also
+ * what reserves the 32 MiB on the device, so a caller that hands the rest
+ * of the device to another allocator makes it before that allocator takes
+ * the memory.  A bounded wait of a step kernel that gives up fails the call
+ * with RSATB_CUDA_ERROR (its fault word is in the static array too).
  * Problems whose temporaries exceed 32 MiB are rejected with
  * RSATB_INVALID_ARGUMENT; calls overlapping on the GPU share the array and
  * race, so serialise them.  No counterpart in the reference: RSATB runs on
@@ -489,7 +502,8 @@ RSATB_API int rsatb_isqrt_autotune(rsatb_ctx_t ctx, int precision, int n_sizes,
  * on every SM timed with CUDA events: the compute roofline of the block SpMM
  * at wide panels.  double_precision: 1 FP64, 0 FP32 (scalar FMAs), 2 FP32
  * issued as packed pairs (fma.rn.f32x2), 3 FP64 on the tensor cores
- * (mma.sync m8n8k4 f64 tiles). */
+ * (mma.sync m8n8k4 f64 tiles), 4 TF32 on the tensor cores (mma.sync m16n8k8
+ * tf32 tiles, FP32 accumulation). */
 RSATB_API int rsatb_measure_fma_peak(rsatb_ctx_t ctx, int double_precision, double* flops);
 
 #ifdef __cplusplus

@@ -277,6 +277,7 @@ int vjp_impl(rsatb_context* ctx, const rsatb_cheb_op* op, const VT* psi, int R, 
     RSATB_CUDA_TRY(cudaMemcpyAsync(h.data(), dots, h.size() * sizeof(double),
                                    cudaMemcpyDeviceToHost, st));
     RSATB_CUDA_TRY(cudaStreamSynchronize(st));
+    RSATB_TRY(ctx_check_fault(ctx));
     if (mu_out)
         for (int n = 0; n < M; ++n) {
             double s = 0.0;

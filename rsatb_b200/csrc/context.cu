@@ -90,7 +90,8 @@ int ctx_check_fault(rsatb_context* ctx) {
     if (h == 0) return RSATB_SUCCESS;
     RSATB_CUDA_TRY(cudaMemsetAsync(w, 0, sizeof(unsigned), ctx->stream));
     return set_error(RSATB_CUDA_ERROR,
-                     "a step kernel gave up waiting for its bulk copies (bounded wait)");
+                     "a step kernel gave up waiting for its bulk copies (bounded wait), in this "
+                     "call or in an earlier asynchronous call on this context");
 }
 
 }  // namespace rsatb_b200
@@ -159,7 +160,9 @@ int rsatb_ctx_synchronize(rsatb_ctx_t ctx) {
     clear_error();
     RSATB_TRY(check_ctx(ctx));
     RSATB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-    return RSATB_SUCCESS;
+    // Bounded waits that gave up in asynchronous calls queued on this context
+    // (mult_dense, apply_op, apply_dual, propagate) are reported here.
+    return ctx_check_fault(ctx);
 }
 
 int64_t rsatb_ctx_launch_count(rsatb_ctx_t ctx) { return ctx ? ctx->launches : 0; }

@@ -596,6 +596,7 @@ int fftcheb_impl(const Ctx& c, const rsatb_bsr_matrix* const* V, const T* psi, i
     RSATB_CUDA_TRY(cudaMemcpyAsync(Kh.data(), K, Kh.size() * sizeof(double),
                                    cudaMemcpyDeviceToHost, st));
     RSATB_CUDA_TRY(cudaStreamSynchronize(st));
+    RSATB_TRY(ctx_check_fault(ctx));
     // Sample average and the ascending energy grid of
     // fftcheb_transport.hpp:602-659: E_k = c + hw cos(pi (M - 1 - k + 1/2) / M).
     for (int k = 0; k < M; ++k) {

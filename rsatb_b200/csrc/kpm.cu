@@ -369,8 +369,10 @@ int rsatb_kpm_dos_moments(rsatb_ctx_t ctx, const rsatb_cheb_op* op, const void* 
             return set_error(RSATB_INVALID_ARGUMENT,
                              "the Solve form S^-1 H is not Hermitian: use the plain recurrence "
                              "(doubled = 0)");
-        return solve_form_moments(ctx, op, psi, n_vectors, vec_dtype, n_moments, mu_out,
-                                  col_mu_out);
+        RSATB_TRY(solve_form_moments(ctx, op, psi, n_vectors, vec_dtype, n_moments, mu_out,
+                                     col_mu_out));
+        RSATB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        return ctx_check_fault(ctx);
     }
     OpShape sh{};
     RSATB_TRY(check_op(op, vec_dtype, &sh));

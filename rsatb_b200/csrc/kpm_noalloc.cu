@@ -17,10 +17,20 @@
 // address is looked up once per device with cudaGetSymbolAddress (with that
 // device current) on the first call on that device, so that first call does
 // the set-up and should come before any stream capture.  All calls share the
-// array and it keeps the last call's contents: the counter is cleared at the
-// start of every call, everything else is written before it is read.  Calls
-// that overlap on the GPU (two streams, two host threads) race on the array;
-// serialise them.
+// array and it keeps the last call's contents: the array's 256-byte header
+// (the completion counter of the dot reductions and the fault word of the
+// step kernels' bounded waits) is cleared at the start of every call,
+// everything else is written before it is read.  The fault word lives in
+// the header, not in the context, so that no context counter is ever
+// allocated on this path; it is read back with the dots, and a wait that
+// gave up fails the call with RSATB_CUDA_ERROR.  Calls that overlap on the
+// GPU (two streams, two host threads) race on the array; serialise them.
+//
+// With lazy module loading (the default since CUDA 12.2) the array is
+// reserved when this file's module is loaded, which the first call's
+// cudaGetSymbolAddress does: on a device whose memory another allocator
+// will take in full, make the first call (for example on a tiny problem)
+// before that allocator reserves the device.
 #include "cheb_kernels.cuh"
 
 #include <cmath>
@@ -64,13 +74,16 @@ int scratch_address(int device, unsigned char** out) {
 size_t round256(size_t b) { return (b + 255) & ~size_t(255); }
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
-StepArgs blank(int W) {
+// Step arguments with the fault word of the static array's header, so that
+// run_step never falls back to the context's (allocated) fault word.
+StepArgs blank(int W, unsigned* fault) {
     StepArgs a{};
     a.W = W;
     a.s_in = 1.0;
     a.s_out = 1.0;
     a.s2 = 1.0;
     a.dot_mode = DOT_NONE;
+    a.fault = fault;
     return a;
 }
 
@@ -146,19 +159,23 @@ extern "C" int rsatb_kpm_dos_moments_noalloc(rsatb_ctx_t ctx, const rsatb_cheb_o
                          need, kNoAllocScratchBytes);
     unsigned char* base = nullptr;
     RSATB_TRY(scratch_address(ctx->device, &base));
+    // Header: the dot reductions' completion counter at byte 0, the step
+    // kernels' fault word at byte 128.
     unsigned* counter = reinterpret_cast<unsigned*>(base);
+    unsigned* fault = reinterpret_cast<unsigned*>(base + 128);
     unsigned char* p = base + 256;
     void* buf[3] = {p, p + vbytes, p + 2 * vbytes};
     void* u = sandwich ? p + 3 * vbytes : nullptr;
     void* w = sandwich ? p + 4 * vbytes : nullptr;
     double* partials = reinterpret_cast<double*>(p + n_panels * vbytes);
     double* dots = reinterpret_cast<double*>(p + n_panels * vbytes + part_bytes);
-    // The last-CTA reductions need a zero counter; the previous call left it
-    // at zero, but a call that failed half-way may not have.
-    RSATB_CUDA_TRY(cudaMemsetAsync(counter, 0, 256, ctx->stream));
+    // The last-CTA reductions need a zero counter and the fault word starts
+    // clear; the previous call left the counter at zero, but a call that
+    // failed half-way may not have.
+    RSATB_CUDA_TRY(cudaMemsetAsync(base, 0, 256, ctx->stream));
 
     {
-        StepArgs a = blank(W);
+        StepArgs a = blank(W, fault);
         a.x = psi;
         a.in = psi;
         a.partials = partials;
@@ -173,7 +190,7 @@ extern "C" int rsatb_kpm_dos_moments_noalloc(rsatb_ctx_t ctx, const rsatb_cheb_o
     for (int s = 1; s <= n_steps; ++s) {
         void* out = buf[slot];
         slot = (slot + 1) % 3;
-        StepArgs last = blank(W);
+        StepArgs last = blank(W, fault);
         last.x = cur;
         last.p = (s == 1) ? nullptr : prev;
         last.psi0 = psi;
@@ -187,7 +204,7 @@ extern "C" int rsatb_kpm_dos_moments_noalloc(rsatb_ctx_t ctx, const rsatb_cheb_o
         last.dots_out = dots + size_t(s) * 2 * W;
         last.counter = counter;
         if (sandwich) {
-            StepArgs a = blank(W);
+            StepArgs a = blank(W, fault);
             a.in = cur;
             a.y = u;
             RSATB_TRY(run_step(ctx, op->Z, vec_dtype, a));
@@ -205,9 +222,16 @@ extern "C" int rsatb_kpm_dos_moments_noalloc(rsatb_ctx_t ctx, const rsatb_cheb_o
     }
 
     std::vector<double> h(size_t(n_steps + 1) * 2 * W);
+    unsigned fault_h = 0;
     RSATB_CUDA_TRY(cudaMemcpyAsync(h.data(), dots, sizeof(double) * h.size(),
                                    cudaMemcpyDeviceToHost, ctx->stream));
+    RSATB_CUDA_TRY(cudaMemcpyAsync(&fault_h, fault, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                                   ctx->stream));
     RSATB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    if (fault_h)
+        return set_error(RSATB_CUDA_ERROR,
+                         "a step kernel gave up waiting for its bulk copies (bounded wait); the "
+                         "moments of this call are not valid");
 
     using cd = std::complex<double>;
     auto coldot = [&](int s, int d, int q) -> cd {

@@ -516,6 +516,8 @@ extern "C" int rsatb_cg_solve(rsatb_ctx_t ctx, rsatb_bsr_t S, rsatb_bsr_t Z, rsa
     int it = 0;
     double res = 0.0;
     RSATB_TRY(cg_solve(s, w, S, Z, ZH, B, X, tol, max_iter, &it, &res));
+    RSATB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    RSATB_TRY(ctx_check_fault(ctx));
     if (iterations) *iterations = it;
     if (max_residual) *max_residual = res;
     return RSATB_SUCCESS;

@@ -5,10 +5,14 @@ device memory is all reserved by another allocator, or a loop that must not
 take cudaMalloc's device-wide synchronisation): it keeps every temporary in a
 fixed 32 MiB static device array.  This file checks, through the C ABI,
 that two calls in a row give the same moments as rsatb_kpm_dos_moments
-(within the 1e-10 moment tolerance of the other KPM tests) and that a
-problem too large for the array is refused.  It is collected last so that a
-failure here never hides the other tests, and it builds everything it needs
-itself, so it also passes alone in a fresh process.
+(within the 1e-10 moment tolerance of the other KPM tests), that the first
+call ever made on a new context takes no device memory (the context has not
+allocated its counters or scratch yet, which is the case the entry point is
+for), that a bounded wait that gives up fails the call instead of returning
+wrong moments, and that a problem too large for the array is refused.  It
+is collected last so that a failure here never hides the other tests, and
+it builds everything it needs itself, so it also passes alone in a fresh
+process.
 """
 from __future__ import annotations
 
@@ -90,3 +94,64 @@ def test_noalloc_refuses_problems_beyond_its_array():
                         dtype_code(psi.dtype), 16, True)
     assert st == 1  # RSATB_INVALID_ARGUMENT
     assert b"32 MiB" in _capi.lib().rsatb_last_error()
+
+
+def test_noalloc_first_call_on_a_fresh_context_takes_no_device_memory():
+    """A caller whose device memory belongs to another allocator makes its
+    first call on a context that has allocated nothing yet.  The call must
+    not allocate either: the free device memory is the same before and after
+    it, and the moments equal the allocating entry point's."""
+    import torch
+    from rsatb_b200 import _capi
+    from rsatb_b200.vbcsr import Context, context, dtype_code
+    lib = _capi.lib()
+    cases = _operators()
+    # Load the library's modules and the static array once (the first call
+    # on a device reserves it), on the shared context.
+    for _, cheby, psi in cases:
+        st, _, _ = _moments(lib.rsatb_kpm_dos_moments_noalloc, context(), cheby.c_op(), psi,
+                            dtype_code(psi.dtype), 64, True)
+        assert st == 0, lib.rsatb_last_error()
+    for name, cheby, psi in cases:
+        fresh = Context(torch.cuda.current_device())
+        try:
+            fresh.bind_stream()
+            torch.cuda.synchronize()
+            free0 = torch.cuda.mem_get_info()[0]
+            st, got, _ = _moments(lib.rsatb_kpm_dos_moments_noalloc, fresh, cheby.c_op(), psi,
+                                  dtype_code(psi.dtype), 64, True)
+            torch.cuda.synchronize()
+            free1 = torch.cuda.mem_get_info()[0]
+            assert st == 0, lib.rsatb_last_error()
+            assert free1 == free0, (name, free0 - free1)
+        finally:
+            lib.rsatb_ctx_destroy(fresh.handle)
+        st, want, _ = _moments(lib.rsatb_kpm_dos_moments, context(), cheby.c_op(), psi,
+                               dtype_code(psi.dtype), 64, True)
+        assert st == 0, lib.rsatb_last_error()
+        assert np.abs(got - want).max() <= TOL * np.abs(want).max(), name
+
+
+def test_noalloc_reports_a_bounded_wait_that_gave_up(monkeypatch):
+    """The bulk-copy step kernel's bounded wait, armed for bytes no copy
+    delivers (a 5 ms limit, no copy issued), sets the fault word in the
+    static array's header; the call then fails with RSATB_CUDA_ERROR instead
+    of returning its moments, and the next call is correct again."""
+    from rsatb_b200 import _capi
+    from rsatb_b200.vbcsr import context, dtype_code
+    lib = _capi.lib()
+    name, cheby, psi = _operators()[2]  # FP32 sandwich, 8x8 blocks, W = 16
+    op = cheby.c_op()
+    code = dtype_code(psi.dtype)
+    monkeypatch.setenv("RSATB_STEP_KERNEL", "bulk")
+    monkeypatch.setenv("RSATB_TEST_BULK_WAIT", "1")
+    st, _, _ = _moments(lib.rsatb_kpm_dos_moments_noalloc, context(), op, psi, code, 32, True)
+    assert st == 16, (st, lib.rsatb_last_error())  # RSATB_CUDA_ERROR
+    assert b"bounded wait" in lib.rsatb_last_error()
+    monkeypatch.delenv("RSATB_TEST_BULK_WAIT")
+    monkeypatch.delenv("RSATB_STEP_KERNEL")
+    st, got, _ = _moments(lib.rsatb_kpm_dos_moments_noalloc, context(), op, psi, code, 32, True)
+    assert st == 0, lib.rsatb_last_error()
+    st, want, _ = _moments(lib.rsatb_kpm_dos_moments, context(), op, psi, code, 32, True)
+    assert st == 0, lib.rsatb_last_error()
+    assert np.abs(got - want).max() <= 1e-6 * np.abs(want).max(), name
