@@ -335,7 +335,6 @@ def cpu_baseline(wl, n_moments: int):
     """The oracle's FP64 recurrence (oracle/kpm_oracle.c) on the host cores,
     on the same operator and samples, over a bounded number of moments."""
     import oracle
-    from rsatb_b200.isqrt import EIGEN_CLAMP  # noqa: F401  (same factor as the GPU)
     H = oracle.Bsr(wl.H.n_block_rows, wl.H.n_block_rows, wl.H.block_size, wl.H.row_ptr,
                    wl.H.col_ind, wl.H.values)
     if wl.Z is not None:
@@ -382,25 +381,81 @@ def build_workload(args, rank):
 
 
 def config_of(wl) -> dict:
-    return {"workload": wl.name + (": diamond LCAO 16^3 conventional cells, 32768 atoms x 8 "
+    """The workload as both arms name it (the spectral window, which each
+    arm estimates for itself, is reported beside the config)."""
+    return {"workload": wl.name + (": diamond LCAO %d^3 conventional cells, %d atoms x 8 "
                                    "orbitals, 8x8 BSR to the 3rd shell (29 blocks/row), "
                                    "operator Z^H H Z with the graph-local S^-1/2"
+                                   % (round((wl.n_rows // 64) ** (1 / 3)), wl.n_rows // 8)
                                    if wl.name == "diamond_sandwich" else ": pz graphene"),
             "n_rows": wl.n_rows, "vectors_per_gpu": wl.R, "n_moments": wl.n_moments,
             "block_size": wl.H.block_size, "nnz_blocks": int(wl.H.nnz_blocks),
-            "bounds_ev": [round(wl.emin, 4), round(wl.emax, 4)],
             "sample_vectors": "complex random phase" if wl.complex_vectors else "Rademacher",
             "l2": "inputs larger than L2 (every panel >= 134 MB > 126 MB L2)"
             if wl.n_rows * wl.R * 4 > 126e6 else "working set may be L2-resident"}
 
 
-def reference_arm(args, dist):
-    """The reference's CPU path (the oracle port; the reference itself cannot
-    be built here) on rank 0, bounded steps."""
-    if dist.rank != 0:
+class HostWorkload:
+    """The bench workload built on the host only (numpy and the oracle), for
+    the reference arm: the same seeded H (and S), the graph-local S^-1/2 by
+    the reference's eigen route, the spectral window by the same Lanczos
+    from the same start vector, the same sample vectors.  Nothing here loads
+    the CUDA library."""
+
+    def __init__(self, args):
+        import oracle
+        from rsatb_b200 import lattice
+        t0 = time.perf_counter()
+        self.setup_seconds = {}
+        self.first_column = 0
+        if args.workload == "graphene":
+            n = 30 if args.small else 60
+            self.name, self.R, self.n_moments, self.orbitals = "graphene_dos", 8, 512, 1
+            self.complex_vectors = True
+            self.H, _, _ = lattice.graphene(n, n)
+            self.Z = None
+        else:
+            L, self.R, self.n_moments = (6, 32, 256) if args.small else (16, 128, 1024)
+            self.name, self.orbitals, self.complex_vectors = "diamond_sandwich", 8, False
+            self.H, S = lattice.diamond_lcao(L=L, seed=7)
+            self.setup_seconds["generate"] = time.perf_counter() - t0
+            t1 = time.perf_counter()
+            zv = oracle.graph_inverse_sqrt_eigen(S.row_ptr, S.col_ind, S.values, S.block_size)
+            self.Z = lattice.BsrArrays(S.row_ptr, S.col_ind, zv, S.block_size)
+            self.setup_seconds["graph_inverse_sqrt_eigen"] = time.perf_counter() - t1
+        t1 = time.perf_counter()
+        H = oracle.Bsr(self.H.n_block_rows, self.H.n_block_rows, self.H.block_size,
+                       self.H.row_ptr, self.H.col_ind, self.H.values)
+        Z = ZH = None
+        if self.Z is not None:
+            Z = oracle.Bsr(self.Z.n_block_rows, self.Z.n_block_rows, self.Z.block_size,
+                           self.Z.row_ptr, self.Z.col_ind, self.Z.values)
+            ZH = oracle.bsr_adjoint(Z)
+        unit = oracle.make_op(H, 0.0, 1.0, Z, ZH)
+        self.emin, self.emax = oracle.lanczos_bounds(lambda X: oracle.apply_op(unit, X),
+                                                     self.H.n_rows)
+        self.setup_seconds["lanczos_bounds"] = time.perf_counter() - t1
+
+    @property
+    def n_rows(self) -> int:
+        return self.H.n_rows
+
+
+def reference_arm(args):
+    """The reference's CPU path on the host cores, rank 0 only: the oracle's
+    FP64 restatement of the recurrence (the reference itself cannot be built
+    here), timed over the same number of moments as the cpu_baseline leg, on
+    a workload built on the host without the CUDA library."""
+    if int(os.environ.get("RANK", "0")) != 0:
         return
-    wl = build_workload(args, 0)
-    n_mom = max(2, args.cpu_moments // 2)
+    if args.workload not in ("diamond", "graphene"):
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "the reference arm covers the KPM DOS workloads "
+                                         "(diamond, graphene); the --workload %s line carries "
+                                         "its own cpu_baseline" % args.workload}), flush=True)
+        return
+    wl = HostWorkload(args)
+    n_mom = args.cpu_moments
     samples = []
     for k in range(args.warmup + args.steps):
         base, _ = cpu_baseline(wl, n_mom)
@@ -415,10 +470,14 @@ def reference_arm(args, dist):
             "ms_per_step": 1e3 * sum(secs) / len(secs), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": config_of(wl), "cpu_baseline": base,
+            "bounds_ev": [round(wl.emin, 4), round(wl.emax, 4)],
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
+            "cuda_library_loaded": "rsatb_b200._capi" in sys.modules,
+            "setup_seconds": {k: round(v, 2) for k, v in wl.setup_seconds.items()},
             "note": "RSATB cannot be built here (vbcsr, PRIMME, MPI, FFTW, HDF5 absent); the "
-                    "timed CPU path is the oracle's FP64 restatement of the same recurrence"}
+                    "timed CPU path is the oracle's FP64 restatement of the same recurrence, "
+                    "on H, Z (eigen route) and the window built on the host"}
     print(json.dumps(line), flush=True)
 
 
@@ -826,6 +885,9 @@ def main():
     if args.forms_only:
         forms_only(args)
         return
+    if args.impl == "reference":
+        reference_arm(args)
+        return
     dist = Dist()
     if args.workload == "isqrt" and args.impl == "ours":
         bench_isqrt(args, dist)
@@ -837,10 +899,6 @@ def main():
         return
     if args.workload == "transport" and args.impl == "ours":
         bench_transport(args, dist)
-        dist.close()
-        return
-    if args.impl == "reference":
-        reference_arm(args, dist)
         dist.close()
         return
     import torch
@@ -879,7 +937,9 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms32, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 (FP64 rescale + moment dots)", "data": "synthetic (seeded generators)",
-            "config": dict(config_of(wl), parallelism=f"samples sharded over {dist.world} GPU(s)"),
+            "config": config_of(wl),
+            "parallelism": f"samples sharded over {dist.world} GPU(s)",
+            "bounds_ev": [round(wl.emin, 4), round(wl.emax, 4)],
             "fp64_path": {"value": round(value64, 1), "ms_per_step": round(ms64, 3),
                           "mixed_over_fp64": round(ms64 / ms32, 3)},
             "dos_err_mixed_vs_fp64": dos_err,

@@ -388,6 +388,126 @@ def isqrt_columns_eigen(A: np.ndarray, col_start: int = 0, k: int | None = None,
     return (V * f) @ V[col_start:col_start + k].T
 
 
+def _graph_isqrt_chunk(args):
+    """Worker of graph_inverse_sqrt_eigen: Z blocks of one chunk of block
+    rows (one batched LAPACK eigh per chunk).  `values` is the block array or
+    the path of a .npy file holding it (read memory-mapped)."""
+    values, members_rows, slot_rows, gather_rows, b = args
+    if isinstance(values, str):
+        values = np.load(values, mmap_mode="r")
+    n, k = members_rows.shape
+    padded = np.concatenate([np.asarray(values), np.zeros((1, b, b))])
+    g = np.where(gather_rows >= 0, gather_rows, values.shape[0])
+    M = padded[g]                                   # (n, k, k, b, b)
+    M = M.transpose(0, 1, 3, 2, 4).reshape(n, k * b, k * b)
+    w, V = np.linalg.eigh(M, UPLO="U")
+    f = np.where(w > EIGEN_CLAMP, 1.0 / np.sqrt(np.maximum(w, EIGEN_CLAMP)), 0.0)
+    idx = slot_rows[:, None] * b + np.arange(b)[None, :]
+    Vs = np.take_along_axis(V, idx[:, :, None], axis=1)       # (n, b, kb)
+    X = np.einsum("nij,nj,nlj->nil", Vs, f, V)                 # rows of M^-1/2
+    return X.reshape(n, b, k, b).transpose(0, 2, 1, 3).reshape(n * k, b, b)
+
+
+def graph_inverse_sqrt_eigen(row_ptr: np.ndarray, col_ind: np.ndarray, values: np.ndarray,
+                             block_size: int, workers: int | None = None,
+                             chunk: int = 256) -> np.ndarray:
+    """The graph-local S^-1/2 factor on the host, FP64: for block row i the
+    dense sub-matrix of S on {i} + its neighbours (rsatb/calc/isqrtm.hpp:
+    149-232, graph_inverse_sqrt) and the block row of its clamped inverse
+    square root at i's position, by the eigen route of
+    isqrt::inverse_sqrt_columns_inplace for n <= 256 (rsatb/calc/
+    isqrt_action.hpp:766-795).  Needs a uniform neighbour count and sorted
+    column indices per row; returns the factor's block values on S's pattern
+    (nnz_blocks, b, b).  The rows are split in chunks over `workers` spawned
+    processes (all host cores by default)."""
+    from concurrent.futures import ProcessPoolExecutor
+    import multiprocessing as mp
+    import tempfile
+    row_ptr = np.asarray(row_ptr, dtype=np.int64)
+    col_ind = np.asarray(col_ind, dtype=np.int64)
+    n = row_ptr.size - 1
+    deg = np.diff(row_ptr)
+    if not np.all(deg == deg[0]):
+        raise ValueError("graph_inverse_sqrt_eigen needs a uniform neighbour count")
+    k = int(deg[0])
+    members = col_ind.reshape(n, k)
+    slot = np.argmax(members == np.arange(n)[:, None], axis=1)
+    key = np.repeat(np.arange(n), k) * n + col_ind
+    b = int(block_size)
+    vals = np.ascontiguousarray(values, dtype=np.float64).reshape(-1, b, b)
+    workers = workers or os.cpu_count() or 1
+    n_chunks = (n + chunk - 1) // chunk
+    parallel = workers > 1 and n_chunks > 1
+
+    def jobs(src):
+        for r0 in range(0, n, chunk):
+            r1 = min(n, r0 + chunk)
+            q = members[r0:r1, :, None] * n + members[r0:r1, None, :]
+            pos = np.minimum(np.searchsorted(key, q), key.size - 1)
+            gather = np.where(key[pos] == q, pos, -1)
+            yield (src, members[r0:r1], slot[r0:r1], gather, b)
+
+    if not parallel:
+        return np.concatenate([_graph_isqrt_chunk(j) for j in jobs(vals)])
+    # Workers read the block values from one memory-mapped file and run
+    # single-threaded LAPACK, one chunk each at a time.
+    saved = {v: os.environ.get(v) for v in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS",
+                                             "MKL_NUM_THREADS")}
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "values.npy")
+        np.save(path, vals)
+        try:
+            for v in saved:
+                os.environ[v] = "1"
+            with ProcessPoolExecutor(max_workers=min(workers, n_chunks),
+                                     mp_context=mp.get_context("spawn")) as pool:
+                parts = list(pool.map(_graph_isqrt_chunk, jobs(path)))
+        finally:
+            for v, old in saved.items():
+                if old is None:
+                    os.environ.pop(v, None)
+                else:
+                    os.environ[v] = old
+    return np.concatenate(parts)
+
+
+def lanczos_bounds(op_apply, n: int, steps: int = 20, seed: int = 2, padding: float = 0.5,
+                   complex_values: bool = False):
+    """Host restatement of the library's spectral-window estimate (a fixed
+    number of Lanczos steps with full reorthogonalisation in FP64, the
+    extreme Ritz values widened by their residual norms and by the
+    reference's 0.5 eV padding, rsatb/setup/spectral_bounds.hpp:67-76,
+    445-490), on the unscaled operator x -> op_apply(x) (N x 1 panels), from
+    the same seeded start vector: Rademacher (complex random phase for a
+    complex operator) of set_random(seed), normalised."""
+    v = set_random(seed, 0 if complex_values else 1, True, np.arange(n), 1, n, 1,
+                   complex_values)[:, 0]
+    dt = np.complex128 if complex_values else np.float64
+    v = (v / np.sqrt(np.vdot(v, v).real)).astype(dt)
+    m = min(steps, n)
+    Q = np.zeros((n, m), dtype=dt)
+    alpha = np.zeros(m)
+    beta = np.zeros(m)
+    q = v
+    for j in range(m):
+        Q[:, j] = q
+        w = op_apply(q[:, None])[:, 0].astype(dt)
+        a = np.vdot(Q[:, j], w).real
+        alpha[j] = a
+        for _ in range(2):
+            w = w - Q[:, :j + 1] @ (Q[:, :j + 1].conj().T @ w)
+        bb = float(np.sqrt(max(np.vdot(w, w).real, 0.0)))
+        beta[j] = bb
+        if bb < 1e-12 * max(1.0, abs(a)):
+            m = j + 1
+            break
+        q = w / bb
+    T = np.diag(alpha[:m]) + np.diag(beta[:m - 1], 1) + np.diag(beta[:m - 1], -1)
+    theta, Y = np.linalg.eigh(T)
+    res = np.abs(beta[m - 1] * Y[-1, :])
+    return float(theta[0] - padding - res[0]), float(theta[-1] + padding + res[-1])
+
+
 def ns_inverse_sqrt_dense(S: np.ndarray, tol: float = 1e-11, maxit: int = 60):
     """Dense FP64 restatement of rsatb::calc::inverse_sqrt's Newton-Schulz
     loop (rsatb/calc/isqrtm.hpp:613-700 and the residual of :370-405 on a
