@@ -508,6 +508,68 @@ def lanczos_bounds(op_apply, n: int, steps: int = 20, seed: int = 2, padding: fl
     return float(theta[0] - padding - res[0]), float(theta[-1] + padding + res[-1])
 
 
+# ------------------------------------------------- exact diagonalisation (ED)
+
+def kpm_moments_ed(H: np.ndarray, psi: np.ndarray, center: float, half_width: float,
+                   n_moments: int, per_column: bool = False):
+    """KPM moments of the dense Hermitian operator H on the sample columns of
+    psi by exact diagonalisation (FP64 LAPACK): with H~ = (H - center) /
+    half_width = U diag(x) U^H, mu_n = (1/R) sum_q sum_k |(U^H psi_q)_k|^2
+    T_n(x_k), the limit the Chebyshev recurrence of kpm_dos_moments
+    (rsatb/calc/dos.hpp:125-190) reaches without rounding.  Real moments
+    (complex dtype, zero imaginary part, like kpm_moments' output)."""
+    x, U = np.linalg.eigh((np.asarray(H) - center * np.eye(H.shape[0])) / half_width)
+    w = np.abs(U.conj().T @ np.asarray(psi)) ** 2            # (n_states, R)
+    th = np.arccos(np.clip(x, -1.0, 1.0))
+    T = np.cos(np.arange(n_moments)[:, None] * th[None, :])  # (n_moments, n_states)
+    col = T @ w                                              # (n_moments, R)
+    mu = col.mean(axis=1).astype(np.complex128)
+    if per_column:
+        return mu, col.astype(np.complex128)
+    return mu
+
+
+def jackson_delta_matrix(E: np.ndarray, levels: np.ndarray, center: float, half_width: float,
+                         n_moments: int, kernel: int = 1) -> np.ndarray:
+    """d[k, n]: the kernel-damped Chebyshev series of delta(E_k - levels_n)
+    in 1/eV, as evaluate_kpm_density builds a density (rsatb/calc/kpm.hpp:
+    206-241: g_0 + 2 sum_m g_m T_m(x) T_m(x_n), over pi sqrt(1 - x^2)), the
+    energy argument x = (E - center) / half_width (the levels' clipped to
+    [-1, 1]) and one more 1/half_width for energy units."""
+    g = kernel_weights(kernel, n_moments)
+    x = (np.asarray(E) - center) / half_width
+    y = np.clip((np.asarray(levels) - center) / half_width, -1.0, 1.0)
+    tx = np.arccos(np.clip(x, -1.0, 1.0))
+    ty = np.arccos(y)
+    out = np.full((x.size, y.size), g[0])
+    for m0 in range(1, n_moments, 256):
+        m = np.arange(m0, min(n_moments, m0 + 256))
+        out += 2.0 * (np.cos(np.outer(tx, m)) * g[m]) @ np.cos(np.outer(m, ty))
+    return out / (np.pi * np.sqrt(np.maximum(1e-14, 1.0 - x ** 2)))[:, None] / half_width
+
+
+def kubo_greenwood_ed(H: np.ndarray, V: np.ndarray, center: float, half_width: float,
+                      n_moments: int, kernel: int = 1):
+    """The exact-trace limit of the FFT-Chebyshev Greenwood accumulation
+    (rsatb/calc/fftcheb_transport.hpp:270-525, 543-660) on the dense
+    Hermitian H and velocity V, by exact diagonalisation: on the ascending
+    Chebyshev-node grid E_k of n_moments points,
+        K(E_k) = (1/4N) sum_nm |V_nm|^2 d(E_k - e_n) d(E_k - e_m)
+    with d the damped delta of jackson_delta_matrix and V_nm in H's
+    eigenbasis.  It is what dc_spectrum_fftcheb returns at prefactor 1 when
+    its samples are the N unit vectors (J = -V / (2 half_width), the delta
+    series' rescaled-to-energy factors, and the 1/R sample average give the
+    1/4N).  Returns (energy, K)."""
+    N = H.shape[0]
+    e, U = np.linalg.eigh(np.asarray(H))
+    Wnm = np.abs(U.conj().T @ np.asarray(V) @ U) ** 2
+    k = np.arange(n_moments)
+    E = center + half_width * np.cos(np.pi * (n_moments - 1 - k + 0.5) / n_moments)
+    d = jackson_delta_matrix(E, e, center, half_width, n_moments, kernel)
+    K = np.einsum("kn,nm,km->k", d, Wnm, d) / (4.0 * N)
+    return E, K
+
+
 def ns_inverse_sqrt_dense(S: np.ndarray, tol: float = 1e-11, maxit: int = 60):
     """Dense FP64 restatement of rsatb::calc::inverse_sqrt's Newton-Schulz
     loop (rsatb/calc/isqrtm.hpp:613-700 and the residual of :370-405 on a

@@ -332,3 +332,45 @@ def test_oracle_integrate_dc_linear_spectrum():
     for T in (0.0, 30.0, 300.0, 3000.0):
         got = oracle.integrate_dc_spectrum(s, e, 0.37, T)
         assert np.abs(got - (a + 0.37 * b)).max() < 1e-10
+
+
+# ------------------------------------------------- exact diagonalisation (ED)
+
+def test_kubo_greenwood_ed_matches_the_reference_ed_sum():
+    """oracle.kubo_greenwood_ed against the reference's own exact-
+    diagonalisation Kubo-Greenwood sum (make_ref_curves.py delta_matrix on
+    the Chebyshev-node grid, committed by tests/golden/make_golden.py):
+    4N K(E_k) = sum_nm |V_nm|^2 dJ dJ to 1e-12 relative, on the grid whose
+    window the reference's window_from_cheb_grid recovers exactly."""
+    z = np.load(GOLDEN / "ed_greenwood.npz")
+    H, V = z["H"], z["V"]
+    c, hw, M = float(z["center"]), float(z["half_width"]), int(z["n_moments"])
+    E, K = oracle.kubo_greenwood_ed(H, V, c, hw, M)
+    assert np.allclose(z["window"], [c, hw], rtol=0, atol=1e-12)
+    assert np.abs(E - z["energy"]).max() < 1e-13
+    assert np.array_equal(oracle.kernel_weights(1, M), z["jackson"]) or \
+        np.abs(oracle.kernel_weights(1, M) - z["jackson"]).max() < 1e-15
+    ref = z["kg_sum"]
+    assert np.abs(4 * H.shape[0] * K - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+def test_kpm_moments_ed_equals_the_recurrence():
+    """The ED moments (eigen-decomposition, T_n at the eigenvalues) against
+    the oracle's Chebyshev recurrence (doubled and plain) on a small
+    complex-Hermitian BSR operator with complex sample columns."""
+    rng = np.random.default_rng(4)
+    n = 60
+    A = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    A = 0.1 * (A + A.conj().T)
+    A[np.abs(A) < 0.12] = 0.0
+    bound = float(np.abs(np.linalg.eigvalsh(A)).max()) + 0.3
+    psi = rng.standard_normal((n, 5)) + 1j * rng.standard_normal((n, 5))
+    rows, cols = np.nonzero(A)
+    row_ptr = np.concatenate([[0], np.cumsum(np.bincount(rows, minlength=n))]).astype(np.int32)
+    Hb = oracle.Bsr(n, n, 1, row_ptr, cols.astype(np.int32),
+                    A[rows, cols].reshape(-1, 1, 1))
+    op = oracle.make_op(Hb, 0.05, bound)
+    want = oracle.kpm_moments_ed(A, psi, 0.05, bound, 64)
+    for doubled in (True, False):
+        got = oracle.kpm_moments(op, psi, 64, doubled=doubled)
+        assert np.abs(got - want).max() <= 1e-11 * np.abs(want[0])
