@@ -11,9 +11,11 @@ HBM; every panel (134-268 MB) is larger than the 126 MB L2.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-With N > 1 (torchrun, one rank per GPU) each rank runs its own 128 sample
-columns (global columns rank*128 ...), the moments are summed with one NCCL
-all-reduce, and the time is the max over ranks.  Prints one JSON line.
+With N > 1 (one rank per GPU; started without a launcher, bench.py runs
+itself under torch.distributed.run with N local ranks) each rank runs its
+own 128 sample columns (global columns rank*128 ...), the moments are summed
+with one NCCL all-reduce, and the time is the max over ranks.  Prints one
+JSON line.
 """
 from __future__ import annotations
 
@@ -43,7 +45,8 @@ def parse_args():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["diamond", "graphene", "isqrt", "transport", "adjoint"],
+    p.add_argument("--workload", choices=["diamond", "graphene", "isqrt", "transport", "adjoint",
+                                          "chain"],
                    default="diamond")
     p.add_argument("--si-L", type=int, default=8, help="silicon conventional cells per side")
     p.add_argument("--tbg-m", type=int, default=31, help="moire index of the TBG cell")
@@ -137,18 +140,25 @@ class ClockSampler:
 # -------------------------------------------------------------- distributed
 
 class Dist:
+    """One rank per GPU (NCCL); without a GPU (the host-only chain
+    workload) the ranks talk over gloo."""
+
     def __init__(self):
         import torch
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
         self.torch = torch
-        if torch.cuda.is_available():
+        self.cuda = torch.cuda.is_available()
+        if self.cuda:
             torch.cuda.set_device(self.local_rank)
         if self.world > 1:
             import torch.distributed as dist
-            dist.init_process_group("nccl", timeout=timedelta(seconds=300),
-                                    device_id=torch.device("cuda", self.local_rank))
+            if self.cuda:
+                dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                        device_id=torch.device("cuda", self.local_rank))
+            else:
+                dist.init_process_group("gloo", timeout=timedelta(seconds=120))
             self.dist = dist
         else:
             self.dist = None
@@ -160,14 +170,17 @@ class Dist:
     def max(self, x: float) -> float:
         if self.dist is None:
             return x
-        t = self.torch.tensor([x], dtype=self.torch.float64, device="cuda")
+        t = self.torch.tensor([x], dtype=self.torch.float64,
+                              device="cuda" if self.cuda else "cpu")
         self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
         return float(t.item())
 
     def sum_array(self, a: np.ndarray) -> np.ndarray:
         if self.dist is None:
             return a
-        t = self.torch.as_tensor(np.ascontiguousarray(a)).cuda()
+        t = self.torch.as_tensor(np.ascontiguousarray(a))
+        if self.cuda:
+            t = t.cuda()
         self.dist.all_reduce(t)
         return t.cpu().numpy()
 
@@ -933,8 +946,64 @@ def bench_adjoint(args, dist):
         print(json.dumps(line), flush=True)
 
 
+def spawn_ranks(args) -> int:
+    """`bench.py --gpus N` started without a launcher: runs the same command
+    under torch.distributed.run with N local ranks (one per GPU, rendezvous
+    on 127.0.0.1), whose rank 0 prints the line; returns their exit status."""
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={args.gpus}", "--master-addr", "127.0.0.1",
+           f"--master-port={port}", str(ROOT / "bench.py"), *sys.argv[1:]]
+    return subprocess.run(cmd, timeout=3600).returncode
+
+
+def chain_moments(n_rows: int, first_column: int, n_cols: int, n_moments: int) -> np.ndarray:
+    """Host workload for the rank plumbing: plain Chebyshev moments
+    mu_n = <psi|T_n(H)|psi> summed over the sample columns first_column ..
+    first_column + n_cols - 1 of a periodic chain H (hopping 1/2, spectrum
+    in [-1, 1]), each column seeded by its global index (numpy)."""
+    cols = [np.random.default_rng(1000 + c).choice([-1.0, 1.0], n_rows) / np.sqrt(n_rows)
+            for c in range(first_column, first_column + n_cols)]
+    psi = np.stack(cols, axis=1)
+    H = lambda x: 0.5 * (np.roll(x, 1, axis=0) + np.roll(x, -1, axis=0))
+    mu = np.zeros(n_moments)
+    t0, t1 = psi, H(psi)
+    mu[0] = float((psi * t0).sum())
+    if n_moments > 1:
+        mu[1] = float((psi * t1).sum())
+    for n in range(2, n_moments):
+        t0, t1 = t1, 2.0 * H(t1) - t0
+        mu[n] = float((psi * t1).sum())
+    return mu
+
+
+def bench_chain(args, dist):
+    """The host-only chain workload: each rank its own R columns, one
+    all-reduce of the moment sums per step, max-over-ranks time."""
+    R, n_rows, n_mom = 4, 4096, 64
+    for _ in range(args.warmup):
+        dist.sum_array(chain_moments(n_rows, dist.rank * R, R, n_mom))
+    dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        mu = dist.sum_array(chain_moments(n_rows, dist.rank * R, R, n_mom)) / (R * dist.world)
+    secs = dist.max((time.perf_counter() - t0) / args.steps)
+    if dist.rank == 0:
+        print(json.dumps({"metric": "chain moments (host plumbing check)",
+                          "value": n_mom * R * dist.world / secs, "unit": UNIT,
+                          "n_gpus": dist.world, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": 1e3 * secs, "moments": mu.tolist(),
+                          "config": {"workload": "chain", "n_rows": n_rows,
+                                     "vectors_per_rank": R, "n_moments": n_mom}}), flush=True)
+
+
 def main():
     args = parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ and args.impl == "ours":
+        sys.exit(spawn_ranks(args))
     if args.spmm_only:
         spmm_only(args)
         return
@@ -945,6 +1014,10 @@ def main():
         reference_arm(args)
         return
     dist = Dist()
+    if args.workload == "chain":
+        bench_chain(args, dist)
+        dist.close()
+        return
     if args.workload == "isqrt" and args.impl == "ours":
         bench_isqrt(args, dist)
         dist.close()
