@@ -8,6 +8,7 @@
 #include "cheb_bulk.cuh"
 #include "cheb_narrow.cuh"
 #include "cheb_dmma.cuh"
+#include "cheb_tf32.cuh"
 
 #include <cstdlib>
 #include <mutex>
@@ -88,8 +89,8 @@ inline int pick_v(int W, bool cv, bool any_b, int block_size, bool dbl) {
 
 constexpr int kNotApplicable = 1000;
 
-// RSATB_STEP_KERNEL=v1|staged|rowsplit|bulk|narrow|dmma forces one kernel family (tuning and
-// A/B tests); unset picks by shape and precision.
+// RSATB_STEP_KERNEL=v1|staged|rowsplit|bulk|narrow|dmma|tf32 forces one kernel family
+// (tuning and A/B tests); unset picks by shape and precision.
 inline int env_kernel() {
     const char* s = std::getenv("RSATB_STEP_KERNEL");
     if (!s) return 0;
@@ -99,6 +100,7 @@ inline int env_kernel() {
     if (s[0] == 'b') return 4;
     if (s[0] == 'n') return 5;
     if (s[0] == 'd') return 6;
+    if (s[0] == 't') return 7;
     return 0;
 }
 inline bool env_force_v1() { return env_kernel() == 1; }
@@ -426,6 +428,40 @@ int launch_bulk(rsatb_context* ctx, StepArgs& a) {
     return kNotApplicable;
 }
 
+template <int W, bool CV, int P, int MINB>
+int launch_tf32_k(rsatb_context* ctx, StepArgs& a) {
+    auto kernel = cheb_step_tf32<W, CV, P, MINB>;
+    const int threads = kTf32Warps * 32;
+    const int64_t need = (a.n_block_rows + kTf32Warps / 2 - 1) / (kTf32Warps / 2);
+    const int per_sm = occupancy(reinterpret_cast<const void*>(kernel), threads, 0);
+    int64_t grid = int64_t(ctx->sm_count) * per_sm;
+    if (need < grid) grid = need;
+    if (grid < 1) grid = 1;
+    kernel<<<unsigned(grid), threads, 0, ctx->stream>>>(a);
+    RSATB_LAUNCH_CHECK(ctx);
+    return RSATB_SUCCESS;
+}
+
+// Split-TF32 tensor-core kernel: FP32 panels, real 8x8 blocks, W in {64,
+// 128, 256}, 16-byte aligned values and operand; kNotApplicable otherwise.
+template <bool CV>
+int launch_tf32(rsatb_context* ctx, StepArgs& a) {
+    if ((reinterpret_cast<uintptr_t>(a.vals) | reinterpret_cast<uintptr_t>(a.in)) & 15u)
+        return kNotApplicable;
+    // RSATB_TF32_SHAPE=p3: three blocks in flight at one CTA per SM less.
+    const char* s = std::getenv("RSATB_TF32_SHAPE");
+    const bool p3 = s && s[0] == 'p' && s[1] == '3';
+    switch (a.W) {
+        case 64:
+            return p3 ? launch_tf32_k<64, CV, 3, 2>(ctx, a) : launch_tf32_k<64, CV, 2, 3>(ctx, a);
+        case 128:
+            return p3 ? launch_tf32_k<128, CV, 3, 1>(ctx, a) : launch_tf32_k<128, CV, 2, 2>(ctx, a);
+        case 256:
+            return p3 ? launch_tf32_k<256, CV, 3, 1>(ctx, a) : launch_tf32_k<256, CV, 2, 1>(ctx, a);
+    }
+    return kNotApplicable;
+}
+
 template <typename VT, typename MT, int B, bool CM, bool CV>
 int launch_b(rsatb_context* ctx, int V, int64_t rows, StepArgs& a);
 
@@ -475,6 +511,13 @@ int launch_typed(rsatb_context* ctx, int block_size, StepArgs& a) {
         // Narrow-panel lock-step kernel: blocks of 8, W <= 16 (when forced).
         if (block_size == 8 && forced == 5) {
             const int st = launch_narrow<VT, CV>(ctx, a);
+            if (st != kNotApplicable) return st;
+        }
+    }
+    if constexpr (sizeof(VT) == 4 && !CM) {
+        // Split-TF32 tensor-core kernel (when forced).
+        if (block_size == 8 && forced == 7) {
+            const int st = launch_tf32<CV>(ctx, a);
             if (st != kNotApplicable) return st;
         }
     }
