@@ -71,6 +71,11 @@ def parse_args():
     p.add_argument("--forms-L", type=int, default=8)
     p.add_argument("--spmm-L", type=int, default=12)
     p.add_argument("--spmm-reps", type=int, default=3)
+    p.add_argument("--spmm-kernels", default="",
+                   help="comma list of FP32 step kernels to A/B in --spmm-only (bulk, tf32, "
+                        "tf32:p3, v1, ...), each with its max error against the FP64 SpMM")
+    p.add_argument("--spmm-widths", default="128,32,16,8",
+                   help="panel widths R of --spmm-only")
     return p.parse_args()
 
 
@@ -562,7 +567,31 @@ def spmm_only(args):
     A64 = BlockSpMat(H.row_ptr, H.col_ind, H.values, 8)
     A32 = A64.astype("f32")
     out = {"n_rows": H.n_rows, "nnz_blocks": int(H.nnz_blocks)}
-    for R in (128, 32, 16, 8):
+    widths = [int(r) for r in args.spmm_widths.split(",") if r]
+    if args.spmm_kernels:
+        # A/B of the FP32 step kernels: time and max error against the FP64
+        # SpMM of the same (FP32-representable) panel.
+        for R in widths:
+            torch.manual_seed(R)
+            X = torch.randn(H.n_rows, R, dtype=torch.float32, device="cuda")
+            Y64 = torch.empty(H.n_rows, R, dtype=torch.float64, device="cuda")
+            A64.mult_dense(X.double(), Y64)
+            ref = Y64.cpu()
+            for k in args.spmm_kernels.split(","):
+                kind, _, shape = k.partition(":")
+                os.environ["RSATB_STEP_KERNEL"] = kind
+                if shape:
+                    os.environ["RSATB_TF32_SHAPE"] = shape
+                ms = time_spmm(A32, H.n_rows, R, torch.float32, reps=max(args.spmm_reps, 20))
+                Y = torch.empty(H.n_rows, R, dtype=torch.float32, device="cuda")
+                A32.mult_dense(X, Y)
+                err = float((Y.double().cpu() - ref).abs().max() / ref.abs().max())
+                out[f"f32_R{R}_{k}"] = {"ms": round(ms, 4), "rel_err_vs_fp64": err}
+                os.environ.pop("RSATB_STEP_KERNEL", None)
+                os.environ.pop("RSATB_TF32_SHAPE", None)
+        print(json.dumps(out), flush=True)
+        return
+    for R in widths:
         for name, A, dt in (("f32", A32, torch.float32), ("f64", A64, torch.float64)):
             ms = time_spmm(A, H.n_rows, R, dt, reps=args.spmm_reps)
             b = spmm_bytes(A, R, torch.empty(0, dtype=dt).element_size())
