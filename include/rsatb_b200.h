@@ -147,6 +147,11 @@ RSATB_API int rsatb_bsr_adjoint(rsatb_ctx_t ctx, rsatb_bsr_t A, rsatb_bsr_t* out
 RSATB_API int rsatb_bsr_convert(rsatb_ctx_t ctx, rsatb_bsr_t A, rsatb_dtype dtype, rsatb_bsr_t* out);
 RSATB_API int rsatb_bsr_info(rsatb_bsr_t A, int* n_block_rows, int* n_block_cols, int* block_size,
                    int64_t* nnz_blocks, int* dtype, unsigned* flags);
+/* The pattern to host memory: row_ptr (n_block_rows + 1 entries) and
+ * col_ind (nnz_blocks entries), vbcsr BlockSpMat::row_ptr() / col_ind().
+ * Synchronises. */
+RSATB_API int rsatb_bsr_pattern(rsatb_ctx_t ctx, rsatb_bsr_t A, int32_t* row_ptr,
+                                int32_t* col_ind);
 /* Device pointer to the values array (nnz_blocks*b*b elements). */
 RSATB_API void* rsatb_bsr_values(rsatb_bsr_t A);
 /* Overwrites the values from host (or device with RSATB_BSR_DEVICE_POINTERS). */
@@ -363,6 +368,22 @@ RSATB_API int rsatb_kpm_moments_vjp(rsatb_ctx_t ctx, const rsatb_cheb_op* op, co
                                     const double* dmu, int checkpoint_stride, double* mu_out,
                                     double* grad_values, rsatb_adjoint_stats* stats);
 
+/* The same VJP for the sandwich form A = (Z^T H Z - center) / half_width
+ * (real symmetric H, Z the graph-local S^-1/2 and ZH = Z^T, every matrix
+ * and psi of one precision): with G = df/dA,
+ *     grad_h = Z G Z^T / half_width   on H's pattern,
+ *     grad_z = H Z (G + G^T) / half_width   on Z's pattern
+ * (device, FP64, in the layouts of H's and Z's values; overwritten).  The
+ * gradient with respect to S follows from grad_z through each row's local
+ * inverse square root (rsatb_b200.adjoint.kpm_moments_vjp_sandwich).  No
+ * counterpart in the reference.  Synchronises the stream. */
+RSATB_API int rsatb_kpm_moments_vjp_sandwich(rsatb_ctx_t ctx, const rsatb_cheb_op* op,
+                                             const void* psi, int n_vectors,
+                                             rsatb_dtype vec_dtype, int n_moments,
+                                             const double* dmu, int checkpoint_stride,
+                                             double* mu_out, double* grad_h, double* grad_z,
+                                             rsatb_adjoint_stats* stats);
+
 /* ------------------------------------------------ FFT-Chebyshev transport */
 
 /* Counters of one rsatb_dc_spectrum_fftcheb call. */
@@ -495,6 +516,45 @@ RSATB_API int rsatb_isqrt_columns_batched(rsatb_ctx_t ctx, int n_problems, const
 RSATB_API int rsatb_isqrt_autotune(rsatb_ctx_t ctx, int precision, int n_sizes,
                                    const int32_t* sizes, int problems_per_size,
                                    int* tc_kernel_out, int32_t* nt_out, double* ms_out);
+
+/* Options of the global sparse Newton-Schulz refinement,
+ * rsatb::calc::InverseSqrtOptions (rsatb/calc/isqrtm.hpp:235-240) plus the
+ * route rule. */
+typedef struct {
+    double tol;    /* stop when max block ||(Z^H S Z - I)[i,j]||_F <= tol (1e-7) */
+    double sptol;  /* Frobenius drop threshold of every product (1e-6); 0 keeps all */
+    int maxit;     /* Newton-Schulz steps at most (20); 0 returns the seed */
+    int route;     /* 0: advance X by P X P when cheaper (every 5th step and
+                    * residuals >= 0.1 reform); 1: always reform X = Z^H S Z */
+} rsatb_ns_refine_options;
+
+/* What the refinement did, rsatb::calc::InverseSqrtReport (isqrtm.hpp:
+ * 243-258), plus the final factor's size. */
+typedef struct {
+    int steps;
+    int converged;             /* the loop residual reached tol */
+    int hit_maxiter;
+    int diverged;              /* residual above 100: the iteration left its radius */
+    int last_advance_propagated;
+    double residual;           /* loop metric: max block Frobenius of X - I */
+    double applied_residual;   /* ||(Z^H S Z - I) v|| on a unit random probe */
+    int64_t nnz_blocks;        /* blocks of the returned factor */
+    int reforms, propagations; /* how X was advanced */
+} rsatb_ns_refine_report;
+
+/* S^-1/2 refined from a seed Z (the graph-local factor) by the cubic
+ * Newton-Schulz purification of rsatb::calc::inverse_sqrt (rsatb/calc/
+ * isqrtm.hpp:262-900): X = Z^H S Z, P = 1.875 I - 1.25 X + 0.375 X^2,
+ * Z <- Z P, every product a block SpGEMM on the device whose blocks of
+ * Frobenius norm below sptol are dropped; X advanced by reformation or by
+ * P X P; stops on tol, a plateau (|norm_prev - norm| <= 0.005 norm), maxit or
+ * divergence.  S and Z_seed: F64 BSR with equal block size (at most 8)
+ * and rows.
+ * *Z_out receives a new matrix (its pattern grows with the products).
+ * report (may be NULL) as above.  Synchronises. */
+RSATB_API int rsatb_inverse_sqrt_refine(rsatb_ctx_t ctx, rsatb_bsr_t S, rsatb_bsr_t Z_seed,
+                                        const rsatb_ns_refine_options* options,
+                                        rsatb_bsr_t* Z_out, rsatb_ns_refine_report* report);
 
 /* ------------------------------------------------------------ measurement */
 

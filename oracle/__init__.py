@@ -570,6 +570,105 @@ def kubo_greenwood_ed(H: np.ndarray, V: np.ndarray, center: float, half_width: f
     return E, K
 
 
+def graph_seed_dense(S: np.ndarray, row_ptr: np.ndarray, col_ind: np.ndarray, b: int):
+    """The graph-local seed of inverse_sqrt on the host, for any pattern
+    (rsatb/calc/isqrtm.hpp:149-232 with the eigen route of
+    isqrt_action.hpp:766-795): block row i of Z is block row i of the clamped
+    inverse square root of S restricted to {i} + neighbours(i) (the columns
+    of S's row i).  S dense (N x N); returns Z dense with S's block pattern."""
+    n = row_ptr.size - 1
+    Z = np.zeros_like(S)
+    for i in range(n):
+        members = np.asarray(col_ind[row_ptr[i]:row_ptr[i + 1]])
+        idx = (members[:, None] * b + np.arange(b)[None, :]).reshape(-1)
+        slot = int(np.flatnonzero(members == i)[0])
+        X = isqrt_columns_eigen(S[np.ix_(idx, idx)], slot * b, b).T  # rows at i
+        Z[i * b:(i + 1) * b, idx] = X
+    return Z
+
+
+def max_block_residual(X: np.ndarray, b: int) -> float:
+    """max over b x b blocks of ||(X - I)[i, j]||_F (rsatb/calc/isqrtm.hpp:
+    360-405; a dense X stores every block)."""
+    n = X.shape[0] // b
+    D = (X - np.eye(X.shape[0])).reshape(n, b, n, b)
+    return float(np.sqrt((D ** 2).sum(axis=(1, 3))).max())
+
+
+def ns_refine_dense(S: np.ndarray, Z0: np.ndarray, b: int, tol: float = 1e-7,
+                    maxit: int = 20) -> tuple[np.ndarray, dict]:
+    """Dense FP64 restatement of inverse_sqrt's refinement loop
+    (rsatb/calc/isqrtm.hpp:620-800) from the seed Z0 with no drop threshold
+    and X reformed every step: X = Z^T S Z (symmetrised), stop when the max
+    block residual is <= tol, after maxit steps, on a plateau
+    (|norm_prev - norm| <= 0.005 norm) or, above 100, as diverged;
+    P = 1.875 I - 1.25 X + 0.375 X^2, Z <- Z P.  Returns (Z, report dict)."""
+    Z = Z0.copy()
+    I = np.eye(S.shape[0])
+
+    def reform(Zc):
+        X = Zc.T @ S @ Zc
+        return 0.5 * (X + X.T)
+
+    X = reform(Z)
+    norm = max_block_residual(X, b)
+    norm_pre, count, diverged = 0.0, 0, False
+    while norm > tol and count < maxit and abs(norm_pre - norm) > 0.005 * norm:
+        if norm > 100.0:
+            diverged = True
+            break
+        norm_pre = norm
+        P = 1.875 * I - 1.25 * X + 0.375 * (X @ X)
+        P = 0.5 * (P + P.T)
+        Z = Z @ P
+        X = reform(Z)
+        norm = max_block_residual(X, b)
+        count += 1
+    return Z, {"steps": count, "converged": norm <= tol, "hit_maxiter": count >= maxit,
+               "diverged": diverged, "residual": norm}
+
+
+def chain_overlap(n: int, diag: float, off: float):
+    """The 1-D chain overlaps of rsatb/calc/test/test_isqrtm.cpp (:21-39,
+    :132-151): diag on the diagonal, off on both neighbours, no periodic
+    wrap; returns (dense S, row_ptr, col_ind) with 1 x 1 blocks."""
+    S = np.diag(np.full(n, float(diag)))
+    i = np.arange(n - 1)
+    S[i, i + 1] = S[i + 1, i] = off
+    rows, cols = np.nonzero(S)
+    row_ptr = np.concatenate([[0], np.cumsum(np.bincount(rows, minlength=n))]).astype(np.int32)
+    return S, row_ptr, cols.astype(np.int32)
+
+
+def graph_seed_grad_s(S: np.ndarray, row_ptr: np.ndarray, col_ind: np.ndarray, b: int,
+                      dZ: np.ndarray) -> np.ndarray:
+    """TEST INFRASTRUCTURE (the reference has no differentiation code): the
+    gradient with respect to S of <dZ, Z(S)>, Z = graph_seed_dense(S, ...),
+    under symmetric perturbations of S: for every row i, with
+    M_i = U diag(w) U^T, E the rows of dZ at i's block placed in i's slot,
+    D_i = U (F o (U^T E U)) U^T, F_kl = (f(w_k) - f(w_l)) / (w_k - w_l) for
+    f(x) = x^-1/2 (f' on the diagonal); the symmetric parts of the D_i summed
+    into a dense N x N result (entries outside S's pattern stay 0)."""
+    n = row_ptr.size - 1
+    G = np.zeros_like(S)
+    for i in range(n):
+        members = np.asarray(col_ind[row_ptr[i]:row_ptr[i + 1]])
+        idx = (members[:, None] * b + np.arange(b)[None, :]).reshape(-1)
+        slot = int(np.flatnonzero(members == i)[0])
+        w, U = np.linalg.eigh(S[np.ix_(idx, idx)])
+        f = 1.0 / np.sqrt(w)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            F = (f[:, None] - f[None, :]) / (w[:, None] - w[None, :])
+        close = np.abs(w[:, None] - w[None, :]) <= 1e-12 * np.abs(w).max()
+        fp = -0.5 * w ** -1.5
+        F = np.where(close, 0.5 * (fp[:, None] + fp[None, :]), F)
+        E = np.zeros((idx.size, idx.size))
+        E[slot * b:(slot + 1) * b, :] = dZ[i * b:(i + 1) * b, idx]
+        D = U @ (F * (U.T @ E @ U)) @ U.T
+        G[np.ix_(idx, idx)] += 0.5 * (D + D.T)
+    return G
+
+
 def ns_inverse_sqrt_dense(S: np.ndarray, tol: float = 1e-11, maxit: int = 60):
     """Dense FP64 restatement of rsatb::calc::inverse_sqrt's Newton-Schulz
     loop (rsatb/calc/isqrtm.hpp:613-700 and the residual of :370-405 on a

@@ -70,6 +70,18 @@ class AdjointStats(C.Structure):
                 ("panels_held", C.c_int)]
 
 
+class NsRefineOptions(C.Structure):
+    _fields_ = [("tol", C.c_double), ("sptol", C.c_double), ("maxit", C.c_int),
+                ("route", C.c_int)]
+
+
+class NsRefineReport(C.Structure):
+    _fields_ = [("steps", C.c_int), ("converged", C.c_int), ("hit_maxiter", C.c_int),
+                ("diverged", C.c_int), ("last_advance_propagated", C.c_int),
+                ("residual", C.c_double), ("applied_residual", C.c_double),
+                ("nnz_blocks", C.c_int64), ("reforms", C.c_int), ("propagations", C.c_int)]
+
+
 # rsatb_ns_precision
 NS_FP64, NS_TF32X3, NS_TF32 = 0, 1, 2
 
@@ -99,6 +111,7 @@ SIGNATURES = {
     "rsatb_bsr_info": (_i, [_vp, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i),
                             C.POINTER(_i64), C.POINTER(_i), C.POINTER(_u)]),
     "rsatb_bsr_values": (_vp, [_vp]),
+    "rsatb_bsr_pattern": (_i, [_vp, _vp, _vp, _vp]),
     "rsatb_bsr_set_values": (_i, [_vp, _vp, _vp, _u]),
     "rsatb_bsr_mult_dense": (_i, [_vp, _vp, _vp, _vp, _i, _i, _d]),
     "rsatb_cheb_apply_op": (_i, [_vp, C.POINTER(ChebOp), _vp, _vp, _i, _i]),
@@ -116,6 +129,8 @@ SIGNATURES = {
     "rsatb_cg_solve": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _d, _i, C.POINTER(_i), _PD]),
     "rsatb_kpm_moments_vjp": (_i, [_vp, C.POINTER(ChebOp), _vp, _i, _i, _i, _PD, _i, _PD, _vp,
                                    C.POINTER(AdjointStats)]),
+    "rsatb_kpm_moments_vjp_sandwich": (_i, [_vp, C.POINTER(ChebOp), _vp, _i, _i, _i, _PD, _i,
+                                            _PD, _vp, _vp, C.POINTER(AdjointStats)]),
     "rsatb_dc_spectrum_fftcheb": (_i, [_vp, C.POINTER(ChebOp), _vp, _vp, _vp, _vp, _i, _i, _i,
                                        _i, _d, _i, _sz, _i, _PD, _PD,
                                        C.POINTER(FftchebStats)]),
@@ -123,6 +138,8 @@ SIGNATURES = {
                                          C.POINTER(IsqrtOptions), _vp, C.POINTER(IsqrtStats)]),
     "rsatb_measure_fma_peak": (_i, [_vp, _i, _PD]),
     "rsatb_isqrt_autotune": (_i, [_vp, _i, _i, _vp, _i, _vp, _vp, _vp]),
+    "rsatb_inverse_sqrt_refine": (_i, [_vp, _vp, _vp, C.POINTER(NsRefineOptions),
+                                       C.POINTER(_vp), C.POINTER(NsRefineReport)]),
 }
 
 

@@ -52,6 +52,8 @@ int grid_for(const rsatb_context* ctx, int64_t n, int threads) {
     return int(g);
 }
 
+}  // namespace
+
 void free_matrix(rsatb_bsr_matrix* A) {
     if (!A) return;
     cudaSetDevice(A->device);
@@ -85,7 +87,6 @@ int alloc_matrix(int device, int nbr, int nbc, int b, int64_t nnzb, int dtype, u
     return RSATB_SUCCESS;
 }
 
-}  // namespace
 }  // namespace rsatb_b200
 
 using namespace rsatb_b200;
@@ -192,6 +193,22 @@ int rsatb_bsr_set_values(rsatb_ctx_t ctx, rsatb_bsr_t A, const void* values, uns
         dtype_size(A->dtype) * size_t(A->nnz_blocks) * A->block_size * A->block_size;
     if (vbytes)
         RSATB_CUDA_TRY(cudaMemcpyAsync(A->values, values, vbytes, cudaMemcpyDefault, ctx->stream));
+    return RSATB_SUCCESS;
+}
+
+int rsatb_bsr_pattern(rsatb_ctx_t ctx, rsatb_bsr_t A, int32_t* row_ptr, int32_t* col_ind) {
+    clear_error();
+    RSATB_TRY(check_ctx(ctx));
+    RSATB_TRY(check_bsr(A, "bsr_pattern"));
+    if (!row_ptr || (A->nnz_blocks && !col_ind))
+        return set_error(RSATB_INVALID_ARGUMENT, "null output array");
+    RSATB_CUDA_TRY(cudaMemcpyAsync(row_ptr, A->row_ptr,
+                                   sizeof(int32_t) * (size_t(A->n_block_rows) + 1),
+                                   cudaMemcpyDeviceToHost, ctx->stream));
+    if (A->nnz_blocks)
+        RSATB_CUDA_TRY(cudaMemcpyAsync(col_ind, A->col_ind, sizeof(int32_t) * size_t(A->nnz_blocks),
+                                       cudaMemcpyDeviceToHost, ctx->stream));
+    RSATB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     return RSATB_SUCCESS;
 }
 

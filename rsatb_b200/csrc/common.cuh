@@ -120,4 +120,10 @@ int ctx_check_fault(rsatb_context* ctx);
 int check_ctx(rsatb_context* ctx);
 int check_bsr(const rsatb_bsr_matrix* A, const char* name);
 
+// A matrix shell with device arrays for nnzb blocks (row_ptr, col_ind and
+// values left unset), and its release.
+int alloc_matrix(int device, int nbr, int nbc, int b, int64_t nnzb, int dtype, unsigned flags,
+                 rsatb_bsr_matrix** out);
+void free_matrix(rsatb_bsr_matrix* A);
+
 }  // namespace rsatb_b200

@@ -1,4 +1,4 @@
-"""Graph-local inverse square root S^-1/2 (the seed of rsatb's inverse_sqrt).
+"""Inverse square root S^-1/2 of a sparse overlap: rsatb's inverse_sqrt.
 
 ``graph_inverse_sqrt`` follows rsatb::calc::graph_inverse_sqrt
 (rsatb/calc/isqrtm.hpp:149-232): for every block row i, the dense overlap
@@ -15,10 +15,15 @@ pattern).  The per-problem action is selected by ``method``:
   by FP64 iterations.
 
 The problems are gathered and solved on the GPU in chunks.
+
+``inverse_sqrt`` is rsatb::calc::inverse_sqrt (rsatb/calc/isqrtm.hpp:262):
+that seed refined by the global sparse Newton-Schulz purification, every
+product a block SpGEMM on the device (``rsatb_inverse_sqrt_refine``).
 """
 from __future__ import annotations
 
 import ctypes as C
+import dataclasses
 
 import numpy as np
 import torch
@@ -220,6 +225,88 @@ def graph_inverse_sqrt(S: BsrArrays, method: str = "eigen", device="cuda",
     # land in S's pattern order.
     zvals = out.reshape(n * k, b, b).cpu().numpy()
     return BsrArrays(S.row_ptr, S.col_ind, zvals, b)
+
+
+def _seed_ragged(S: BsrArrays, device="cuda") -> BsrArrays:
+    """graph_inverse_sqrt for patterns whose rows have different neighbour
+    counts (chains with ends, unstructured graphs): the rows are grouped by
+    neighbour count and each group takes the clamped eigen route."""
+    n, b = S.n_block_rows, S.block_size
+    rp = np.asarray(S.row_ptr, dtype=np.int64)
+    ci = np.asarray(S.col_ind, dtype=np.int64)
+    deg = np.diff(rp)
+    key = np.repeat(np.arange(n), deg) * n + ci
+    vals = torch.as_tensor(np.ascontiguousarray(S.values), dtype=torch.float64, device=device)
+    zvals = np.zeros((ci.size, b, b))
+    for k in np.unique(deg):
+        rows = np.flatnonzero(deg == k)
+        members = ci[rp[rows][:, None] + np.arange(k)[None, :]]
+        slot = np.argmax(members == rows[:, None], axis=1)
+        q = members[:, :, None] * n + members[:, None, :]
+        pos = np.minimum(np.searchsorted(key, q), key.size - 1)
+        gather = torch.as_tensor(np.where(key[pos] == q, pos, -1), device=device)
+        M = _gather_dense(vals, gather, b)
+        X = clamped_inverse_sqrt_rows(M, torch.as_tensor(slot, device=device), b)
+        blocks = X.reshape(rows.size, b, int(k), b).permute(0, 2, 1, 3).cpu().numpy()
+        for r, i in enumerate(rows):
+            zvals[rp[i]:rp[i] + k] = blocks[r]
+    return BsrArrays(S.row_ptr, S.col_ind, zvals, b)
+
+
+@dataclasses.dataclass
+class InverseSqrtOptions:
+    """rsatb::calc::InverseSqrtOptions (rsatb/calc/isqrtm.hpp:235-240), and
+    the route rule of the X update (0: propagate P X P when its first product
+    is smaller, every fifth step and residuals >= 0.1 reform; 1: always
+    reform)."""
+    tol: float = 1e-7
+    sptol: float = 1e-6
+    maxit: int = 20
+    route: int = 0
+
+
+@dataclasses.dataclass
+class InverseSqrtReport:
+    """rsatb::calc::InverseSqrtReport (rsatb/calc/isqrtm.hpp:243-258)."""
+    steps: int
+    converged: bool
+    hit_maxiter: bool
+    diverged: bool
+    last_advance_propagated: bool
+    residual: float
+    applied_residual: float
+    nnz_blocks: int
+    reforms: int
+    propagations: int
+
+
+def inverse_sqrt(S, options: InverseSqrtOptions | None = None, seed=None):
+    """S^-1/2 of the FP64 BSR overlap S (BsrArrays): the graph-local seed
+    (``graph_inverse_sqrt``, or ``seed`` if given) refined on the device by
+    the sparse Newton-Schulz purification of inverse_sqrt
+    (rsatb/calc/isqrtm.hpp:262-900).  Returns (Z as a device BlockSpMat, its
+    pattern grown by the products; InverseSqrtReport)."""
+    from .vbcsr import BlockSpMat
+    opt = options or InverseSqrtOptions()
+    if seed is None:
+        deg = np.diff(np.asarray(S.row_ptr))
+        seed = graph_inverse_sqrt(S) if np.all(deg == deg[0]) else _seed_ragged(S)
+    Sd = BlockSpMat(S.row_ptr, S.col_ind, S.values, S.block_size, dtype=np.float64)
+    Zd = BlockSpMat(seed.row_ptr, seed.col_ind, seed.values, seed.block_size, dtype=np.float64)
+    copt = _capi.NsRefineOptions(float(opt.tol), float(opt.sptol), int(opt.maxit),
+                                 int(opt.route))
+    rep = _capi.NsRefineReport()
+    h = C.c_void_p()
+    ctx = Sd.ctx
+    ctx.bind_stream()
+    check(lib().rsatb_inverse_sqrt_refine(ctx.handle, Sd.handle, Zd.handle, C.byref(copt),
+                                          C.byref(h), C.byref(rep)))
+    Z = BlockSpMat(None, None, None, 0, device=ctx.device, _handle=h)
+    report = InverseSqrtReport(rep.steps, bool(rep.converged), bool(rep.hit_maxiter),
+                               bool(rep.diverged), bool(rep.last_advance_propagated),
+                               rep.residual, rep.applied_residual, rep.nnz_blocks, rep.reforms,
+                               rep.propagations)
+    return Z, report
 
 
 def graph_inverse_sqrt_host(S: BsrArrays) -> BsrArrays:

@@ -172,6 +172,17 @@ class BlockSpMat:
                                          C.c_void_p(src), nbytes))
         return out.view(self.nnz_blocks, self.block_size, self.block_size)
 
+    def to_arrays(self):
+        """The matrix on the host as lattice.BsrArrays (row_ptr, col_ind and
+        values (nnz_blocks, b, b) copied from the device)."""
+        from .lattice import BsrArrays
+        rp = np.zeros(self.n_block_rows + 1, dtype=np.int32)
+        ci = np.zeros(max(self.nnz_blocks, 1), dtype=np.int32)
+        check(lib().rsatb_bsr_pattern(self.ctx.handle, self.handle, rp.ctypes.data,
+                                      ci.ctypes.data))
+        vals = self.values_tensor().cpu().numpy()
+        return BsrArrays(rp, ci[:self.nnz_blocks], vals, self.block_size, self.n_block_cols)
+
     def set_values(self, values: torch.Tensor) -> None:
         """Overwrites the block values from a device tensor of matching size."""
         v = values.contiguous()

@@ -374,3 +374,25 @@ def test_kpm_moments_ed_equals_the_recurrence():
     for doubled in (True, False):
         got = oracle.kpm_moments(op, psi, 64, doubled=doubled)
         assert np.abs(got - want).max() <= 1e-11 * np.abs(want[0])
+
+
+# ------------------------------------------- sparse Newton-Schulz refinement
+
+def test_ns_refine_dense_keeps_test_isqrtm_chain_semantics():
+    """The dense restatement of inverse_sqrt's loop from the graph-local seed
+    on test_isqrtm.cpp's 24-site chains: off-diagonal 0.6 (indefinite) is
+    reported DIVERGED, 0.49 converges to tol 1e-10, and one step towards an
+    unreachable tol is capped (neither converged nor diverged)."""
+    def run(off, maxit, tol):
+        S, rp, ci = oracle.chain_overlap(24, 1.0, off)
+        Z0 = oracle.graph_seed_dense(S, rp, ci, 1)
+        return oracle.ns_refine_dense(S, Z0, 1, tol=tol, maxit=maxit)
+
+    _, r = run(0.60, 20, 1e-10)
+    assert not r["converged"] and r["diverged"]
+    Z, r = run(0.49, 20, 1e-10)
+    assert r["converged"] and not r["diverged"]
+    S, _, _ = oracle.chain_overlap(24, 1.0, 0.49)
+    assert np.abs(Z.T @ S @ Z - np.eye(24)).max() < 1e-9
+    _, r = run(0.49, 1, 1e-16)
+    assert not r["converged"] and not r["diverged"] and r["hit_maxiter"]
