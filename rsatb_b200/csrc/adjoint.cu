@@ -12,6 +12,14 @@
 // so df/dH_ij = (df/dA)_ij / hw on the stored pattern: a sampled dense-dense
 // product (SDDMM) of the lambda and t panels.
 //
+// Sandwich form, A = (Z^T H Z - c) / hw (real H symmetric): with
+// G = df/dA = sum_n w_n lambda_{n+1} t_n^T as above,
+//     df/dH = Z G Z^T / hw                     (SDDMM of Z lambda and Z t),
+//     df/dZ = H Z (G + G^T) / hw               (SDDMMs of H Z lambda with t
+//                                               and of H Z t with lambda),
+// each on the stored pattern of its matrix; the four Z / H Z images of a
+// segment's panels are formed by plain SpMMs before its SDDMMs.
+//
 // Memory: t_n is recomputed in segments of C moments from checkpoints
 // (t_{kC}, t_{kC-1}) kept by the forward pass (C ~ sqrt(N)), so the
 // backward pass holds O(sqrt(N)) panels, not N.  Each backward step is one
@@ -125,9 +133,10 @@ StepArgs zero_args(int W) {
 
 template <typename VT>
 int vjp_impl(rsatb_context* ctx, const rsatb_cheb_op* op, const VT* psi, int R, int vdt, int M,
-             const double* dmu, int C, double* mu_out, double* grad,
+             const double* dmu, int C, double* mu_out, double* grad, double* grad_z,
              rsatb_adjoint_stats* stats) {
     const rsatb_bsr_matrix* H = op->H;
+    const bool sandwich = op->form == RSATB_FORM_SANDWICH;
     const int b = H->block_size;
     const int64_t N = int64_t(H->n_block_rows) * b;
     const int W = R;
@@ -145,7 +154,10 @@ int vjp_impl(rsatb_context* ctx, const rsatb_cheb_op* op, const VT* psi, int R, 
     const size_t max_ctas = size_t(ctx->sm_count) * 8;
     const size_t dots_b = (size_t(M) * W * sizeof(double) + 255) & ~size_t(255);
     const size_t part_b = (max_ctas * 2 * W * sizeof(double) + 255) & ~size_t(255);
-    const size_t n_pan = 2 * size_t(n_seg) + 2 * size_t(C) + 3 + 1 + 3;
+    // sandwich: two step intermediates and the Z t, Z lambda, H Z t, H Z
+    // lambda images of a segment
+    const size_t n_extra = sandwich ? 2 + 4 * size_t(C) : 0;
+    const size_t n_pan = 2 * size_t(n_seg) + 2 * size_t(C) + 3 + 1 + 3 + n_extra;
     void* sp = nullptr;
     RSATB_TRY(ctx_scratch(ctx, n_pan * pal + dots_b + part_b, &sp));
     char* base = static_cast<char*>(sp);
@@ -157,10 +169,20 @@ int vjp_impl(rsatb_context* ctx, const rsatb_cheb_op* op, const VT* psi, int R, 
     VT* lam = reinterpret_cast<VT*>(base + (2 * size_t(n_seg) + 2 * C) * pal);
     VT* zero = reinterpret_cast<VT*>(base + (2 * size_t(n_seg) + 2 * C + 3) * pal);
     VT* f = reinterpret_cast<VT*>(base + (2 * size_t(n_seg) + 2 * C + 4) * pal);
+    VT* su = sandwich ? reinterpret_cast<VT*>(base + (2 * size_t(n_seg) + 2 * C + 7) * pal)
+                      : nullptr;
+    VT* sw = sandwich ? su + pal / sizeof(VT) : nullptr;
+    VT* zt = sandwich ? sw + pal / sizeof(VT) : nullptr;       // C panels each
+    VT* zl = sandwich ? zt + size_t(C) * (pal / sizeof(VT)) : nullptr;
+    VT* hzt = sandwich ? zl + size_t(C) * (pal / sizeof(VT)) : nullptr;
+    VT* hzl = sandwich ? hzt + size_t(C) * (pal / sizeof(VT)) : nullptr;
     double* dots = reinterpret_cast<double*>(base + n_pan * pal);
     double* partials = reinterpret_cast<double*>(base + n_pan * pal + dots_b);
     RSATB_CUDA_TRY(cudaMemsetAsync(zero, 0, pbytes, st));
     RSATB_CUDA_TRY(cudaMemsetAsync(grad, 0, size_t(H->nnz_blocks) * b * b * sizeof(double), st));
+    if (sandwich)
+        RSATB_CUDA_TRY(cudaMemsetAsync(grad_z, 0,
+                                       size_t(op->Z->nnz_blocks) * b * b * sizeof(double), st));
 
     const double inv_hw = 1.0 / op->half_width;
     auto step = [&](const VT* in, const VT* prev, VT* out, double s2, double g_p, const VT* q,
@@ -183,7 +205,22 @@ int vjp_impl(rsatb_context* ctx, const rsatb_cheb_op* op, const VT* psi, int R, 
             a.dots_out = dot_slot;
             a.counter = counter;
         }
-        return run_step(ctx, H, vdt, a);
+        if (!sandwich) return run_step(ctx, H, vdt, a);
+        StepArgs m = zero_args(W);  // su = Z in, sw = H su, then Z^T sw with the epilogue
+        m.in = in;
+        m.y = su;
+        RSATB_TRY(run_step(ctx, op->Z, vdt, m));
+        m.in = su;
+        m.y = sw;
+        RSATB_TRY(run_step(ctx, H, vdt, m));
+        a.in = sw;
+        return run_step(ctx, op->ZH, vdt, a);
+    };
+    auto mult = [&](const rsatb_bsr_matrix* A, const VT* in, VT* out) -> int {
+        StepArgs m = zero_args(W);
+        m.in = in;
+        m.y = out;
+        return run_step(ctx, A, vdt, m);
     };
     const size_t ps = pal / sizeof(VT);  // panel stride in elements
     auto ckpt = [&](int k, int which) { return ck + (2 * size_t(k) + which) * ps; };
@@ -268,8 +305,23 @@ int vjp_impl(rsatb_context* ctx, const rsatb_cheb_op* op, const VT* psi, int R, 
                 l1 = out;
             }
         }
-        RSATB_TRY(launch_sddmm<VT>(ctx, H, R, nb0, nb1 - nb0, M - 2, inv_hw, lseg, tseg, int64_t(ps),
-                                   grad));
+        if (!sandwich) {
+            RSATB_TRY(launch_sddmm<VT>(ctx, H, R, nb0, nb1 - nb0, M - 2, inv_hw, lseg, tseg,
+                                       int64_t(ps), grad));
+        } else {
+            for (int q = 0; q < nb1 - nb0; ++q) {
+                RSATB_TRY(mult(op->Z, tseg + size_t(q) * ps, zt + size_t(q) * ps));
+                RSATB_TRY(mult(op->Z, lseg + size_t(q) * ps, zl + size_t(q) * ps));
+                RSATB_TRY(mult(H, zt + size_t(q) * ps, hzt + size_t(q) * ps));
+                RSATB_TRY(mult(H, zl + size_t(q) * ps, hzl + size_t(q) * ps));
+            }
+            RSATB_TRY(launch_sddmm<VT>(ctx, H, R, nb0, nb1 - nb0, M - 2, inv_hw, zl, zt,
+                                       int64_t(ps), grad));
+            RSATB_TRY(launch_sddmm<VT>(ctx, op->Z, R, nb0, nb1 - nb0, M - 2, inv_hw, hzl, tseg,
+                                       int64_t(ps), grad_z));
+            RSATB_TRY(launch_sddmm<VT>(ctx, op->Z, R, nb0, nb1 - nb0, M - 2, inv_hw, hzt, lseg,
+                                       int64_t(ps), grad_z));
+        }
     }
     RSATB_CUDA_TRY(cudaEventRecord(e2, st));
 
@@ -292,7 +344,7 @@ int vjp_impl(rsatb_context* ctx, const rsatb_cheb_op* op, const VT* psi, int R, 
         stats->segments = n_seg;
         stats->forward_ms = a;
         stats->backward_ms = c;
-        stats->panels_held = 2 * n_seg + 2 * C + 7;
+        stats->panels_held = int(n_pan);
     }
     return RSATB_SUCCESS;
 }
@@ -302,17 +354,25 @@ int vjp_impl(rsatb_context* ctx, const rsatb_cheb_op* op, const VT* psi, int R, 
 
 using namespace rsatb_b200;
 
-extern "C" int rsatb_kpm_moments_vjp(rsatb_ctx_t ctx, const rsatb_cheb_op* op, const void* psi,
-                                     int n_vectors, rsatb_dtype vec_dtype, int n_moments,
-                                     const double* dmu, int checkpoint_stride, double* mu_out,
-                                     double* grad_values, rsatb_adjoint_stats* stats) {
-    clear_error();
+namespace {
+
+int vjp_entry(rsatb_ctx_t ctx, const rsatb_cheb_op* op, const void* psi, int n_vectors,
+              rsatb_dtype vec_dtype, int n_moments, const double* dmu, int checkpoint_stride,
+              double* mu_out, double* grad_values, double* grad_z, rsatb_adjoint_stats* stats) {
     RSATB_TRY(check_ctx(ctx));
     if (!op || !psi || !dmu || !grad_values)
         return set_error(RSATB_INVALID_ARGUMENT, "null argument");
-    if (op->form != RSATB_FORM_ORTHOGONAL)
-        return set_error(RSATB_NOT_SUPPORTED, "the adjoint runs for the Orthogonal form only");
     RSATB_TRY(check_bsr(op->H, "H"));
+    if (op->form == RSATB_FORM_SANDWICH) {
+        RSATB_TRY(check_bsr(op->Z, "Z"));
+        RSATB_TRY(check_bsr(op->ZH, "ZH"));
+        if (!grad_z)
+            return set_error(RSATB_INVALID_ARGUMENT, "the sandwich adjoint needs grad_z");
+        if (op->Z->dtype != op->H->dtype || op->ZH->dtype != op->H->dtype ||
+            op->Z->block_size != op->H->block_size ||
+            op->Z->n_block_rows != op->H->n_block_rows || (op->Z->flags | op->ZH->flags))
+            return set_error(RSATB_INVALID_ARGUMENT, "Z, Z^H and H differ in shape or type");
+    }
     const rsatb_bsr_matrix* H = op->H;
     if (H->n_block_rows != H->n_block_cols)
         return set_error(RSATB_INVALID_ARGUMENT, "H must be square");
@@ -332,7 +392,36 @@ extern "C" int rsatb_kpm_moments_vjp(rsatb_ctx_t ctx, const rsatb_cheb_op* op, c
     if (dtype_is_double(vec_dtype))
         return vjp_impl<double>(ctx, op, static_cast<const double*>(psi), n_vectors,
                                 int(vec_dtype), n_moments, dmu, checkpoint_stride, mu_out,
-                                grad_values, stats);
+                                grad_values, grad_z, stats);
     return vjp_impl<float>(ctx, op, static_cast<const float*>(psi), n_vectors, int(vec_dtype),
-                           n_moments, dmu, checkpoint_stride, mu_out, grad_values, stats);
+                           n_moments, dmu, checkpoint_stride, mu_out, grad_values, grad_z,
+                           stats);
+}
+
+}  // namespace
+
+extern "C" int rsatb_kpm_moments_vjp(rsatb_ctx_t ctx, const rsatb_cheb_op* op, const void* psi,
+                                     int n_vectors, rsatb_dtype vec_dtype, int n_moments,
+                                     const double* dmu, int checkpoint_stride, double* mu_out,
+                                     double* grad_values, rsatb_adjoint_stats* stats) {
+    clear_error();
+    if (ctx && op && op->form != RSATB_FORM_ORTHOGONAL)
+        return set_error(RSATB_NOT_SUPPORTED,
+                         "rsatb_kpm_moments_vjp runs the Orthogonal form; the sandwich form "
+                         "is rsatb_kpm_moments_vjp_sandwich");
+    return vjp_entry(ctx, op, psi, n_vectors, vec_dtype, n_moments, dmu, checkpoint_stride,
+                     mu_out, grad_values, nullptr, stats);
+}
+
+extern "C" int rsatb_kpm_moments_vjp_sandwich(rsatb_ctx_t ctx, const rsatb_cheb_op* op,
+                                              const void* psi, int n_vectors,
+                                              rsatb_dtype vec_dtype, int n_moments,
+                                              const double* dmu, int checkpoint_stride,
+                                              double* mu_out, double* grad_h, double* grad_z,
+                                              rsatb_adjoint_stats* stats) {
+    clear_error();
+    if (ctx && op && op->form != RSATB_FORM_SANDWICH)
+        return set_error(RSATB_INVALID_ARGUMENT, "the operator is not in the sandwich form");
+    return vjp_entry(ctx, op, psi, n_vectors, vec_dtype, n_moments, dmu, checkpoint_stride,
+                     mu_out, grad_h, grad_z, stats);
 }
