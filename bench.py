@@ -305,15 +305,18 @@ def roofline(wl, hbm_peak, peak_note, fma_peaks):
     flops = spmm_flops(Z32, wl.R, wl.complex_vectors)
     gbs = nbytes / (ms * 1e-3) / 1e9
     tfs = flops / (ms * 1e-3) / 1e12
-    # DRAM bytes of one launch of this kernel at this shape (diamond 16^3,
-    # 8x8 blocks, R = 128, FP32) from an ncu capture
-    # (profiles/cheb_step_f32_traffic_diamond_L16.md): read + write.
+    # DRAM bytes (read + write) of one launch of this kernel at this shape
+    # (diamond 16^3, 8x8 blocks, R = 128, FP32), from an ncu capture of that
+    # launch; a profiler counter, so not measured inside this run.
     traffic = None
     if wl.n_rows == 262144 and wl.R == 128 and wl.H.block_size == 8 and not wl.complex_vectors:
         traffic = 403398400 + 118504192
     peak32 = max(fma_peaks["f32"], fma_peaks["f32x2"])
     out = {"bound": "hbm", "achieved": round(gbs, 1), "peak": hbm_peak, "unit": "GB/s",
            "frac": round(gbs / hbm_peak, 4), "traffic": traffic,
+           "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch "
+                             "at this shape (a separate profiled run, not this one)"
+                             if traffic else None,
            "kernel": "fused BSR Chebyshev step, Y = A X, FP32, R=%d, %dx%d blocks" % (
                wl.R, wl.H.block_size, wl.H.block_size),
            "algorithmic_bytes_per_launch": nbytes, "ms_per_launch": round(ms, 4),

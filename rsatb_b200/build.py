@@ -80,7 +80,7 @@ def build(verbose: bool = False, force: bool = False, jobs: int | None = None) -
     if force or todo or not LIB_PATH.exists() or LIB_PATH.stat().st_mtime < newest:
         libdir = cuda_lib_dir()
         cmd = [nvcc_path(), *ARCH, "-shared", "-o", str(LIB_PATH), *map(str, objs),
-               "-L", str(libdir), "-lcufft", "-lcublas",
+               "-L", str(libdir), "-lcufft",
                "-Xlinker", f"-rpath,{libdir}"]
         proc = subprocess.run(cmd, capture_output=True, text=True)
         if proc.returncode != 0:

@@ -33,10 +33,12 @@ from .vbcsr import BlockSpMat, set_random
 class PreconditionerOptions:
     """rsatb::model::PreconditionerOptions (rsatb/model/setup.hpp:33-51):
     operator_form 'solve' (S^-1 H, a CG with S per application) or
-    'sandwich' (Z^H H Z).  tol, sptol and maxiter configure the reference's
-    construction of Z, which happens outside this package (Z is passed in);
-    cg_tol and cg_max_iter are the Solve form's CG settings (LinearSolver's
-    1e-8 and 1000)."""
+    'sandwich' (Z^H H Z).  tol, sptol and maxiter configure the construction
+    of Z from S when the sandwich form is given S rather than Z, as the
+    reference's build_preconditioner does (rsatb/model/operator_set.hpp:369):
+    the graph-local seed, then maxiter Newton-Schulz steps on the device
+    (isqrt.inverse_sqrt); cg_tol and cg_max_iter are the Solve form's CG
+    settings (LinearSolver's 1e-8 and 1000)."""
     operator_form: str = "solve"
     tol: float = 1e-7
     sptol: float = 1e-5
@@ -47,10 +49,13 @@ class PreconditionerOptions:
 
 @dataclass
 class SetupOptions:
-    """rsatb::model::SetupOptions (pybind_rsatb.cpp:263-341): sampling and
-    spectral bounds.  Only the Gamma point is served (real operators);
-    ``precision`` ('f64' or 'mixed': FP32 vectors and operators, FP64 dots)
-    is this package's addition."""
+    """rsatb::model::SetupOptions (pybind_rsatb.cpp:263-341): k-points,
+    sampling and spectral bounds.  k-points other than Gamma need the
+    operator as real-space images (bloch.ImageOperator), from which H(k) is
+    summed on the device; bounds_zero_tol and bounds_max_matvecs drive the
+    Lanczos window estimate as BoundsOptions does.  ``precision`` ('f64' or
+    'mixed': FP32 vectors and operators, FP64 dots) is this package's
+    addition."""
     kpoints: list = field(default_factory=lambda: [[0.0, 0.0, 0.0]])
     nsamples: int = 1
     sample_seed: int = 20240917
@@ -118,6 +123,7 @@ class RSATB:
                 raise NotImplementedError("the sandwich form takes one matrix, not images")
             self.H = self.images.at_k(self.kpoints[0])
         self.Z = _as_device(Z) if Z is not None else None
+        self.factor_report = None  # InverseSqrtReport when Z is built from S
         self.S = _as_device(S) if S is not None else None
         form = self.options.preconditioner.operator_form.strip().lower()
         if form not in ("solve", "sandwich"):
@@ -126,8 +132,12 @@ class RSATB:
         # which of S and Z the operator uses (ParseOperatorForm, setup.hpp:54).
         # 'solve' takes S (and Z, if given, preconditions its CG, the
         # reference's default route); 'sandwich' takes Z alone.
-        if self.S is not None and form != "solve":
-            raise ValueError("S was given but operator_form is 'sandwich' (pass Z alone)")
+        if self.S is not None and form == "sandwich":
+            # build_preconditioner: Z from S (seed + maxiter refinement steps);
+            # the sandwich never references S itself.
+            if self.Z is None:
+                self.Z, self.factor_report = self._factor_from_overlap(S)
+            self.S = None
         if self.Z is not None and self.S is None and form != "sandwich":
             raise ValueError("operator_form 'solve' needs S (Z alone gives the sandwich form)")
         if self.S is not None and self.images is not None:
@@ -152,6 +162,13 @@ class RSATB:
             self._bounds = self._estimate_bounds()
 
     # -- operators --------------------------------------------------------
+
+    def _factor_from_overlap(self, S):
+        from .isqrt import InverseSqrtOptions, inverse_sqrt
+        po = self.options.preconditioner
+        arrays = S.to_arrays() if isinstance(S, BlockSpMat) else S
+        return inverse_sqrt(arrays, InverseSqrtOptions(tol=po.tol, sptol=po.sptol,
+                                                       maxit=po.maxiter))
 
     def _operator(self, kidx: int) -> BlockSpMat:
         if self.images is None or kidx == 0:
@@ -197,7 +214,10 @@ class RSATB:
         keeps one window for all of them, OperatorSet::emin/emax)."""
         lo, hi = np.inf, -np.inf
         for kidx in self._local_kidx():
-            a, b = estimate_spectral_bounds(self._cheby(-1.0, 1.0, False, kidx))
+            opt = self.options
+            a, b = estimate_spectral_bounds(self._cheby(-1.0, 1.0, False, kidx), tol=1e-3,
+                                            zero_tol=opt.bounds_zero_tol,
+                                            max_matvecs=opt.bounds_max_matvecs)
             lo, hi = min(lo, a), max(hi, b)
         if self._dist()[1] > 1:
             import torch.distributed as dist

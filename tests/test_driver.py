@@ -280,10 +280,79 @@ def test_compute_dos_solve_form():
     want = 2.0 * oracle.density(mu, x, 0.5 / nt)
     assert rel_err(dos, want) < 1e-8
     with pytest.raises(ValueError):
-        RSATB(H, SetupOptions(preconditioner=PreconditionerOptions(operator_form="sandwich")),
-              S=S)
-    with pytest.raises(ValueError):
         PreconditionerOptions(operator_form="cg") and RSATB(
             H, SetupOptions(preconditioner=PreconditionerOptions(operator_form="cg"),
                             energy_bounds=(emin, emax)))
 
+
+
+@pytest.mark.gpu
+def test_sandwich_factor_built_from_overlap():
+    """operator_form='sandwich' given S (and no Z) builds Z as the
+    reference's build_preconditioner does: the graph-local seed, then
+    maxiter Newton-Schulz steps on the device.  maxiter = 0 is the seed: the
+    DOS equals the one with the seed passed in as Z.  With maxiter > 0 the
+    refined factor's congruence Z^T S Z is closer to the identity."""
+    import torch
+    from rsatb_b200 import lattice
+    from rsatb_b200.driver import PreconditionerOptions, RSATB, SetupOptions
+    from rsatb_b200.isqrt import graph_inverse_sqrt
+    torch.cuda.set_device(0)
+    H, S = lattice.diamond_lcao(L=2, seed=3)
+    Sd = S.to_dense()
+
+    def opts(maxiter):
+        return SetupOptions(nsamples=2, sample_seed=4, energy_bounds=(-12.0, 12.0),
+                            preconditioner=PreconditionerOptions(operator_form="sandwich",
+                                                                 maxiter=maxiter, tol=1e-9,
+                                                                 sptol=1e-9))
+
+    seeded = RSATB(H, opts(0), S=S)
+    assert seeded.factor_report.steps == 0 and seeded.S is None
+    given = RSATB(H, opts(0), Z=graph_inverse_sqrt(S))
+    d0, _ = seeded.compute_dos(0.8)
+    d1, _ = given.compute_dos(0.8)
+    assert rel_err(d0, d1) < 1e-12
+    refined = RSATB(H, opts(3), S=S)
+    assert 1 <= refined.factor_report.steps <= 3
+
+    def congruence(Zm):
+        Zd = Zm.to_arrays().to_dense()
+        return np.abs(Zd.T @ Sd @ Zd - np.eye(Sd.shape[0])).max()
+
+    assert congruence(refined.Z) < 0.1 * congruence(seeded.Z)
+
+
+@pytest.mark.gpu
+def test_converging_bounds_follow_the_reference_contract():
+    """estimate_spectral_bounds with tol (the facade's mode): Lanczos until
+    both extreme Ritz pairs reach residual 1e-3 of the spectral scale, the
+    0.5 eV padding outside; a zero operator gives (-0.5, 0.5); a solve that
+    cannot converge within max_matvecs falls back to +-||H||_F (orthogonal)
+    or raises (sandwich), as ExtremalEigenvalues does
+    (rsatb/setup/spectral_bounds.hpp:311-400)."""
+    import torch
+    from rsatb_b200 import lattice
+    from rsatb_b200.bounds import estimate_spectral_bounds
+    from rsatb_b200.calc import Chebyshev, ISQRTMPreconditioner
+    from rsatb_b200.isqrt import graph_inverse_sqrt
+    from rsatb_b200.vbcsr import BlockSpMat
+    torch.cuda.set_device(0)
+    H, _, _ = lattice.graphene(20, 20)
+    w = np.linalg.eigvalsh(H.to_dense())
+    A = BlockSpMat(H.row_ptr, H.col_ind, H.values, 1)
+    info = {}
+    lo, hi = estimate_spectral_bounds(Chebyshev(A, -1, 1), tol=1e-3, zero_tol=1e-12, info=info)
+    assert info["converged"] and info["matvecs"] < 400
+    assert lo < w[0] and hi > w[-1] and w[0] - lo < 0.6 and hi - w[-1] < 0.6
+    Z0 = BlockSpMat(H.row_ptr, H.col_ind, 0.0 * H.values, 1)
+    assert estimate_spectral_bounds(Chebyshev(Z0, -1, 1), tol=1e-3, zero_tol=1e-12) == (-0.5, 0.5)
+    fro = float(np.sqrt((H.values ** 2).sum()))
+    lo, hi = estimate_spectral_bounds(Chebyshev(A, -1, 1), tol=1e-3, max_matvecs=2)
+    assert abs(lo + fro + 0.5) < 1e-9 and abs(hi - fro - 0.5) < 1e-9
+    Hd, S = lattice.diamond_lcao(L=2, seed=3)
+    Z = graph_inverse_sqrt(S)
+    c = Chebyshev(BlockSpMat(Hd.row_ptr, Hd.col_ind, Hd.values, 8), -1, 1,
+                  preconditioner=ISQRTMPreconditioner(BlockSpMat(Z.row_ptr, Z.col_ind, Z.values, 8)))
+    with pytest.raises(RuntimeError, match="max_matvecs"):
+        estimate_spectral_bounds(c, tol=1e-3, max_matvecs=2)
