@@ -426,6 +426,24 @@ RSATB_API int rsatb_dc_spectrum_fftcheb(rsatb_ctx_t ctx, const rsatb_cheb_op* op
                                         int kernel, double* sigma_out, double* energy_out,
                                         rsatb_fftcheb_stats* stats);
 
+/* Quasi-eigenstate Greenwood spectrum, rsatb::calc::dc_spectrum_qe
+ * (rsatb/calc/fftcheb_transport.hpp:662-884): the fftcheb Greenwood
+ * bilinear form evaluated at a window of grid nodes only, with no row store
+ * and no row transform.  The right chains T_m(Op) J_b psi and the left
+ * J_a T_m(Op) psi are summed into per-node vectors with the node weights
+ * (g_m / pi)(2 - [m = 0]) T_m(e_j) in batches of moments, and each node's
+ * value is one dot of its two vectors over rows and samples.  nodes (host,
+ * n_nodes, may be NULL with n_nodes = 0 for every node) index the
+ * ascending output grid; out-of-range indices are RSATB_INVALID_ARGUMENT.
+ * sigma_out (n_moments x 6, zero outside the window: xx, yy, zz filled)
+ * and energy_out (n_moments, ascending) as for rsatb_dc_spectrum_fftcheb.
+ * Memory: two FP64 vectors of 3 x N x R complex per node.  Synchronises. */
+RSATB_API int rsatb_dc_spectrum_qe(rsatb_ctx_t ctx, const rsatb_cheb_op* op, rsatb_bsr_t Vx,
+                                   rsatb_bsr_t Vy, rsatb_bsr_t Vz, const void* psi,
+                                   int n_vectors, rsatb_dtype vec_dtype, int n_moments,
+                                   double prefactor, int kernel, const int32_t* nodes,
+                                   int n_nodes, double* sigma_out, double* energy_out);
+
 /* ------------------------------------------- batched dense inverse square root */
 
 /* Arithmetic of the batched Newton-Schulz solve. */

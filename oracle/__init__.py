@@ -280,6 +280,63 @@ def bloch_dense(rows, cols, shifts, blocks, n_block_rows: int, k, weights=None,
 
 # ------------------------------------------------- finite-temperature sigma
 
+def qe_dense(H: np.ndarray, V, psi: np.ndarray, center: float, half_width: float,
+             n_moments: int, nodes_ascending=None, kernel: int = 1, prefactor: float = 1.0):
+    """dc_spectrum_qe / accumulate_qe_block (rsatb/calc/fftcheb_transport.hpp:
+    662-884) restated densely for an orthogonal operator (TEST
+    INFRASTRUCTURE): the right chains R_m = T_m(A) J_b psi summed into the
+    node vectors q_j with w_m(j) = (2 - [m = 0]) g_m / pi T_m(e_j), then the
+    left chain's J_a^H T_m(A) psi contracted against them with the same
+    weights over 1 - e_j^2 (at least 1e-14), the sample average, and sigma =
+    prefactor Re(kernel) at the window's nodes (zero elsewhere).
+    H, V[a]: dense (complex); psi: N x R.  Returns (sigma[M, 6], energy)."""
+    M = n_moments
+    N = H.shape[0]
+    R = psi.shape[1]
+    nodes = np.arange(M) if nodes_ascending is None else np.unique(np.asarray(nodes_ascending))
+    src = M - 1 - nodes
+    A = (np.asarray(H) - center * np.eye(N)) / half_width
+    g = kernel_weights(kernel, M)
+    th = np.pi * (src + 0.5) / M
+    eps = np.cos(th)
+    denom = np.maximum(1e-14, 1.0 - eps * eps)
+    vs = 1.0 / (2.0 * half_width)
+    J = [-vs * (np.asarray(V[a]) @ psi) for a in range(3)]
+    w = np.array([[(1.0 if m == 0 else 2.0) * g[m] / np.pi * np.cos(m * t) for t in th]
+                  for m in range(M)])                                   # (M, NE)
+    q = np.zeros((3, nodes.size, N, R), dtype=np.complex128)
+    r_prev = [x.copy() for x in J]
+    r_curr = None
+    for m in range(M):
+        if m == 1:
+            r_curr = [A @ x for x in r_prev]
+        elif m >= 2:
+            r_next = [2.0 * A @ r_curr[a] - r_prev[a] for a in range(3)]
+            r_prev, r_curr = r_curr, r_next
+        rm = r_prev if m == 0 else r_curr
+        for a in range(3):
+            q[a] += w[m][:, None, None] * rm[a][None]
+    K = np.zeros((M, 6), dtype=np.complex128)
+    l_prev, l_curr = psi.astype(np.complex128), None
+    for m in range(M):
+        if m == 1:
+            l_curr = A.conj().T @ l_prev
+        elif m >= 2:
+            l_next = 2.0 * A.conj().T @ l_curr - l_prev
+            l_prev, l_curr = l_curr, l_next
+        lm = l_prev if m == 0 else l_curr
+        for a in range(3):
+            la = -vs * (np.asarray(V[a]).conj().T @ lm)
+            comp = (0, 3, 5)[a]
+            part = np.einsum("nr,jnr->j", la.conj(), q[a])
+            K[src, comp] += w[m] * part / denom
+    K /= R
+    energy = center + half_width * np.cos(np.pi * (M - 1 - np.arange(M) + 0.5) / M)
+    sigma = np.zeros((M, 6))
+    sigma[nodes] = prefactor * K[src].real
+    return sigma, energy
+
+
 def integrate_dc_spectrum(sigma: np.ndarray, energy: np.ndarray, mu: float,
                           temp: float) -> np.ndarray:
     """rsatb/calc/fftcheb_transport.hpp:950-1040 (with fermi_dirac_energy

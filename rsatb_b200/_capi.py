@@ -134,6 +134,8 @@ SIGNATURES = {
     "rsatb_dc_spectrum_fftcheb": (_i, [_vp, C.POINTER(ChebOp), _vp, _vp, _vp, _vp, _i, _i, _i,
                                        _i, _d, _i, _sz, _i, _PD, _PD,
                                        C.POINTER(FftchebStats)]),
+    "rsatb_dc_spectrum_qe": (_i, [_vp, C.POINTER(ChebOp), _vp, _vp, _vp, _vp, _i, _i, _i, _d, _i,
+                                  _vp, _i, _PD, _PD]),
     "rsatb_isqrt_columns_batched": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                          C.POINTER(IsqrtOptions), _vp, C.POINTER(IsqrtStats)]),
     "rsatb_measure_fma_peak": (_i, [_vp, _i, _PD]),

@@ -25,6 +25,7 @@
 
 #include <cufft.h>
 
+#include <algorithm>
 #include <cmath>
 #include <complex>
 #include <vector>
@@ -635,6 +636,227 @@ int fftcheb_impl(const Ctx& c, const rsatb_bsr_matrix* const* V, const T* psi, i
     return RSATB_SUCCESS;
 }
 
+// ------------------------------------------------------------ QE route
+//
+// Quasi-eigenstate Greenwood (dc_spectrum_qe, fftcheb_transport.hpp:
+// 662-884): the same bilinear form as the fftcheb Greenwood route,
+// sigma(e_j) = sum_{m,m'} w_m(j) w_m'(j) <L_m|R_m'> / max(1e-14, 1 - e_j^2),
+// w_m(j) = (m ? 2 : 1) g_m / pi T_m(e_j), evaluated at a window of nodes j
+// only.  The weights are real, so it factors as <P_j|Q_j> with the left and
+// right quasi-eigenstates P_j = sum_m w_m(j) L_m and Q_j = sum_m w_m(j) R_m:
+// each pass adds a batch of QE_BATCH consecutive moment panels into all the
+// node vectors in one launch (each node vector read and written once per
+// batch, FP64 whatever the panel precision), and one fixed-order dot per
+// (node, axis) finishes.  No row store and no transform.
+
+constexpr int kQeBatch = 8;
+
+template <typename T>
+struct QePanels {
+    const T* p[3 * kQeBatch];  // right: one [row][axis][sample] panel per
+                               // moment; left: three [row][sample] per moment
+};
+
+// Q[j][a][row][s] += sum_b w[b][j] X_b(a, row, s) for the nb moments of a
+// batch; one thread per (a, row, s).
+template <typename T, bool RIGHT>
+__global__ void qe_accumulate(int64_t n_rows, int R, int nb, int NE, QePanels<T> X,
+                              const double* __restrict__ w, double2* __restrict__ Q) {
+    const int64_t n_el = 3 * n_rows * R;
+    for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < n_el;
+         e += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t s = e % R;
+        const int64_t t = e / R;
+        const int64_t row = t % n_rows;
+        const int a = int(t / n_rows);
+        double xr[kQeBatch], xi[kQeBatch];
+#pragma unroll
+        for (int b = 0; b < kQeBatch; ++b) {
+            xr[b] = xi[b] = 0.0;
+            if (b < nb) {
+                const T* src = RIGHT ? X.p[b] + 2 * ((row * 3 + a) * R + s)
+                                     : X.p[3 * b + a] + 2 * (row * R + s);
+                xr[b] = double(src[0]);
+                xi[b] = double(src[1]);
+            }
+        }
+        for (int j = 0; j < NE; ++j) {
+            double2 q = Q[int64_t(j) * n_el + e];
+#pragma unroll
+            for (int b = 0; b < kQeBatch; ++b) {
+                if (b < nb) {
+                    const double wb = __ldg(w + b * NE + j);
+                    q.x = fma(wb, xr[b], q.x);
+                    q.y = fma(wb, xi[b], q.y);
+                }
+            }
+            Q[int64_t(j) * n_el + e] = q;
+        }
+    }
+}
+
+// D[j][a] = sum_{row, s} conj(P[j][a][row][s]) Q[j][a][row][s]: one CTA per
+// (node, axis), fixed-order tree reduction.
+__global__ void __launch_bounds__(256) qe_node_dots(int64_t per_axis, const double2* P,
+                                                    const double2* Q, double* D) {
+    __shared__ double red[2][256];
+    const int64_t base = int64_t(blockIdx.x) * per_axis;
+    double ar = 0.0, ai = 0.0;
+    for (int64_t q = threadIdx.x; q < per_axis; q += blockDim.x) {
+        const double2 x = P[base + q], y = Q[base + q];
+        ar += x.x * y.x + x.y * y.y;
+        ai += x.x * y.y - x.y * y.x;
+    }
+    red[0][threadIdx.x] = ar;
+    red[1][threadIdx.x] = ai;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) {
+            red[0][threadIdx.x] += red[0][threadIdx.x + w];
+            red[1][threadIdx.x] += red[1][threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        D[2 * blockIdx.x] = red[0][0];
+        D[2 * blockIdx.x + 1] = red[1][0];
+    }
+}
+
+template <typename T>
+int qe_impl(const Ctx& c, const rsatb_bsr_matrix* const* V, const T* psi, int R, int M,
+            const std::vector<int>& nodes, double prefactor, int kernel, double* sigma_out,
+            double* energy_out) {
+    rsatb_context* ctx = c.ctx;
+    cudaStream_t st = ctx->stream;
+    const int b = c.op->H->block_size;
+    const int nbr = c.op->H->n_block_rows;
+    const int64_t N = int64_t(nbr) * b;
+    const int W1 = 2 * R, W3 = 6 * R;
+    const size_t cplx = 2 * sizeof(T);
+    const int NE = int(nodes.size());
+    const int RB = kQeBatch + 2;  // right ring: the batch plus the recurrence's predecessors
+
+    std::vector<double> g(M);
+    kpm_kernel_weights(kernel, M, g.data());
+    // weights w[m][j] and the node energies (src = M - 1 - ascending index)
+    std::vector<double> wts(size_t(M) * NE), denom(NE);
+    for (int j = 0; j < NE; ++j) {
+        const int src = M - 1 - nodes[j];
+        const double th = M_PI * (double(src) + 0.5) / double(M);
+        const double e = std::cos(th);
+        denom[j] = std::max(1e-14, 1.0 - e * e);
+        for (int m = 0; m < M; ++m)
+            wts[size_t(m) * NE + j] = (m == 0 ? 1.0 : 2.0) * g[m] / M_PI * std::cos(double(m) * th);
+    }
+    DevBuf bW, bJ, bR, bL, bLA, bU, bWs, bQ, bP, bD;
+    RSATB_TRY(bW.alloc(wts.size() * sizeof(double)));
+    RSATB_CUDA_TRY(cudaMemcpyAsync(bW.p, wts.data(), wts.size() * sizeof(double),
+                                   cudaMemcpyHostToDevice, st));
+    RSATB_TRY(bJ.alloc(size_t(N) * 3 * R * cplx));
+    RSATB_TRY(bR.alloc(size_t(RB) * N * 3 * R * cplx));
+    RSATB_TRY(bL.alloc(size_t(3) * N * R * cplx));
+    RSATB_TRY(bLA.alloc(size_t(kQeBatch) * 3 * N * R * cplx));
+    if (c.sandwich) {
+        RSATB_TRY(bU.alloc(size_t(N) * 3 * R * cplx));
+        RSATB_TRY(bWs.alloc(size_t(N) * 3 * R * cplx));
+    }
+    const int64_t n_el = 3 * N * R;
+    RSATB_TRY(bQ.alloc(size_t(NE) * n_el * sizeof(double2)));
+    RSATB_TRY(bP.alloc(size_t(NE) * n_el * sizeof(double2)));
+    RSATB_TRY(bD.alloc(size_t(NE) * 3 * sizeof(double2)));
+    RSATB_CUDA_TRY(cudaMemsetAsync(bQ.p, 0, size_t(NE) * n_el * sizeof(double2), st));
+    RSATB_CUDA_TRY(cudaMemsetAsync(bP.p, 0, size_t(NE) * n_el * sizeof(double2), st));
+    T* J[3];
+    for (int a = 0; a < 3; ++a) J[a] = bJ.as<T>() + size_t(a) * N * 2 * R;
+    auto rslot = [&](int m) { return bR.as<T>() + size_t(m % RB) * N * 6 * R; };
+    T* l[3];
+    for (int i = 0; i < 3; ++i) l[i] = bL.as<T>() + size_t(i) * N * 2 * R;
+    auto laslot = [&](int bidx, int a) {
+        return bLA.as<T>() + (size_t(bidx) * 3 + a) * N * 2 * R;
+    };
+    const unsigned grid = grid_for(n_el, ctx->sm_count);
+    auto flush = [&](bool right, int m_last, int nb) -> int {
+        QePanels<T> X{};
+        const int m0 = m_last - nb + 1;
+        for (int q = 0; q < nb; ++q) {
+            if (right) {
+                X.p[q] = rslot(m0 + q);
+            } else {
+                for (int a = 0; a < 3; ++a) X.p[3 * q + a] = laslot((m0 + q) % kQeBatch, a);
+            }
+        }
+        const double* w = bW.as<double>() + size_t(m0) * NE;
+        double2* dst = right ? bQ.as<double2>() : bP.as<double2>();
+        if (right)
+            qe_accumulate<T, true><<<grid, 256, 0, st>>>(N, R, nb, NE, X, w, dst);
+        else
+            qe_accumulate<T, false><<<grid, 256, 0, st>>>(N, R, nb, NE, X, w, dst);
+        RSATB_LAUNCH_CHECK(ctx);
+        return RSATB_SUCCESS;
+    };
+
+    // Right pass: R_0 = (J_a psi) packed [row][axis][sample], R_m by the
+    // recurrence on the N x 3R panel.
+    for (int a = 0; a < 3; ++a)
+        RSATB_TRY(current_rows(c, V[a], W1, psi, J[a], 0, nbr, bU.p, bWs.p));
+    pack_axes_kernel<T><<<grid_for(N * 3 * R, ctx->sm_count), 256, 0, st>>>(N, R, J[0], J[1],
+                                                                           J[2], rslot(0));
+    RSATB_LAUNCH_CHECK(ctx);
+    for (int m = 0; m < M; ++m) {
+        if (m == 1)
+            RSATB_TRY(op_step(c, W3, rslot(0), nullptr, rslot(1), bU.p, bWs.p, 1.0, 0.0));
+        else if (m >= 2)
+            RSATB_TRY(op_step(c, W3, rslot(m - 1), rslot(m - 2), rslot(m), bU.p, bWs.p, 2.0,
+                              -1.0));
+        if ((m + 1) % kQeBatch == 0 || m == M - 1)
+            RSATB_TRY(flush(true, m, m % kQeBatch + 1));
+    }
+    // Left pass: L_m = J_a T_m(Op) psi (J_a^H = J_a: V_a and the sandwich's
+    // Z^H V_a Z are Hermitian).
+    const T* lp = nullptr;
+    const T* lc = psi;
+    int li = 0;
+    for (int m = 0; m < M; ++m) {
+        if (m >= 1) {
+            T* lo = l[li];
+            li = (li + 1) % 3;
+            if (m == 1) RSATB_TRY(op_step(c, W1, lc, nullptr, lo, bU.p, bWs.p, 1.0, 0.0));
+            else RSATB_TRY(op_step(c, W1, lc, lp, lo, bU.p, bWs.p, 2.0, -1.0));
+            lp = lc;
+            lc = lo;
+        }
+        for (int a = 0; a < 3; ++a)
+            RSATB_TRY(current_rows(c, V[a], W1, lc, laslot(m % kQeBatch, a), 0, nbr, bU.p,
+                                   bWs.p));
+        if ((m + 1) % kQeBatch == 0 || m == M - 1)
+            RSATB_TRY(flush(false, m, m % kQeBatch + 1));
+    }
+    qe_node_dots<<<unsigned(NE * 3), 256, 0, st>>>(N * R, bP.as<double2>(), bQ.as<double2>(),
+                                                  bD.as<double>());
+    RSATB_LAUNCH_CHECK(ctx);
+    std::vector<double> D(size_t(NE) * 6);
+    RSATB_CUDA_TRY(cudaMemcpyAsync(D.data(), bD.p, D.size() * sizeof(double),
+                                   cudaMemcpyDeviceToHost, st));
+    RSATB_CUDA_TRY(cudaStreamSynchronize(st));
+    RSATB_TRY(ctx_check_fault(ctx));
+    // Ascending energies (fftcheb_transport.hpp:940-954); sigma zero outside
+    // the node window, Re of the sample-averaged kernel inside.
+    for (int k = 0; k < M; ++k) {
+        const int src = M - 1 - k;
+        energy_out[k] = c.op->center +
+                        c.op->half_width * std::cos(M_PI * (double(src) + 0.5) / double(M));
+    }
+    std::fill(sigma_out, sigma_out + size_t(M) * 6, 0.0);
+    for (int j = 0; j < NE; ++j)
+        for (int a = 0; a < 3; ++a) {
+            const int comp = a == 0 ? 0 : (a == 1 ? 3 : 5);
+            sigma_out[size_t(nodes[j]) * 6 + comp] =
+                prefactor * D[2 * (size_t(j) * 3 + a)] / denom[j] / double(R);
+        }
+    return RSATB_SUCCESS;
+}
+
 }  // namespace
 }  // namespace rsatb_b200
 
@@ -691,4 +913,62 @@ extern "C" int rsatb_dc_spectrum_fftcheb(rsatb_ctx_t ctx, const rsatb_cheb_op* o
     return fftcheb_impl<float>(c, V, static_cast<const float*>(psi), n_vectors, n_moments,
                                formulation, prefactor, partition_sections, max_workspace_bytes,
                                kernel, sigma_out, energy_out, stats);
+}
+
+extern "C" int rsatb_dc_spectrum_qe(rsatb_ctx_t ctx, const rsatb_cheb_op* op, rsatb_bsr_t Vx,
+                                    rsatb_bsr_t Vy, rsatb_bsr_t Vz, const void* psi,
+                                    int n_vectors, rsatb_dtype vec_dtype, int n_moments,
+                                    double prefactor, int kernel, const int32_t* nodes,
+                                    int n_nodes, double* sigma_out, double* energy_out) {
+    clear_error();
+    RSATB_TRY(check_ctx(ctx));
+    if (!op || !psi || !sigma_out || !energy_out || (n_nodes > 0 && !nodes))
+        return set_error(RSATB_INVALID_ARGUMENT, "null argument");
+    if (op->form != RSATB_FORM_ORTHOGONAL && op->form != RSATB_FORM_SANDWICH)
+        return set_error(RSATB_NOT_SUPPORTED, "operator form %d is not available on the device",
+                         op->form);
+    const bool sandwich = op->form == RSATB_FORM_SANDWICH;
+    const rsatb_bsr_matrix* mats[6] = {op->H, sandwich ? op->Z : op->H,
+                                       sandwich ? op->ZH : op->H, Vx, Vy, Vz};
+    const char* names[6] = {"H", "Z", "ZH", "Vx", "Vy", "Vz"};
+    for (int i = 0; i < 6; ++i) {
+        RSATB_TRY(check_bsr(mats[i], names[i]));
+        if (mats[i]->n_block_rows != op->H->n_block_rows ||
+            mats[i]->n_block_cols != op->H->n_block_rows ||
+            mats[i]->block_size != op->H->block_size)
+            return set_error(RSATB_INVALID_ARGUMENT, "%s does not match H's shape", names[i]);
+        if (dtype_is_double(mats[i]->dtype) != dtype_is_double(vec_dtype))
+            return set_error(RSATB_INVALID_ARGUMENT, "%s precision differs from the vectors'",
+                             names[i]);
+    }
+    if (!dtype_is_complex(vec_dtype))
+        return set_error(RSATB_INVALID_ARGUMENT, "transport needs complex sample vectors");
+    if (!(op->half_width > 0.0))
+        return set_error(RSATB_INVALID_ARGUMENT, "half_width must be positive");
+    if (n_vectors <= 0 || n_moments <= 0)
+        return set_error(RSATB_INVALID_ARGUMENT, "n_vectors and n_moments must be positive");
+    if (6 * n_vectors > 1536)
+        return set_error(RSATB_NOT_SUPPORTED, "%d samples exceed one block (256 at most)",
+                         n_vectors);
+    if (!aligned16(psi)) return set_error(RSATB_INVALID_ARGUMENT, "psi must be 16-byte aligned");
+    // The node window: ascending output-grid indices, sorted and unique;
+    // empty means every node (dc_spectrum_qe's nodes_ascending).
+    std::vector<int> nd;
+    if (n_nodes <= 0) {
+        nd.resize(n_moments);
+        for (int k = 0; k < n_moments; ++k) nd[k] = k;
+    } else {
+        nd.assign(nodes, nodes + n_nodes);
+        std::sort(nd.begin(), nd.end());
+        nd.erase(std::unique(nd.begin(), nd.end()), nd.end());
+        if (nd.front() < 0 || nd.back() >= n_moments)
+            return set_error(RSATB_INVALID_ARGUMENT, "dc_spectrum_qe: node index out of range");
+    }
+    const rsatb_bsr_matrix* V[3] = {Vx, Vy, Vz};
+    Ctx c{ctx, op, sandwich, int(vec_dtype)};
+    if (dtype_is_double(vec_dtype))
+        return qe_impl<double>(c, V, static_cast<const double*>(psi), n_vectors, n_moments, nd,
+                               prefactor, kernel, sigma_out, energy_out);
+    return qe_impl<float>(c, V, static_cast<const float*>(psi), n_vectors, n_moments, nd,
+                          prefactor, kernel, sigma_out, energy_out);
 }

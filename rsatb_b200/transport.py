@@ -60,6 +60,36 @@ def dc_spectrum_fftcheb(cheby: Chebyshev, Vx: BlockSpMat, Vy: BlockSpMat, Vz: Bl
     return out
 
 
+def dc_spectrum_qe(cheby: Chebyshev, Vx: BlockSpMat, Vy: BlockSpMat, Vz: BlockSpMat,
+                   psi: torch.Tensor, n_moments: int, prefactor: float = 1.0,
+                   kernel: KpmKernel = KpmKernel.Jackson, nodes_ascending=None):
+    """rsatb::calc::dc_spectrum_qe (rsatb/calc/fftcheb_transport.hpp:
+    662-884): the Greenwood sigma at the nodes_ascending window of the
+    ascending grid (all nodes when None) by quasi-eigenstates, without the
+    row store; same (sigma[n_moments, 6], energy[n_moments]) as
+    dc_spectrum_fftcheb, sigma zero outside the window."""
+    if n_moments <= 0:
+        raise ValueError("n_moments must be positive")
+    if not psi.is_cuda or psi.dim() != 2 or not psi.is_contiguous() or not psi.is_complex():
+        raise ValueError("psi must be a contiguous (N, R) complex CUDA tensor")
+    if psi.shape[0] != cheby.n_rows:
+        raise ValueError("psi rows differ from the operator size")
+    nodes = (np.zeros(0, np.int32) if nodes_ascending is None else
+             np.ascontiguousarray(np.asarray(nodes_ascending, dtype=np.int32)))
+    ctx = cheby.H.ctx
+    ctx.bind_stream()
+    op = cheby.c_op()
+    sigma = np.zeros(n_moments * 6)
+    energy = np.zeros(n_moments)
+    P = C.POINTER(C.c_double)
+    check(lib().rsatb_dc_spectrum_qe(
+        ctx.handle, C.byref(op), Vx.handle, Vy.handle, Vz.handle, C.c_void_p(psi.data_ptr()),
+        psi.shape[1], dtype_code(psi.dtype), int(n_moments), float(prefactor), int(kernel),
+        nodes.ctypes.data if nodes.size else None, int(nodes.size), sigma.ctypes.data_as(P),
+        energy.ctypes.data_as(P)))
+    return sigma.reshape(n_moments, 6), energy
+
+
 def integrate_dc_spectrum(sigma, energy, mu: float, temp: float, device=None) -> np.ndarray:
     """sigma(mu, T) (6 components) from a zero-temperature spectrum
     sigma[n_energy, 6] on `energy` (fftcheb_transport.hpp:950-1040), on the

@@ -396,3 +396,28 @@ def test_ns_refine_dense_keeps_test_isqrtm_chain_semantics():
     assert np.abs(Z.T @ S @ Z - np.eye(24)).max() < 1e-9
     _, r = run(0.49, 1, 1e-16)
     assert not r["converged"] and not r["diverged"] and r["hit_maxiter"]
+
+
+def test_qe_restatement_equals_fftcheb_greenwood():
+    """oracle.qe_dense (accumulate_qe_block restated) against the oracle's
+    fftcheb Greenwood route, itself pinned to test_fftcheb_transport.cpp's
+    toys: the same bilinear form, equal to rounding on every node and on a
+    window (zero outside it)."""
+    rng = np.random.default_rng(14)
+    n, R, M = 24, 3, 40
+    H = rng.standard_normal((n, n)) * 0.3
+    H = H + H.T
+    W = [rng.standard_normal((n, n)) * 0.2 for _ in range(3)]
+    W = [w - w.T for w in W]                  # V_a = i W_a, imaginary Hermitian
+    psi = np.exp(2j * np.pi * rng.random((n, R))) / np.sqrt(n)
+    bound = float(np.abs(np.linalg.eigvalsh(H)).max()) + 0.5
+    op = oracle.make_op(oracle.Bsr.from_dense(H), 0.0, bound)
+    Vb = [oracle.Bsr.from_dense(w, imag=True) for w in W]
+    want, en = oracle.fftcheb(op, Vb, psi, M)
+    got, en2 = oracle.qe_dense(H, [1j * w for w in W], psi, 0.0, bound, M)
+    assert np.abs(en - en2).max() < 1e-13
+    assert np.abs(got - want).max() <= 1e-11 * np.abs(want).max()
+    nodes = np.array([3, 11, 12, 30])
+    win, _ = oracle.qe_dense(H, [1j * w for w in W], psi, 0.0, bound, M, nodes)
+    assert np.abs(win[nodes] - want[nodes]).max() <= 1e-11 * np.abs(want).max()
+    assert np.all(np.delete(win, nodes, axis=0) == 0.0)

@@ -198,3 +198,73 @@ def test_integrate_dc_spectrum_matches_oracle(torch_cuda, temp):
     if temp > 0:
         with pytest.raises(Exception):
             integrate_dc_spectrum(s, e[::-1].copy(), 0.0, temp)
+
+
+# ------------------------------------------------------------------ QE route
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_qe_route_matches_oracle_and_fftcheb(torch_cuda, precision):
+    """dc_spectrum_qe on a window of nodes: the oracle's dense restatement
+    of accumulate_qe_block (1e-10 of the window's peak in FP64, 1e-4 with
+    FP32 vectors) and the fftcheb Greenwood route on the same nodes, which
+    is the same bilinear form (the reference's note: they agree to
+    rounding); zero outside the window."""
+    torch = torch_cuda
+    from rsatb_b200.calc import Chebyshev
+    from rsatb_b200.transport import dc_spectrum_fftcheb, dc_spectrum_qe
+    H, V = _tbg()
+    emin, emax = _bounds(H)
+    M, R = 64, 3
+    psi = _phases(H.n_rows, R, seed=8)
+    nodes = np.arange(20, 34)
+    c = Chebyshev(_dev(H), emin, emax)
+    Vd = [_dev(v, imaginary=True) for v in V]
+    dt = torch.complex128
+    if precision == "f32":
+        c, Vd, dt = c.astype("f32"), [v.astype("f32") for v in Vd], torch.complex64
+    p = torch.as_tensor(psi).cuda().to(dt).contiguous()
+    sig, en = dc_spectrum_qe(c, *Vd, p, M, nodes_ascending=nodes)
+    Vo = [1j * v.to_dense() for v in V]
+    want, en_o = oracle.qe_dense(H.to_dense(), Vo, psi, (emax + emin) / 2, (emax - emin) / 2, M,
+                                 nodes)
+    assert np.abs(en - en_o).max() < 1e-12
+    tol = 1e-10 if precision == "f64" else 1e-4
+    assert rel_err(sig, want) < tol
+    outside = np.setdiff1d(np.arange(M), nodes)
+    assert np.all(sig[outside] == 0.0)
+    if precision == "f64":
+        full, _ = dc_spectrum_fftcheb(c, *Vd, p, M)
+        assert rel_err(sig[nodes], full[nodes]) < 1e-10
+        every, _ = dc_spectrum_qe(c, *Vd, p, M)
+        assert rel_err(every, full) < 1e-10
+
+
+def test_qe_route_sandwich_and_errors(torch_cuda):
+    """The sandwich form through the QE route equals the fftcheb route;
+    a node outside the grid is refused."""
+    torch = torch_cuda
+    from rsatb_b200._capi import RsatbError
+    from rsatb_b200.calc import Chebyshev, ISQRTMPreconditioner
+    from rsatb_b200.transport import dc_spectrum_fftcheb, dc_spectrum_qe
+    H, V = _tbg()
+    emin, emax = _bounds(H)
+    n = H.n_rows
+    rng = np.random.default_rng(2)
+    Zd = np.eye(n) + 0.01 * rng.standard_normal((n, n))
+    mask = np.abs(H.to_dense()) > 0
+    np.fill_diagonal(mask, True)
+    Zd = np.where(mask, Zd, 0.0)
+    from rsatb_b200.lattice import BsrArrays
+    rows, cols = np.nonzero(Zd)
+    rp = np.concatenate([[0], np.cumsum(np.bincount(rows, minlength=n))]).astype(np.int32)
+    Z = BsrArrays(rp, cols.astype(np.int32), Zd[rows, cols].reshape(-1, 1, 1).copy(), 1)
+    c = Chebyshev(_dev(H), emin - 1.0, emax + 1.0, preconditioner=ISQRTMPreconditioner(_dev(Z)))
+    Vd = [_dev(v, imaginary=True) for v in V]
+    p = torch.as_tensor(_phases(n, 2, seed=3)).cuda().contiguous()
+    M = 48
+    full, _ = dc_spectrum_fftcheb(c, *Vd, p, M)
+    nodes = np.array([5, 17, 30, 47])
+    sig, _ = dc_spectrum_qe(c, *Vd, p, M, nodes_ascending=nodes)
+    assert rel_err(sig[nodes], full[nodes]) < 1e-10
+    with pytest.raises(RsatbError, match="out of range"):
+        dc_spectrum_qe(c, *Vd, p, M, nodes_ascending=[0, M])
