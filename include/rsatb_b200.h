@@ -221,20 +221,29 @@ typedef struct {
 RSATB_API int rsatb_cheb_apply_op(rsatb_ctx_t ctx, const rsatb_cheb_op* op, const void* X, void* Y,
                         int n_vectors, rsatb_dtype vec_dtype);
 
-/* Y = scale * (V dressed by the operator form) X: V X (Orthogonal) or
- * Z^H V Z X (Sandwich).  Chebyshev::apply_dual (rsatb/calc/cheby.hpp:
+/* Y = scale * (V dressed by the operator form) X: V X (Orthogonal),
+ * Z^H V Z X (Sandwich) or S^-1 V X (Solve: one CG with S, V X its target
+ * and initial guess).  Chebyshev::apply_dual NORMAL (rsatb/calc/cheby.hpp:
  * 249-291) for a plain velocity matrix V (RSATB_BSR_IMAGINARY_UNIT for the
- * i W of a real k-point); mode is immaterial for these two forms.  X, Y:
- * device N x n_vectors panels, 16-byte aligned, distinct. */
+ * i W of a real k-point).  X, Y: device N x n_vectors panels, 16-byte
+ * aligned, distinct. */
 RSATB_API int rsatb_cheb_apply_dual(rsatb_ctx_t ctx, const rsatb_cheb_op* op, rsatb_bsr_t V,
                                     const void* X, void* Y, int n_vectors, rsatb_dtype vec_dtype,
                                     double scale);
+/* The same in ChebyMode::ADJOINT: scale * V S^-1 X for the Solve form (the
+ * CG from zero), equal to rsatb_cheb_apply_dual for the two Hermitian
+ * forms. */
+RSATB_API int rsatb_cheb_apply_dual_adjoint(rsatb_ctx_t ctx, const rsatb_cheb_op* op,
+                                            rsatb_bsr_t V, const void* X, void* Y,
+                                            int n_vectors, rsatb_dtype vec_dtype, double scale);
 
 /* Y = sum_{n < n_coeffs} c_n T_n(Op~) X, Chebyshev::propagate
  * (rsatb/calc/cheby.hpp:367-441): coeffs holds n_coeffs complex values as
  * (re, im) pairs; a real panel takes Re(c_n), as the reference's CoeffCast
  * does for a real scalar type.  n_coeffs == 0 leaves Y unchanged.  X, Y:
- * device panels, 16-byte aligned, distinct. */
+ * device panels, 16-byte aligned, distinct.  The Solve form runs one CG per
+ * application, each started from its output panel's previous contents
+ * (T_{n-3}; the first two from zero). */
 RSATB_API int rsatb_cheb_propagate(rsatb_ctx_t ctx, const rsatb_cheb_op* op, const void* X,
                                    void* Y, int n_vectors, rsatb_dtype vec_dtype,
                                    const double* coeffs, int n_coeffs);

@@ -116,6 +116,7 @@ SIGNATURES = {
     "rsatb_bsr_mult_dense": (_i, [_vp, _vp, _vp, _vp, _i, _i, _d]),
     "rsatb_cheb_apply_op": (_i, [_vp, C.POINTER(ChebOp), _vp, _vp, _i, _i]),
     "rsatb_cheb_apply_dual": (_i, [_vp, C.POINTER(ChebOp), _vp, _vp, _vp, _i, _i, _d]),
+    "rsatb_cheb_apply_dual_adjoint": (_i, [_vp, C.POINTER(ChebOp), _vp, _vp, _vp, _i, _i, _d]),
     "rsatb_cheb_propagate": (_i, [_vp, C.POINTER(ChebOp), _vp, _vp, _i, _i, _PD, _i]),
     "rsatb_kpm_dos_moments": (_i, [_vp, C.POINTER(ChebOp), _vp, _i, _i, _i, _i, _PD, _PD]),
     "rsatb_kpm_dos_moments_noalloc": (_i, [_vp, C.POINTER(ChebOp), _vp, _i, _i, _i, _i, _PD,

@@ -88,7 +88,8 @@ class Chebyshev:
     ``cg_tol`` 1e-8 and at most ``cg_max_iter`` 1000 iterations, as
     LinearSolver's defaults), preconditioned by the factor of
     ``preconditioner`` when one is given as well.  The Solve form serves
-    ``apply_op`` and the plain moment recurrence.
+    ``apply_op`` (NORMAL), ``apply_dual`` (both modes), ``propagate`` and
+    the plain moment recurrence.
     """
 
     def __init__(self, H: BlockSpMat, emin: float, emax: float,
@@ -169,12 +170,15 @@ class Chebyshev:
 
     def apply_dual(self, V: BlockSpMat, X: torch.Tensor, Y: torch.Tensor,
                    mode: ChebyMode = ChebyMode.NORMAL, scale: float = 1.0) -> torch.Tensor:
-        """Y = scale * (V dressed by the form) X: V X (Orthogonal) or Z^H V Z X
-        (Sandwich) (cheby.hpp:249-291); mode is immaterial for these forms."""
+        """Y = scale * (V dressed by the form) X: V X (Orthogonal), Z^H V Z X
+        (Sandwich), S^-1 V X (Solve; ADJOINT: V S^-1 X) (cheby.hpp:249-291);
+        mode is immaterial for the two Hermitian forms."""
         ctx = self.H.ctx
         ctx.bind_stream()
         op = self.c_op()
-        check(lib().rsatb_cheb_apply_dual(ctx.handle, C.byref(op), V.handle,
+        fn = (lib().rsatb_cheb_apply_dual_adjoint if mode == ChebyMode.ADJOINT
+              else lib().rsatb_cheb_apply_dual)
+        check(fn(ctx.handle, C.byref(op), V.handle,
                                           C.c_void_p(X.data_ptr()), C.c_void_p(Y.data_ptr()),
                                           X.shape[1], dtype_code(X.dtype), float(scale)))
         return Y
@@ -182,7 +186,10 @@ class Chebyshev:
     def propagate(self, V_in: torch.Tensor, V_out: torch.Tensor, coeffs,
                   mode: ChebyMode = ChebyMode.NORMAL) -> torch.Tensor:
         """V_out = sum_n c_n T_n(Op~) V_in (cheby.hpp:367-441); coeffs complex
-        (a real panel takes their real parts)."""
+        (a real panel takes their real parts).  The Solve form runs a CG per
+        application (NORMAL only, as its apply_op)."""
+        if self.form == ChebyOpForm.Solve and mode == ChebyMode.ADJOINT:
+            raise NotImplementedError("the Solve form serves NORMAL applications only")
         c = np.ascontiguousarray(np.asarray(coeffs, dtype=np.complex128))
         flat = np.ascontiguousarray(np.stack([c.real, c.imag], axis=-1).reshape(-1))
         ctx = self.H.ctx

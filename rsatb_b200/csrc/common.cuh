@@ -72,6 +72,9 @@ struct rsatb_context {
     std::string kpm_graph_key;
     std::string kpm_seen_key;
     int64_t kpm_graph_launches = 0;
+    // Pinned host staging (grow-only) for small asynchronous read-backs.
+    void* pinned = nullptr;
+    size_t pinned_bytes = 0;
 };
 
 struct rsatb_bsr_matrix {
@@ -113,6 +116,9 @@ int ctx_counters(rsatb_context* ctx, int n, unsigned** out);
 // The context's device fault word (the last of its 64 counters): kernels
 // whose bounded waits give up set it non-zero.
 int ctx_fault_word(rsatb_context* ctx, unsigned** out);
+// Pinned host memory of at least `bytes` (grow-only, released with the
+// context).
+int ctx_pinned(rsatb_context* ctx, size_t bytes, void** out);
 // After the stream has been synchronised: reads and clears the fault word;
 // RSATB_CUDA_ERROR when a kernel recorded a fault.
 int ctx_check_fault(rsatb_context* ctx);

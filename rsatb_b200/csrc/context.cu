@@ -74,6 +74,22 @@ int ctx_counters(rsatb_context* ctx, int n, unsigned** out) {
     return RSATB_SUCCESS;
 }
 
+int ctx_pinned(rsatb_context* ctx, size_t bytes, void** out) {
+    if (ctx->pinned_bytes < bytes) {
+        if (ctx->pinned) {
+            RSATB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+            RSATB_CUDA_TRY(cudaFreeHost(ctx->pinned));
+            ctx->pinned = nullptr;
+            ctx->pinned_bytes = 0;
+        }
+        const size_t grow = bytes < 4096 ? 4096 : bytes + bytes / 2;
+        RSATB_CUDA_TRY(cudaHostAlloc(&ctx->pinned, grow, cudaHostAllocDefault));
+        ctx->pinned_bytes = grow;
+    }
+    *out = ctx->pinned;
+    return RSATB_SUCCESS;
+}
+
 int ctx_fault_word(rsatb_context* ctx, unsigned** out) {
     unsigned* c = nullptr;
     RSATB_TRY(ctx_counters(ctx, 1, &c));
@@ -139,6 +155,7 @@ int rsatb_ctx_destroy(rsatb_ctx_t ctx) {
     cudaStreamSynchronize(ctx->stream);
     if (ctx->scratch) cudaFree(ctx->scratch);
     if (ctx->counters) cudaFree(ctx->counters);
+    if (ctx->pinned) cudaFreeHost(ctx->pinned);
     if (ctx->kpm_graph) cudaGraphExecDestroy(ctx->kpm_graph);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;

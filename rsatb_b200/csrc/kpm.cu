@@ -29,6 +29,11 @@ int solve_form_apply(rsatb_context* ctx, const rsatb_cheb_op* op, const void* X,
 int solve_form_moments(rsatb_context* ctx, const rsatb_cheb_op* op, const void* psi,
                        int n_vectors, int vdt, int n_moments, double* mu_out,
                        double* col_mu_out);
+int solve_form_apply_dual(rsatb_context* ctx, const rsatb_cheb_op* op,
+                          const rsatb_bsr_matrix* V, const void* X, void* Y, int n_vectors,
+                          int vdt, double scale, bool adjoint);
+int solve_form_propagate(rsatb_context* ctx, const rsatb_cheb_op* op, const void* X, void* Y,
+                         int n_vectors, int vdt, const double* coeffs, int n_coeffs);
 
 int run_coldot(rsatb_context* ctx, int vdt, int64_t n_rows, const StepArgs& a) {
     return dtype_is_double(vdt) ? launch_coldot_f64(ctx, vdt, n_rows, a)
@@ -534,11 +539,19 @@ int rsatb_kpm_dos_moments(rsatb_ctx_t ctx, const rsatb_cheb_op* op, const void* 
     return RSATB_SUCCESS;
 }
 
-int rsatb_cheb_apply_dual(rsatb_ctx_t ctx, const rsatb_cheb_op* op, rsatb_bsr_t V,
-                          const void* X, void* Y, int n_vectors, rsatb_dtype vec_dtype,
-                          double scale) {
-    clear_error();
+static int apply_dual_impl(rsatb_ctx_t ctx, const rsatb_cheb_op* op, rsatb_bsr_t V,
+                           const void* X, void* Y, int n_vectors, rsatb_dtype vec_dtype,
+                           double scale, bool adjoint) {
     RSATB_TRY(check_ctx(ctx));
+    if (op && op->form == RSATB_FORM_SOLVE) {
+        if (!X || !Y) return set_error(RSATB_INVALID_ARGUMENT, "null multivector");
+        if (!aligned16(X) || !aligned16(Y))
+            return set_error(RSATB_INVALID_ARGUMENT, "multivectors must be 16-byte aligned");
+        if (X == Y) return set_error(RSATB_INVALID_ARGUMENT, "apply_dual cannot run in place");
+        int W = 0;
+        RSATB_TRY(panel_width(n_vectors, vec_dtype, &W));
+        return solve_form_apply_dual(ctx, op, V, X, Y, n_vectors, vec_dtype, scale, adjoint);
+    }
     OpShape sh{};
     RSATB_TRY(check_op(op, vec_dtype, &sh));
     RSATB_TRY(check_matrix_square(V, "V"));
@@ -575,11 +588,36 @@ int rsatb_cheb_apply_dual(rsatb_ctx_t ctx, const rsatb_cheb_op* op, rsatb_bsr_t 
     return run_step(ctx, op->ZH, vec_dtype, a);      // y = scale Z^H V Z x
 }
 
+int rsatb_cheb_apply_dual(rsatb_ctx_t ctx, const rsatb_cheb_op* op, rsatb_bsr_t V,
+                          const void* X, void* Y, int n_vectors, rsatb_dtype vec_dtype,
+                          double scale) {
+    clear_error();
+    return apply_dual_impl(ctx, op, V, X, Y, n_vectors, vec_dtype, scale, false);
+}
+
+int rsatb_cheb_apply_dual_adjoint(rsatb_ctx_t ctx, const rsatb_cheb_op* op, rsatb_bsr_t V,
+                                  const void* X, void* Y, int n_vectors, rsatb_dtype vec_dtype,
+                                  double scale) {
+    clear_error();
+    return apply_dual_impl(ctx, op, V, X, Y, n_vectors, vec_dtype, scale, true);
+}
+
 int rsatb_cheb_propagate(rsatb_ctx_t ctx, const rsatb_cheb_op* op, const void* X, void* Y,
                          int n_vectors, rsatb_dtype vec_dtype, const double* coeffs,
                          int n_coeffs) {
     clear_error();
     RSATB_TRY(check_ctx(ctx));
+    if (op && op->form == RSATB_FORM_SOLVE) {
+        if (n_coeffs < 0) return set_error(RSATB_INVALID_ARGUMENT, "n_coeffs < 0");
+        if (n_coeffs == 0) return RSATB_SUCCESS;
+        if (!X || !Y || !coeffs) return set_error(RSATB_INVALID_ARGUMENT, "null argument");
+        if (!aligned16(X) || !aligned16(Y))
+            return set_error(RSATB_INVALID_ARGUMENT, "multivectors must be 16-byte aligned");
+        if (X == Y) return set_error(RSATB_INVALID_ARGUMENT, "propagate cannot run in place");
+        int W = 0;
+        RSATB_TRY(panel_width(n_vectors, vec_dtype, &W));
+        return solve_form_propagate(ctx, op, X, Y, n_vectors, vec_dtype, coeffs, n_coeffs);
+    }
     OpShape sh{};
     RSATB_TRY(check_op(op, vec_dtype, &sh));
     int W = 0;

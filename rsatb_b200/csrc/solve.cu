@@ -11,11 +11,13 @@
 // KPM recurrence over this operator is the plain one (dos.hpp:172-187):
 // S^-1 H is not Hermitian, so the doubling identity does not apply.
 //
-// On the device: S P and H x are the fused BSR step kernels with no
-// epilogue; the per-column dots are FP64 and deterministic (fixed-order
-// partial sums per CTA, then over CTAs); alpha and beta are formed on the
-// device; the host reads the column residuals once per iteration for the
-// stopping test.  With the graph-local factor Z (ISQRTMPreconditioner, whose
+// On the device: S P and H x are the fused BSR step kernels, S P with its
+// column dots <p|Sp> fused into the step; the update of X and R computes
+// alpha per column and the new <r|r> in the same launch; every dot is FP64
+// and deterministic (fixed-order partial sums per CTA, then the last CTA
+// over CTAs).  An iteration is three launches and one 8 x R-byte copy of
+// the residuals, which the host reads one iteration behind for the stopping
+// test.  With the graph-local factor Z (ISQRTMPreconditioner, whose
 // type is Symmetric) the CG runs on Z^H S Z Y = Z^H B and X = Z Y.
 #include "cheb_kernels.cuh"
 
@@ -26,6 +28,7 @@
 namespace rsatb_b200 {
 
 int run_step(rsatb_context* ctx, const rsatb_bsr_matrix* A, int vdt, const StepArgs& a);
+int run_coldot(rsatb_context* ctx, int vdt, int64_t n_rows, const StepArgs& a);
 
 namespace {
 
@@ -34,100 +37,114 @@ constexpr int kMaxCols = 256;  // columns a dot CTA covers at once
 
 bool aligned16s(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
-// part[b][c] = sum over the rows CTA b takes of conj(A_rc) B_rc.
+// Column c of a dot in the layout of the fused step kernels' dots: W real
+// values per row, so a complex column is the pair (re, im) at 2c and a real
+// one the value at c (imaginary part 0).
+template <bool CV>
+__device__ __forceinline__ double2 col_value(const double* d, int c) {
+    if constexpr (CV) return make_double2(d[2 * c], d[2 * c + 1]);
+    return make_double2(d[c], 0.0);
+}
+
+// X_c += alpha_c P_c, R_c -= alpha_c AP_c with alpha_c = rr_c / pap_c (0 for
+// a converged column, |rr_c| < tol2, or a broken-down one, |pap_c| < 1e-14
+// |rr_c|), and rr_out_c = <R_c|R_c> of the updated R: thread (sub, column)
+// of a CTA walks every (subs x gridDim.x)-th row, the CTA sums its rows in
+// a fixed order, and the last CTA to finish (ticket counter) sums the CTA
+// partials in a fixed order and resets the counter.  Deterministic.
 template <typename T, bool CV>
 __global__ void __launch_bounds__(kDotThreads)
-col_dot_partials(const T* __restrict__ A, const T* __restrict__ B, int64_t n_rows, int ncols,
-                 double2* __restrict__ part) {
-    __shared__ double2 red[kDotThreads];
-    const int W = CV ? 2 * ncols : ncols;
+cg_update_kernel(T* __restrict__ X, const T* __restrict__ P, T* __restrict__ R,
+                 const T* __restrict__ AP, const double* __restrict__ rr,
+                 const double* __restrict__ pap, double tol2, int64_t n_rows, int ncols,
+                 double* __restrict__ part, double* __restrict__ rr_out,
+                 unsigned* __restrict__ counter) {
+    __shared__ double red[kDotThreads];
+    __shared__ unsigned ticket;
     const int subs = kDotThreads / ncols;
     const int col = threadIdx.x % ncols, sub = threadIdx.x / ncols;
-    double re = 0.0, im = 0.0;
+    double acc = 0.0;
     if (sub < subs) {
+        const double2 r2 = col_value<CV>(rr, col), q2 = col_value<CV>(pap, col);
+        const double nr = hypot(r2.x, r2.y), np = hypot(q2.x, q2.y);
+        double ar = 0.0, ai = 0.0;
+        if (!(nr < tol2 || np < 1e-14 * nr)) {
+            const double d = q2.x * q2.x + q2.y * q2.y;
+            ar = (r2.x * q2.x + r2.y * q2.y) / d;
+            ai = (r2.y * q2.x - r2.x * q2.y) / d;
+        }
+#pragma unroll 4
         for (int64_t r = int64_t(blockIdx.x) * subs + sub; r < n_rows;
              r += int64_t(gridDim.x) * subs) {
             if constexpr (CV) {
-                const double ar = A[r * W + 2 * col], ai = A[r * W + 2 * col + 1];
-                const double br = B[r * W + 2 * col], bi = B[r * W + 2 * col + 1];
-                re += ar * br + ai * bi;
-                im += ar * bi - ai * br;
+                const int64_t e = r * ncols + col;
+                const double pr = P[2 * e], pi = P[2 * e + 1];
+                const double qr = AP[2 * e], qi = AP[2 * e + 1];
+                X[2 * e] = T(double(X[2 * e]) + (ar * pr - ai * pi));
+                X[2 * e + 1] = T(double(X[2 * e + 1]) + (ar * pi + ai * pr));
+                const T nr_ = T(double(R[2 * e]) - (ar * qr - ai * qi));
+                const T ni_ = T(double(R[2 * e + 1]) - (ar * qi + ai * qr));
+                R[2 * e] = nr_;
+                R[2 * e + 1] = ni_;
+                acc += double(nr_) * double(nr_) + double(ni_) * double(ni_);
             } else {
-                re += double(A[r * W + col]) * double(B[r * W + col]);
+                const int64_t e = r * ncols + col;
+                X[e] = T(double(X[e]) + ar * double(P[e]));
+                const T v = T(double(R[e]) - ar * double(AP[e]));
+                R[e] = v;
+                acc += double(v) * double(v);
             }
         }
     }
-    red[threadIdx.x] = make_double2(re, im);
+    red[threadIdx.x] = acc;
     __syncthreads();
     if (threadIdx.x < ncols) {
-        double sr = 0.0, si = 0.0;
-        for (int q = 0; q < subs; ++q) {
-            sr += red[q * ncols + threadIdx.x].x;
-            si += red[q * ncols + threadIdx.x].y;
+        double t = 0.0;
+        for (int q = 0; q < subs; ++q) t += red[q * ncols + threadIdx.x];
+        part[int64_t(blockIdx.x) * ncols + threadIdx.x] = t;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) ticket = atomicAdd(counter, 1u);
+    __syncthreads();
+    if (ticket != gridDim.x - 1) return;
+    __threadfence();
+    // Eight independent partial sums per thread, so eight L2 loads are in
+    // flight at once (a single chain costs one L2 round trip per CTA).
+    double t8[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    if (sub < subs) {
+        unsigned g = sub;
+        for (; g + 7 * subs < gridDim.x; g += 8 * subs) {
+#pragma unroll
+            for (int u = 0; u < 8; ++u) t8[u] += __ldcg(part + int64_t(g + u * subs) * ncols + col);
         }
-        part[int64_t(blockIdx.x) * ncols + threadIdx.x] = make_double2(sr, si);
+        for (; g < gridDim.x; g += subs) t8[0] += __ldcg(part + int64_t(g) * ncols + col);
     }
-}
-
-__global__ void col_dot_finish(const double2* __restrict__ part, int G, int ncols,
-                               double2* __restrict__ out) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= ncols) return;
-    double sr = 0.0, si = 0.0;
-    for (int g = 0; g < G; ++g) {
-        sr += part[int64_t(g) * ncols + c].x;
-        si += part[int64_t(g) * ncols + c].y;
-    }
-    out[c] = make_double2(sr, si);
-}
-
-// alpha_c = rr_c / pap_c, or 0 for a converged or broken-down column.
-__global__ void cg_alpha_kernel(const double2* __restrict__ rr, const double2* __restrict__ pap,
-                                int ncols, double tol2, double2* __restrict__ alpha) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= ncols) return;
-    const double nr = hypot(rr[c].x, rr[c].y), np = hypot(pap[c].x, pap[c].y);
-    if (nr < tol2 || np < 1e-14 * nr) {
-        alpha[c] = make_double2(0.0, 0.0);
-        return;
-    }
-    const double d = pap[c].x * pap[c].x + pap[c].y * pap[c].y;
-    alpha[c] = make_double2((rr[c].x * pap[c].x + rr[c].y * pap[c].y) / d,
-                            (rr[c].y * pap[c].x - rr[c].x * pap[c].y) / d);
-}
-
-// X_c += alpha_c P_c, R_c -= alpha_c AP_c.  One thread per (row, column).
-template <typename T, bool CV>
-__global__ void cg_update_kernel(T* __restrict__ X, const T* __restrict__ P, T* __restrict__ R,
-                                 const T* __restrict__ AP, const double2* __restrict__ alpha,
-                                 int64_t n_elems, int ncols) {
-    for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < n_elems;
-         e += int64_t(gridDim.x) * blockDim.x) {
-        const double2 a = alpha[e % ncols];
+    red[threadIdx.x] = ((t8[0] + t8[1]) + (t8[2] + t8[3])) + ((t8[4] + t8[5]) + (t8[6] + t8[7]));
+    __syncthreads();
+    if (threadIdx.x < ncols) {
+        double u = 0.0;
+        for (int q = 0; q < subs; ++q) u += red[q * ncols + threadIdx.x];
         if constexpr (CV) {
-            const double pr = P[2 * e], pi = P[2 * e + 1];
-            const double qr = AP[2 * e], qi = AP[2 * e + 1];
-            X[2 * e] = T(double(X[2 * e]) + (a.x * pr - a.y * pi));
-            X[2 * e + 1] = T(double(X[2 * e + 1]) + (a.x * pi + a.y * pr));
-            R[2 * e] = T(double(R[2 * e]) - (a.x * qr - a.y * qi));
-            R[2 * e + 1] = T(double(R[2 * e + 1]) - (a.x * qi + a.y * qr));
+            rr_out[2 * threadIdx.x] = u;
+            rr_out[2 * threadIdx.x + 1] = 0.0;
         } else {
-            X[e] = T(double(X[e]) + a.x * double(P[e]));
-            R[e] = T(double(R[e]) - a.x * double(AP[e]));
+            rr_out[threadIdx.x] = u;
         }
     }
+    if (threadIdx.x == 0) *counter = 0u;  // ready for the next launch
 }
 
 // beta_c = rr_new_c / rr_old_c (0 when rr_old_c vanishes); P_c = R_c + beta_c P_c.
 template <typename T, bool CV>
 __global__ void cg_direction_kernel(T* __restrict__ P, const T* __restrict__ R,
-                                    const double2* __restrict__ rr_old,
-                                    const double2* __restrict__ rr_new, int64_t n_elems,
+                                    const double* __restrict__ rr_old,
+                                    const double* __restrict__ rr_new, int64_t n_elems,
                                     int ncols) {
     for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < n_elems;
          e += int64_t(gridDim.x) * blockDim.x) {
         const int c = int(e % ncols);
-        const double2 o = rr_old[c], n = rr_new[c];
+        const double2 o = col_value<CV>(rr_old, c), n = col_value<CV>(rr_new, c);
         double br = 0.0, bi = 0.0;
         if (hypot(o.x, o.y) >= 1e-300) {
             const double d = o.x * o.x + o.y * o.y;
@@ -140,6 +157,24 @@ __global__ void cg_direction_kernel(T* __restrict__ P, const T* __restrict__ R,
             P[2 * e + 1] = T(double(R[2 * e + 1]) + (br * pi + bi * pr));
         } else {
             P[e] = T(double(R[e]) + br * double(P[e]));
+        }
+    }
+}
+
+// Y += c X with the complex coefficient c = (cr, ci) over n complex values
+// (cv), or Y += Re(c) X over n real values (Chebyshev's CoeffCast for a real
+// scalar type, rsatb/calc/cheby.hpp:113-121).
+template <typename T>
+__global__ void coeff_axpy_kernel(int64_t n, bool cv, double cr, double ci,
+                                  const T* __restrict__ X, T* __restrict__ Y) {
+    for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < n;
+         e += int64_t(gridDim.x) * blockDim.x) {
+        if (cv) {
+            const double xr = double(X[2 * e]), xi = double(X[2 * e + 1]);
+            Y[2 * e] = T(double(Y[2 * e]) + cr * xr - ci * xi);
+            Y[2 * e + 1] = T(double(Y[2 * e + 1]) + cr * xi + ci * xr);
+        } else {
+            Y[e] = T(double(Y[e]) + cr * double(X[e]));
         }
     }
 }
@@ -163,13 +198,15 @@ struct SolveWork {
     void* u2;   // S Z p
     void* Yp;   // solution of the preconditioned system
     void* Bp;   // its right-hand side Z^H b
-    double2* part;
-    double2* d_rr;
-    double2* d_rr2;
-    double2* d_pap;
-    double2* d_alpha;
-    double2* d_dot;
-    int grid;  // dot CTAs
+    // Dots in the step kernels' layout (W doubles per dot; see col_value).
+    double* part;     // CTA partials, sm_count x 8 x 2 x W
+    double* d_rr;
+    double* d_rr2;
+    double* d_pap;
+    double* d_dot;    // [dot_slots][W]
+    unsigned* counter;
+    unsigned* fault;
+    int grid;  // CTAs of the update kernel
 };
 
 struct SolveCall {
@@ -186,21 +223,30 @@ unsigned elem_grid(const SolveCall& s, int64_t n) {
                                                            int64_t(s.ctx->sm_count) * 8)));
 }
 
-template <typename T, bool CV>
-int dots_t(const SolveCall& s, const SolveWork& w, const void* A, const void* B, double2* out) {
-    col_dot_partials<T, CV><<<w.grid, kDotThreads, 0, s.ctx->stream>>>(
-        static_cast<const T*>(A), static_cast<const T*>(B), s.n_rows, s.ncols, w.part);
-    RSATB_LAUNCH_CHECK(s.ctx);
-    col_dot_finish<<<(s.ncols + 127) / 128, 128, 0, s.ctx->stream>>>(w.part, w.grid, s.ncols, out);
-    RSATB_LAUNCH_CHECK(s.ctx);
-    return RSATB_SUCCESS;
+// out[0..W) = per-column <A|B> in the step kernels' layout.
+int dots(const SolveCall& s, const SolveWork& w, const void* A, const void* B, double* out) {
+    StepArgs a{};
+    a.W = s.W;
+    a.x = A;
+    a.in = B;
+    a.partials = w.part;
+    a.dots_out = out;
+    a.counter = w.counter;
+    a.fault = w.fault;
+    return run_coldot(s.ctx, s.vdt, s.n_rows, a);
 }
 
-int dots(const SolveCall& s, const SolveWork& w, const void* A, const void* B, double2* out) {
+int coeff_axpy(const SolveCall& s, double cr, double ci, const void* X, void* Y) {
     const bool cv = dtype_is_complex(s.vdt);
+    const int64_t n = s.n_rows * s.W / (cv ? 2 : 1);
     if (dtype_is_double(s.vdt))
-        return cv ? dots_t<double, true>(s, w, A, B, out) : dots_t<double, false>(s, w, A, B, out);
-    return cv ? dots_t<float, true>(s, w, A, B, out) : dots_t<float, false>(s, w, A, B, out);
+        coeff_axpy_kernel<double><<<elem_grid(s, n), 256, 0, s.ctx->stream>>>(
+            n, cv, cr, ci, static_cast<const double*>(X), static_cast<double*>(Y));
+    else
+        coeff_axpy_kernel<float><<<elem_grid(s, n), 256, 0, s.ctx->stream>>>(
+            n, cv, cr, ci, static_cast<const float*>(X), static_cast<float*>(Y));
+    RSATB_LAUNCH_CHECK(s.ctx);
+    return RSATB_SUCCESS;
 }
 
 int axpby(const SolveCall& s, double a, const void* X, double b, void* Y) {
@@ -216,18 +262,19 @@ int axpby(const SolveCall& s, double a, const void* X, double b, void* Y) {
 }
 
 template <typename T, bool CV>
-int update_t(const SolveCall& s, const SolveWork& w, void* X) {
-    const int64_t n = s.n_rows * s.ncols;
-    cg_update_kernel<T, CV><<<elem_grid(s, n), 256, 0, s.ctx->stream>>>(
+int update_t(const SolveCall& s, const SolveWork& w, void* X, const double* rr, double tol2,
+             double* rr_out) {
+    cg_update_kernel<T, CV><<<w.grid, kDotThreads, 0, s.ctx->stream>>>(
         static_cast<T*>(X), static_cast<const T*>(w.P), static_cast<T*>(w.R),
-        static_cast<const T*>(w.AP), w.d_alpha, n, s.ncols);
+        static_cast<const T*>(w.AP), rr, w.d_pap, tol2, s.n_rows, s.ncols, w.part, rr_out,
+        w.counter);
     RSATB_LAUNCH_CHECK(s.ctx);
     return RSATB_SUCCESS;
 }
 
 template <typename T, bool CV>
-int direction_t(const SolveCall& s, const SolveWork& w, const double2* rr_old,
-                const double2* rr_new) {
+int direction_t(const SolveCall& s, const SolveWork& w, const double* rr_old,
+                const double* rr_new) {
     const int64_t n = s.n_rows * s.ncols;
     cg_direction_kernel<T, CV><<<elem_grid(s, n), 256, 0, s.ctx->stream>>>(
         static_cast<T*>(w.P), static_cast<const T*>(w.R), rr_old, rr_new, n, s.ncols);
@@ -235,14 +282,17 @@ int direction_t(const SolveCall& s, const SolveWork& w, const double2* rr_old,
     return RSATB_SUCCESS;
 }
 
-int update(const SolveCall& s, const SolveWork& w, void* X) {
+int update(const SolveCall& s, const SolveWork& w, void* X, const double* rr, double tol2,
+           double* rr_out) {
     const bool cv = dtype_is_complex(s.vdt);
     if (dtype_is_double(s.vdt))
-        return cv ? update_t<double, true>(s, w, X) : update_t<double, false>(s, w, X);
-    return cv ? update_t<float, true>(s, w, X) : update_t<float, false>(s, w, X);
+        return cv ? update_t<double, true>(s, w, X, rr, tol2, rr_out)
+                  : update_t<double, false>(s, w, X, rr, tol2, rr_out);
+    return cv ? update_t<float, true>(s, w, X, rr, tol2, rr_out)
+              : update_t<float, false>(s, w, X, rr, tol2, rr_out);
 }
 
-int direction(const SolveCall& s, const SolveWork& w, const double2* o, const double2* n) {
+int direction(const SolveCall& s, const SolveWork& w, const double* o, const double* n) {
     const bool cv = dtype_is_complex(s.vdt);
     if (dtype_is_double(s.vdt))
         return cv ? direction_t<double, true>(s, w, o, n) : direction_t<double, false>(s, w, o, n);
@@ -264,13 +314,28 @@ StepArgs plain_args(int W, const void* in, void* y) {
 }
 
 // out = S in, or Z^H S Z in when a symmetric preconditioner Z is given
-// (SymPrecondMat::mult_dense, rsatb/calc/preconditioner.hpp:249-262).
+// (SymPrecondMat::mult_dense, rsatb/calc/preconditioner.hpp:249-262).  With
+// dot_out, the last step also writes <in|out> per column there.
 int apply_A(const SolveCall& s, const SolveWork& w, const rsatb_bsr_matrix* S,
-            const rsatb_bsr_matrix* Z, const rsatb_bsr_matrix* ZH, const void* in, void* out) {
-    if (!Z) return run_step(s.ctx, S, s.vdt, plain_args(s.W, in, out));
+            const rsatb_bsr_matrix* Z, const rsatb_bsr_matrix* ZH, const void* in, void* out,
+            double* dot_out = nullptr) {
+    StepArgs last = plain_args(s.W, nullptr, out);
+    last.fault = w.fault;
+    if (dot_out) {
+        last.dot_mode = DOT_PLAIN;
+        last.psi0 = in;
+        last.partials = w.part;
+        last.dots_out = dot_out;
+        last.counter = w.counter;
+    }
+    if (!Z) {
+        last.in = in;
+        return run_step(s.ctx, S, s.vdt, last);
+    }
     RSATB_TRY(run_step(s.ctx, Z, s.vdt, plain_args(s.W, in, w.u1)));
     RSATB_TRY(run_step(s.ctx, S, s.vdt, plain_args(s.W, w.u1, w.u2)));
-    return run_step(s.ctx, ZH, s.vdt, plain_args(s.W, w.u2, out));
+    last.in = w.u2;
+    return run_step(s.ctx, ZH, s.vdt, last);
 }
 
 // Batched CG for A X = B from X's contents (solver.hpp:216-312), A = S or
@@ -283,29 +348,56 @@ int cg_core(const SolveCall& s, const SolveWork& w, const rsatb_bsr_matrix* S,
     RSATB_CUDA_TRY(cudaMemcpyAsync(w.R, B, s.vbytes, cudaMemcpyDeviceToDevice, s.ctx->stream));
     RSATB_TRY(axpby(s, -1.0, w.AP, 1.0, w.R));
     RSATB_CUDA_TRY(cudaMemcpyAsync(w.P, w.R, s.vbytes, cudaMemcpyDeviceToDevice, s.ctx->stream));
-    double2* rr = w.d_rr;
-    double2* rr_new = w.d_rr2;
+    double* rr = w.d_rr;
+    double* rr_new = w.d_rr2;
     RSATB_TRY(dots(s, w, w.R, w.R, rr));
-    std::vector<double2> h(s.ncols);
+    // The column residuals of iteration k are copied to pinned memory and
+    // read after iteration k + 1 has been queued, so the device never waits
+    // for the host's test.  A column whose residual is below tol is frozen
+    // by the alpha kernel (alpha = 0: X and R unchanged), so once every
+    // column has converged the extra queued iteration changes nothing and
+    // the result equals a test after every iteration.
+    const bool cv = dtype_is_complex(s.vdt);
+    const int dw = cv ? 2 * s.ncols : s.ncols;  // doubles per dot
+    void* pin = nullptr;
+    RSATB_TRY(ctx_pinned(s.ctx, 2 * sizeof(double) * dw, &pin));
+    double* hbuf[2] = {static_cast<double*>(pin), static_cast<double*>(pin) + dw};
+    cudaEvent_t ev[2];
+    RSATB_CUDA_TRY(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
+    const cudaError_t e_ev = cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming);
+    if (e_ev != cudaSuccess) cudaEventDestroy(ev[0]);
+    RSATB_CUDA_TRY(e_ev);
+    struct EvG {
+        cudaEvent_t* e;
+        ~EvG() {
+            cudaEventDestroy(e[0]);
+            cudaEventDestroy(e[1]);
+        }
+    } evg{ev};
     int it = 0;
     double max_err = 0.0;
-    for (int k = 0; k < max_iter; ++k) {
-        RSATB_TRY(apply_A(s, w, S, Z, ZH, w.P, w.AP));
-        RSATB_TRY(dots(s, w, w.P, w.AP, w.d_pap));
-        cg_alpha_kernel<<<(s.ncols + 127) / 128, 128, 0, s.ctx->stream>>>(rr, w.d_pap, s.ncols,
-                                                                         tol * tol, w.d_alpha);
-        RSATB_LAUNCH_CHECK(s.ctx);
-        RSATB_TRY(update(s, w, X));
-        RSATB_TRY(dots(s, w, w.R, w.R, rr_new));
-        RSATB_CUDA_TRY(cudaMemcpyAsync(h.data(), rr_new, sizeof(double2) * s.ncols,
-                                       cudaMemcpyDeviceToHost, s.ctx->stream));
-        RSATB_CUDA_TRY(cudaStreamSynchronize(s.ctx->stream));
+    bool done = false;
+    auto read = [&](int k) -> int {  // the test of iteration k (already queued)
+        RSATB_CUDA_TRY(cudaEventSynchronize(ev[k & 1]));
         max_err = 0.0;
-        for (const double2& v : h) max_err = std::max(max_err, std::sqrt(std::hypot(v.x, v.y)));
+        const double* h = hbuf[k & 1];
+        for (int c = 0; c < s.ncols; ++c)
+            max_err = std::max(max_err, std::sqrt(cv ? std::hypot(h[2 * c], h[2 * c + 1])
+                                                     : std::fabs(h[c])));
         it = k + 1;
-        if (!(max_err >= tol)) break;  // converged (or NaN: stop and report it)
+        done = !(max_err >= tol);  // converged (or NaN: stop and report it)
+        return RSATB_SUCCESS;
+    };
+    for (int k = 0; k < max_iter && !done; ++k) {
+        RSATB_TRY(apply_A(s, w, S, Z, ZH, w.P, w.AP, w.d_pap));
+        RSATB_TRY(update(s, w, X, rr, tol * tol, rr_new));
+        RSATB_CUDA_TRY(cudaMemcpyAsync(hbuf[k & 1], rr_new, sizeof(double) * dw,
+                                       cudaMemcpyDeviceToHost, s.ctx->stream));
+        RSATB_CUDA_TRY(cudaEventRecord(ev[k & 1], s.ctx->stream));
         RSATB_TRY(direction(s, w, rr, rr_new));
         std::swap(rr, rr_new);
+        if (k > 0) RSATB_TRY(read(k - 1));
+        if (!done && k + 1 == max_iter) RSATB_TRY(read(k));
     }
     if (iters_out) *iters_out += it;
     if (resid_out) *resid_out = std::max(*resid_out, max_err);
@@ -328,7 +420,7 @@ int cg_solve(const SolveCall& s, const SolveWork& w, const rsatb_bsr_matrix* S,
 }
 
 int solve_setup(rsatb_context* ctx, const rsatb_bsr_matrix* S, int vdt, int n_vectors,
-                int extra_panels, SolveCall* s, SolveWork* w, void** panels) {
+                int extra_panels, SolveCall* s, SolveWork* w, void** panels, int dot_slots = 1) {
     RSATB_TRY(check_bsr(S, "S"));
     if (S->n_block_rows != S->n_block_cols)
         return set_error(RSATB_INVALID_ARGUMENT, "S must be square");
@@ -349,12 +441,18 @@ int solve_setup(rsatb_context* ctx, const rsatb_bsr_matrix* S, int vdt, int n_ve
     const size_t vb = (s->vbytes + 255) & ~size_t(255);
     const int subs = kDotThreads / n_vectors;
     w->grid = int(std::max<int64_t>(1, std::min<int64_t>((s->n_rows + subs - 1) / subs,
-                                                         int64_t(ctx->sm_count) * 4)));
-    const size_t part_b = ((sizeof(double2) * size_t(w->grid) * n_vectors) + 255) & ~size_t(255);
-    const size_t col_b = ((sizeof(double2) * n_vectors) + 255) & ~size_t(255);
+                                                         int64_t(ctx->sm_count) * 2)));
+    // CTA partials of the fused step kernels' dots (at most sm_count x 8
+    // CTAs, two dots of W values) and of the update kernel (grid x R).
+    const size_t part_b =
+        (sizeof(double) * std::max(size_t(ctx->sm_count) * 8 * 2 * s->W,
+                                   size_t(w->grid) * n_vectors) + 255) & ~size_t(255);
+    const size_t col_b = ((sizeof(double) * s->W) + 255) & ~size_t(255);
     const int n_panels = 8 + extra_panels;
     void* base = nullptr;
-    RSATB_TRY(ctx_scratch(ctx, n_panels * vb + part_b + 5 * col_b, &base));
+    RSATB_TRY(ctx_scratch(ctx, n_panels * vb + part_b + (3 + dot_slots) * col_b, &base));
+    RSATB_TRY(ctx_counters(ctx, 1, &w->counter));
+    RSATB_TRY(ctx_fault_word(ctx, &w->fault));
     char* p = static_cast<char*>(base);
     w->R = p;
     w->P = p + vb;
@@ -366,13 +464,12 @@ int solve_setup(rsatb_context* ctx, const rsatb_bsr_matrix* S, int vdt, int n_ve
     w->Bp = p + 7 * vb;
     for (int i = 0; i < extra_panels; ++i) panels[i] = p + (8 + i) * vb;
     char* q = p + n_panels * vb;
-    w->part = reinterpret_cast<double2*>(q);
+    w->part = reinterpret_cast<double*>(q);
     q += part_b;
-    w->d_rr = reinterpret_cast<double2*>(q);
-    w->d_rr2 = reinterpret_cast<double2*>(q + col_b);
-    w->d_pap = reinterpret_cast<double2*>(q + 2 * col_b);
-    w->d_alpha = reinterpret_cast<double2*>(q + 3 * col_b);
-    w->d_dot = reinterpret_cast<double2*>(q + 4 * col_b);
+    w->d_rr = reinterpret_cast<double*>(q);
+    w->d_rr2 = reinterpret_cast<double*>(q + col_b);
+    w->d_pap = reinterpret_cast<double*>(q + 2 * col_b);
+    w->d_dot = reinterpret_cast<double*>(q + 3 * col_b);
     return RSATB_SUCCESS;
 }
 
@@ -420,6 +517,69 @@ int apply_solve(const SolveCall& s, const SolveWork& w, const rsatb_cheb_op* op,
 
 }  // namespace
 
+// Y = scale * S^-1 V X (NORMAL: V X is the CG's target and initial guess)
+// or scale * V S^-1 X (adjoint: the solve from zero), Chebyshev::apply_dual
+// for the Solve form (rsatb/calc/cheby.hpp:270-287).
+int solve_form_apply_dual(rsatb_context* ctx, const rsatb_cheb_op* op,
+                          const rsatb_bsr_matrix* V, const void* X, void* Y, int n_vectors,
+                          int vdt, double scale, bool adjoint) {
+    RSATB_TRY(check_solve_op(op, vdt));
+    RSATB_TRY(check_bsr(V, "V"));
+    if (V->n_block_rows != op->H->n_block_rows || V->block_size != op->H->block_size)
+        return set_error(RSATB_INVALID_ARGUMENT, "V and H sizes differ");
+    SolveCall s{};
+    SolveWork w{};
+    void* t[1] = {nullptr};
+    RSATB_TRY(solve_setup(ctx, op->S, vdt, n_vectors, 1, &s, &w, t));
+    int iters = 0;
+    double resid = 0.0;
+    if (!adjoint) {
+        RSATB_TRY(run_step(ctx, V, vdt, plain_args(s.W, X, Y)));  // Y = V X
+        RSATB_CUDA_TRY(cudaMemcpyAsync(t[0], Y, s.vbytes, cudaMemcpyDeviceToDevice, ctx->stream));
+        RSATB_TRY(cg_solve(s, w, op->S, op->Z, op->ZH, t[0], Y, op_tol(op), op_iters(op), &iters,
+                           &resid));
+    } else {
+        RSATB_CUDA_TRY(cudaMemsetAsync(t[0], 0, s.vbytes, ctx->stream));
+        RSATB_TRY(cg_solve(s, w, op->S, op->Z, op->ZH, X, t[0], op_tol(op), op_iters(op), &iters,
+                           &resid));
+        RSATB_TRY(run_step(ctx, V, vdt, plain_args(s.W, t[0], Y)));  // Y = V S^-1 X
+    }
+    return axpby(s, 0.0, X, scale, Y);
+}
+
+// Y = sum_n c_n T_n(Op~) X with Op~ = (S^-1 H - c) / hw, one CG per
+// application (Chebyshev::propagate, rsatb/calc/cheby.hpp:399-441): each
+// solve starts from the contents of its output panel, which after the
+// rotation holds T_{n-3} (the first two from zero).
+int solve_form_propagate(rsatb_context* ctx, const rsatb_cheb_op* op, const void* X, void* Y,
+                         int n_vectors, int vdt, const double* coeffs, int n_coeffs) {
+    RSATB_TRY(check_solve_op(op, vdt));
+    SolveCall s{};
+    SolveWork w{};
+    void* t[3] = {nullptr, nullptr, nullptr};
+    RSATB_TRY(solve_setup(ctx, op->S, vdt, n_vectors, 3, &s, &w, t));
+    RSATB_CUDA_TRY(cudaMemcpyAsync(t[0], X, s.vbytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    RSATB_CUDA_TRY(cudaMemsetAsync(t[1], 0, s.vbytes, ctx->stream));
+    RSATB_CUDA_TRY(cudaMemsetAsync(t[2], 0, s.vbytes, ctx->stream));
+    RSATB_CUDA_TRY(cudaMemsetAsync(Y, 0, s.vbytes, ctx->stream));
+    RSATB_TRY(coeff_axpy(s, coeffs[0], coeffs[1], t[0], Y));
+    if (n_coeffs == 1) return RSATB_SUCCESS;
+    int iters = 0;
+    double resid = 0.0;
+    RSATB_TRY(apply_solve(s, w, op, t[0], t[1], &iters, &resid));
+    RSATB_TRY(coeff_axpy(s, coeffs[2], coeffs[3], t[1], Y));
+    for (int n = 2; n < n_coeffs; ++n) {
+        RSATB_TRY(apply_solve(s, w, op, t[1], t[2], &iters, &resid));
+        RSATB_TRY(axpby(s, -1.0, t[0], 2.0, t[2]));
+        RSATB_TRY(coeff_axpy(s, coeffs[2 * n], coeffs[2 * n + 1], t[2], Y));
+        void* old0 = t[0];
+        t[0] = t[1];
+        t[1] = t[2];
+        t[2] = old0;
+    }
+    return RSATB_SUCCESS;
+}
+
 // Entry points behind rsatb_cheb_apply_op and rsatb_kpm_dos_moments for
 // the Solve form.
 int solve_form_apply(rsatb_context* ctx, const rsatb_cheb_op* op, const void* X, void* Y,
@@ -440,25 +600,35 @@ int solve_form_moments(rsatb_context* ctx, const rsatb_cheb_op* op, const void* 
     SolveCall s{};
     SolveWork w{};
     void* t[3] = {nullptr, nullptr, nullptr};
-    RSATB_TRY(solve_setup(ctx, op->S, vdt, n_vectors, 3, &s, &w, t));
+    // One dot slot per moment on the device, read back once at the end.
+    RSATB_TRY(solve_setup(ctx, op->S, vdt, n_vectors, 3, &s, &w, t, n_moments));
     const int R = n_vectors;
-    std::vector<double2> h(R);
+    const size_t slot = ((sizeof(double) * s.W) + 255) & ~size_t(255);
     auto record = [&](int n, const void* a, const void* b) -> int {
-        RSATB_TRY(dots(s, w, a, b, w.d_dot));
-        RSATB_CUDA_TRY(cudaMemcpyAsync(h.data(), w.d_dot, sizeof(double2) * R,
+        return dots(s, w, a, b,
+                    reinterpret_cast<double*>(reinterpret_cast<char*>(w.d_dot) + n * slot));
+    };
+    auto finish = [&]() -> int {
+        std::vector<double> h(slot / sizeof(double) * size_t(n_moments));
+        RSATB_CUDA_TRY(cudaMemcpyAsync(h.data(), w.d_dot, slot * size_t(n_moments),
                                        cudaMemcpyDeviceToHost, ctx->stream));
         RSATB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-        double sr = 0.0, si = 0.0;
-        for (int c = 0; c < R; ++c) {
-            sr += h[c].x;
-            si += h[c].y;
-            if (col_mu_out) {
-                col_mu_out[2 * (size_t(n) * R + c)] = h[c].x;
-                col_mu_out[2 * (size_t(n) * R + c) + 1] = h[c].y;
+        const bool cv = dtype_is_complex(vdt);
+        for (int n = 0; n < n_moments; ++n) {
+            const double* d = h.data() + n * (slot / sizeof(double));
+            double sr = 0.0, si = 0.0;
+            for (int c = 0; c < R; ++c) {
+                const double re = cv ? d[2 * c] : d[c], im = cv ? d[2 * c + 1] : 0.0;
+                sr += re;
+                si += im;
+                if (col_mu_out) {
+                    col_mu_out[2 * (size_t(n) * R + c)] = re;
+                    col_mu_out[2 * (size_t(n) * R + c) + 1] = im;
+                }
             }
+            mu_out[2 * n] = sr / R;
+            mu_out[2 * n + 1] = si / R;
         }
-        mu_out[2 * n] = sr / R;
-        mu_out[2 * n + 1] = si / R;
         return RSATB_SUCCESS;
     };
     // t0 = psi, t1 = t2 = 0 (the first solves start from zero).
@@ -466,7 +636,7 @@ int solve_form_moments(rsatb_context* ctx, const rsatb_cheb_op* op, const void* 
     RSATB_CUDA_TRY(cudaMemsetAsync(t[1], 0, s.vbytes, ctx->stream));
     RSATB_CUDA_TRY(cudaMemsetAsync(t[2], 0, s.vbytes, ctx->stream));
     RSATB_TRY(record(0, psi, psi));
-    if (n_moments == 1) return RSATB_SUCCESS;
+    if (n_moments == 1) return finish();
     int iters = 0;
     double resid = 0.0;
     RSATB_TRY(apply_solve(s, w, op, t[0], t[1], &iters, &resid));
@@ -482,7 +652,7 @@ int solve_form_moments(rsatb_context* ctx, const rsatb_cheb_op* op, const void* 
         t[1] = t[2];
         t[2] = old0;
     }
-    return RSATB_SUCCESS;
+    return finish();
 }
 
 }  // namespace rsatb_b200

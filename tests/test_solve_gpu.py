@@ -99,7 +99,7 @@ def test_solve_form_moments_match_oracle(torch_cuda, diamond, cg_tol, tol):
     assert np.abs(mu.imag).max() == 0.0
 
 
-def test_solve_form_refuses_doubling_and_other_entries(torch_cuda, diamond):
+def test_solve_form_refuses_doubling(torch_cuda, diamond):
     torch = torch_cuda
     from rsatb_b200._capi import RsatbError
     from rsatb_b200.calc import Chebyshev, _moments
@@ -108,9 +108,6 @@ def test_solve_form_refuses_doubling_and_other_entries(torch_cuda, diamond):
     psi = torch.ones(Hd.shape[0], 2, dtype=torch.float64, device="cuda")
     with pytest.raises(RsatbError):
         _moments(c, psi, 8, doubled=True)
-    Y = torch.empty_like(psi)
-    with pytest.raises(RsatbError):
-        c.propagate(psi, Y, [1.0, 0.5])
 
 
 def _factor(S):
@@ -152,3 +149,52 @@ def test_preconditioned_solve_form_moments(torch_cuda, diamond):
                                           (emax + emin) / 2, (emax - emin) / 2, 32)
     assert np.abs(mu.real - want).max() < 1e-9 * abs(want[0])
 
+
+
+@pytest.mark.parametrize("preconditioned", [False, True])
+def test_solve_form_apply_dual_and_propagate(torch_cuda, diamond, preconditioned):
+    """Chebyshev::apply_dual for the Solve form: scale S^-1 V X (NORMAL)
+    and scale V S^-1 X (ADJOINT); propagate: sum_n c_n T_n(Op~) X with
+    Op~ = (S^-1 H - c) / hw and complex coefficients, one CG per
+    application; against dense FP64 solves, with the plain and the
+    Z-preconditioned CG (CG tolerance 1e-12)."""
+    torch = torch_cuda
+    from rsatb_b200.calc import ChebyMode, Chebyshev, ISQRTMPreconditioner
+    from rsatb_b200.isqrt import graph_inverse_sqrt
+    from rsatb_b200.lattice import BsrArrays
+    H, S, Hd, Sd, emin, emax = diamond
+    rng = np.random.default_rng(6)
+    v = rng.standard_normal(H.values.shape)
+    Vd = BsrArrays(H.row_ptr, H.col_ind, v, 8).to_dense()
+    Vd = 0.5 * (Vd + Vd.T)
+    rows = np.repeat(np.arange(H.n_block_rows), np.diff(H.row_ptr))
+    vv = np.stack([Vd[i * 8:(i + 1) * 8, j * 8:(j + 1) * 8] for i, j in zip(rows, H.col_ind)])
+    V = _dev(BsrArrays(H.row_ptr, H.col_ind, vv, 8))
+    pre = None
+    if preconditioned:
+        Z = graph_inverse_sqrt(S)
+        pre = ISQRTMPreconditioner(_dev(Z))
+    c = Chebyshev(_dev(H), emin, emax, preconditioner=pre, overlap=_dev(S), cg_tol=1e-12)
+    X = rng.standard_normal((H.n_rows, 4))
+    Xd = torch.as_tensor(X).cuda()
+    Y = torch.zeros_like(Xd)
+    c.apply_dual(V, Xd, Y, scale=0.7)
+    assert rel_err(Y.cpu().numpy(), 0.7 * np.linalg.solve(Sd, Vd @ X)) < 1e-9
+    Y.zero_()
+    c.apply_dual(V, Xd, Y, mode=ChebyMode.ADJOINT, scale=0.7)
+    assert rel_err(Y.cpu().numpy(), 0.7 * Vd @ np.linalg.solve(Sd, X)) < 1e-9
+    coeffs = np.array([0.3 - 0.1j, -0.2 + 0.4j, 0.15, 0.05j, -0.07 + 0.02j])
+    Xc = (X + 1j * rng.standard_normal(X.shape)).astype(np.complex128)
+    Pc = torch.as_tensor(Xc).cuda()
+    out = torch.zeros_like(Pc)
+    c.propagate(Pc, out, coeffs)
+    cen, hw = (emax + emin) / 2, (emax - emin) / 2
+    At = (np.linalg.solve(Sd, Hd) - cen * np.eye(Hd.shape[0])) / hw
+    t0, t1 = Xc, At @ Xc
+    want = coeffs[0] * t0 + coeffs[1] * t1
+    for n in range(2, coeffs.size):
+        t0, t1 = t1, 2 * At @ t1 - t0
+        want = want + coeffs[n] * t1
+    assert rel_err(out.cpu().numpy(), want) < 1e-8
+    with pytest.raises(NotImplementedError):
+        c.propagate(Pc, out, coeffs, mode=ChebyMode.ADJOINT)
