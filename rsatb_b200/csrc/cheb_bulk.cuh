@@ -18,7 +18,13 @@
 //    XG = false brings X_j through the ring as well (measured slower: every
 //    X byte then crosses shared memory twice);
 //  * the FMAs are issued as packed pairs (fma.rn.f32x2), half the issue
-//    slots of scalar FMAs at the same per-output operation order.
+//    slots of scalar FMAs at the same per-output operation order;
+//  * DUP: after its stage lands, the warp rewrites its A blocks in shared
+//    memory transposed and with every value twice, [c][r] as (a, a) pairs,
+//    so one 128-bit load gives the packed operands {a_rc, a_rc} and
+//    {a_r+1,c, a_r+1,c} of two rows: a quarter of the 32-bit loads of the
+//    row-major slot, and no register moves to build the broadcast pairs
+//    (the arithmetic, and so every result bit, is the same).
 //
 // Every mbarrier wait is bounded by the global timer; a wait that gives up
 // poisons the dots with NaN, sets *fault and leaves the loop.  The epilogue
@@ -46,18 +52,44 @@ struct BulkShape {
     static constexpr int STAGE = S * ASLOT + (XG ? 0 : S * XSLOT);
     static constexpr int XBASE = S * ASLOT;
     static constexpr unsigned BYTES = 256u + (XG ? 0u : unsigned(32 * W));  // per block row
+    // DUP slot (floats): 8 columns c of 20 (8 pairs + 4 pad: rows 16-byte
+    // aligned, the pair stores of a warp spread over the banks), + 4 pad so
+    // the S slots of a warp start in different banks.
+    static constexpr int DROW = 20;
+    static constexpr int DSLOT = 8 * DROW + 4;
 };
 
-// Shared memory of one CTA: the warps' rings, then the per-thread FP64 dot
-// partials [threads][16] (d0 of both column groups, then d1).
+// Shared memory of one CTA: the warps' rings, the per-thread FP64 dot
+// partials [threads][16] (d0 of both column groups, then d1), then the
+// warps' DUP slots.
 template <int W, bool XG, int NS>
-constexpr size_t bulk_smem_bytes() {
+constexpr size_t bulk_dup_offset() {
     return size_t(kBulkWarps) * NS * BulkShape<W, XG>::STAGE +
            size_t(kBulkWarps) * 32 * 16 * sizeof(double);
 }
+template <int W, bool XG, int NS>
+constexpr size_t bulk_smem_bytes() {
+    return bulk_dup_offset<W, XG, NS>() +
+           size_t(kBulkWarps) * BulkShape<W, XG>::S * BulkShape<W, XG>::DSLOT * sizeof(float);
+}
 
-// MINB: resident CTAs per SM the register budget is sized for.
-template <int W, bool CV, int NS, bool XG, int MINB>
+// (d0, d1) += (a0, a1) * (b0, b1) as one fma.rn.f32x2 (a0 = a1 for a
+// broadcast A value held as a register pair).
+__device__ __forceinline__ void fma2p(float& d0, float& d1, float a0, float a1, float b0,
+                                      float b1) {
+    asm("{\n\t.reg .b64 ra, rb, rd;\n\t"
+        "mov.b64 ra, {%2, %3};\n\t"
+        "mov.b64 rb, {%4, %5};\n\t"
+        "mov.b64 rd, {%0, %1};\n\t"
+        "fma.rn.f32x2 rd, ra, rb, rd;\n\t"
+        "mov.b64 {%0, %1}, rd;\n\t}"
+        : "+f"(d0), "+f"(d1)
+        : "f"(a0), "f"(a1), "f"(b0), "f"(b1));
+}
+
+// MINB: resident CTAs per SM the register budget is sized for; DUP: A read
+// from the transposed, duplicated slot (see above).
+template <int W, bool CV, int NS, bool XG, int MINB, bool DUP>
 __global__ void __launch_bounds__(kBulkWarps * 32, MINB) cheb_step_bulk(StepArgs a) {
     using Sh = BulkShape<W, XG>;
     constexpr int G = Sh::G, S = Sh::S;
@@ -68,6 +100,8 @@ __global__ void __launch_bounds__(kBulkWarps * 32, MINB) cheb_step_bulk(StepArgs
     unsigned char* ring = smem + size_t(warp) * NS * Sh::STAGE;
     double* dsm = reinterpret_cast<double*>(smem + size_t(kBulkWarps) * NS * Sh::STAGE) +
                   size_t(threadIdx.x) * 16;
+    float* dup = reinterpret_cast<float*>(smem + bulk_dup_offset<W, XG, NS>()) +
+                 size_t(warp) * S * Sh::DSLOT;
     const int s = lane / G, g = lane % G;
     const int u = lane % S;  // the block row this lane copies (lanes < S issue)
     const int64_t nbr = a.n_block_rows;
@@ -171,10 +205,25 @@ __global__ void __launch_bounds__(kBulkWarps * 32, MINB) cheb_step_bulk(StepArgs
             failed = true;
             break;
         }
+        if constexpr (DUP) {
+            // Rewrite the stage's S blocks as [c][r] (a, a) pairs (slots of
+            // rows that have no block here hold stale values nobody reads).
+            const float* sa = reinterpret_cast<const float*>(ring + st * Sh::STAGE);
+#pragma unroll
+            for (int u = 0; u < 2 * S; ++u) {
+                const int idx = lane + 32 * u;
+                const int b = idx >> 6, e = idx & 63;
+                const float v = sa[b * (Sh::ASLOT / 4) + e];
+                *reinterpret_cast<float2*>(dup + b * Sh::DSLOT + (e & 7) * Sh::DROW + 2 * (e >> 3)) =
+                    make_float2(v, v);
+            }
+            __syncwarp();
+        }
         if (live) {
             const unsigned char* stage = ring + st * Sh::STAGE;
             const float* As = reinterpret_cast<const float*>(stage + s * Sh::ASLOT);
             const float* Xs = reinterpret_cast<const float*>(stage + Sh::XBASE + s * Sh::XSLOT);
+            const float* Ds = dup + s * Sh::DSLOT;
 #pragma unroll
             for (int c = 0; c < 8; ++c) {
                 float4 x0, x1;
@@ -185,13 +234,31 @@ __global__ void __launch_bounds__(kBulkWarps * 32, MINB) cheb_step_bulk(StepArgs
                     x0 = *reinterpret_cast<const float4*>(Xs + c * W + 4 * g);
                     x1 = *reinterpret_cast<const float4*>(Xs + c * W + W / 2 + 4 * g);
                 }
+                if constexpr (DUP) {
 #pragma unroll
-                for (int r = 0; r < 8; ++r) {
-                    const float av = As[r * 8 + c];
-                    fma2(acc[r][0], acc[r][1], av, x0.x, x0.y);
-                    fma2(acc[r][2], acc[r][3], av, x0.z, x0.w);
-                    fma2(acc[r][4], acc[r][5], av, x1.x, x1.y);
-                    fma2(acc[r][6], acc[r][7], av, x1.z, x1.w);
+                    for (int rp = 0; rp < 4; ++rp) {
+                        const float4 aa =
+                            *reinterpret_cast<const float4*>(Ds + c * Sh::DROW + 4 * rp);
+                        float* u0 = acc[2 * rp];
+                        float* u1 = acc[2 * rp + 1];
+                        fma2p(u0[0], u0[1], aa.x, aa.y, x0.x, x0.y);
+                        fma2p(u0[2], u0[3], aa.x, aa.y, x0.z, x0.w);
+                        fma2p(u0[4], u0[5], aa.x, aa.y, x1.x, x1.y);
+                        fma2p(u0[6], u0[7], aa.x, aa.y, x1.z, x1.w);
+                        fma2p(u1[0], u1[1], aa.z, aa.w, x0.x, x0.y);
+                        fma2p(u1[2], u1[3], aa.z, aa.w, x0.z, x0.w);
+                        fma2p(u1[4], u1[5], aa.z, aa.w, x1.x, x1.y);
+                        fma2p(u1[6], u1[7], aa.z, aa.w, x1.z, x1.w);
+                    }
+                } else {
+#pragma unroll
+                    for (int r = 0; r < 8; ++r) {
+                        const float av = As[r * 8 + c];
+                        fma2(acc[r][0], acc[r][1], av, x0.x, x0.y);
+                        fma2(acc[r][2], acc[r][3], av, x0.z, x0.w);
+                        fma2(acc[r][4], acc[r][5], av, x1.x, x1.y);
+                        fma2(acc[r][6], acc[r][7], av, x1.z, x1.w);
+                    }
                 }
             }
         }

@@ -236,7 +236,8 @@ inline int pick_v_staged(int W, bool cv, int block_size, bool dbl) {
 // (RSATB_BULK_OCC=4: sized for 4 resident CTAs per SM instead of 3).
 inline int bulk_stages() {
     const char* s = std::getenv("RSATB_BULK_NS");
-    return (s && std::atoi(s) == 3) ? 3 : 2;
+    const int n = s ? std::atoi(s) : 2;
+    return (n == 3 || n == 4) ? n : 2;
 }
 inline bool bulk_x_global() {
     const char* s = std::getenv("RSATB_BULK_X");
@@ -246,11 +247,21 @@ inline bool bulk_occ4() {
     const char* s = std::getenv("RSATB_BULK_OCC");
     return s && std::atoi(s) == 4;
 }
+// A from the duplicated transposed slot (DUP): the default at W = 256,
+// where it measured 0.92 against 1.11 ms per launch on the diamond 16^3
+// BSR; at W = 32 to 128 the row-major slot is faster (0.427 against
+// 0.451 ms at W = 128).  RSATB_BULK_A=dup|row forces one (A/B only).
+inline bool bulk_a_dup(int W) {
+    const char* s = std::getenv("RSATB_BULK_A");
+    if (s && s[0] == 'd') return true;
+    if (s && s[0] == 'r') return false;
+    return W >= 256;
+}
 
-template <int W, bool CV, int NS, bool XG, int MINB>
+template <int W, bool CV, int NS, bool XG, int MINB, bool DUP = false>
 int launch_bulk_k(rsatb_context* ctx, StepArgs& a) {
     using Sh = BulkShape<W, XG>;
-    auto kernel = cheb_step_bulk<W, CV, NS, XG, MINB>;
+    auto kernel = cheb_step_bulk<W, CV, NS, XG, MINB, DUP>;
     const int threads = kBulkWarps * 32;
     const size_t smem = bulk_smem_bytes<W, XG, NS>();
     if (smem > 227 * 1024) return kNotApplicable;
@@ -282,12 +293,20 @@ int launch_bulk_w(rsatb_context* ctx, StepArgs& a) {
     // of the bounded-wait fault report).
     const char* wc = std::getenv("RSATB_TEST_BULK_WAIT");
     a.wait_check = (wc && wc[0] == '1') ? 1 : 0;
-    const bool ns3 = bulk_stages() == 3;
+    const int ns = bulk_stages();
     if (!bulk_x_global())
-        return ns3 ? launch_bulk_k<W, CV, 3, false, 2>(ctx, a)
-                   : launch_bulk_k<W, CV, 2, false, 3>(ctx, a);
+        return ns == 3 ? launch_bulk_k<W, CV, 3, false, 2>(ctx, a)
+                       : launch_bulk_k<W, CV, 2, false, 3>(ctx, a);
     if (bulk_occ4()) return launch_bulk_k<W, CV, 2, true, 4>(ctx, a);
-    return ns3 ? launch_bulk_k<W, CV, 3, true, 3>(ctx, a) : launch_bulk_k<W, CV, 2, true, 3>(ctx, a);
+    const bool dup = bulk_a_dup(W);
+    if (ns == 3)
+        return dup ? launch_bulk_k<W, CV, 3, true, 3, true>(ctx, a)
+                   : launch_bulk_k<W, CV, 3, true, 3, false>(ctx, a);
+    if (ns == 4)
+        return dup ? launch_bulk_k<W, CV, 4, true, 3, true>(ctx, a)
+                   : launch_bulk_k<W, CV, 4, true, 3, false>(ctx, a);
+    return dup ? launch_bulk_k<W, CV, 2, true, 3, true>(ctx, a)
+               : launch_bulk_k<W, CV, 2, true, 3, false>(ctx, a);
 }
 
 // Ring depth of the narrow-panel kernel (RSATB_NARROW_NS: 2 or 3).

@@ -299,7 +299,10 @@ NARROW = [(96, 8, 6, False, False, 8, False), (96, 8, 6, False, False, 4, True),
           # bulk-copy kernel widths W = 64 and 256 and ragged group counts
           # (97 block rows: not a multiple of the 2..32 block rows per warp)
           (97, 8, 7, False, False, 64, False), (97, 8, 7, False, False, 128, True),
-          (97, 8, 7, False, False, 256, False), (97, 8, 7, False, False, 2, True)]
+          (97, 8, 7, False, False, 256, False), (97, 8, 7, False, False, 2, True),
+          # narrow tensor-core widths W = 32 and complex W = 16, 32
+          (97, 8, 7, False, False, 32, False), (97, 8, 7, False, False, 8, True),
+          (97, 8, 7, False, False, 16, True)]
 
 
 @pytest.mark.parametrize("kernel", ["staged", "rowsplit", "bulk", "bulk_smem", "narrow", "dmma",
