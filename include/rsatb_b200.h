@@ -583,6 +583,41 @@ RSATB_API int rsatb_inverse_sqrt_refine(rsatb_ctx_t ctx, rsatb_bsr_t S, rsatb_bs
                                         const rsatb_ns_refine_options* options,
                                         rsatb_bsr_t* Z_out, rsatb_ns_refine_report* report);
 
+/* ------------------------------------------------------- spectral bounds */
+
+/* Options of rsatb_lanczos_extremes; zero fields take the defaults. */
+typedef struct {
+    int steps;          /* fixed Lanczos steps when tol <= 0 (0: 20) */
+    double tol;         /* > 0: stop once both extreme Ritz pairs have residual
+                           <= tol * max|theta| (PRIMME's 1e-3 in the reference) */
+    int max_matvecs;    /* cap with tol (0: 10000); at most 400 basis vectors */
+    uint64_t seed;      /* start vector of rsatb_set_random (0: 2) */
+} rsatb_lanczos_options;
+
+typedef struct {
+    double theta_min, theta_max;  /* extreme Ritz values of the unscaled operator */
+    double res_min, res_max;      /* their residual norms |beta_m y_m| */
+    int matvecs;                  /* operator applications */
+    int converged;                /* tol met (or an invariant subspace found) */
+} rsatb_lanczos_result;
+
+/* Extreme eigenvalues of the operator of `op` applied unscaled (its window is
+ * ignored): Lanczos with full FP64 reorthogonalisation on the device, the
+ * basis S-orthonormal for the Solve form (H x = lambda S x), the tridiagonal
+ * eigenproblem on the host (implicit QL).  The spectral-bounds estimate of
+ * rsatb/setup/spectral_bounds.hpp:311-490 (ExtremalEigenvalues) without
+ * PRIMME; the caller pads and applies the fallback rules.  Allocates its
+ * basis (n x m FP64) with cudaMalloc and frees it; synchronises. */
+RSATB_API int rsatb_lanczos_extremes(rsatb_ctx_t ctx, const rsatb_cheb_op* op,
+                                     const rsatb_lanczos_options* options,
+                                     rsatb_lanczos_result* result);
+
+/* Eigenvalues (ascending) of the symmetric tridiagonal matrix diag[0..m),
+ * off[0..m-1) and the last components of its normalised eigenvectors (host
+ * only; the Ritz solve of rsatb_lanczos_extremes). */
+RSATB_API int rsatb_tridiag_eigen(int m, const double* diag, const double* off,
+                                  double* eigenvalues, double* last_components);
+
 /* ------------------------------------------------------------ measurement */
 
 /* FMA-pipe throughput of this device in FLOP/s, from independent FMA chains

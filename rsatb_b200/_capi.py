@@ -82,6 +82,17 @@ class NsRefineReport(C.Structure):
                 ("nnz_blocks", C.c_int64), ("reforms", C.c_int), ("propagations", C.c_int)]
 
 
+class LanczosOptions(C.Structure):
+    _fields_ = [("steps", C.c_int), ("tol", C.c_double), ("max_matvecs", C.c_int),
+                ("seed", C.c_uint64)]
+
+
+class LanczosResult(C.Structure):
+    _fields_ = [("theta_min", C.c_double), ("theta_max", C.c_double),
+                ("res_min", C.c_double), ("res_max", C.c_double),
+                ("matvecs", C.c_int), ("converged", C.c_int)]
+
+
 # rsatb_ns_precision
 NS_FP64, NS_TF32X3, NS_TF32 = 0, 1, 2
 
@@ -143,6 +154,9 @@ SIGNATURES = {
     "rsatb_isqrt_autotune": (_i, [_vp, _i, _i, _vp, _i, _vp, _vp, _vp]),
     "rsatb_inverse_sqrt_refine": (_i, [_vp, _vp, _vp, C.POINTER(NsRefineOptions),
                                        C.POINTER(_vp), C.POINTER(NsRefineReport)]),
+    "rsatb_lanczos_extremes": (_i, [_vp, C.POINTER(ChebOp), C.POINTER(LanczosOptions),
+                                    C.POINTER(LanczosResult)]),
+    "rsatb_tridiag_eigen": (_i, [_i, _PD, _PD, _PD, _PD]),
 }
 
 
