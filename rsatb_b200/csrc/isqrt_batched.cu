@@ -8,17 +8,19 @@
 // operands, so both tensor-core operands are K-major):
 //     W = Z S^T            (= Z S, S symmetric)
 //     X = Z W^T            (= Z S Z^T)  -> ||X - I||_F, stopping rules
-//     P = 1.875 I - 1.25 X + 0.375 X X^T
-//     Z' = ((P + P^T)/2) Z (FP64)
+//     P = 1.875 I - 1.25 X + 0.375 X X^T, made exactly symmetric
+//     Z' = P Z
 // from Z0 = I / sqrt(s), s = max row sum of |S| >= lambda_max.
 //
-// Phases: an optional tensor-core phase (W, X and P in TF32 or split TF32
-// on tcgen05 with FP32 accumulation; the update of Z in FP64) followed by
-// FP64 iterations (SIMT GEMMs).  The iteration is equivariant under
-// Z -> Q Z for orthogonal Q, so rounding in the update of Z would leave a
-// rotation that no later step corrects; with that one product in FP64 and a
-// symmetric left factor, the low-precision errors only perturb X and are
-// removed by the following steps.  Each phase of a chunk is one captured
+// Phases: an optional tensor-core phase (all four products in TF32 or
+// split TF32 on tcgen05 with FP32 accumulation) followed by FP64 iterations
+// (FP64 tensor-core GEMMs).  The iteration is equivariant under Z -> Q Z for
+// orthogonal Q, so an antisymmetric part of the rounded left factor P would
+// leave a rotation that no later step corrects: P is computed on the tiles
+// of its upper triangle only and mirrored, so it is exactly symmetric, and
+// a symmetric perturbation only moves Z normal to the solution set, which
+// the following steps undo.  Z' = P Z takes Z^T as its K-major B operand,
+// which the update itself stores (transposed) for the next step.  Each phase of a chunk is one captured
 // CUDA graph; a problem that stops early is gated off in every later kernel
 // by its `active` flag and its iterate is retired (copied out) at once.
 #include "ns_batched.cuh"
@@ -26,6 +28,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <numeric>
 #include <vector>
 
@@ -56,27 +59,37 @@ __global__ void pack_kernel(const Prob* probs, const int64_t* in_off, const doub
     }
 }
 
-// Gershgorin scale and the starting iterate Z0 = I / sqrt(s) in FP64 (and
-// as TF32 hi/lo for a tensor-core phase); state reset.
+// Scale s >= lambda_max, the smaller of two upper bounds, the Gershgorin
+// bound max_r sum_c |S_rc| and the Frobenius norm (the tighter s, the fewer
+// steps: X0 = S / s has its smallest eigenvalue lambda_min / s), and the
+// starting iterate Z0 = I / sqrt(s) in FP64 (and as TF32 hi/lo for a
+// tensor-core phase); state reset.
 __global__ void init_kernel(const Prob* probs, const double* s64, State* st, float* z_hi,
                             float* z_lo, double* z64, double* scale, int cap) {
     const Prob pr = probs[blockIdx.x];
     const int np = pr.n_pad, n = pr.n;
-    __shared__ double red[256];
-    double m = 0.0;
+    __shared__ double red[256], red2[256];
+    double m = 0.0, f2 = 0.0;
     for (int r = threadIdx.x; r < n; r += blockDim.x) {
         double s = 0.0;
         const double* row = s64 + pr.off + int64_t(r) * np;
-        for (int c = 0; c < n; ++c) s += fabs(row[c]);
+        for (int c = 0; c < n; ++c) {
+            s += fabs(row[c]);
+            f2 += row[c] * row[c];
+        }
         m = fmax(m, s);
     }
     red[threadIdx.x] = m;
+    red2[threadIdx.x] = f2;
     __syncthreads();
     for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-        if (threadIdx.x < w) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + w]);
+        if (threadIdx.x < w) {
+            red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + w]);
+            red2[threadIdx.x] += red2[threadIdx.x + w];
+        }
         __syncthreads();
     }
-    const double s = red[0];
+    const double s = fmin(red[0], sqrt(red2[0]));
     const double z0 = s > 0.0 ? 1.0 / sqrt(s) : 0.0;
     for (int64_t e = threadIdx.x; e < int64_t(np) * np; e += blockDim.x) {
         const int r = int(e / np), c = int(e - int64_t(r) * np);
@@ -188,6 +201,17 @@ __global__ void retire_low_kernel(const Prob* probs, const State* st, const doub
     const int np = pr.n_pad;
     for (int64_t e = threadIdx.x; e < int64_t(np) * np; e += blockDim.x)
         dst[pr.off + e] = src[pr.off + e];
+}
+
+// z64 = z_hi + z_lo for every problem: the split-TF32 update keeps the
+// iterate as a hi/lo pair only, and a problem's tiles are skipped once it
+// stops, so the pair still holds the iterate it stopped at.
+__global__ void low_to_f64_kernel(const Prob* probs, const float* z_hi, const float* z_lo,
+                                  double* z64) {
+    const Prob pr = probs[blockIdx.x];
+    const int np = pr.n_pad;
+    for (int64_t e = threadIdx.x; e < int64_t(np) * np; e += blockDim.x)
+        z64[pr.off + e] = double(z_hi[pr.off + e]) + double(z_lo[pr.off + e]);
 }
 
 // Result of a problem the FP64 phase just stopped: columns
@@ -416,15 +440,24 @@ struct Chunk {
 };
 
 struct Arrays {
-    // tensor-core phase (nullptr when absent)
+    // tensor-core phase (nullptr when absent); zt: Z^T, the B operand of the
+    // split-TF32 update Z' = P Z (two buffers: one read, one written)
     float *s_hi, *s_lo, *z_hi, *z_lo, *w_hi, *w_lo, *x_hi, *x_lo,
-        *p_hi, *p_lo;
+        *p_hi, *p_lo, *zt_hi[2], *zt_lo[2];
     // FP64 phase
     double *s64, *z64[2], *w64, *x64, *p64;
 };
 
 size_t chunk_bytes(int64_t elems, bool low) {
-    return size_t(elems) * ((low ? 10 * 4 : 0) + 6 * 8);
+    return size_t(elems) * ((low ? 14 * 4 : 0) + 6 * 8);
+}
+
+// The tensor-core phase's update Z' = P Z: split TF32 on the tensor cores
+// with P made exactly symmetric (the default), or in FP64 with (P + P^T)/2
+// summed as it is read (RSATB_NS_UPDATE=fp64).
+bool fp64_update() {
+    const char* s = std::getenv("RSATB_NS_UPDATE");
+    return s && s[0] == 'f';
 }
 
 // A tensor-core phase that stops above this residual has not resolved the
@@ -457,6 +490,7 @@ struct Dev {
     int* low_count;
     unsigned* error;
     TcItem* tc_items;
+    TcItem* tc_items_upper;  // the tiles that touch the upper triangle
     F64Item* f64_items;
     int n_tc_items;
     int n_f64_items;
@@ -472,11 +506,14 @@ T* carve(char*& cur, size_t count) {
 
 // One tensor-core GEMM over the whole chunk, in launches of at most
 // kMaxBuckets buckets.
-int tc_gemm(rsatb_context* ctx, const Chunk& ch, const Dev& d,
+// items / group_item_begin: the full tile list or the upper-triangle one
+// (sym); ct_hi / ct_lo: optional transposed store of C.
+int tc_gemm(rsatb_context* ctx, const Chunk& ch, const Dev& d, const TcItem* items,
             const std::vector<int>& group_item_begin, const float* a_hi, const float* a_lo,
             const float* b_hi, const float* b_lo, float* c_hi, float* c_lo, double* c64,
             int mode, const float* xe_hi, const float* xe_lo, bool split, bool ws,
-            rsatb_isqrt_stats* stats) {
+            rsatb_isqrt_stats* stats, float* ct_hi = nullptr, float* ct_lo = nullptr,
+            bool sym = false) {
     const int nb = int(ch.buckets.size());
     for (int g0 = 0, gi = 0; g0 < nb; g0 += kMaxBuckets, ++gi) {
         TcMaps maps;
@@ -490,7 +527,7 @@ int tc_gemm(rsatb_context* ctx, const Chunk& ch, const Dev& d,
         }
         TcArgs args{};
         args.probs = d.probs;
-        args.items = d.tc_items + group_item_begin[gi];
+        args.items = items + group_item_begin[gi];
         args.n_items = group_item_begin[gi + 1] - group_item_begin[gi];
         args.state = d.state;
         args.c_hi = c_hi;
@@ -500,6 +537,9 @@ int tc_gemm(rsatb_context* ctx, const Chunk& ch, const Dev& d,
         args.xe_lo = xe_lo;
         args.res2 = d.res2;
         args.mode = mode;
+        args.ct_hi = ct_hi;
+        args.ct_lo = ct_lo;
+        args.sym = sym ? 1 : 0;
         args.split = split ? 1 : 0;
         args.error = d.error;
         RSATB_TRY(launch_tc_gemm(ctx, maps, args, ws));
@@ -570,8 +610,8 @@ int run_chunk(rsatb_context* ctx, const Opts& o, const Chunk& ch, const int* col
 
     // Work items, ordered by bucket (the buckets of a launch group are
     // contiguous), largest problems first.
-    std::vector<TcItem> tc_items;
-    std::vector<int> group_begin{0};
+    std::vector<TcItem> tc_items, tc_upper;
+    std::vector<int> group_begin{0}, group_begin_upper{0};
     std::vector<F64Item> f64_items;
     for (size_t b = 0; b < ch.buckets.size(); ++b) {
         const Bucket& bk = ch.buckets[b];
@@ -579,13 +619,18 @@ int run_chunk(rsatb_context* ctx, const Opts& o, const Chunk& ch, const int* col
             const int p = bk.first + z;
             if (low)
                 for (int m0 = 0; m0 < bk.n_pad; m0 += 128)
-                    for (int n0 = 0; n0 < bk.n_pad; n0 += bk.nt)
-                        tc_items.push_back(TcItem{p, int(b % kMaxBuckets), z, m0, n0, bk.nt});
+                    for (int n0 = 0; n0 < bk.n_pad; n0 += bk.nt) {
+                        const TcItem it{p, int(b % kMaxBuckets), z, m0, n0, bk.nt};
+                        tc_items.push_back(it);
+                        if (n0 + bk.nt > m0) tc_upper.push_back(it);  // reaches col >= row
+                    }
             for (int m0 = 0; m0 < bk.n_pad; m0 += 64)
                 for (int n0 = 0; n0 < bk.n_pad; n0 += 64) f64_items.push_back(F64Item{p, m0, n0});
         }
-        if ((b + 1) % kMaxBuckets == 0 || b + 1 == ch.buckets.size())
+        if ((b + 1) % kMaxBuckets == 0 || b + 1 == ch.buckets.size()) {
             group_begin.push_back(int(tc_items.size()));
+            group_begin_upper.push_back(int(tc_upper.size()));
+        }
     }
 
     // Workspace.
@@ -595,8 +640,9 @@ int run_chunk(rsatb_context* ctx, const Opts& o, const Chunk& ch, const int* col
              3 * align256(P * sizeof(int)) + align256(P * sizeof(State)) +
              2 * align256(P * sizeof(double)) + 256 +
              align256(tc_items.size() * sizeof(TcItem)) +
+             align256(tc_upper.size() * sizeof(TcItem)) +
              align256(f64_items.size() * sizeof(F64Item));
-    bytes += (low ? 10 * align256(E * sizeof(float)) : 0) + 6 * align256(E * sizeof(double));
+    bytes += (low ? 14 * align256(E * sizeof(float)) : 0) + 6 * align256(E * sizeof(double));
     void* ws = nullptr;
     RSATB_TRY(ctx_scratch(ctx, bytes, &ws));
     char* cur = static_cast<char*>(ws);
@@ -612,6 +658,7 @@ int run_chunk(rsatb_context* ctx, const Opts& o, const Chunk& ch, const int* col
     d.scale = carve<double>(cur, P);
     d.error = carve<unsigned>(cur, 64);
     d.tc_items = carve<TcItem>(cur, tc_items.size());
+    d.tc_items_upper = carve<TcItem>(cur, tc_upper.size());
     d.f64_items = carve<F64Item>(cur, f64_items.size());
     d.n_tc_items = int(tc_items.size());
     d.n_f64_items = int(f64_items.size());
@@ -628,6 +675,10 @@ int run_chunk(rsatb_context* ctx, const Opts& o, const Chunk& ch, const int* col
         a.x_lo = carve<float>(cur, E);
         a.p_hi = carve<float>(cur, E);
         a.p_lo = carve<float>(cur, E);
+        for (int i = 0; i < 2; ++i) {
+            a.zt_hi[i] = carve<float>(cur, E);
+            a.zt_lo[i] = carve<float>(cur, E);
+        }
     }
     a.s64 = carve<double>(cur, E);
     a.z64[0] = carve<double>(cur, E);
@@ -661,6 +712,10 @@ int run_chunk(rsatb_context* ctx, const Opts& o, const Chunk& ch, const int* col
         RSATB_CUDA_TRY(cudaMemcpyAsync(d.tc_items, tc_items.data(),
                                        tc_items.size() * sizeof(TcItem), cudaMemcpyHostToDevice,
                                        s));
+    if (!tc_upper.empty())
+        RSATB_CUDA_TRY(cudaMemcpyAsync(d.tc_items_upper, tc_upper.data(),
+                                       tc_upper.size() * sizeof(TcItem), cudaMemcpyHostToDevice,
+                                       s));
     RSATB_CUDA_TRY(cudaMemcpyAsync(d.f64_items, f64_items.data(),
                                    f64_items.size() * sizeof(F64Item), cudaMemcpyHostToDevice, s));
     RSATB_CUDA_TRY(cudaMemsetAsync(d.res2, 0, P * sizeof(double), s));
@@ -672,6 +727,12 @@ int run_chunk(rsatb_context* ctx, const Opts& o, const Chunk& ch, const int* col
     init_kernel<<<P, 256, 0, s>>>(d.probs, a.s64, d.state, a.z_hi, a.z_lo, a.z64[0], d.scale,
                                   low ? o.max_iter : o.max_fp64);
     RSATB_LAUNCH_CHECK(ctx);
+    if (low) {  // Z0 = I / sqrt(s) is symmetric: Z0^T = Z0
+        RSATB_CUDA_TRY(cudaMemcpyAsync(a.zt_hi[0], a.z_hi, E * sizeof(float),
+                                       cudaMemcpyDeviceToDevice, s));
+        RSATB_CUDA_TRY(cudaMemcpyAsync(a.zt_lo[0], a.z_lo, E * sizeof(float),
+                                       cudaMemcpyDeviceToDevice, s));
+    }
     const int cb = (P + 255) / 256;
 
     cudaEvent_t ev[3];
@@ -684,42 +745,67 @@ int run_chunk(rsatb_context* ctx, const Opts& o, const Chunk& ch, const int* col
     } guard{ev};
     RSATB_CUDA_TRY(cudaEventRecord(ev[0], s));
 
-    // P is consumed in FP64 only: the tensor-core kernel that can skip its
-    // TF32 hi/lo copy does so.
+    // With the FP64 update P is consumed in FP64 only: the tensor-core
+    // kernel that can skip its TF32 hi/lo copy does so.
     const bool use_ws_tc = o.ws;
+    const bool update64 = fp64_update();
     if (low) {
         RSATB_TRY(prepare_tc_gemm());
         RSATB_TRY(run_phase(ctx, o.graph, [&]() -> int {
             for (int k = 0; k <= o.max_iter; ++k) {
                 const int c = k & 1;
                 // W = Z S^T, X = Z W^T (+ residual) on the tensor cores
-                RSATB_TRY(tc_gemm(ctx, ch, d, group_begin, a.z_hi, a.z_lo, a.s_hi, a.s_lo,
-                                  a.w_hi, a.w_lo, nullptr, EPI_STORE, nullptr, nullptr, split, o.ws,
-                                  stats));
-                RSATB_TRY(tc_gemm(ctx, ch, d, group_begin, a.z_hi, a.z_lo, a.w_hi, a.w_lo,
-                                  a.x_hi, a.x_lo, nullptr, EPI_RESID, nullptr, nullptr, split, o.ws,
-                                  stats));
+                RSATB_TRY(tc_gemm(ctx, ch, d, d.tc_items, group_begin, a.z_hi, a.z_lo, a.s_hi,
+                                  a.s_lo, a.w_hi, a.w_lo, nullptr, EPI_STORE, nullptr, nullptr,
+                                  split, o.ws, stats));
+                // X on every tile (its upper triangle mirrored, as P is, measured
+                // the same: 21,300 against 21,400 matrices/s at 20,000 problems).
+                RSATB_TRY(tc_gemm(ctx, ch, d, d.tc_items, group_begin, a.z_hi, a.z_lo, a.w_hi,
+                                  a.w_lo, a.x_hi, a.x_lo, nullptr, EPI_RESID, nullptr, nullptr,
+                                  split, o.ws, stats));
                 control_kernel<<<cb, 256, 0, s>>>(P, d.state, d.res2, o.tol, 1);
                 RSATB_LAUNCH_CHECK(ctx);
-                if (c == 1) {
+                if (c == 1 && update64) {
                     retire_low_kernel<<<P, 256, 0, s>>>(d.probs, d.state, a.z64[1], a.z64[0]);
                     RSATB_LAUNCH_CHECK(ctx);
                 }
                 if (k == o.max_iter) break;
-                // P = 1.875 I - 1.25 X + 0.375 X X^T on the tensor cores (and in
-                // FP64), then Z' = ((P + P^T)/2) Z in FP64: a symmetric factor on
-                // the left only moves Z off the solution set {Q S^-1/2}, which
-                // later steps undo, while rounding in the product itself would
-                // add a rotation Q that no step removes.
-                RSATB_TRY(tc_gemm(ctx, ch, d, group_begin, a.x_hi, a.x_lo, a.x_hi, a.x_lo,
-                                  use_ws_tc ? nullptr : a.p_hi, use_ws_tc ? nullptr : a.p_lo,
-                                  a.p64, EPI_POLY, a.x_hi, a.x_lo, split, o.ws, stats));
-                const int st_z = f64_gemm<false, true>(ctx, d, a.p64, a.z64[c], a.z64[c ^ 1],
-                                                       EPI_STORE, nullptr, stats, a.z_hi, a.z_lo);
-                RSATB_TRY(st_z);
+                // P = 1.875 I - 1.25 X + 0.375 X X^T on the tensor cores, then
+                // Z' = P Z with P exactly symmetric.  A symmetric factor on the
+                // left only moves Z off the solution set {Q S^-1/2}, which later
+                // steps undo; the antisymmetric part of a rounded P would add a
+                // rotation Q that no step removes (split TF32 with an
+                // unsymmetrised P: 6e-4 from the eigen route at kappa 1e5,
+                // symmetrised: 2.4e-5, as with the FP64 update).
+                if (!update64) {
+                    // Upper-triangle tiles of P, each element also stored
+                    // mirrored; Z' = P Z against Z^T (both operands K-major),
+                    // storing Z' and Z'^T (the FP64 iterate is formed once,
+                    // after the phase).
+                    RSATB_TRY(tc_gemm(ctx, ch, d, d.tc_items_upper, group_begin_upper, a.x_hi,
+                                      a.x_lo, a.x_hi, a.x_lo, a.p_hi, a.p_lo, nullptr, EPI_POLY,
+                                      a.x_hi, a.x_lo, split, o.ws, stats, nullptr, nullptr, true));
+                    RSATB_TRY(tc_gemm(ctx, ch, d, d.tc_items, group_begin, a.p_hi, a.p_lo,
+                                      a.zt_hi[c], a.zt_lo[c], a.z_hi, a.z_lo, nullptr,
+                                      EPI_STORE, nullptr, nullptr, split, o.ws, stats,
+                                      a.zt_hi[c ^ 1], a.zt_lo[c ^ 1]));
+                } else {
+                    RSATB_TRY(tc_gemm(ctx, ch, d, d.tc_items, group_begin, a.x_hi, a.x_lo, a.x_hi,
+                                      a.x_lo, use_ws_tc ? nullptr : a.p_hi,
+                                      use_ws_tc ? nullptr : a.p_lo, a.p64, EPI_POLY, a.x_hi,
+                                      a.x_lo, split, o.ws, stats));
+                    const int st_z = f64_gemm<false, true>(ctx, d, a.p64, a.z64[c], a.z64[c ^ 1],
+                                                           EPI_STORE, nullptr, stats, a.z_hi,
+                                                           a.z_lo);
+                    RSATB_TRY(st_z);
+                }
             }
             return RSATB_SUCCESS;
         }));
+    }
+    if (low && !update64) {
+        low_to_f64_kernel<<<P, 256, 0, s>>>(d.probs, a.z_hi, a.z_lo, a.z64[0]);
+        RSATB_LAUNCH_CHECK(ctx);
     }
     RSATB_CUDA_TRY(cudaEventRecord(ev[1], s));
 

@@ -63,6 +63,11 @@ struct TcArgs {
     const float* xe_hi;      // EPI_POLY: X (hi + lo) for P = 1.875 I - 1.25 X + 0.375 X X^T
     const float* xe_lo;
     double* res2;            // EPI_RESID: per-problem sum of (C - I)^2 over the valid corner
+    float* ct_hi;            // optional transposed store of C (hi, lo), nullptr: none
+    float* ct_lo;
+    int sym;                 // 1: only (row, col >= row) is stored, each also at (col, row):
+                             // C leaves exactly symmetric (the items cover the upper
+                             // triangle of tiles only)
     int mode;
     int split;               // 1: hi*hi + hi*lo + lo*hi; 0: hi*hi
     unsigned* error;         // set non-zero when a bounded wait gave up

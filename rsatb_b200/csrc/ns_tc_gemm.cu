@@ -36,6 +36,87 @@ __device__ __forceinline__ void record_error(unsigned* error, unsigned code) {
     if (error) atomicOr(error, code);
 }
 
+// Stores one thread's 16 consecutive values of C (row `row`, columns col0..
+// col0 + 15 of the padded problem): the hi/lo pair and the optional FP64
+// copy at (row, col), and the optional transposed hi/lo at (col, row); with
+// args.sym only the upper triangle (col >= row) is stored, each element
+// also at (col, row), so C leaves exactly symmetric.  The transposed and
+// mirrored stores of a warp (32 consecutive rows, one column) are
+// coalesced.
+// X (hi + lo) at 16 consecutive elements for the polynomial epilogue, as
+// 128-bit loads.
+__device__ __forceinline__ void load_x16(const TcArgs& args, int64_t base, float (&xe)[16]) {
+    const float4* h = reinterpret_cast<const float4*>(args.xe_hi + base);
+    const float4* l = reinterpret_cast<const float4*>(args.xe_lo + base);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const float4 a = h[q], b = l[q];
+        xe[4 * q] = a.x + b.x;
+        xe[4 * q + 1] = a.y + b.y;
+        xe[4 * q + 2] = a.z + b.z;
+        xe[4 * q + 3] = a.w + b.w;
+    }
+}
+
+__device__ __forceinline__ void store_rows(const TcArgs& args, int64_t base,
+                                           const float (&hi)[16], const float (&lo)[16]) {
+    if (args.c_hi) {
+        float4* ch = reinterpret_cast<float4*>(args.c_hi + base);
+        float4* cl = reinterpret_cast<float4*>(args.c_lo + base);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            ch[q] = make_float4(hi[4 * q], hi[4 * q + 1], hi[4 * q + 2], hi[4 * q + 3]);
+            cl[q] = make_float4(lo[4 * q], lo[4 * q + 1], lo[4 * q + 2], lo[4 * q + 3]);
+        }
+    }
+    if (args.c64) {
+        double2* cd = reinterpret_cast<double2*>(args.c64 + base);
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+            cd[q] = make_double2(double(hi[2 * q]) + double(lo[2 * q]),
+                                 double(hi[2 * q + 1]) + double(lo[2 * q + 1]));
+    }
+}
+
+__device__ __forceinline__ void store_chunk(const TcArgs& args, const Prob& pr, int row, int col0,
+                                            const float (&hi)[16], const float (&lo)[16]) {
+    const int np = pr.n_pad;
+    const int64_t base = pr.off + int64_t(row) * np + col0;
+    if (args.sym) {
+        if (col0 + 15 < row) return;  // below the diagonal: the mirror of another thread's
+        if (col0 >= row) {
+            store_rows(args, base, hi, lo);  // the whole chunk is on or above the diagonal
+        } else {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                if (col0 + j < row) continue;
+                args.c_hi[base + j] = hi[j];
+                args.c_lo[base + j] = lo[j];
+                if (args.c64) args.c64[base + j] = double(hi[j]) + double(lo[j]);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {  // mirror: for fixed j a warp writes 32 consecutive rows
+            const int col = col0 + j;
+            if (col <= row) continue;
+            const int64_t t = pr.off + int64_t(col) * np + row;
+            args.c_hi[t] = hi[j];
+            args.c_lo[t] = lo[j];
+            if (args.c64) args.c64[t] = double(hi[j]) + double(lo[j]);
+        }
+        return;
+    }
+    store_rows(args, base, hi, lo);
+    if (args.ct_hi) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const int64_t t = pr.off + int64_t(col0 + j) * np + row;
+            args.ct_hi[t] = hi[j];
+            args.ct_lo[t] = lo[j];
+        }
+    }
+}
+
 __global__ void __launch_bounds__(128, 1)
     tc_gemm_kernel(const __grid_constant__ TcMaps maps, const TcArgs args) {
     using namespace umma;
@@ -158,38 +239,24 @@ __global__ void __launch_bounds__(128, 1)
                 const int col0 = item.n0 + c;
                 if (!in_mat || col0 >= np) continue;
                 const int64_t base = pr.off + int64_t(row) * np + col0;
-                float hi[16], lo[16];
+                float hi[16], lo[16], xe[16];
+                if (args.mode == EPI_POLY) load_x16(args, base, xe);
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
                     const int col = col0 + j;
                     const bool valid = vrow && col < pr.n;
                     float x = v[j];
-                    if (args.mode == EPI_POLY) {
-                        const float xe = args.xe_hi[base + j] + args.xe_lo[base + j];
-                        x = fmaf(0.375f, x, fmaf(-1.25f, xe, row == col ? 1.875f : 0.0f));
-                    }
+                    if (args.mode == EPI_POLY)
+                        x = fmaf(0.375f, x, fmaf(-1.25f, xe[j], row == col ? 1.875f : 0.0f));
                     if (!valid) x = 0.0f;
-                    if (args.mode == EPI_RESID && valid) {
+                    if (args.mode == EPI_RESID && valid && (!args.sym || col >= row)) {
                         const double d = double(x) - (row == col ? 1.0 : 0.0);
-                        r2 += d * d;
+                        r2 += (args.sym && col > row) ? 2.0 * d * d : d * d;
                     }
                     hi[j] = to_tf32(x);
                     lo[j] = x - hi[j];
                 }
-                float4* ch = reinterpret_cast<float4*>(args.c_hi + base);
-                float4* cl = reinterpret_cast<float4*>(args.c_lo + base);
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    ch[q] = make_float4(hi[4 * q], hi[4 * q + 1], hi[4 * q + 2], hi[4 * q + 3]);
-                    cl[q] = make_float4(lo[4 * q], lo[4 * q + 1], lo[4 * q + 2], lo[4 * q + 3]);
-                }
-                if (args.c64) {
-                    double2* cd = reinterpret_cast<double2*>(args.c64 + base);
-#pragma unroll
-                    for (int q = 0; q < 8; ++q)
-                        cd[q] = make_double2(double(hi[2 * q]) + double(lo[2 * q]),
-                                             double(hi[2 * q + 1]) + double(lo[2 * q + 1]));
-                }
+                store_chunk(args, pr, row, col0, hi, lo);
             }
             if (args.mode == EPI_RESID) {
 #pragma unroll
@@ -237,40 +304,24 @@ __device__ __forceinline__ void ws_epilogue(const TcArgs& args, const TcItem& it
         const int col0 = item.n0 + c;
         if (!in_mat || col0 >= np) continue;
         const int64_t base = pr.off + int64_t(row) * np + col0;
-        float hi[16], lo[16];
+        float hi[16], lo[16], xe[16];
+        if (args.mode == EPI_POLY) load_x16(args, base, xe);
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
             const int col = col0 + j;
             const bool valid = vrow && col < pr.n;
             float x = v[j];
-            if (args.mode == EPI_POLY) {
-                const float xe = args.xe_hi[base + j] + args.xe_lo[base + j];
-                x = fmaf(0.375f, x, fmaf(-1.25f, xe, row == col ? 1.875f : 0.0f));
-            }
+            if (args.mode == EPI_POLY)
+                x = fmaf(0.375f, x, fmaf(-1.25f, xe[j], row == col ? 1.875f : 0.0f));
             if (!valid) x = 0.0f;
-            if (args.mode == EPI_RESID && valid) {
+            if (args.mode == EPI_RESID && valid && (!args.sym || col >= row)) {
                 const double d = double(x) - (row == col ? 1.0 : 0.0);
-                r2 += d * d;
+                r2 += (args.sym && col > row) ? 2.0 * d * d : d * d;
             }
             hi[j] = to_tf32(x);
             lo[j] = x - hi[j];
         }
-        if (args.c_hi) {
-            float4* ch = reinterpret_cast<float4*>(args.c_hi + base);
-            float4* cl = reinterpret_cast<float4*>(args.c_lo + base);
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                ch[q] = make_float4(hi[4 * q], hi[4 * q + 1], hi[4 * q + 2], hi[4 * q + 3]);
-                cl[q] = make_float4(lo[4 * q], lo[4 * q + 1], lo[4 * q + 2], lo[4 * q + 3]);
-            }
-        }
-        if (args.c64) {
-            double2* cd = reinterpret_cast<double2*>(args.c64 + base);
-#pragma unroll
-            for (int q = 0; q < 8; ++q)
-                cd[q] = make_double2(double(hi[2 * q]) + double(lo[2 * q]),
-                                     double(hi[2 * q + 1]) + double(lo[2 * q + 1]));
-        }
+        store_chunk(args, pr, row, col0, hi, lo);
     }
     if (args.mode == EPI_RESID) {
 #pragma unroll
