@@ -297,37 +297,71 @@ __device__ __forceinline__ void ws_epilogue(const TcArgs& args, const TcItem& it
     const bool vrow = row < pr.n;
     const int np = pr.n_pad;
     double r2 = 0.0;
-    // two warps share a TMEM lane quarter: they take alternate 16-column chunks
+    // Two warps share a TMEM lane quarter: they take alternate 16-column
+    // chunks, the next chunk's TMEM load in flight while one is stored.
+    const uint32_t lanes = tacc + (uint32_t(quarter * 32) << 16);
+    uint32_t cur[16], nxt[16];
+    if (16 * half < item.nt) {
+        tmem_ld16_issue(lanes + uint32_t(16 * half), cur);
+        tmem_wait_ld();
+    }
     for (int c = 16 * half; c < item.nt; c += 32) {
+        const bool more = c + 32 < item.nt;  // warp-uniform
+        if (more) tmem_ld16_issue(lanes + uint32_t(c + 32), nxt);
         float v[16];
-        tmem_ld16(tacc + (uint32_t(quarter * 32) << 16) + uint32_t(c), v);
-        const int col0 = item.n0 + c;
-        if (!in_mat || col0 >= np) continue;
-        const int64_t base = pr.off + int64_t(row) * np + col0;
-        float hi[16], lo[16], xe[16];
-        if (args.mode == EPI_POLY) load_x16(args, base, xe);
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-            const int col = col0 + j;
-            const bool valid = vrow && col < pr.n;
-            float x = v[j];
-            if (args.mode == EPI_POLY)
-                x = fmaf(0.375f, x, fmaf(-1.25f, xe[j], row == col ? 1.875f : 0.0f));
-            if (!valid) x = 0.0f;
-            if (args.mode == EPI_RESID && valid && (!args.sym || col >= row)) {
-                const double d = double(x) - (row == col ? 1.0 : 0.0);
-                r2 += (args.sym && col > row) ? 2.0 * d * d : d * d;
+        for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(cur[j]);
+        const int col0 = item.n0 + c;
+        if (in_mat && col0 < np) {
+            const int64_t base = pr.off + int64_t(row) * np + col0;
+            float hi[16], lo[16], xe[16];
+            if (args.mode == EPI_POLY) load_x16(args, base, xe);
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const int col = col0 + j;
+                const bool valid = vrow && col < pr.n;
+                float x = v[j];
+                if (args.mode == EPI_POLY)
+                    x = fmaf(0.375f, x, fmaf(-1.25f, xe[j], row == col ? 1.875f : 0.0f));
+                if (!valid) x = 0.0f;
+                if (args.mode == EPI_RESID && valid && (!args.sym || col >= row)) {
+                    const double d = double(x) - (row == col ? 1.0 : 0.0);
+                    r2 += (args.sym && col > row) ? 2.0 * d * d : d * d;
+                }
+                hi[j] = to_tf32(x);
+                lo[j] = x - hi[j];
             }
-            hi[j] = to_tf32(x);
-            lo[j] = x - hi[j];
+            store_chunk(args, pr, row, col0, hi, lo);
         }
-        store_chunk(args, pr, row, col0, hi, lo);
+        if (more) {  // the next chunk's load was in flight during the stores
+            tmem_wait_ld();
+#pragma unroll
+            for (int j = 0; j < 16; ++j) cur[j] = nxt[j];
+        }
     }
     if (args.mode == EPI_RESID) {
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) r2 += __shfl_xor_sync(0xffffffffu, r2, o);
         if (lane == 0 && r2 != 0.0) atomicAdd(args.res2 + item.p, r2);
     }
+}
+
+// A work item with what every role needs of it, read one item ahead so the
+// global loads of the next item overlap the current tile (all roles walk
+// the same item sequence and skip the same inactive problems).
+struct ItemView {
+    TcItem item;
+    Prob pr;
+    int active;
+};
+__device__ __forceinline__ ItemView view_item(const TcArgs& args, int it) {
+    ItemView v{};
+    if (it < args.n_items) {
+        v.item = args.items[it];
+        v.active = args.state[v.item.p].active;
+        v.pr = args.probs[v.item.p];
+    }
+    return v;
 }
 
 __global__ void __launch_bounds__(320, 1)
@@ -369,10 +403,13 @@ __global__ void __launch_bounds__(320, 1)
         if (lane == 0) {
             // ---- TMA producer
             uint32_t g = 0;
+            ItemView nx = view_item(args, blockIdx.x);
             for (int it = blockIdx.x; it < args.n_items && !abort_flag; it += gridDim.x) {
-                const TcItem item = args.items[it];
-                if (!args.state[item.p].active) continue;
-                const int nk = args.probs[item.p].n_pad / 32;
+                const ItemView cur = nx;
+                nx = view_item(args, it + gridDim.x);
+                const TcItem item = cur.item;
+                if (!cur.active) continue;
+                const int nk = cur.pr.n_pad / 32;
                 const uint32_t tx = uint32_t(kTileA + item.nt * 128) * (args.split ? 2u : 1u);
                 for (int kc = 0; kc < nk; ++kc, ++g) {
                     const int s = int(g % kWsStages);
@@ -400,10 +437,13 @@ __global__ void __launch_bounds__(320, 1)
         if (lane == 0) {
             // ---- MMA issuer
             uint32_t g = 0, t = 0;
+            ItemView nx = view_item(args, blockIdx.x);
             for (int it = blockIdx.x; it < args.n_items && !abort_flag; it += gridDim.x) {
-                const TcItem item = args.items[it];
-                if (!args.state[item.p].active) continue;
-                const int nk = args.probs[item.p].n_pad / 32;
+                const ItemView cur = nx;
+                nx = view_item(args, it + gridDim.x);
+                const TcItem item = cur.item;
+                if (!cur.active) continue;
+                const int nk = cur.pr.n_pad / 32;
                 const uint32_t b = t & 1u, tph = (t >> 1) & 1u;
                 ++t;
                 if (!mbar_wait(&acc_empty[b], tph ^ 1u, kWaitLimitNs)) {
@@ -452,10 +492,13 @@ __global__ void __launch_bounds__(320, 1)
         const int quarter = warp & 3;
         const int half = (warp - 2) >> 2;
         uint32_t t = 0;
+        ItemView nx = view_item(args, blockIdx.x);
         for (int it = blockIdx.x; it < args.n_items && !abort_flag; it += gridDim.x) {
-            const TcItem item = args.items[it];
-            if (!args.state[item.p].active) continue;
-            const Prob pr = args.probs[item.p];
+            const ItemView cur = nx;
+            nx = view_item(args, it + gridDim.x);
+            const TcItem item = cur.item;
+            if (!cur.active) continue;
+            const Prob pr = cur.pr;
             const uint32_t b = t & 1u, tph = (t >> 1) & 1u;
             ++t;
             if (!mbar_wait(&acc_full[b], tph, kWaitLimitNs)) {
