@@ -56,6 +56,8 @@ def parse_args():
     p.add_argument("--isqrt-n", type=int, default=100_000,
                    help="problems of the batched inverse-sqrt workload")
     p.add_argument("--isqrt-precision", choices=["tf32x3", "tf32", "fp64"], default="tf32x3")
+    p.add_argument("--isqrt-family", choices=["continuous", "gapped"], default="continuous",
+                   help="spectrum family of the batched inverse-sqrt problems")
     p.add_argument("--isqrt-ws-gb", type=float, default=24.0,
                    help="device workspace per chunk of the batched inverse sqrt")
     p.add_argument("--small", action="store_true", help="reduced sizes, for a quick check")
@@ -665,7 +667,7 @@ def bench_isqrt(args, dist):
     from rsatb_b200 import workloads
     from rsatb_b200.isqrt import inverse_sqrt_columns_batched
     t0 = time.perf_counter()
-    batch = workloads.batched_spd(args.isqrt_n, seed=7 + dist.rank)
+    batch = workloads.batched_spd(args.isqrt_n, family=args.isqrt_family, seed=7 + dist.rank)
     torch.cuda.synchronize()
     gen_s = time.perf_counter() - t0
     n = batch.n
@@ -734,9 +736,10 @@ def bench_isqrt(args, dist):
             "dtype": {"tf32x3": "split TF32 (FP32 accumulate) + FP64 refinement",
                       "tf32": "TF32 (FP32 accumulate) + FP64 refinement",
                       "fp64": "f64"}[args.isqrt_precision],
-            "data": "synthetic (seeded Q diag(l) Q^T, continuous spectra)",
+            "data": f"synthetic (seeded Q diag(l) Q^T, {args.isqrt_family} spectra)",
             "config": {"workload": "batched_isqrt: SPD n~U[40,400], kappa log-uniform "
                                    "[1e2,1e5], 16 columns from n/3 per problem",
+                       "spectrum_family": args.isqrt_family,
                        "problems_per_gpu": int(n.size), "sum_n_cubed": float((n.astype(
                            np.float64) ** 3).sum()), "workspace_gb_per_chunk": args.isqrt_ws_gb},
             "status_failures": int((status != 0).sum()),
