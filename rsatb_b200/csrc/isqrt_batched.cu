@@ -165,6 +165,15 @@ __global__ void restart_kernel(const Prob* probs, const State* st, const double*
 // stop_on_rise (tensor-core phase) a residual that did not fall also stops:
 // in exact arithmetic every eigenvalue error of X shrinks each step, so a
 // rise means the low-precision floor was reached.
+//
+// The plateau and rise tests apply once ||X - I||_F < kQuadratic.  The
+// reference runs this loop from a seed already near S^-1/2; here it starts
+// from Z0 = I / sqrt(s), where every eigenvalue x of X in (0, 1] climbs
+// monotonically (x -> x p(x)^2, about 3.5 x while x is small) and a
+// near-null cluster (the gapped spectra of LCAO overlaps) holds the
+// Frobenius norm almost still for several steps: a stall of the norm there
+// is not a stall of the iteration.
+constexpr double kQuadratic = 0.5;
 __global__ void control_kernel(int np_count, State* st, double* res2, double tol,
                                int stop_on_rise) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -174,8 +183,10 @@ __global__ void control_kernel(int np_count, State* st, double* res2, double tol
     if (x.active) {
         const double norm = sqrt(res2[p]);
         x.norm = norm;
-        bool go = norm > tol && x.count < x.cap && fabs(x.norm_pre - norm) > 0.005 * norm;
-        if (stop_on_rise && x.count > 0 && norm >= x.norm_pre) go = false;
+        const bool near = norm < kQuadratic;
+        bool go = norm > tol && x.count < x.cap &&
+                  (!near || fabs(x.norm_pre - norm) > 0.005 * norm);
+        if (near && stop_on_rise && x.count > 0 && norm >= x.norm_pre) go = false;
         if (!(norm <= 100.0)) {  // also catches NaN
             x.active = 0;
             x.retire = 1;
