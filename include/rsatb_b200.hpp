@@ -181,6 +181,16 @@ public:
         check(rsatb_bsr_adjoint(ctx_->handle(), h_, &out));
         return BlockSpMat(ctx_, out);
     }
+    // Takes ownership of a matrix an entry point created (rsatb_inverse_sqrt_refine).
+    static BlockSpMat adopt(Context& ctx, rsatb_bsr_t h) { return BlockSpMat(&ctx, h); }
+    int64_t nnz_blocks() const { return info().nnz; }
+    // Block row offsets and block columns (row_ptr, col_ind) on the host.
+    void pattern(std::vector<int32_t>& row_ptr, std::vector<int32_t>& col_ind) const {
+        const Info i = info();
+        row_ptr.resize(size_t(i.n_block_rows) + 1);
+        col_ind.resize(size_t(i.nnz));
+        check(rsatb_bsr_pattern(ctx_->handle(), h_, row_ptr.data(), col_ind.data()));
+    }
 
 private:
     struct Info {
@@ -277,6 +287,47 @@ public:
                                   X.num_vectors(), dtype_of<T>::value));
     }
 
+    // Y = sum_n c_n T_n(Op~) X, Chebyshev::propagate (rsatb/calc/cheby.hpp:
+    // 367-441); a real panel takes Re(c_n).
+    void propagate(const DistMultiVector<T>& X, DistMultiVector<T>& Y,
+                   const std::vector<std::complex<double>>& coeffs) const {
+        std::vector<double> c(2 * coeffs.size());
+        for (size_t n = 0; n < coeffs.size(); ++n) {
+            c[2 * n] = coeffs[n].real();
+            c[2 * n + 1] = coeffs[n].imag();
+        }
+        const rsatb_cheb_op op = c_op();
+        check(rsatb_cheb_propagate(H.context().handle(), &op, X.data(), Y.data(),
+                                   X.num_vectors(), dtype_of<T>::value, c.data(),
+                                   int(coeffs.size())));
+    }
+    // Y = scale * (V dressed by the form) X, Chebyshev::apply_dual
+    // (rsatb/calc/cheby.hpp:249-291): V, Z^H V Z or S^-1 V (ADJOINT: V S^-1).
+    void apply_dual(const BlockSpMat<T>& V, const DistMultiVector<T>& X, DistMultiVector<T>& Y,
+                    double scale = 1.0, ChebyMode mode = ChebyMode::NORMAL) const {
+        const rsatb_cheb_op op = c_op();
+        if (mode == ChebyMode::ADJOINT)
+            check(rsatb_cheb_apply_dual_adjoint(H.context().handle(), &op, V.handle(), X.data(),
+                                                Y.data(), X.num_vectors(), dtype_of<T>::value,
+                                                scale));
+        else
+            check(rsatb_cheb_apply_dual(H.context().handle(), &op, V.handle(), X.data(),
+                                        Y.data(), X.num_vectors(), dtype_of<T>::value, scale));
+    }
+    // mu_n = <psi|T_n(Op~)|psi> averaged over the columns by the plain
+    // recurrence, Chebyshev::compute_moments (rsatb/calc/cheby.hpp:479-514).
+    std::vector<std::complex<double>> compute_moments(const DistMultiVector<T>& psi,
+                                                      int n_moments) const {
+        if (n_moments <= 0) return {};
+        const rsatb_cheb_op op = c_op();
+        std::vector<double> mu(2 * size_t(n_moments));
+        check(rsatb_kpm_dos_moments(H.context().handle(), &op, psi.data(), psi.num_vectors(),
+                                    dtype_of<T>::value, n_moments, 0, mu.data(), nullptr));
+        std::vector<std::complex<double>> out(n_moments);
+        for (int n = 0; n < n_moments; ++n) out[n] = {mu[2 * n], mu[2 * n + 1]};
+        return out;
+    }
+
     rsatb_cheb_op c_op() const {
         rsatb_cheb_op op{};
         op.form = form == ChebyOpForm::Sandwich ? RSATB_FORM_SANDWICH
@@ -312,6 +363,50 @@ std::vector<std::complex<double>> kpm_dos_moments(Chebyshev<T>& cheby,
     std::vector<std::complex<double>> out(n_moments);
     for (int n = 0; n < n_moments; ++n) out[n] = {mu[2 * n], mu[2 * n + 1]};
     return out;
+}
+
+// Extreme eigenvalues of the operator cheby iterates, applied unscaled (its
+// window is ignored), by Lanczos on the device: the PRIMME call of
+// EstimateSpectralBounds (rsatb/setup/spectral_bounds.hpp:311-490).  The
+// caller pads by |residual| and BoundsOptions::padding and applies the
+// reference's fallback when converged == 0.
+template <typename T>
+rsatb_lanczos_result lanczos_extremes(const Chebyshev<T>& cheby, double tol = 1e-3,
+                                      int max_matvecs = 10000, uint64_t seed = 2) {
+    const rsatb_cheb_op op = cheby.c_op();
+    rsatb_lanczos_options o{};
+    o.tol = tol;
+    o.max_matvecs = max_matvecs;
+    o.seed = seed;
+    rsatb_lanczos_result r{};
+    check(rsatb_lanczos_extremes(cheby.H.context().handle(), &op, &o, &r));
+    return r;
+}
+
+// rsatb::calc::inverse_sqrt (rsatb/calc/isqrtm.hpp:262) for a real FP64
+// overlap from a seed factor Z0 (the graph-local S^-1/2): Newton-Schulz with
+// block SpGEMMs, the drop threshold sptol and the reference's stopping rules.
+struct InverseSqrtOptions {
+    double tol = 1e-7;
+    double sptol = 1e-6;
+    int maxit = 20;
+    int route = 0;  // 0: X reformed or propagated by cost, 1: always reformed
+};
+using InverseSqrtReport = rsatb_ns_refine_report;
+
+inline BlockSpMat<double> inverse_sqrt(const BlockSpMat<double>& S, const BlockSpMat<double>& Z0,
+                                       const InverseSqrtOptions& opts = {},
+                                       InverseSqrtReport* report = nullptr) {
+    rsatb_ns_refine_options o{};
+    o.tol = opts.tol;
+    o.sptol = opts.sptol;
+    o.maxit = opts.maxit;
+    o.route = opts.route;
+    rsatb_ns_refine_report rep{};
+    rsatb_bsr_t Z = nullptr;
+    check(rsatb_inverse_sqrt_refine(S.context().handle(), S.handle(), Z0.handle(), &o, &Z, &rep));
+    if (report) *report = rep;
+    return BlockSpMat<double>::adopt(S.context(), Z);
 }
 
 // rho(x_j) from the moments with the Jackson (or another) kernel
