@@ -409,6 +409,33 @@ inline BlockSpMat<double> inverse_sqrt(const BlockSpMat<double>& S, const BlockS
     return BlockSpMat<double>::adopt(S.context(), Z);
 }
 
+// The DC spectrum by the FFT-Chebyshev method, rsatb::calc::
+// dc_spectrum_fftcheb (rsatb/calc/fftcheb_transport.hpp:543): Vx, Vy, Vz
+// the velocity matrices (H's shape and type), psi the complex samples.
+// sigma_out receives n_moments x 6 (xx xy xz yy yz zz; Greenwood fills the
+// diagonal) scaled by prefactor, energy_out the ascending energies.
+enum class DCFormulation { Greenwood = 0, Bastin = 1 };
+
+template <typename T>
+void dc_spectrum_fftcheb(const Chebyshev<T>& cheby, const BlockSpMat<T>& Vx,
+                         const BlockSpMat<T>& Vy, const BlockSpMat<T>& Vz,
+                         const DistMultiVector<T>& psi, int n_moments,
+                         DCFormulation formulation, double prefactor, int partition_sections,
+                         size_t max_workspace_mb, std::vector<double>& sigma_out,
+                         std::vector<double>& energy_out,
+                         rsatb_kpm_kernel kernel = RSATB_KPM_JACKSON) {
+    static_assert(dtype_of<T>::value == RSATB_C128 || dtype_of<T>::value == RSATB_C64,
+                  "dc_spectrum_fftcheb takes complex sample vectors");
+    const rsatb_cheb_op op = cheby.c_op();
+    sigma_out.assign(6 * size_t(n_moments), 0.0);
+    energy_out.assign(size_t(n_moments), 0.0);
+    check(rsatb_dc_spectrum_fftcheb(cheby.H.context().handle(), &op, Vx.handle(), Vy.handle(),
+                                    Vz.handle(), psi.data(), psi.num_vectors(),
+                                    dtype_of<T>::value, n_moments, int(formulation), prefactor,
+                                    partition_sections, max_workspace_mb << 20, kernel,
+                                    sigma_out.data(), energy_out.data(), nullptr));
+}
+
 // rho(x_j) from the moments with the Jackson (or another) kernel
 // (rsatb/calc/kpm.hpp:206-241), x clamped by edge_inset.
 inline std::vector<double> evaluate_kpm_density(Context& ctx,

@@ -172,8 +172,11 @@ int launch_staged(rsatb_context* ctx, StepArgs& a) {
     if (smem > 227 * 1024) return kNotApplicable;
     auto kernel = cheb_step_staged<VT, MT, B, V, CM, CV, STAGES>;
     // Raise the dynamic shared-memory limit of this instantiation as far as
-    // this launch needs (a process-wide setting of the function).
-    static size_t attr_bytes = 48 * 1024;
+    // this launch needs (a process-wide setting of the function).  Opted in
+    // from the first launch: the kernel also holds static shared memory (the
+    // dot finish), so 48 KB of dynamic memory alone already exceeds the
+    // default limit.
+    static size_t attr_bytes = 0;
     if (smem > attr_bytes) {
         cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                int(smem));

@@ -165,3 +165,51 @@ def test_calc_consumer_matches_dense_references(tmp_path):
     steps, converged, residual, nnz, nnz_pattern, check = d["refine"]
     assert converged == 1.0 and residual <= 1e-10 and nnz == nnz_pattern and nnz > 0
     assert check <= 1e-8
+
+
+TRANSPORT_SRC = ROOT / "tests" / "cpp" / "transport_consumer.cpp"
+TRANSPORT_EXE = ROOT / "_build" / "transport_consumer"
+
+
+def test_transport_consumer_compiles_against_the_headers():
+    exe = build_consumer(TRANSPORT_SRC, TRANSPORT_EXE)
+    out = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert out.returncode == 2 and "usage" in out.stderr
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("formulation", [0, 1])
+def test_transport_consumer_matches_the_oracle(tmp_path, formulation):
+    """calc::dc_spectrum_fftcheb from C++ (complex H and V_a = i W_a) against
+    the oracle's restatement of dc_spectrum_fftcheb with the real H and the
+    imaginary-unit velocities, Greenwood and Bastin, to 1e-10."""
+    import oracle
+    from _util import to_oracle
+    from rsatb_b200 import lattice
+    exe = build_consumer(TRANSPORT_SRC, TRANSPORT_EXE)
+    H, pos, cell, disp = lattice.twisted_bilayer_graphene(m=1, tiles=(4, 4))
+    V = lattice.commutator_velocity(H, disp)
+    w = np.linalg.eigvalsh(H.to_dense())
+    emin, emax, R, M = w[0] - 0.5, w[-1] + 0.5, 3, 33
+    rng = np.random.default_rng(5)
+    psi = np.exp(2j * np.pi * rng.random((H.n_rows, R))) / np.sqrt(H.n_rows)
+    with open(tmp_path / "in.bin", "wb") as f:
+        np.array([H.n_block_rows, H.block_size, H.nnz_blocks, R, M, formulation],
+                 dtype=np.int32).tofile(f)
+        np.array([emin, emax], dtype=np.float64).tofile(f)
+        np.asarray(H.row_ptr, dtype=np.int32).tofile(f)
+        np.asarray(H.col_ind, dtype=np.int32).tofile(f)
+        for A in (H, *V):
+            np.ascontiguousarray(A.values, dtype=np.float64).tofile(f)
+        np.ascontiguousarray(psi, dtype=np.complex128).view(np.float64).tofile(f)
+    out = subprocess.run([str(exe), str(tmp_path / "in.bin")], capture_output=True, text=True,
+                         timeout=300)
+    assert out.returncode == 0, out.stderr
+    d = json.loads(out.stdout)
+    sig = np.array(d["sigma"]).reshape(M, 6)
+    c, hw = (emax + emin) / 2, (emax - emin) / 2
+    op = oracle.make_op(to_oracle(H), c, hw)
+    sig_o, en_o = oracle.fftcheb(op, [to_oracle(v, imag=True) for v in V], psi, M,
+                                 formulation=formulation, prefactor=1.0, sections=1)
+    assert np.allclose(np.array(d["energy"]), en_o, rtol=0, atol=1e-13)
+    assert np.linalg.norm(sig - sig_o) <= 1e-10 * np.linalg.norm(sig_o)

@@ -338,7 +338,10 @@ NARROW = [(96, 8, 6, False, False, 8, False), (96, 8, 6, False, False, 4, True),
           (97, 8, 7, False, False, 256, False), (97, 8, 7, False, False, 2, True),
           # narrow tensor-core widths W = 32 and complex W = 16, 32
           (97, 8, 7, False, False, 32, False), (97, 8, 7, False, False, 8, True),
-          (97, 8, 7, False, False, 16, True)]
+          (97, 8, 7, False, False, 16, True),
+          # complex H of 1x1 blocks, 3 complex columns: the staged kernel's
+          # 48 KB of dynamic shared memory plus its static dot-finish arrays
+          (60, 1, 5, True, False, 3, True)]
 
 
 @pytest.mark.parametrize("kernel", ["staged", "rowsplit", "bulk", "bulk_smem", "narrow", "dmma",
