@@ -1,0 +1,80 @@
+"""The step kernel's default dispatch over a grid of shapes: block sizes 1,
+2, 3, 5, 8; real, complex and imaginary-unit matrices; real and complex
+panels of 1 to 64 columns; FP64 and FP32.  Every case runs the SpMM
+(rsatb_bsr_mult_dense) against the oracle's SpMM and the doubled KPM
+recurrence (rsatb_kpm_dos_moments, whose step kernels carry the fused dots)
+against the oracle's moments (Hermitian matrices).  The point is the launch
+path itself: each shape reaches one kernel family and launch configuration
+(mapping, shared memory opt-in, grid), and a shape no other test reaches
+must still launch and agree."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle
+from _util import random_hermitian_bsr, rel_err, to_oracle
+
+pytestmark = pytest.mark.gpu
+
+WIDTHS = [1, 2, 3, 4, 5, 7, 8, 12, 16, 24, 32, 40, 64]
+KINDS = [("real", False, False, False), ("complex", True, False, True),
+         ("imaginary", False, True, True), ("real_cplx_panel", False, False, True)]
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    torch.cuda.set_device(0)
+    return torch
+
+
+def _dtype(torch, precision, cv):
+    return {("f64", True): torch.complex128, ("f64", False): torch.float64,
+            ("f32", True): torch.complex64, ("f32", False): torch.float32}[(precision, cv)]
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+@pytest.mark.parametrize("kind", KINDS, ids=[k[0] for k in KINDS])
+@pytest.mark.parametrize("b", [1, 2, 3, 5, 8])
+def test_default_dispatch_sweep(torch_cuda, b, kind, precision):
+    torch = torch_cuda
+    from rsatb_b200.calc import Chebyshev, kpm_dos_moments
+    from rsatb_b200.vbcsr import BlockSpMat
+    _, cm, imag, cv = kind
+    n = 37
+    A = random_hermitian_bsr(n, b, 4, seed=100 + b, complex_values=cm, scale=0.3)
+    if imag:
+        A = A.with_values(A.values.real.copy())
+    Ao = to_oracle(A, imag=imag)
+    Ad = BlockSpMat(A.row_ptr, A.col_ind, A.values, b, A.n_block_cols, imaginary=imag)
+    if precision == "f32":
+        Ad = Ad.astype("f32")
+    # i W of a symmetric W is anti-Hermitian: it is swept through the SpMM
+    # only (velocity matrices never enter the recurrence as the operator).
+    bound = 1.0 if imag else np.abs(np.linalg.eigvalsh(A.to_dense())).max() + 0.5
+    c = Chebyshev(Ad, -bound, bound)
+    op = oracle.make_op(Ao, 0.0, bound)
+    rng = np.random.default_rng(b * 17 + len(kind[0]))
+    tol_mv = 1e-13 if precision == "f64" else 2e-5
+    tol_mu = 1e-10 if precision == "f64" else 2e-5
+    failures = []
+    for R in WIDTHS:
+        X = rng.standard_normal((n * b, R))
+        if cv:
+            X = X + 1j * rng.standard_normal((n * b, R))
+        Xd = torch.as_tensor(X).cuda().to(_dtype(torch, precision, cv)).contiguous()
+        Yd = torch.empty_like(Xd)
+        Ad.mult_dense(Xd, Yd, alpha=0.5)
+        err = rel_err(Yd.cpu().numpy(), oracle.spmm(Ao, X, alpha=0.5))
+        if not err < tol_mv:
+            failures.append(("spmm", R, err))
+        if imag:
+            continue
+        Xq = Xd.to(torch.complex128 if cv else torch.float64).cpu().numpy()
+        mu = kpm_dos_moments(c, Xd, 10)
+        want = oracle.kpm_moments(op, Xq, 10)
+        err = np.abs(mu - want).max() / abs(want[0])
+        if not err < tol_mu:
+            failures.append(("moments", R, err))
+    assert not failures, failures
