@@ -78,3 +78,38 @@ def test_default_dispatch_sweep(torch_cuda, b, kind, precision):
         if not err < tol_mu:
             failures.append(("moments", R, err))
     assert not failures, failures
+
+
+@pytest.mark.parametrize("cm", [False, True], ids=["real", "complex"])
+@pytest.mark.parametrize("b", [1, 3, 8])
+def test_cg_solve_sweep(torch_cuda, b, cm):
+    """The batched CG (rsatb_cg_solve: the fused S P + <p|Sp>, the update with
+    alpha and the new residual, the direction) over column counts that do
+    and do not divide the 256 threads of its dot CTAs (1, 3, 8, 17, 64),
+    real and complex Hermitian S, against the dense solve to 1e-9."""
+    torch = torch_cuda
+    from rsatb_b200.calc import cg_solve
+    from rsatb_b200.vbcsr import BlockSpMat
+    n = 29
+    A = random_hermitian_bsr(n, b, 3, seed=7 + b, complex_values=cm, scale=0.2)
+    w = np.linalg.eigvalsh(A.to_dense())
+    shift = 1.0 - w[0]  # S = A + shift I, smallest eigenvalue 1
+    vals = A.values.copy()
+    for i in range(n):
+        for k in range(A.row_ptr[i], A.row_ptr[i + 1]):
+            if A.col_ind[k] == i:
+                vals[k] += shift * np.eye(b)
+    S = A.with_values(vals)
+    Sd = BlockSpMat(S.row_ptr, S.col_ind, S.values, b)
+    dense = S.to_dense()
+    rng = np.random.default_rng(b)
+    dt = torch.complex128 if cm else torch.float64
+    for R in (1, 3, 8, 17, 64):
+        Bh = rng.standard_normal((n * b, R))
+        if cm:
+            Bh = Bh + 1j * rng.standard_normal((n * b, R))
+        B = torch.as_tensor(Bh).cuda().to(dt).contiguous()
+        X = torch.zeros_like(B)
+        it, res = cg_solve(Sd, B, X, tol=1e-12, max_iter=500)
+        want = np.linalg.solve(dense, Bh)
+        assert rel_err(X.cpu().numpy(), want) < 1e-9, (R, it, res)
