@@ -113,3 +113,48 @@ def test_cg_solve_sweep(torch_cuda, b, cm):
         it, res = cg_solve(Sd, B, X, tol=1e-12, max_iter=500)
         want = np.linalg.solve(dense, Bh)
         assert rel_err(X.cpu().numpy(), want) < 1e-9, (R, it, res)
+
+
+def _antisymmetric(A):
+    """Real W with W^T = -W on A's (symmetric) pattern: V = i W is Hermitian."""
+    vals = np.zeros_like(A.values, dtype=np.float64)
+    rows = np.repeat(np.arange(A.n_block_rows), np.diff(A.row_ptr))
+    index = {(int(i), int(j)): k for k, (i, j) in enumerate(zip(rows, A.col_ind))}
+    for (i, j), k in index.items():
+        blk = A.values[k].real
+        if i == j:
+            vals[k] = 0.5 * (blk - blk.T)
+        elif i < j:
+            vals[k] = blk
+            vals[index[(j, i)]] = -blk.T
+    return A.with_values(vals)
+
+
+@pytest.mark.parametrize("b", [1, 2, 5])
+def test_fftcheb_sweep(torch_cuda, b):
+    """rsatb_dc_spectrum_fftcheb (Greenwood and Bastin) for block sizes 1, 2,
+    5 and sample counts 1, 2, 5 (left panels of 2R, right panels of 6R real
+    values) against the oracle's dc_spectrum_fftcheb to 1e-10."""
+    torch = torch_cuda
+    from rsatb_b200.calc import Chebyshev
+    from rsatb_b200.transport import dc_spectrum_fftcheb
+    from rsatb_b200.vbcsr import BlockSpMat
+    n = 23
+    H = random_hermitian_bsr(n, b, 3, seed=31 + b, complex_values=False, scale=0.4)
+    Ws = [_antisymmetric(random_hermitian_bsr(n, b, 3, seed=31 + b, complex_values=False,
+                                              scale=0.2 + 0.1 * a)) for a in range(3)]
+    w = np.linalg.eigvalsh(H.to_dense())
+    emin, emax = w[0] - 0.3, w[-1] + 0.3
+    c = Chebyshev(BlockSpMat(H.row_ptr, H.col_ind, H.values, b), emin, emax)
+    Vd = [BlockSpMat(W.row_ptr, W.col_ind, W.values, b, imaginary=True) for W in Ws]
+    op = oracle.make_op(to_oracle(H), (emax + emin) / 2, (emax - emin) / 2)
+    Vo = [to_oracle(W, imag=True) for W in Ws]
+    rng = np.random.default_rng(b)
+    for R, M, form in ((1, 7, 0), (2, 16, 1), (5, 9, 0), (5, 12, 1)):
+        psi = np.exp(2j * np.pi * rng.random((n * b, R))) / np.sqrt(n * b)
+        p = torch.as_tensor(psi).cuda().contiguous()
+        sig, en = dc_spectrum_fftcheb(c, *Vd, p, M, formulation=form)
+        sig_o, en_o = oracle.fftcheb(op, Vo, psi, M, formulation=form, prefactor=1.0,
+                                     sections=1)
+        assert np.allclose(en, en_o, rtol=0, atol=1e-13)
+        assert rel_err(sig, sig_o) < 1e-10, (R, M, form)
