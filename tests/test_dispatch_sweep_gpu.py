@@ -158,3 +158,32 @@ def test_fftcheb_sweep(torch_cuda, b):
                                      sections=1)
         assert np.allclose(en, en_o, rtol=0, atol=1e-13)
         assert rel_err(sig, sig_o) < 1e-10, (R, M, form)
+
+
+@pytest.mark.parametrize("b", [1, 2, 3, 4, 5, 8])
+def test_vjp_sweep(torch_cuda, b):
+    """rsatb_kpm_moments_vjp for every built block size and sample counts 1,
+    3, 8 (the recurrence kernels and the SDDMM at each width) against the
+    oracle's dense FP64 reference gradient to 1e-10."""
+    torch = torch_cuda
+    from rsatb_b200.adjoint import kpm_moments_vjp
+    from rsatb_b200.calc import Chebyshev
+    from rsatb_b200.vbcsr import BlockSpMat
+    n = 19
+    H = random_hermitian_bsr(n, b, 3, seed=51 + b, complex_values=False, scale=0.4)
+    Hd = H.to_dense()
+    w = np.linalg.eigvalsh(Hd)
+    emin, emax = w[0] - 0.3, w[-1] + 0.3
+    c = Chebyshev(BlockSpMat(H.row_ptr, H.col_ind, H.values, b), emin, emax)
+    cc, hw = (emax + emin) / 2, (emax - emin) / 2
+    rows = np.repeat(np.arange(n), np.diff(H.row_ptr))
+    rng = np.random.default_rng(b)
+    for R, M in ((1, 5), (3, 12), (8, 9)):
+        psi = rng.choice([-1.0, 1.0], size=(n * b, R)) / np.sqrt(n * b)
+        dmu = rng.standard_normal(M)
+        grad, mu, _ = kpm_moments_vjp(c, torch.as_tensor(psi).cuda(), M, dmu, 0)
+        G = oracle.kpm_moments_vjp_dense(Hd, psi, cc, hw, M, dmu)
+        want = np.stack([G[i * b:(i + 1) * b, j * b:(j + 1) * b]
+                         for i, j in zip(rows, H.col_ind)])
+        assert np.abs(mu - oracle.kpm_plain_moments_dense(Hd, psi, cc, hw, M)).max() < 1e-12
+        assert rel_err(grad.cpu().numpy().reshape(want.shape), want) < 1e-10, (R, M)
