@@ -187,3 +187,31 @@ def test_vjp_sweep(torch_cuda, b):
                          for i, j in zip(rows, H.col_ind)])
         assert np.abs(mu - oracle.kpm_plain_moments_dense(Hd, psi, cc, hw, M)).max() < 1e-12
         assert rel_err(grad.cpu().numpy().reshape(want.shape), want) < 1e-10, (R, M)
+
+
+@pytest.mark.parametrize("b", [1, 2, 3, 5, 8])
+def test_refine_sweep(torch_cuda, b):
+    """The sparse Newton-Schulz refinement (rsatb_inverse_sqrt_refine: the
+    block SpGEMM at every block size up to 8, the runtime-size numeric phase
+    below 8) from the seed c I on S's pattern, against the oracle's dense
+    restatement of the loop: same steps, factor to 1e-10."""
+    from rsatb_b200.isqrt import InverseSqrtOptions, inverse_sqrt
+    n = 26
+    A = random_hermitian_bsr(n, b, 3, seed=71 + b, complex_values=False, scale=0.15)
+    w = np.linalg.eigvalsh(A.to_dense())
+    vals = A.values.copy()
+    seed_vals = np.zeros_like(vals)
+    s_max = w[-1] + (1.0 - w[0])
+    for i in range(n):
+        for k in range(A.row_ptr[i], A.row_ptr[i + 1]):
+            if A.col_ind[k] == i:
+                vals[k] += (1.0 - w[0]) * np.eye(b)  # spectrum in [1, s_max]
+                seed_vals[k] = np.eye(b) / np.sqrt(s_max)
+    S = A.with_values(vals)
+    Z0 = A.with_values(seed_vals)
+    Z, rep = inverse_sqrt(S, InverseSqrtOptions(tol=1e-11, sptol=0.0, maxit=30, route=1),
+                          seed=Z0)
+    Zd = Z.to_arrays().to_dense()
+    Z_ref, r_ref = oracle.ns_refine_dense(S.to_dense(), Z0.to_dense(), b, tol=1e-11, maxit=30)
+    assert rep.converged == r_ref["converged"] and rep.steps == r_ref["steps"], (rep, r_ref)
+    assert np.abs(Zd - Z_ref).max() <= 1e-10 * np.abs(Z_ref).max()
