@@ -215,3 +215,33 @@ def test_refine_sweep(torch_cuda, b):
     Z_ref, r_ref = oracle.ns_refine_dense(S.to_dense(), Z0.to_dense(), b, tol=1e-11, maxit=30)
     assert rep.converged == r_ref["converged"] and rep.steps == r_ref["steps"], (rep, r_ref)
     assert np.abs(Zd - Z_ref).max() <= 1e-10 * np.abs(Z_ref).max()
+
+
+@pytest.mark.parametrize("b", [1, 2, 5])
+def test_qe_sweep(torch_cuda, b):
+    """The quasi-eigenstate route (rsatb_dc_spectrum_qe) for block sizes 1,
+    2, 5, sample counts 1 and 3, all nodes and a window of them, equal to the
+    FFT-Chebyshev Greenwood spectrum on the same nodes to 1e-10."""
+    torch = torch_cuda
+    from rsatb_b200.calc import Chebyshev
+    from rsatb_b200.transport import dc_spectrum_fftcheb, dc_spectrum_qe
+    from rsatb_b200.vbcsr import BlockSpMat
+    n = 21
+    H = random_hermitian_bsr(n, b, 3, seed=91 + b, complex_values=False, scale=0.4)
+    Ws = [_antisymmetric(random_hermitian_bsr(n, b, 3, seed=91 + b, complex_values=False,
+                                              scale=0.3 + 0.1 * a)) for a in range(3)]
+    w = np.linalg.eigvalsh(H.to_dense())
+    c = Chebyshev(BlockSpMat(H.row_ptr, H.col_ind, H.values, b), w[0] - 0.3, w[-1] + 0.3)
+    Vd = [BlockSpMat(W.row_ptr, W.col_ind, W.values, b, imaginary=True) for W in Ws]
+    rng = np.random.default_rng(b)
+    for R, M, nodes in ((1, 11, None), (3, 20, [2, 3, 7, 15, 19])):
+        psi = np.exp(2j * np.pi * rng.random((n * b, R))) / np.sqrt(n * b)
+        p = torch.as_tensor(psi).cuda().contiguous()
+        sig_f, en_f = dc_spectrum_fftcheb(c, *Vd, p, M)
+        sig_q, en_q = dc_spectrum_qe(c, *Vd, p, M, nodes_ascending=nodes)
+        idx = np.arange(M) if nodes is None else np.array(nodes)
+        assert np.allclose(en_q, en_f, rtol=0, atol=1e-13)
+        assert rel_err(sig_q[idx], sig_f[idx]) < 1e-10, (R, M)
+        if nodes is not None:
+            rest = np.setdiff1d(np.arange(M), idx)
+            assert np.all(sig_q[rest] == 0.0)
