@@ -31,7 +31,25 @@ struct State {
     int status;       // rsatb_status
     int cap;          // iteration cap of the current phase
     int restart;      // FP64 phase restarts from Z0 (the tensor-core phase failed)
+    int lift;         // next P uses the lift polynomial (tensor-core phase, ||X - I||_F large)
 };
+
+// P = a I + b X + c X X^T.  The reference's polynomial (15/8, -5/4, 3/8),
+// rsatb/calc/isqrtm.hpp:646-667, maps an eigenvalue x of X to
+// x p(x)^2 = 1 + (5/8) e^3 at x = 1 + e (cubic) and lifts a small x by
+// p(0)^2 = 3.52 per step.  The lift polynomial (5/2, -5/2, 1) is the member
+// of the family p(1) = 1, p'(1) = -1/2 (x = 1 a fixed point with quadratic
+// convergence, 1 + (5/4) e^2) with p(0)^2 = 6.25: it maps [0, 9/8] into
+// itself (its maximum, 9/8, at x = 1/2), so from the start, where the scale
+// puts every eigenvalue in (0, 1], it lifts the small ones in
+// log(1/x) / log(6.25) steps instead of log(1/x) / log(3.52) without
+// leaving [0, 9/8]; the cubic polynomial finishes from there.
+struct PolyCoef {
+    float a, b, c;
+};
+__host__ __device__ inline PolyCoef poly_coef(int lift) {
+    return lift ? PolyCoef{2.5f, -2.5f, 1.0f} : PolyCoef{1.875f, -1.25f, 0.375f};
+}
 
 enum EpiMode { EPI_STORE = 0, EPI_RESID = 1, EPI_POLY = 2 };
 
@@ -60,7 +78,7 @@ struct TcArgs {
     float* c_hi;             // C = A B^T: TF32-rounded value
     float* c_lo;             // and the residual value - c_hi (exact)
     double* c64;             // optional FP64 copy of C (c_hi + c_lo), nullptr: none
-    const float* xe_hi;      // EPI_POLY: X (hi + lo) for P = 1.875 I - 1.25 X + 0.375 X X^T
+    const float* xe_hi;      // EPI_POLY: X (hi + lo) for P = a I + b X + c X X^T (poly_coef)
     const float* xe_lo;
     double* res2;            // EPI_RESID: per-problem sum of (C - I)^2 over the valid corner
     float* ct_hi;            // optional transposed store of C (hi, lo), nullptr: none

@@ -232,6 +232,7 @@ __global__ void __launch_bounds__(128, 1)
             const bool in_mat = row < pr.n_pad;
             const bool vrow = row < pr.n;
             const int np = pr.n_pad;
+            const PolyCoef pc = poly_coef(args.mode == EPI_POLY && args.state[item.p].lift);
             double r2 = 0.0;
             for (int c = 0; c < item.nt; c += 16) {
                 float v[16];
@@ -247,7 +248,7 @@ __global__ void __launch_bounds__(128, 1)
                     const bool valid = vrow && col < pr.n;
                     float x = v[j];
                     if (args.mode == EPI_POLY)
-                        x = fmaf(0.375f, x, fmaf(-1.25f, xe[j], row == col ? 1.875f : 0.0f));
+                        x = fmaf(pc.c, x, fmaf(pc.b, xe[j], row == col ? pc.a : 0.0f));
                     if (!valid) x = 0.0f;
                     if (args.mode == EPI_RESID && valid && (!args.sym || col >= row)) {
                         const double d = double(x) - (row == col ? 1.0 : 0.0);
@@ -296,6 +297,7 @@ __device__ __forceinline__ void ws_epilogue(const TcArgs& args, const TcItem& it
     const bool in_mat = row < pr.n_pad;
     const bool vrow = row < pr.n;
     const int np = pr.n_pad;
+    const PolyCoef pc = poly_coef(args.mode == EPI_POLY && args.state[item.p].lift);
     double r2 = 0.0;
     // Two warps share a TMEM lane quarter: they take alternate 16-column
     // chunks, the next chunk's TMEM load in flight while one is stored.
@@ -322,7 +324,7 @@ __device__ __forceinline__ void ws_epilogue(const TcArgs& args, const TcItem& it
                 const bool valid = vrow && col < pr.n;
                 float x = v[j];
                 if (args.mode == EPI_POLY)
-                    x = fmaf(0.375f, x, fmaf(-1.25f, xe[j], row == col ? 1.875f : 0.0f));
+                    x = fmaf(pc.c, x, fmaf(pc.b, xe[j], row == col ? pc.a : 0.0f));
                 if (!valid) x = 0.0f;
                 if (args.mode == EPI_RESID && valid && (!args.sym || col >= row)) {
                     const double d = double(x) - (row == col ? 1.0 : 0.0);
