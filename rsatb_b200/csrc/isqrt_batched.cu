@@ -186,13 +186,22 @@ __global__ void restart_kernel(const Prob* probs, const State* st, const double*
 // benchmark's spectra (n ~ U[40, 400], kappa ~ [1e2, 1e5]), it cuts the
 // n^3-weighted mean of the steps to ||X - I||_F < 1e-4 from 10.2 to 7.8
 // (continuous) and from 11.3 to 8.4 (gapped).
+//
+// With floor_stop (tensor-core phase) a step of the cubic polynomial from
+// norm_pre < kFloorFrom that ends above twice its exact-arithmetic bound
+// also stops: for |e| < 1/2 an eigenvalue error e of X becomes at most
+// 1.25 (5/8) |e|^3, so ||X - I||_F falls to at most 0.78 norm_pre^3, and a
+// residual above 1.5625 norm_pre^3 is the rounding floor of the phase.  It
+// saves the step the rise test needs to see the floor.
 constexpr double kQuadratic = 0.5;
 constexpr double kLift = 1.0;
+constexpr double kFloorFrom = 0.1;
 __global__ void control_kernel(int np_count, State* st, double* res2, double tol,
-                               int stop_on_rise, int lift) {
+                               int stop_on_rise, int lift, int floor_stop) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= np_count) return;
     State x = st[p];
+    const int applied_lift = x.lift;  // the polynomial of the step just taken
     x.retire = 0;
     x.lift = 0;
     if (x.active) {
@@ -202,6 +211,9 @@ __global__ void control_kernel(int np_count, State* st, double* res2, double tol
         bool go = norm > tol && x.count < x.cap &&
                   (!near || fabs(x.norm_pre - norm) > 0.005 * norm);
         if (near && stop_on_rise && x.count > 0 && norm >= x.norm_pre) go = false;
+        if (floor_stop && x.count > 0 && !applied_lift && x.norm_pre < kFloorFrom &&
+            norm > 1.5625 * x.norm_pre * x.norm_pre * x.norm_pre)
+            go = false;
         if (!(norm <= 100.0)) {  // also catches NaN
             x.active = 0;
             x.retire = 1;
@@ -501,6 +513,13 @@ bool fp64_update() {
 // reference's polynomial throughout (RSATB_NS_LIFT=0).
 bool lift_enabled() {
     const char* s = std::getenv("RSATB_NS_LIFT");
+    return !(s && s[0] == '0');
+}
+
+// The floor test of the tensor-core phase (the default; RSATB_NS_FLOOR=0:
+// the plateau and rise tests only).
+bool floor_stop_enabled() {
+    const char* s = std::getenv("RSATB_NS_FLOOR");
     return !(s && s[0] == '0');
 }
 
@@ -811,6 +830,7 @@ int run_chunk(rsatb_context* ctx, const Opts& o, const Chunk& ch, const int* col
     const bool use_ws_tc = o.ws;
     const bool update64 = fp64_update();
     const int lift = lift_enabled() ? 1 : 0;
+    const int floor_stop = floor_stop_enabled() ? 1 : 0;
     if (low) {
         RSATB_TRY(prepare_tc_gemm());
         RSATB_TRY(run_phase(ctx, o.graph, [&]() -> int {
@@ -825,7 +845,8 @@ int run_chunk(rsatb_context* ctx, const Opts& o, const Chunk& ch, const int* col
                 RSATB_TRY(tc_gemm(ctx, ch, d, d.tc_items, group_begin, a.z_hi, a.z_lo, a.w_hi,
                                   a.w_lo, a.x_hi, a.x_lo, nullptr, EPI_RESID, nullptr, nullptr,
                                   split, o.ws, stats));
-                control_kernel<<<cb, 256, 0, s>>>(P, d.state, d.res2, o.tol, 1, lift);
+                control_kernel<<<cb, 256, 0, s>>>(P, d.state, d.res2, o.tol, 1, lift,
+                                                  floor_stop);
                 RSATB_LAUNCH_CHECK(ctx);
                 if (c == 1 && update64) {
                     retire_low_kernel<<<P, 256, 0, s>>>(d.probs, d.state, a.z64[1], a.z64[0]);
@@ -898,7 +919,7 @@ int run_chunk(rsatb_context* ctx, const Opts& o, const Chunk& ch, const int* col
             RSATB_TRY(f64_gemm<true>(ctx, d, a.z64[c], a.s64, a.w64, EPI_STORE, nullptr, stats));
             RSATB_TRY(f64_gemm<true>(ctx, d, a.z64[c], a.w64, a.x64, EPI_RESID, nullptr, stats,
                                      nullptr, nullptr, true));
-            control_kernel<<<cb, 256, 0, s>>>(P, d.state, d.res2, o.tol, 0, 0);
+            control_kernel<<<cb, 256, 0, s>>>(P, d.state, d.res2, o.tol, 0, 0, 0);
             RSATB_LAUNCH_CHECK(ctx);
             retire_out_kernel<<<P, 256, 0, s>>>(d.probs, d.state, a.z64[c], d.col_start,
                                                 d.k_cols, d.out_off, out);
