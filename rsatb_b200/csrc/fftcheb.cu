@@ -20,7 +20,10 @@
 //   FFT (cuFFT, sequences interleaved: stride = batch) of the half-grid
 //   phased even extension, built and read back with coalesced accesses;
 // * the contraction gives each energy k to one CTA per chunk: no atomics,
-//   the same summation order on every run.
+//   the same summation order on every run;
+// * at M = 2048 (Greenwood) the row stage is one hand-written kernel after a
+//   coalesced gather: extension, 4096-point transform and contraction
+//   without the FP64 extension buffer's round trips (greenwood_fused_kernel).
 #include "cheb_kernels.cuh"
 
 #include <cufft.h>
@@ -28,6 +31,7 @@
 #include <algorithm>
 #include <cmath>
 #include <complex>
+#include <type_traits>
 #include <vector>
 
 namespace rsatb_b200 {
@@ -223,6 +227,250 @@ __global__ void __launch_bounds__(256) greenwood_contract_kernel(int M, int64_t 
             K[2 * (int64_t(k) * 6 + comp)] += red[a][0][0] * inv;
             K[2 * (int64_t(k) * 6 + comp) + 1] += red[a][1][0] * inv;
         }
+}
+
+// ---------------------------------------------------------------------------
+// Fused Greenwood row stage for M = 2048 (a 4096-point transform): the even
+// extension, the DCT-III (the inverse 2M-point DFT of extend_kernel's
+// sequence, outputs k < M) and the contraction in one kernel, FP64
+// arithmetic, so the moments are read once and nothing else touches HBM.
+//
+// One CTA of 256 threads transforms one sequence at a time as 16 x 16 x 16
+// (n = n0 + 16 n1 + 256 n2, k = k0 + 16 k1 + 256 k2, w = e^{2 pi i / 4096}):
+//   pass A  thread (n0, n1): 16-point DFT over n2 -> k0, times w^{(n0 + 16 n1) k0}
+//   pass B  thread (n0, k0): 16-point DFT over n1 -> k1, times w^{16 n0 k1}
+//   pass C  thread (k0, k1): 16-point DFT over n0 -> k2; k < 2048 is k2 < 8
+// with the values between passes exchanged through shared memory (planes of
+// 257 entries, so the 16-byte accesses of a quarter warp fall on distinct
+// banks).  Pass A builds the extension as it loads: E_n = ph_n x_n (n < M),
+// 0 (n = M), conj(ph_{2M-n}) x_{2M-n} (n > M), ph_m = w_m e^{i pi m / 2M}.
+// Each thread keeps the left sequence's 8 outputs, transforms the right
+// sequence and accumulates conj(L3_k) R3_k for its 8 energies in FP64 over
+// the CTA's sequences (a fixed grid-stride order); fused_reduce_kernel sums
+// the CTAs in a fixed order, so results do not depend on timing.
+//
+// The store is moment-major (each moment's rows written coalesced by the
+// recurrence), so one sequence is 2048 values 8 or 16 bytes apiece at a
+// stride of the slot size; gather_sequences_kernel first turns a chunk of
+// consecutive sequences into sequence-major rows with a tiled transpose
+// (both sides coalesced), from which pass A reads 256 contiguous values per
+// warp instruction.
+constexpr int kFusedM = 2048;
+constexpr int kFusedThreads = 256;
+constexpr int kXchPlane = 257;
+constexpr size_t kFusedSmem =
+    size_t(16 * kXchPlane + 1024 + kFusedM) * sizeof(double2);  // exchange, w^j, ph
+
+__device__ __forceinline__ double2 c_add(double2 a, double2 b) {
+    return make_double2(a.x + b.x, a.y + b.y);
+}
+__device__ __forceinline__ double2 c_sub(double2 a, double2 b) {
+    return make_double2(a.x - b.x, a.y - b.y);
+}
+__device__ __forceinline__ double2 c_mul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 c_mul_conj_a(double2 a, double2 b) {  // conj(a) b
+    return make_double2(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ double2 c_mul_i(double2 a) { return make_double2(-a.y, a.x); }
+
+// out[k] = sum_j in[j] i^{jk}, k = 0..3, in place.
+__device__ __forceinline__ void dft4_inv(double2& a0, double2& a1, double2& a2, double2& a3) {
+    const double2 s02 = c_add(a0, a2), d02 = c_sub(a0, a2);
+    const double2 s13 = c_add(a1, a3), d13 = c_mul_i(c_sub(a1, a3));
+    a0 = c_add(s02, s13);
+    a2 = c_sub(s02, s13);
+    a1 = c_add(d02, d13);
+    a3 = c_sub(d02, d13);
+}
+
+// 16-point DFT with the + sign, in place, as 4 x 4: j = j0 + 4 j1,
+// k = c + 4 r.  Output k sits at v[4 (k % 4) + k / 4] (dft16_at).
+__device__ __forceinline__ void dft16_inv(double2 (&v)[16]) {
+    constexpr double c8 = 0.92387953251128674;  // cos(pi / 8)
+    constexpr double s8 = 0.38268343236508978;  // sin(pi / 8)
+    constexpr double r2 = 0.70710678118654752;  // cos(pi / 4)
+#pragma unroll
+    for (int j0 = 0; j0 < 4; ++j0) dft4_inv(v[j0], v[j0 + 4], v[j0 + 8], v[j0 + 12]);
+    // v[j0 + 4 c] *= e^{2 pi i j0 c / 16}
+    v[1 + 4] = c_mul(v[1 + 4], make_double2(c8, s8));     // 1
+    v[2 + 4] = c_mul(v[2 + 4], make_double2(r2, r2));     // 2
+    v[3 + 4] = c_mul(v[3 + 4], make_double2(s8, c8));     // 3
+    v[1 + 8] = c_mul(v[1 + 8], make_double2(r2, r2));     // 2
+    v[2 + 8] = c_mul_i(v[2 + 8]);                         // 4
+    v[3 + 8] = c_mul(v[3 + 8], make_double2(-r2, r2));    // 6
+    v[1 + 12] = c_mul(v[1 + 12], make_double2(s8, c8));   // 3
+    v[2 + 12] = c_mul(v[2 + 12], make_double2(-r2, r2));  // 6
+    v[3 + 12] = c_mul(v[3 + 12], make_double2(-c8, -s8)); // 9
+#pragma unroll
+    for (int c = 0; c < 4; ++c) dft4_inv(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
+}
+__device__ __forceinline__ int dft16_at(int k) { return 4 * (k & 3) + (k >> 2); }
+
+// w^n = e^{2 pi i n / 4096} from the quarter table q[j] = w^j, j < 1024.
+__device__ __forceinline__ double2 twiddle4096(const double2* q, int n) {
+    const double2 b = q[n & 1023];
+    switch ((n >> 10) & 3) {
+        case 0: return b;
+        case 1: return make_double2(-b.y, b.x);
+        case 2: return make_double2(-b.x, -b.y);
+        default: return make_double2(b.y, -b.x);
+    }
+}
+
+__device__ __forceinline__ double2 load_c(const float* S, int64_t e) {
+    const float2 f = __ldg(reinterpret_cast<const float2*>(S) + e);
+    return make_double2(double(f.x), double(f.y));
+}
+__device__ __forceinline__ double2 load_c(const double* S, int64_t e) {
+    return __ldg(reinterpret_cast<const double2*>(S) + e);
+}
+
+// The 8 outputs k0 + 16 k1 + 256 k2 (k2 < 8) of thread (k0, k1) for the
+// sequence whose element m is S[m + base] (complex index; sequence-major).
+template <typename T>
+__device__ __forceinline__ void fused_transform(const T* S, int64_t base, const double2* qtw,
+                                                const double2* ph, double2* xch,
+                                                double2 (&out)[8]) {
+    const int t = threadIdx.x;
+    double2 v[16];
+    // pass A: thread (n0, n1) = (t % 16, t / 16) holds E_{t + 256 n2}
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        const int n = t + 256 * j;
+        if (j < 8) {
+            v[j] = c_mul(ph[n], load_c(S, base + n));
+        } else if (n == kFusedM) {
+            v[j] = make_double2(0.0, 0.0);
+        } else {
+            const int m = 2 * kFusedM - n;
+            const double2 p = ph[m];
+            v[j] = c_mul(make_double2(p.x, -p.y), load_c(S, base + m));
+        }
+    }
+    dft16_inv(v);
+    {
+        const int n0 = t & 15, n1 = t >> 4;
+#pragma unroll
+        for (int k0 = 0; k0 < 16; ++k0)
+            xch[n0 * kXchPlane + k0 * 16 + n1] =
+                c_mul(v[dft16_at(k0)], twiddle4096(qtw, t * k0));
+    }
+    __syncthreads();
+    // pass B: thread (n0, k0) = (t % 16, t / 16)
+    {
+        const int n0 = t & 15, k0 = t >> 4;
+#pragma unroll
+        for (int n1 = 0; n1 < 16; ++n1) v[n1] = xch[n0 * kXchPlane + k0 * 16 + n1];
+        dft16_inv(v);
+        __syncthreads();
+#pragma unroll
+        for (int k1 = 0; k1 < 16; ++k1)
+            xch[k0 * kXchPlane + k1 * 16 + n0] =
+                c_mul(v[dft16_at(k1)], twiddle4096(qtw, 16 * n0 * k1));
+    }
+    __syncthreads();
+    // pass C: thread (k0, k1) = (t % 16, t / 16)
+    {
+        const int k0 = t & 15, k1 = t >> 4;
+#pragma unroll
+        for (int n0 = 0; n0 < 16; ++n0) v[n0] = xch[k0 * kXchPlane + k1 * 16 + n0];
+        dft16_inv(v);
+#pragma unroll
+        for (int k2 = 0; k2 < 8; ++k2) out[k2] = v[dft16_at(k2)];
+    }
+    __syncthreads();  // xch is rewritten by the next transform
+}
+
+// The tables of the transform: tab[j] = w^j (j < 1024), tab[1024 + m] = ph_m.
+__global__ void fused_tables_kernel(const double* w, double2* tab) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double s, c;
+    if (i < 1024) {
+        sincospi(double(i) / 2048.0, &s, &c);  // w^j = e^{2 pi i j / 4096}
+        tab[i] = make_double2(c, s);
+    } else if (i < 1024 + kFusedM) {
+        const int m = i - 1024;
+        sincospi(double(m) / (2.0 * kFusedM), &s, &c);  // e^{i pi m / 2M}
+        tab[i] = make_double2(w[m] * c, w[m] * s);
+    }
+}
+
+// Tq[side][i][m] = S_side[m * slot + q0 + i] for i < nqc (complex entries):
+// 32 x 32 tiles through shared memory, blockIdx.z the side (left, right).
+template <typename T>
+__global__ void __launch_bounds__(256) gather_sequences_kernel(int64_t q0, int64_t nqc,
+                                                               int64_t slot, const T* SL,
+                                                               const T* SR, T* Tq) {
+    using C = typename std::conditional<std::is_same<T, float>::value, float2, double2>::type;
+    __shared__ C tile[32][33];
+    const C* S = reinterpret_cast<const C*>(blockIdx.z ? SR : SL);
+    C* out = reinterpret_cast<C*>(Tq) + int64_t(blockIdx.z) * nqc * kFusedM;
+    const int64_t i0 = int64_t(blockIdx.x) * 32;
+    const int m0 = blockIdx.y * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const int m = m0 + ty + 8 * r;
+        if (i0 + tx < nqc) tile[ty + 8 * r][tx] = S[int64_t(m) * slot + q0 + i0 + tx];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const int64_t i = i0 + ty + 8 * r;
+        if (i < nqc) out[i * kFusedM + m0 + tx] = tile[tx][ty + 8 * r];
+    }
+}
+
+// Gathered sequences i < nqc of one chunk (Tq, left then right);
+// partial[cta][k] += sum over the CTA's sequences of conj(L3_k) R3_k.
+template <typename T>
+__global__ void __launch_bounds__(kFusedThreads, 1)
+    greenwood_fused_kernel(int64_t nqc, const T* Tq, const double2* tab, double2* partial) {
+    extern __shared__ double2 fsm[];
+    double2* xch = fsm;
+    double2* qtw = xch + 16 * kXchPlane;
+    double2* ph = qtw + 1024;
+    for (int j = threadIdx.x; j < 1024 + kFusedM; j += blockDim.x) qtw[j] = tab[j];
+    __syncthreads();
+    double2 acc[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) acc[i] = make_double2(0.0, 0.0);
+    const int64_t right = nqc * kFusedM;
+    for (int64_t i = blockIdx.x; i < nqc; i += gridDim.x) {
+        double2 l3[8], r3[8];
+        fused_transform(Tq, i * kFusedM, qtw, ph, xch, l3);
+        fused_transform(Tq, right + i * kFusedM, qtw, ph, xch, r3);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[j] = c_add(acc[j], c_mul_conj_a(l3[j], r3[j]));
+    }
+    double2* p = partial + int64_t(blockIdx.x) * kFusedM + threadIdx.x;
+#pragma unroll
+    for (int k2 = 0; k2 < 8; ++k2) p[256 * k2] = c_add(p[256 * k2], acc[k2]);
+}
+
+// K[k][comp] += sum over the n_cta partials (in CTA order) / max(1e-14, 1 - eps_k^2).
+__global__ void fused_reduce_kernel(int n_cta, const double2* partial, int comp, double* K) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= kFusedM) return;
+    double re = 0.0, im = 0.0;
+    for (int c = 0; c < n_cta; ++c) {
+        const double2 p = partial[int64_t(c) * kFusedM + k];
+        re += p.x;
+        im += p.y;
+    }
+    const double eps = cos(M_PI * (double(k) + 0.5) / double(kFusedM));
+    const double wden = 1.0 - eps * eps;
+    const double inv = 1.0 / (wden > 1e-14 ? wden : 1e-14);
+    K[2 * (int64_t(k) * 6 + comp)] += re * inv;
+    K[2 * (int64_t(k) * 6 + comp) + 1] += im * inv;
+}
+
+// The fused row stage serves Greenwood at M = 2048 unless RSATB_FFTCHEB_FUSED=0.
+bool fused_enabled() {
+    const char* s = std::getenv("RSATB_FFTCHEB_FUSED");
+    return !(s && s[0] == '0');
 }
 
 // Owning device buffer released on scope exit.
@@ -444,6 +692,26 @@ int fftcheb_impl(const Ctx& c, const rsatb_bsr_matrix* const* V, const T* psi, i
     }
     RSATB_CUDA_TRY(cudaMemsetAsync(K, 0, size_t(M) * 12 * sizeof(double), st));
 
+    // Fused row stage (Greenwood, M = 2048): one CTA per SM, partial sums
+    // per CTA and energy; chunks of fused_qc sequences gathered into the
+    // extension buffer (sequence-major, both sides).
+    const bool fused = !bastin && M == kFusedM && fused_enabled();
+    const int fused_grid = ctx->sm_count;
+    const int64_t fused_qc = std::max<int64_t>(
+        1, std::min<int64_t>(8192, int64_t(size_t(n_tf) * 2 * 2 * size_t(M) * nq_max *
+                                           sizeof(double2) / (2 * size_t(M) * cplx))));
+    DevBuf bPart, bTab;
+    if (fused) {
+        RSATB_TRY(bPart.alloc(size_t(fused_grid) * kFusedM * sizeof(double2)));
+        RSATB_TRY(bTab.alloc(size_t(1024 + kFusedM) * sizeof(double2)));
+        fused_tables_kernel<<<(1024 + kFusedM) / 256, 256, 0, st>>>(bWts.as<double>(),
+                                                                    bTab.as<double2>());
+        RSATB_LAUNCH_CHECK(ctx);
+        RSATB_CUDA_TRY(cudaFuncSetAttribute(greenwood_fused_kernel<T>,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            int(kFusedSmem)));
+    }
+
     // cuFFT plans: full chunks and the last, shorter chunk of a section.
     Plan plans[2];
     int64_t plan_nq[2] = {0, 0};
@@ -544,9 +812,32 @@ int fftcheb_impl(const Ctx& c, const rsatb_bsr_matrix* const* V, const T* psi, i
         cudaEventElapsedTime(&t, ev0, ev1);
         rec_ms += t;
 
-        // Row stage in chunks of rows.
+        // Row stage: fused at M = 2048 (Greenwood), else in chunks of rows
+        // through the extension, cuFFT and the contraction.
         RSATB_CUDA_TRY(cudaEventRecord(ev0, st));
-        for (int64_t c0 = 0; c0 < rows; c0 += chunk_rows) {
+        if (fused) {
+            const int64_t per_axis = rows * R;
+            T* Tq = reinterpret_cast<T*>(EL);
+            for (int a = 0; a < 3; ++a) {
+                RSATB_CUDA_TRY(cudaMemsetAsync(
+                    bPart.p, 0, size_t(fused_grid) * kFusedM * sizeof(double2), st));
+                for (int64_t i0 = 0; i0 < per_axis; i0 += fused_qc) {
+                    const int64_t n = std::min<int64_t>(fused_qc, per_axis - i0);
+                    const dim3 gg(unsigned((n + 31) / 32), kFusedM / 32, 2);
+                    gather_sequences_kernel<T><<<gg, 256, 0, st>>>(int64_t(a) * per_axis + i0, n,
+                                                                   sslot, SL, SR, Tq);
+                    RSATB_LAUNCH_CHECK(ctx);
+                    greenwood_fused_kernel<T><<<fused_grid, kFusedThreads, kFusedSmem, st>>>(
+                        n, Tq, bTab.as<double2>(), bPart.as<double2>());
+                    RSATB_LAUNCH_CHECK(ctx);
+                    ++chunks;
+                }
+                fused_reduce_kernel<<<kFusedM / 256, 256, 0, st>>>(
+                    fused_grid, bPart.as<double2>(), a == 0 ? 0 : (a == 1 ? 3 : 5), K);
+                RSATB_LAUNCH_CHECK(ctx);
+            }
+        }
+        for (int64_t c0 = 0; !fused && c0 < rows; c0 += chunk_rows) {
             const int64_t cr = std::min<int64_t>(chunk_rows, rows - c0);
             const int64_t nq = 3 * cr * R;
             cufftHandle plan;
