@@ -779,7 +779,8 @@ def bench_transport(args, dist):
     t = -2.7 eV, interlayer 0.48 exp(-(d - 3.35)/0.45) within 6 A), commutator
     velocities at Gamma, random-phase samples sharded over the GPUs.  One step
     = one dc_spectrum_fftcheb call over this GPU's samples: FP32 vectors with
-    FP64 transform and contraction; the FP64 path is timed beside it."""
+    the fused row stage's FP32 transform with FP64 products and sums; the FP64
+    path is timed beside it."""
     import torch
     import oracle
     from rsatb_b200 import lattice
@@ -851,7 +852,7 @@ def bench_transport(args, dist):
                 ms32 * 1e-3), 1), "unit": "sample-moments/s", "n_gpus": dist.world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms32, 2),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32 vectors, FP64 transform and contraction",
+            "dtype": "f32 vectors and transform, FP64 contraction sums",
             "data": "synthetic (seeded TBG generator, random phases)",
             "config": {"workload": f"transport_tbg: m={args.tbg_m} moire cell tiled "
                                    f"{args.tbg_tiles}x{args.tbg_tiles}",

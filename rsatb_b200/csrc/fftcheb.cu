@@ -258,27 +258,44 @@ __global__ void __launch_bounds__(256) greenwood_contract_kernel(int M, int64_t 
 constexpr int kFusedM = 2048;
 constexpr int kFusedThreads = 256;
 constexpr int kXchPlane = 257;
-constexpr size_t kFusedSmem =
-    size_t(16 * kXchPlane + 1024 + kFusedM) * sizeof(double2);  // exchange, w^j, ph
+// Shared memory of the fused kernel: exchange planes, w^j (j < 1024), ph.
+template <typename C>
+constexpr size_t fused_smem() {
+    return size_t(16 * kXchPlane + 1024 + kFusedM) * sizeof(C);
+}
 
-__device__ __forceinline__ double2 c_add(double2 a, double2 b) {
-    return make_double2(a.x + b.x, a.y + b.y);
+// Complex arithmetic on float2 (FP32 transform) and double2 (FP64 transform).
+template <typename C> struct Cx;
+template <> struct Cx<float2> {
+    using S = float;
+    __device__ static float2 make(float x, float y) { return make_float2(x, y); }
+};
+template <> struct Cx<double2> {
+    using S = double;
+    __device__ static double2 make(double x, double y) { return make_double2(x, y); }
+};
+template <typename C>
+__device__ __forceinline__ C c_add(C a, C b) {
+    return Cx<C>::make(a.x + b.x, a.y + b.y);
 }
-__device__ __forceinline__ double2 c_sub(double2 a, double2 b) {
-    return make_double2(a.x - b.x, a.y - b.y);
+template <typename C>
+__device__ __forceinline__ C c_sub(C a, C b) {
+    return Cx<C>::make(a.x - b.x, a.y - b.y);
 }
-__device__ __forceinline__ double2 c_mul(double2 a, double2 b) {
-    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+template <typename C>
+__device__ __forceinline__ C c_mul(C a, C b) {
+    return Cx<C>::make(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
-__device__ __forceinline__ double2 c_mul_conj_a(double2 a, double2 b) {  // conj(a) b
-    return make_double2(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
+template <typename C>
+__device__ __forceinline__ C c_mul_i(C a) {
+    return Cx<C>::make(-a.y, a.x);
 }
-__device__ __forceinline__ double2 c_mul_i(double2 a) { return make_double2(-a.y, a.x); }
 
 // out[k] = sum_j in[j] i^{jk}, k = 0..3, in place.
-__device__ __forceinline__ void dft4_inv(double2& a0, double2& a1, double2& a2, double2& a3) {
-    const double2 s02 = c_add(a0, a2), d02 = c_sub(a0, a2);
-    const double2 s13 = c_add(a1, a3), d13 = c_mul_i(c_sub(a1, a3));
+template <typename C>
+__device__ __forceinline__ void dft4_inv(C& a0, C& a1, C& a2, C& a3) {
+    const C s02 = c_add(a0, a2), d02 = c_sub(a0, a2);
+    const C s13 = c_add(a1, a3), d13 = c_mul_i(c_sub(a1, a3));
     a0 = c_add(s02, s13);
     a2 = c_sub(s02, s13);
     a1 = c_add(d02, d13);
@@ -287,66 +304,72 @@ __device__ __forceinline__ void dft4_inv(double2& a0, double2& a1, double2& a2, 
 
 // 16-point DFT with the + sign, in place, as 4 x 4: j = j0 + 4 j1,
 // k = c + 4 r.  Output k sits at v[4 (k % 4) + k / 4] (dft16_at).
-__device__ __forceinline__ void dft16_inv(double2 (&v)[16]) {
-    constexpr double c8 = 0.92387953251128674;  // cos(pi / 8)
-    constexpr double s8 = 0.38268343236508978;  // sin(pi / 8)
-    constexpr double r2 = 0.70710678118654752;  // cos(pi / 4)
+template <typename C>
+__device__ __forceinline__ void dft16_inv(C (&v)[16]) {
+    using S = typename Cx<C>::S;
+    constexpr S c8 = S(0.92387953251128674);  // cos(pi / 8)
+    constexpr S s8 = S(0.38268343236508978);  // sin(pi / 8)
+    constexpr S r2 = S(0.70710678118654752);  // cos(pi / 4)
 #pragma unroll
     for (int j0 = 0; j0 < 4; ++j0) dft4_inv(v[j0], v[j0 + 4], v[j0 + 8], v[j0 + 12]);
     // v[j0 + 4 c] *= e^{2 pi i j0 c / 16}
-    v[1 + 4] = c_mul(v[1 + 4], make_double2(c8, s8));     // 1
-    v[2 + 4] = c_mul(v[2 + 4], make_double2(r2, r2));     // 2
-    v[3 + 4] = c_mul(v[3 + 4], make_double2(s8, c8));     // 3
-    v[1 + 8] = c_mul(v[1 + 8], make_double2(r2, r2));     // 2
-    v[2 + 8] = c_mul_i(v[2 + 8]);                         // 4
-    v[3 + 8] = c_mul(v[3 + 8], make_double2(-r2, r2));    // 6
-    v[1 + 12] = c_mul(v[1 + 12], make_double2(s8, c8));   // 3
-    v[2 + 12] = c_mul(v[2 + 12], make_double2(-r2, r2));  // 6
-    v[3 + 12] = c_mul(v[3 + 12], make_double2(-c8, -s8)); // 9
+    v[1 + 4] = c_mul(v[1 + 4], Cx<C>::make(c8, s8));     // 1
+    v[2 + 4] = c_mul(v[2 + 4], Cx<C>::make(r2, r2));     // 2
+    v[3 + 4] = c_mul(v[3 + 4], Cx<C>::make(s8, c8));     // 3
+    v[1 + 8] = c_mul(v[1 + 8], Cx<C>::make(r2, r2));     // 2
+    v[2 + 8] = c_mul_i(v[2 + 8]);                        // 4
+    v[3 + 8] = c_mul(v[3 + 8], Cx<C>::make(-r2, r2));    // 6
+    v[1 + 12] = c_mul(v[1 + 12], Cx<C>::make(s8, c8));   // 3
+    v[2 + 12] = c_mul(v[2 + 12], Cx<C>::make(-r2, r2));  // 6
+    v[3 + 12] = c_mul(v[3 + 12], Cx<C>::make(-c8, -s8)); // 9
 #pragma unroll
     for (int c = 0; c < 4; ++c) dft4_inv(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
 }
 __device__ __forceinline__ int dft16_at(int k) { return 4 * (k & 3) + (k >> 2); }
 
 // w^n = e^{2 pi i n / 4096} from the quarter table q[j] = w^j, j < 1024.
-__device__ __forceinline__ double2 twiddle4096(const double2* q, int n) {
-    const double2 b = q[n & 1023];
+template <typename C>
+__device__ __forceinline__ C twiddle4096(const C* q, int n) {
+    const C b = q[n & 1023];
     switch ((n >> 10) & 3) {
         case 0: return b;
-        case 1: return make_double2(-b.y, b.x);
-        case 2: return make_double2(-b.x, -b.y);
-        default: return make_double2(b.y, -b.x);
+        case 1: return Cx<C>::make(-b.y, b.x);
+        case 2: return Cx<C>::make(-b.x, -b.y);
+        default: return Cx<C>::make(b.y, -b.x);
     }
 }
 
-__device__ __forceinline__ double2 load_c(const float* S, int64_t e) {
+// Element e of a store as the transform's complex type.
+template <typename C>
+__device__ __forceinline__ C load_c(const float* S, int64_t e) {
     const float2 f = __ldg(reinterpret_cast<const float2*>(S) + e);
-    return make_double2(double(f.x), double(f.y));
+    return Cx<C>::make(typename Cx<C>::S(f.x), typename Cx<C>::S(f.y));
 }
-__device__ __forceinline__ double2 load_c(const double* S, int64_t e) {
-    return __ldg(reinterpret_cast<const double2*>(S) + e);
+template <typename C>
+__device__ __forceinline__ C load_c(const double* S, int64_t e) {
+    const double2 f = __ldg(reinterpret_cast<const double2*>(S) + e);
+    return Cx<C>::make(typename Cx<C>::S(f.x), typename Cx<C>::S(f.y));
 }
 
 // The 8 outputs k0 + 16 k1 + 256 k2 (k2 < 8) of thread (k0, k1) for the
 // sequence whose element m is S[m + base] (complex index; sequence-major).
-template <typename T>
-__device__ __forceinline__ void fused_transform(const T* S, int64_t base, const double2* qtw,
-                                                const double2* ph, double2* xch,
-                                                double2 (&out)[8]) {
+template <typename C, typename T>
+__device__ __forceinline__ void fused_transform(const T* S, int64_t base, const C* qtw,
+                                                const C* ph, C* xch, C (&out)[8]) {
     const int t = threadIdx.x;
-    double2 v[16];
+    C v[16];
     // pass A: thread (n0, n1) = (t % 16, t / 16) holds E_{t + 256 n2}
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
         const int n = t + 256 * j;
         if (j < 8) {
-            v[j] = c_mul(ph[n], load_c(S, base + n));
+            v[j] = c_mul(ph[n], load_c<C>(S, base + n));
         } else if (n == kFusedM) {
-            v[j] = make_double2(0.0, 0.0);
+            v[j] = Cx<C>::make(0, 0);
         } else {
             const int m = 2 * kFusedM - n;
-            const double2 p = ph[m];
-            v[j] = c_mul(make_double2(p.x, -p.y), load_c(S, base + m));
+            const C p = ph[m];
+            v[j] = c_mul(Cx<C>::make(p.x, -p.y), load_c<C>(S, base + m));
         }
     }
     dft16_inv(v);
@@ -423,31 +446,39 @@ __global__ void __launch_bounds__(256) gather_sequences_kernel(int64_t q0, int64
     }
 }
 
-// Gathered sequences i < nqc of one chunk (Tq, left then right);
-// partial[cta][k] += sum over the CTA's sequences of conj(L3_k) R3_k.
-template <typename T>
-__global__ void __launch_bounds__(kFusedThreads, 1)
+// Gathered sequences i < nqc of one chunk (Tq, left then right), transform
+// in the precision of C; partial[cta][k] += sum over the CTA's sequences of
+// conj(L3_k) R3_k, the products and the sums in FP64.  Two CTAs per SM for
+// the FP32 transform (half the registers and shared memory), one for FP64.
+template <typename T, typename C>
+__global__ void __launch_bounds__(kFusedThreads, sizeof(C) == 8 ? 2 : 1)
     greenwood_fused_kernel(int64_t nqc, const T* Tq, const double2* tab, double2* partial) {
-    extern __shared__ double2 fsm[];
-    double2* xch = fsm;
-    double2* qtw = xch + 16 * kXchPlane;
-    double2* ph = qtw + 1024;
-    for (int j = threadIdx.x; j < 1024 + kFusedM; j += blockDim.x) qtw[j] = tab[j];
+    extern __shared__ __align__(16) unsigned char fsm_raw[];
+    C* xch = reinterpret_cast<C*>(fsm_raw);
+    C* qtw = xch + 16 * kXchPlane;
+    C* ph = qtw + 1024;
+    for (int j = threadIdx.x; j < 1024 + kFusedM; j += blockDim.x)
+        qtw[j] = Cx<C>::make(typename Cx<C>::S(tab[j].x), typename Cx<C>::S(tab[j].y));
     __syncthreads();
     double2 acc[8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) acc[i] = make_double2(0.0, 0.0);
     const int64_t right = nqc * kFusedM;
     for (int64_t i = blockIdx.x; i < nqc; i += gridDim.x) {
-        double2 l3[8], r3[8];
+        C l3[8], r3[8];
         fused_transform(Tq, i * kFusedM, qtw, ph, xch, l3);
         fused_transform(Tq, right + i * kFusedM, qtw, ph, xch, r3);
 #pragma unroll
-        for (int j = 0; j < 8; ++j) acc[j] = c_add(acc[j], c_mul_conj_a(l3[j], r3[j]));
+        for (int j = 0; j < 8; ++j) {
+            const double lx = l3[j].x, ly = l3[j].y, rx = r3[j].x, ry = r3[j].y;
+            acc[j].x += lx * rx + ly * ry;  // conj(L3) R3
+            acc[j].y += lx * ry - ly * rx;
+        }
     }
     double2* p = partial + int64_t(blockIdx.x) * kFusedM + threadIdx.x;
 #pragma unroll
-    for (int k2 = 0; k2 < 8; ++k2) p[256 * k2] = c_add(p[256 * k2], acc[k2]);
+    for (int k2 = 0; k2 < 8; ++k2) p[256 * k2] = make_double2(p[256 * k2].x + acc[k2].x,
+                                                              p[256 * k2].y + acc[k2].y);
 }
 
 // K[k][comp] += sum over the n_cta partials (in CTA order) / max(1e-14, 1 - eps_k^2).
@@ -471,6 +502,12 @@ __global__ void fused_reduce_kernel(int n_cta, const double2* partial, int comp,
 bool fused_enabled() {
     const char* s = std::getenv("RSATB_FFTCHEB_FUSED");
     return !(s && s[0] == '0');
+}
+
+// RSATB_FFTCHEB_FP64=1: the FP64 transform for FP32 vectors too.
+bool fused_fp64_forced() {
+    const char* s = std::getenv("RSATB_FFTCHEB_FP64");
+    return s && s[0] == '1';
 }
 
 // Owning device buffer released on scope exit.
@@ -696,7 +733,10 @@ int fftcheb_impl(const Ctx& c, const rsatb_bsr_matrix* const* V, const T* psi, i
     // per CTA and energy; chunks of fused_qc sequences gathered into the
     // extension buffer (sequence-major, both sides).
     const bool fused = !bastin && M == kFusedM && fused_enabled();
-    const int fused_grid = ctx->sm_count;
+    // FP32 vectors take the FP32 transform (FP64 products and sums) unless
+    // RSATB_FFTCHEB_FP64=1; FP64 vectors the FP64 one.
+    const bool fused32 = fused && std::is_same<T, float>::value && !fused_fp64_forced();
+    const int fused_grid = ctx->sm_count * (fused32 ? 2 : 1);
     const int64_t fused_qc = std::max<int64_t>(
         1, std::min<int64_t>(8192, int64_t(size_t(n_tf) * 2 * 2 * size_t(M) * nq_max *
                                            sizeof(double2) / (2 * size_t(M) * cplx))));
@@ -707,9 +747,13 @@ int fftcheb_impl(const Ctx& c, const rsatb_bsr_matrix* const* V, const T* psi, i
         fused_tables_kernel<<<(1024 + kFusedM) / 256, 256, 0, st>>>(bWts.as<double>(),
                                                                     bTab.as<double2>());
         RSATB_LAUNCH_CHECK(ctx);
-        RSATB_CUDA_TRY(cudaFuncSetAttribute(greenwood_fused_kernel<T>,
+        RSATB_CUDA_TRY(cudaFuncSetAttribute(greenwood_fused_kernel<T, double2>,
                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            int(kFusedSmem)));
+                                            int(fused_smem<double2>())));
+        if constexpr (std::is_same<T, float>::value)
+            RSATB_CUDA_TRY(cudaFuncSetAttribute(greenwood_fused_kernel<T, float2>,
+                                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                int(fused_smem<float2>())));
     }
 
     // cuFFT plans: full chunks and the last, shorter chunk of a section.
@@ -827,8 +871,19 @@ int fftcheb_impl(const Ctx& c, const rsatb_bsr_matrix* const* V, const T* psi, i
                     gather_sequences_kernel<T><<<gg, 256, 0, st>>>(int64_t(a) * per_axis + i0, n,
                                                                    sslot, SL, SR, Tq);
                     RSATB_LAUNCH_CHECK(ctx);
-                    greenwood_fused_kernel<T><<<fused_grid, kFusedThreads, kFusedSmem, st>>>(
-                        n, Tq, bTab.as<double2>(), bPart.as<double2>());
+                    bool done = false;
+                    if constexpr (std::is_same<T, float>::value) {
+                        if (fused32) {
+                            greenwood_fused_kernel<T, float2>
+                                <<<fused_grid, kFusedThreads, fused_smem<float2>(), st>>>(
+                                    n, Tq, bTab.as<double2>(), bPart.as<double2>());
+                            done = true;
+                        }
+                    }
+                    if (!done)
+                        greenwood_fused_kernel<T, double2>
+                            <<<fused_grid, kFusedThreads, fused_smem<double2>(), st>>>(
+                                n, Tq, bTab.as<double2>(), bPart.as<double2>());
                     RSATB_LAUNCH_CHECK(ctx);
                     ++chunks;
                 }
