@@ -197,7 +197,7 @@ constexpr double kQuadratic = 0.5;
 constexpr double kLift = 1.0;
 constexpr double kFloorFrom = 0.1;
 __global__ void control_kernel(int np_count, State* st, double* res2, double tol,
-                               int stop_on_rise, int lift, int floor_stop) {
+                               int stop_on_rise, int lift, int floor_stop, int* live) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= np_count) return;
     State x = st[p];
@@ -225,6 +225,7 @@ __global__ void control_kernel(int np_count, State* st, double* res2, double tol
             x.norm_pre = norm;
             x.count += 1;
             x.lift = (lift && norm >= kLift) ? 1 : 0;
+            *live = 1;  // every writer stores the same value
         }
     }
     res2[p] = 0.0;
@@ -325,7 +326,8 @@ __global__ void __launch_bounds__(128) gemm_f64_kernel(const Prob* probs, const 
                                                        const double* A, const double* B,
                                                        double* C, int mode, const double* Xe,
                                                        double* res2, float* c_hi,
-                                                       float* c_lo, int sym) {
+                                                       float* c_lo, int sym, const int* live) {
+    if (live && *live == 0) return;  // every problem has stopped
     using Sh = F64Shape<BT, SYM_A>;
     constexpr int KC = Sh::KC, LDR = Sh::LDR, LDK = Sh::LDK;
     extern __shared__ __align__(16) double f64_smem[];
@@ -556,6 +558,12 @@ struct Dev {
     TcItem* tc_items_upper;  // the tiles that touch the upper triangle
     F64Item* f64_items;
     F64Item* f64_items_upper;  // the 64 x 64 tiles on or above the diagonal
+    // live[k] (tensor-core phase) and live_f64[k] (FP64 phase): set by the
+    // control step of iteration k when a problem goes on; the GEMMs after it
+    // return at once when it stays 0 (the graph keeps the full loop).
+    int* live;
+    int* live_f64;
+    int n_live;
     int n_tc_items;
     int n_f64_items;
     int n_f64_upper;
@@ -578,7 +586,7 @@ int tc_gemm(rsatb_context* ctx, const Chunk& ch, const Dev& d, const TcItem* ite
             const float* b_hi, const float* b_lo, float* c_hi, float* c_lo, double* c64,
             int mode, const float* xe_hi, const float* xe_lo, bool split, bool ws,
             rsatb_isqrt_stats* stats, float* ct_hi = nullptr, float* ct_lo = nullptr,
-            bool sym = false) {
+            bool sym = false, const int* live = nullptr) {
     const int nb = int(ch.buckets.size());
     for (int g0 = 0, gi = 0; g0 < nb; g0 += kMaxBuckets, ++gi) {
         TcMaps maps;
@@ -607,6 +615,7 @@ int tc_gemm(rsatb_context* ctx, const Chunk& ch, const Dev& d, const TcItem* ite
         args.sym = sym ? 1 : 0;
         args.split = split ? 1 : 0;
         args.error = d.error;
+        args.live = live;
         RSATB_TRY(launch_tc_gemm(ctx, maps, args, ws));
         if (stats) stats->gemm_launches++;
     }
@@ -618,14 +627,15 @@ int tc_gemm(rsatb_context* ctx, const Chunk& ch, const Dev& d, const TcItem* ite
 template <bool BT, bool SYM_A = false>
 int f64_gemm(rsatb_context* ctx, const Dev& d, const double* A, const double* B, double* C,
              int mode, const double* Xe, rsatb_isqrt_stats* stats, float* c_hi = nullptr,
-             float* c_lo = nullptr, bool sym = false) {
+             float* c_lo = nullptr, bool sym = false, const int* live = nullptr) {
     const F64Item* items = sym ? d.f64_items_upper : d.f64_items;
     const int n_items = sym ? d.n_f64_upper : d.n_f64_items;
     if (n_items == 0) return RSATB_SUCCESS;
     int grid = ctx->sm_count * 6;
     if (n_items < grid) grid = n_items;
     gemm_f64_kernel<BT, SYM_A><<<grid, 128, F64Shape<BT, SYM_A>::SMEM, ctx->stream>>>(
-        d.probs, items, n_items, d.state, A, B, C, mode, Xe, d.res2, c_hi, c_lo, sym ? 1 : 0);
+        d.probs, items, n_items, d.state, A, B, C, mode, Xe, d.res2, c_hi, c_lo, sym ? 1 : 0,
+        live);
     RSATB_LAUNCH_CHECK(ctx);
     if (stats) stats->gemm_launches++;
     return RSATB_SUCCESS;
@@ -717,7 +727,9 @@ int run_chunk(rsatb_context* ctx, const Opts& o, const Chunk& ch, const int* col
              align256(tc_items.size() * sizeof(TcItem)) +
              align256(tc_upper.size() * sizeof(TcItem)) +
              align256(f64_items.size() * sizeof(F64Item)) +
-             align256(f64_upper.size() * sizeof(F64Item));
+             align256(f64_upper.size() * sizeof(F64Item)) +
+             align256(size_t(o.max_iter + 2 + std::max(o.max_fp64, o.max_fp64_restart) + 2) *
+                      sizeof(int));
     bytes += (low ? 14 * align256(E * sizeof(float)) : 0) + 6 * align256(E * sizeof(double));
     void* ws = nullptr;
     RSATB_TRY(ctx_scratch(ctx, bytes, &ws));
@@ -737,6 +749,9 @@ int run_chunk(rsatb_context* ctx, const Opts& o, const Chunk& ch, const int* col
     d.tc_items_upper = carve<TcItem>(cur, tc_upper.size());
     d.f64_items = carve<F64Item>(cur, f64_items.size());
     d.f64_items_upper = carve<F64Item>(cur, f64_upper.size());
+    d.n_live = o.max_iter + 2 + std::max(o.max_fp64, o.max_fp64_restart) + 2;
+    d.live = carve<int>(cur, size_t(d.n_live));
+    d.live_f64 = d.live + (o.max_iter + 2);
     d.n_tc_items = int(tc_items.size());
     d.n_f64_items = int(f64_items.size());
     d.n_f64_upper = int(f64_upper.size());
@@ -800,6 +815,7 @@ int run_chunk(rsatb_context* ctx, const Opts& o, const Chunk& ch, const int* col
                                    f64_upper.size() * sizeof(F64Item), cudaMemcpyHostToDevice, s));
     RSATB_CUDA_TRY(cudaMemsetAsync(d.res2, 0, P * sizeof(double), s));
     RSATB_CUDA_TRY(cudaMemsetAsync(d.error, 0, sizeof(unsigned), s));
+    RSATB_CUDA_TRY(cudaMemsetAsync(d.live, 0, size_t(d.n_live) * sizeof(int), s));
 
     // Pack S and the starting iterate.
     pack_kernel<<<P, 256, 0, s>>>(d.probs, d.in_off, M, a.s64, a.s_hi, a.s_lo);
@@ -836,17 +852,19 @@ int run_chunk(rsatb_context* ctx, const Opts& o, const Chunk& ch, const int* col
         RSATB_TRY(run_phase(ctx, o.graph, [&]() -> int {
             for (int k = 0; k <= o.max_iter; ++k) {
                 const int c = k & 1;
+                const int* live_in = k ? d.live + (k - 1) : nullptr;  // after control k - 1
+                const int* live_k = d.live + k;                        // after control k
                 // W = Z S^T, X = Z W^T (+ residual) on the tensor cores
                 RSATB_TRY(tc_gemm(ctx, ch, d, d.tc_items, group_begin, a.z_hi, a.z_lo, a.s_hi,
                                   a.s_lo, a.w_hi, a.w_lo, nullptr, EPI_STORE, nullptr, nullptr,
-                                  split, o.ws, stats));
+                                  split, o.ws, stats, nullptr, nullptr, false, live_in));
                 // X on every tile (its upper triangle mirrored, as P is, measured
                 // the same: 21,300 against 21,400 matrices/s at 20,000 problems).
                 RSATB_TRY(tc_gemm(ctx, ch, d, d.tc_items, group_begin, a.z_hi, a.z_lo, a.w_hi,
                                   a.w_lo, a.x_hi, a.x_lo, nullptr, EPI_RESID, nullptr, nullptr,
-                                  split, o.ws, stats));
+                                  split, o.ws, stats, nullptr, nullptr, false, live_in));
                 control_kernel<<<cb, 256, 0, s>>>(P, d.state, d.res2, o.tol, 1, lift,
-                                                  floor_stop);
+                                                  floor_stop, d.live + k);
                 RSATB_LAUNCH_CHECK(ctx);
                 if (c == 1 && update64) {
                     retire_low_kernel<<<P, 256, 0, s>>>(d.probs, d.state, a.z64[1], a.z64[0]);
@@ -868,19 +886,21 @@ int run_chunk(rsatb_context* ctx, const Opts& o, const Chunk& ch, const int* col
                     // after the phase).
                     RSATB_TRY(tc_gemm(ctx, ch, d, d.tc_items_upper, group_begin_upper, a.x_hi,
                                       a.x_lo, a.x_hi, a.x_lo, a.p_hi, a.p_lo, nullptr, EPI_POLY,
-                                      a.x_hi, a.x_lo, split, o.ws, stats, nullptr, nullptr, true));
+                                      a.x_hi, a.x_lo, split, o.ws, stats, nullptr, nullptr, true,
+                                      live_k));
                     RSATB_TRY(tc_gemm(ctx, ch, d, d.tc_items, group_begin, a.p_hi, a.p_lo,
                                       a.zt_hi[c], a.zt_lo[c], a.z_hi, a.z_lo, nullptr,
                                       EPI_STORE, nullptr, nullptr, split, o.ws, stats,
-                                      a.zt_hi[c ^ 1], a.zt_lo[c ^ 1]));
+                                      a.zt_hi[c ^ 1], a.zt_lo[c ^ 1], false, live_k));
                 } else {
                     RSATB_TRY(tc_gemm(ctx, ch, d, d.tc_items, group_begin, a.x_hi, a.x_lo, a.x_hi,
                                       a.x_lo, use_ws_tc ? nullptr : a.p_hi,
                                       use_ws_tc ? nullptr : a.p_lo, a.p64, EPI_POLY, a.x_hi,
-                                      a.x_lo, split, o.ws, stats));
+                                      a.x_lo, split, o.ws, stats, nullptr, nullptr, false,
+                                      live_k));
                     const int st_z = f64_gemm<false, true>(ctx, d, a.p64, a.z64[c], a.z64[c ^ 1],
                                                            EPI_STORE, nullptr, stats, a.z_hi,
-                                                           a.z_lo);
+                                                           a.z_lo, false, live_k);
                     RSATB_TRY(st_z);
                 }
             }
@@ -916,10 +936,14 @@ int run_chunk(rsatb_context* ctx, const Opts& o, const Chunk& ch, const int* col
     RSATB_TRY(run_phase(ctx, o.graph, [&]() -> int {
         for (int k = 0; k <= fp64_steps; ++k) {
             const int c = k & 1;
-            RSATB_TRY(f64_gemm<true>(ctx, d, a.z64[c], a.s64, a.w64, EPI_STORE, nullptr, stats));
+            const int* live_in = k ? d.live_f64 + (k - 1) : nullptr;
+            const int* live_k = d.live_f64 + k;
+            RSATB_TRY(f64_gemm<true>(ctx, d, a.z64[c], a.s64, a.w64, EPI_STORE, nullptr, stats,
+                                     nullptr, nullptr, false, live_in));
             RSATB_TRY(f64_gemm<true>(ctx, d, a.z64[c], a.w64, a.x64, EPI_RESID, nullptr, stats,
-                                     nullptr, nullptr, true));
-            control_kernel<<<cb, 256, 0, s>>>(P, d.state, d.res2, o.tol, 0, 0, 0);
+                                     nullptr, nullptr, true, live_in));
+            control_kernel<<<cb, 256, 0, s>>>(P, d.state, d.res2, o.tol, 0, 0, 0,
+                                              d.live_f64 + k);
             RSATB_LAUNCH_CHECK(ctx);
             retire_out_kernel<<<P, 256, 0, s>>>(d.probs, d.state, a.z64[c], d.col_start,
                                                 d.k_cols, d.out_off, out);
@@ -928,9 +952,10 @@ int run_chunk(rsatb_context* ctx, const Opts& o, const Chunk& ch, const int* col
             // X and P exactly symmetric (upper tiles, mirrored): Z' = P Z
             // takes P as it is.
             RSATB_TRY(f64_gemm<true>(ctx, d, a.x64, a.x64, a.p64, EPI_POLY, a.x64, stats,
-                                     nullptr, nullptr, true));
+                                     nullptr, nullptr, true, live_k));
             const int st_z = f64_gemm<false, false>(ctx, d, a.p64, a.z64[c], a.z64[c ^ 1],
-                                                   EPI_STORE, nullptr, stats);
+                                                   EPI_STORE, nullptr, stats, nullptr, nullptr,
+                                                   false, live_k);
             RSATB_TRY(st_z);
         }
         return RSATB_SUCCESS;
@@ -1249,7 +1274,12 @@ extern "C" int rsatb_isqrt_autotune(rsatb_ctx_t ctx, int precision, int n_sizes,
             }
         }
     }
-    // The kernel with the smaller summed best time, then its best tile per size.
+    // The kernel family, then its best tile per size.  The built-in family
+    // (the warp-specialised kernel) stays unless the other one is faster by
+    // more than 15 % on the samples: a few problems per size hide what the
+    // warp specialisation buys on full chunks (the epilogue of one tile under
+    // the main loop of the next), and a noisy pick of the single-role kernel
+    // cost a quarter of the throughput of the 100,000-problem batch.
     double total[2] = {0.0, 0.0};
     for (int si = 0; si < n_sizes; ++si)
         for (int kk = 0; kk < 2; ++kk) {
@@ -1260,7 +1290,8 @@ extern "C" int rsatb_isqrt_autotune(rsatb_ctx_t ctx, int precision, int n_sizes,
             }
             total[kk] += b;
         }
-    const int kk = total[1] < total[0] ? 1 : 0;
+    const int builtin = default_tc_ws() ? 0 : 1, other = 1 - builtin;
+    const int kk = total[other] < 0.85 * total[builtin] ? other : builtin;
     *tc_kernel_out = kk + 1;
     for (int si = 0; si < n_sizes; ++si) {
         const int np = (sizes[si] + 31) / 32 * 32;

@@ -89,6 +89,8 @@ struct TcArgs {
     int mode;
     int split;               // 1: hi*hi + hi*lo + lo*hi; 0: hi*hi
     unsigned* error;         // set non-zero when a bounded wait gave up
+    const int* live;         // optional: 0 when no problem of the chunk is still iterating
+                             // (the launch returns at once), nullptr: always run
 };
 
 // One batched C = A B^T on the tensor cores for the items of up to

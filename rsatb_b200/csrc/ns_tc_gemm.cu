@@ -120,6 +120,7 @@ __device__ __forceinline__ void store_chunk(const TcArgs& args, const Prob& pr, 
 __global__ void __launch_bounds__(128, 1)
     tc_gemm_kernel(const __grid_constant__ TcMaps maps, const TcArgs args) {
     using namespace umma;
+    if (args.live && *args.live == 0) return;  // every problem has stopped
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -369,6 +370,7 @@ __device__ __forceinline__ ItemView view_item(const TcArgs& args, int it) {
 __global__ void __launch_bounds__(320, 1)
     tc_gemm_ws_kernel(const __grid_constant__ TcMaps maps, const TcArgs args) {
     using namespace umma;
+    if (args.live && *args.live == 0) return;  // every problem has stopped
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
