@@ -232,8 +232,10 @@ __global__ void __launch_bounds__(256) greenwood_contract_kernel(int M, int64_t 
 // ---------------------------------------------------------------------------
 // Fused Greenwood row stage for M = 2048 (a 4096-point transform): the even
 // extension, the DCT-III (the inverse 2M-point DFT of extend_kernel's
-// sequence, outputs k < M) and the contraction in one kernel, FP64
-// arithmetic, so the moments are read once and nothing else touches HBM.
+// sequence, outputs k < M) and the contraction in one kernel, so no
+// extended sequence or transform output goes through HBM.  The transform
+// runs in FP64 for FP64 vectors and in FP32 for FP32 vectors; the products
+// conj(L3) R3 and their sums are FP64 in both.
 //
 // One CTA of 256 threads transforms one sequence at a time as 16 x 16 x 16
 // (n = n0 + 16 n1 + 256 n2, k = k0 + 16 k1 + 256 k2, w = e^{2 pi i / 4096}):
