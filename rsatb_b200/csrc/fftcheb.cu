@@ -341,6 +341,29 @@ __device__ __forceinline__ C twiddle4096(const C* q, int n) {
     }
 }
 
+// The powers b^k, k = 0..15, of a twiddle b as b4^(k / 4) b^(k % 4), from b
+// and b4 = b^4 (two reads of the quarter table, whose strided lanes would
+// otherwise conflict on the shared-memory banks sixteen at a time): at most
+// four roundings more than a table entry.
+template <typename C>
+struct Pow16 {
+    C lo[4], hi[4];
+    __device__ __forceinline__ Pow16(C b, C b4) {
+        lo[0] = hi[0] = Cx<C>::make(1, 0);
+        lo[1] = b;
+        lo[2] = c_mul(b, b);
+        lo[3] = c_mul(lo[2], b);
+        hi[1] = b4;
+        hi[2] = c_mul(b4, b4);
+        hi[3] = c_mul(hi[2], b4);
+    }
+    __device__ __forceinline__ C operator()(int k) const {
+        if (k < 4) return lo[k];
+        if ((k & 3) == 0) return hi[k >> 2];
+        return c_mul(hi[k >> 2], lo[k & 3]);
+    }
+};
+
 // Element e of a store as the transform's complex type.
 template <typename C>
 __device__ __forceinline__ C load_c(const float* S, int64_t e) {
@@ -377,10 +400,10 @@ __device__ __forceinline__ void fused_transform(const T* S, int64_t base, const 
     dft16_inv(v);
     {
         const int n0 = t & 15, n1 = t >> 4;
+        const Pow16<C> tw(twiddle4096(qtw, t), twiddle4096(qtw, 4 * t));  // w^{t k0}
 #pragma unroll
         for (int k0 = 0; k0 < 16; ++k0)
-            xch[n0 * kXchPlane + k0 * 16 + n1] =
-                c_mul(v[dft16_at(k0)], twiddle4096(qtw, t * k0));
+            xch[n0 * kXchPlane + k0 * 16 + n1] = c_mul(v[dft16_at(k0)], tw(k0));
     }
     __syncthreads();
     // pass B: thread (n0, k0) = (t % 16, t / 16)
@@ -389,11 +412,11 @@ __device__ __forceinline__ void fused_transform(const T* S, int64_t base, const 
 #pragma unroll
         for (int n1 = 0; n1 < 16; ++n1) v[n1] = xch[n0 * kXchPlane + k0 * 16 + n1];
         dft16_inv(v);
+        const Pow16<C> tw(twiddle4096(qtw, 16 * n0), twiddle4096(qtw, 64 * n0));  // w^{16 n0 k1}
         __syncthreads();
 #pragma unroll
         for (int k1 = 0; k1 < 16; ++k1)
-            xch[k0 * kXchPlane + k1 * 16 + n0] =
-                c_mul(v[dft16_at(k1)], twiddle4096(qtw, 16 * n0 * k1));
+            xch[k0 * kXchPlane + k1 * 16 + n0] = c_mul(v[dft16_at(k1)], tw(k1));
     }
     __syncthreads();
     // pass C: thread (k0, k1) = (t % 16, t / 16)
