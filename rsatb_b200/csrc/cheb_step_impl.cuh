@@ -98,7 +98,7 @@ inline int pick_v(int W, bool cv, bool any_b, int block_size, bool dbl) {
 
 constexpr int kNotApplicable = 1000;
 
-// RSATB_STEP_KERNEL=v1|staged|rowsplit|bulk|narrow|dmma|tf32 forces one kernel family
+// RSATB_STEP_KERNEL=v1|staged|rowsplit|bulk|narrow|dmma|tf32|generic forces one kernel family
 // (tuning and A/B tests); unset picks by shape and precision.
 inline int env_kernel() {
     const char* s = std::getenv("RSATB_STEP_KERNEL");
@@ -110,6 +110,7 @@ inline int env_kernel() {
     if (s[0] == 'n') return 5;
     if (s[0] == 'd') return 6;
     if (s[0] == 't') return 7;
+    if (s[0] == 'g') return 8;  // the register kernel
     return 0;
 }
 inline bool env_force_v1() { return env_kernel() == 1; }
@@ -564,9 +565,12 @@ int launch_typed(rsatb_context* ctx, int block_size, StepArgs& a) {
     // Measured choice (diamond 8x8 blocks, B200), after the tensor-core and
     // bulk-copy kernels above: FP64 takes the staged kernel (other block
     // sizes), FP32 the staged kernel for complex panels of W = 16 and the
-    // register kernel otherwise.
+    // register kernel otherwise.  FP64 scalar rows take the register kernel
+    // (twisted-bilayer transport, complex W = 32 and 96: 225 against 519 ms
+    // for 256 moments).
     const bool want_staged =
-        forced == 2 || (forced == 0 && (sizeof(VT) == 8 || (a.W == 16 && CV)));
+        forced == 2 ||
+        (forced == 0 && ((sizeof(VT) == 8 && block_size != 1) || (a.W == 16 && CV)));
     if (special && want_staged) {
         const int Vs = pick_v_staged(a.W, CV, block_size, sizeof(VT) == 8);
         int st = kNotApplicable;
