@@ -565,12 +565,13 @@ int launch_typed(rsatb_context* ctx, int block_size, StepArgs& a) {
     // Measured choice (diamond 8x8 blocks, B200), after the tensor-core and
     // bulk-copy kernels above: FP64 takes the staged kernel (other block
     // sizes), FP32 the staged kernel for complex panels of W = 16 and the
-    // register kernel otherwise.  FP64 scalar rows take the register kernel
-    // (twisted-bilayer transport, complex W = 32 and 96: 225 against 519 ms
-    // for 256 moments).
+    // register kernel otherwise.  Scalar rows take the register kernel in
+    // both precisions (twisted-bilayer transport recurrence: FP64 complex
+    // W = 32 and 96, 225 against 519 ms for 256 moments; FP32 complex W = 16
+    // and 48, 175 against 259 ms for 512).
     const bool want_staged =
         forced == 2 ||
-        (forced == 0 && ((sizeof(VT) == 8 && block_size != 1) || (a.W == 16 && CV)));
+        (forced == 0 && block_size != 1 && (sizeof(VT) == 8 || (a.W == 16 && CV)));
     if (special && want_staged) {
         const int Vs = pick_v_staged(a.W, CV, block_size, sizeof(VT) == 8);
         int st = kNotApplicable;
