@@ -676,9 +676,16 @@ int fftcheb_impl(const Ctx& c, const rsatb_bsr_matrix* const* V, const T* psi, i
                          "workspace of %zu bytes holds no section (needs %zu + %zu per block row)",
                          workspace, fixed, store_per_brow);
     // FFT chunk: rows whose 2 x (2M x 3 rows R) double2 extensions fit a
-    // quarter of what remains after the fixed buffers.
+    // quarter of what remains after the fixed buffers.  The fused row stage
+    // (Greenwood, M = 2048) needs only its gathered chunk of up to 8,192
+    // sequence pairs, and the store takes the rest (larger sections: fewer
+    // passes of the recurrence).
     const size_t avail = workspace - fixed;
-    const size_t fft_budget = avail / 4;
+    const bool fused = !bastin && M == kFusedM && fused_enabled();
+    const size_t fused_chunk_bytes = 2 * size_t(8192) * size_t(M) * cplx;
+    const size_t fft_budget =
+        fused ? std::max(2 * size_t(M) * cplx, std::min(avail / 4, fused_chunk_bytes))
+              : avail / 4;
     const size_t fft_per_row =
         size_t(n_tf) * 2 * 2 * size_t(M) * 3 * R * sizeof(double2) * 2;  // + cuFFT work
     int64_t chunk_rows = int64_t(fft_budget / fft_per_row);
@@ -708,7 +715,9 @@ int fftcheb_impl(const Ctx& c, const rsatb_bsr_matrix* const* V, const T* psi, i
     const int64_t slot = 3 * sec_rows_max * R;  // complex entries per moment slot
     RSATB_TRY(bS.alloc(2 * size_t(M) * slot * cplx));
     const int64_t nq_max = 3 * chunk_rows * R;
-    RSATB_TRY(bE.alloc(size_t(n_tf) * 2 * 2 * size_t(M) * nq_max * sizeof(double2)));
+    const size_t e_bytes =
+        fused ? fft_budget : size_t(n_tf) * 2 * 2 * size_t(M) * nq_max * sizeof(double2);
+    RSATB_TRY(bE.alloc(e_bytes));
     RSATB_TRY(bK.alloc(size_t(M) * 12 * sizeof(double)));
     RSATB_TRY(bWts.alloc(size_t(M) * sizeof(double)));
     DevBuf bPw;
@@ -725,7 +734,7 @@ int fftcheb_impl(const Ctx& c, const rsatb_bsr_matrix* const* V, const T* psi, i
     T* SL = bS.as<T>();
     T* SR = SL + 2 * size_t(M) * slot;
     double2* EL = bE.as<double2>();
-    double2* ER = EL + 2 * size_t(M) * nq_max;
+    double2* ER = fused ? nullptr : EL + 2 * size_t(M) * nq_max;
     // Bastin: phi1 and phi2 of both sides follow.
     double2* EL1 = bastin ? ER + 2 * size_t(M) * nq_max : nullptr;
     double2* ER1 = bastin ? EL1 + 2 * size_t(M) * nq_max : nullptr;
@@ -757,14 +766,16 @@ int fftcheb_impl(const Ctx& c, const rsatb_bsr_matrix* const* V, const T* psi, i
     // Fused row stage (Greenwood, M = 2048): one CTA per SM, partial sums
     // per CTA and energy; chunks of fused_qc sequences gathered into the
     // extension buffer (sequence-major, both sides).
-    const bool fused = !bastin && M == kFusedM && fused_enabled();
     // FP32 vectors take the FP32 transform (FP64 products and sums) unless
     // RSATB_FFTCHEB_FP64=1; FP64 vectors the FP64 one.
     const bool fused32 = fused && std::is_same<T, float>::value && !fused_fp64_forced();
     const int fused_grid = ctx->sm_count * (fused32 ? 2 : 1);
-    const int64_t fused_qc = std::max<int64_t>(
-        1, std::min<int64_t>(8192, int64_t(size_t(n_tf) * 2 * 2 * size_t(M) * nq_max *
-                                           sizeof(double2) / (2 * size_t(M) * cplx))));
+    int64_t fused_qc = std::max<int64_t>(
+        1, std::min<int64_t>(8192, int64_t(e_bytes / (2 * size_t(M) * cplx))));
+    if (const char* cap = std::getenv("RSATB_FFTCHEB_CHUNK")) {  // smaller chunks (tests)
+        const int64_t c = std::atoll(cap);
+        if (c > 0 && c < fused_qc) fused_qc = c;
+    }
     DevBuf bPart, bTab;
     if (fused) {
         RSATB_TRY(bPart.alloc(size_t(fused_grid) * kFusedM * sizeof(double2)));

@@ -283,9 +283,10 @@ def test_fused_row_stage_at_2048_moments(torch_cuda, precision, monkeypatch):
     fused, en, st = _gpu(torch_cuda, H, V, psi, 2048, emin, emax, precision=precision)
     fused3, _, st3 = _gpu(torch_cuda, H, V, psi, 2048, emin, emax, precision=precision,
                           partition_sections=3)
-    # a 20 MB workspace: several sections, several gathered chunks per axis
-    small, _, st_s = _gpu(torch_cuda, H, V, psi, 2048, emin, emax, precision=precision,
-                          max_workspace_mb=20.0)
+    # gathered chunks of 100 sequence pairs: nine per axis
+    monkeypatch.setenv("RSATB_FFTCHEB_CHUNK", "100")
+    small, _, st_s = _gpu(torch_cuda, H, V, psi, 2048, emin, emax, precision=precision)
+    monkeypatch.delenv("RSATB_FFTCHEB_CHUNK")
     monkeypatch.setenv("RSATB_FFTCHEB_FP64", "1")
     fused64, _, _ = _gpu(torch_cuda, H, V, psi, 2048, emin, emax, precision=precision)
     monkeypatch.setenv("RSATB_FFTCHEB_FUSED", "0")
@@ -295,7 +296,7 @@ def test_fused_row_stage_at_2048_moments(torch_cuda, precision, monkeypatch):
     assert rel_err(fused64, chunked) < 1e-12
     assert rel_err(fused, chunked) < (1e-12 if precision == "f64" else 1e-6)
     assert rel_err(fused3, fused) < 1e-12
-    assert st_s["fft_chunks"] > 3 * st_s["sections"] and rel_err(small, fused) < 1e-12
+    assert st_s["fft_chunks"] == 27 and rel_err(small, fused) < 1e-12
     assert np.all(fused[:, [1, 2, 4]] == 0.0)
     if precision == "f64":
         sig_o, en_o = _oracle(H, V, psi, 2048, emin, emax)
