@@ -699,6 +699,7 @@ int fftcheb_impl(const Ctx& c, const rsatb_bsr_matrix* const* V, const T* psi, i
     }
     if (sec_brows > nb) sec_brows = nb;
     const int n_sections = int((nb + sec_brows - 1) / sec_brows);
+    sec_brows = (nb + n_sections - 1) / n_sections;  // balanced: the store is no larger than needed
     if (chunk_rows > sec_brows * b) chunk_rows = sec_brows * b;
 
     // Buffers.
