@@ -81,6 +81,26 @@ __global__ void store_right_kernel(int64_t row0, int64_t rows, int R, const T* p
     }
 }
 
+// The same copy in 16-byte units: the R samples of one (row, axis) are one
+// contiguous run in both layouts, of 2 R sizeof(T) / 16 units (R even for
+// FP32; every run, slot and panel then starts on a 16-byte boundary).
+template <typename T>
+__global__ void store_right_vec_kernel(int64_t row0, int64_t rows, int R, const T* panel,
+                                       T* slot) {
+    const int upr = int(2 * R * sizeof(T) / 16);  // units per run
+    const int64_t total = rows * 3 * upr;
+    const float4* src = reinterpret_cast<const float4*>(panel);
+    float4* dst = reinterpret_cast<float4*>(slot);
+    for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total;
+         e += int64_t(gridDim.x) * blockDim.x) {
+        const int u = int(e % upr);
+        const int64_t run = e / upr;  // destination run a * rows + row
+        const int64_t row = run % rows;
+        const int a = int(run / rows);
+        dst[e] = src[((row0 + row) * 3 + a) * upr + u];
+    }
+}
+
 // Even extension with the half-grid phase of fft.hpp:125-154 for a chunk of
 // sequences: sequence q (0 <= q < nq, q = (a * chunk_rows + row) * R + s,
 // rows offset row_off inside the section) of store S (slot stride
@@ -883,8 +903,13 @@ int fftcheb_impl(const Ctx& c, const rsatb_bsr_matrix* const* V, const T* psi, i
             for (int a = 0; a < 3; ++a)
                 RSATB_TRY(current_rows(c, V[a], W1, lm, sl + 2 * size_t(a) * rows * R, sb0, sb1,
                                        bU.p, bW.p));
-            store_right_kernel<T><<<grid_for(sslot, ctx->sm_count), 256, 0, st>>>(
-                rows0, rows, R, r[rm], SR + 2 * size_t(m) * sslot);
+            if (sizeof(T) == 8 || R % 2 == 0)
+                store_right_vec_kernel<T>
+                    <<<grid_for(sslot * 2 * int64_t(sizeof(T)) / 16, ctx->sm_count), 256, 0, st>>>(
+                        rows0, rows, R, r[rm], SR + 2 * size_t(m) * sslot);
+            else
+                store_right_kernel<T><<<grid_for(sslot, ctx->sm_count), 256, 0, st>>>(
+                    rows0, rows, R, r[rm], SR + 2 * size_t(m) * sslot);
             RSATB_LAUNCH_CHECK(ctx);
         }
         RSATB_CUDA_TRY(cudaEventRecord(ev1, st));
